@@ -1,0 +1,116 @@
+/* spaQR-B200: C ABI of the B200-native hierarchical sparsified QR.
+ *
+ * The entry points replace the reference's C++ surface one for one:
+ *
+ *   Tree(int nlevels, int skip)           include/tree.h:113-120  -> spq_create
+ *   set_tol / set_scale / set_order /
+ *   set_hsl / set_square / set_Xcoo       include/tree.h:124-130  -> spq_set_*
+ *   void partition(SpMat& A)              include/tree.h:139      -> spq_partition
+ *   void assemble(SpMat& A)               include/tree.h:140      -> spq_assemble
+ *   int factorize()                       include/tree.h:143      -> spq_factorize
+ *   void solve(VectorXd b, VectorXd& x)   include/tree.h:144      -> spq_solve
+ *   void solve_nrml(VectorXd b, ...)      include/tree.h:147      -> spq_solve_nrml
+ *   gmres(A, b, x, precond, iters,
+ *         restart, tol, verb)             include/is.h:14-15      -> spq_gmres
+ *   cgls(A, b, x, precond, iters, tol,..) include/is.h:18-19      -> spq_cgls
+ *   ~Tree()                               src/tree.cpp:1520-1546  -> spq_destroy
+ *   A = A*D*10 column normalisation       spaQR.cpp:131-147       -> spq_column_normalize
+ *   linspace_nd(n, d) coordinates         src/util.cpp:852-881    -> spq_set_coords_grid
+ *
+ * Matrices are CSC with 0-based int32 indices and sorted row indices inside each
+ * column (the layout of Eigen::SparseMatrix<double, ColMajor, int>), m >= n.
+ * Every call returns an int status (SPQ_OK = 0); spq_last_error() describes the
+ * last failure of the calling thread. A handle owns all of its device memory and
+ * one CUDA stream; calls on one handle must not overlap.
+ */
+#ifndef SPAQR_B200_H
+#define SPAQR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spq_tree spq_tree;
+
+enum spq_status {
+    SPQ_OK = 0,
+    SPQ_ERR_ARG = 1,         /* invalid argument or size */
+    SPQ_ERR_STATE = 2,       /* call out of order (e.g. solve before factorize) */
+    SPQ_ERR_CUDA = 3,        /* CUDA runtime error (no device, launch failure, ...) */
+    SPQ_ERR_NUMERIC = 4,     /* NaN/Inf or a zero pivot reported by a kernel */
+    SPQ_ERR_ALLOC = 5,       /* device or host allocation failed */
+    SPQ_ERR_UNSUPPORTED = 6, /* option outside the built path (e.g. non-geometric partition) */
+    SPQ_ERR_NOCONV = 7       /* Krylov solver did not reach the tolerance */
+};
+
+enum spq_precision {
+    SPQ_FP64 = 0, /* plain form: factorization and solve sweeps in FP64 */
+    SPQ_FP32 = 1  /* FP32 factorization and sweeps; Krylov, SpMV and residuals stay FP64 */
+};
+
+const char* spq_last_error(void);
+int spq_version(void);
+int spq_device_count(int* count);
+
+/* Tree(nlevels, skip) (include/tree.h:113). */
+int spq_create(spq_tree** out, int nlevels, int skip);
+int spq_destroy(spq_tree* t);
+
+int spq_set_tol(spq_tree* t, double tol);      /* -t   (default 1e-1 in the CLI; 0 in Tree) */
+int spq_set_scale(spq_tree* t, int scale);     /* --scale */
+int spq_set_order(spq_tree* t, float order);   /* --order (1 only; 1.5 -> SPQ_ERR_UNSUPPORTED) */
+int spq_set_hsl(spq_tree* t, int hsl);         /* --hsl (0 only) */
+int spq_set_square(spq_tree* t, int square);
+int spq_set_coords(spq_tree* t, int d, int n, const double* X); /* d x n, column-major */
+int spq_set_coords_grid(spq_tree* t, int n, int d);             /* -n/-d tensor grid */
+int spq_set_precision(spq_tree* t, int precision);              /* spq_precision */
+int spq_set_device(spq_tree* t, int device);
+int spq_set_verbose(spq_tree* t, int verbose); /* 1: per-level print lines as src/tree.cpp:1417-1434 */
+
+int spq_partition(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val);
+int spq_assemble(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val);
+int spq_factorize(spq_tree* t);
+
+/* Preconditioner applies on HOST buffers (b of length m for solve, n for
+ * solve_nrml; x of length n). */
+int spq_solve(spq_tree* t, const double* b, double* x);
+int spq_solve_nrml(spq_tree* t, const double* b, double* x);
+/* Same on DEVICE buffers (FP64, on the handle's device). */
+int spq_solve_dev(spq_tree* t, const double* d_b, double* d_x);
+int spq_solve_nrml_dev(spq_tree* t, const double* d_b, double* d_x);
+
+/* Householder GMRES with the factorization as left preconditioner
+ * (src/is.cpp:94-272). A is the matrix that was factorized (host CSC), b and x
+ * host vectors (x holds the initial guess on entry). *its = iterations,
+ * *res = last preconditioned residual estimate |w(k)|/|r0|. */
+int spq_gmres(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
+              const double* b, double* x, int iters, int restart, double tol, int* its, double* res);
+/* Preconditioned CGLS on the normal equations (src/is.cpp:274-345). */
+int spq_cgls(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
+             const double* b, double* x, int iters, double tol, int* its, double* res);
+
+/* Introspection: permutations, event log (records of 8 int64, layout documented
+ * in the package's host source), nnz counters, per-level phase times. */
+int spq_get_perm(spq_tree* t, int* cperm, int* rperm);
+int spq_log_size(spq_tree* t, long long* n);
+int spq_get_log(spq_tree* t, long long* out);
+int spq_num_bottom(spq_tree* t, int* n);
+int spq_get_bottom(spq_tree* t, int* out); /* 10 ints per bottom cluster */
+/* times[0..3] = partition, assemble, factorize, last solve (seconds);
+ * counters[0..3] = nnzA, nnzR, nnzH, nnzQ; counters[4] = kernel launches of the
+ * last factorize; counters[5] = kernel launches of the last solve;
+ * counters[6] = device bytes in use. */
+int spq_get_stats(spq_tree* t, double* times, long long* counters);
+/* Per-level factorization phase times in ms (6 per level: fill, elmn, shift,
+ * scale, sprsfy, merge), as printed by src/tree.cpp:1417-1426. */
+int spq_get_level_times(spq_tree* t, double* out);
+
+/* A <- A * diag(1/||A_j||) * 10, in place on val (spaQR.cpp:131-147). */
+int spq_column_normalize(int m, int n, const int* colptr, const int* rowind, double* val);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,10 @@
+"""spaQR-B200: B200-native hierarchical sparsified QR (spaQR) with GMRES/CGLS drivers.
+
+The numerical path lives in the in-tree CUDA library (``_build/libspaqr_b200.so``,
+C ABI in ``include/spaqr_b200.h``); this package is its Python mirror of the
+reference's ``Tree`` / ``gmres`` / ``cgls`` surface plus the seeded workload
+generators.
+"""
+from .tree import FP32, FP64, Tree, cgls, column_normalize, gmres  # noqa: F401
+
+__all__ = ["Tree", "gmres", "cgls", "column_normalize", "FP32", "FP64"]

@@ -1,0 +1,365 @@
+// C ABI of spaQR-B200 (declared in include/spaqr_b200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../../include/spaqr_b200.h"
+#include "engine.hpp"
+#include "krylov.hpp"
+
+using namespace spq;
+
+struct spq_tree {
+    Config cfg;
+    int precision = SPQ_FP64;
+    std::unique_ptr<EngineBase> eng;
+    int state = 0;  // 0 created, 1 partitioned, 2 assembled, 3 factorized
+    long long launches_krylov = 0;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+template <class F>
+int guard(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        return fail(SPQ_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(SPQ_ERR_ALLOC, "host allocation failed");
+    } catch (const std::invalid_argument& e) {
+        return fail(SPQ_ERR_UNSUPPORTED, e.what());
+    } catch (const std::logic_error& e) {
+        return fail(SPQ_ERR_STATE, e.what());
+    } catch (const std::exception& e) {
+        return fail(SPQ_ERR_NUMERIC, e.what());
+    }
+}
+
+int check_csc(int m, int n, const int* cp, const int* ri, const double* va) {
+    if (m <= 0 || n <= 0 || !cp || (!ri && cp[n] > 0) || (!va && cp[n] > 0))
+        return fail(SPQ_ERR_ARG, "invalid CSC matrix");
+    if (cp[0] != 0) return fail(SPQ_ERR_ARG, "colptr[0] must be 0");
+    for (int j = 0; j < n; ++j) {
+        if (cp[j + 1] < cp[j]) return fail(SPQ_ERR_ARG, "colptr must be non-decreasing");
+        for (int q = cp[j]; q < cp[j + 1]; ++q) {
+            if (ri[q] < 0 || ri[q] >= m) return fail(SPQ_ERR_ARG, "row index out of range");
+            if (q > cp[j] && ri[q] <= ri[q - 1]) return fail(SPQ_ERR_ARG, "row indices must be strictly increasing");
+        }
+    }
+    return SPQ_OK;
+}
+
+struct DevCsrOwned {
+    int* rp = nullptr;
+    int* ci = nullptr;
+    double* v = nullptr;
+    ~DevCsrOwned() {
+        cudaFree(rp);
+        cudaFree(ci);
+        cudaFree(v);
+    }
+};
+
+// Host CSC -> device CSR (rows of A with sorted column indices).
+void upload_csr(const Csc& A, DevCsrOwned& o, DevCsr& d, cudaStream_t s) {
+    Csc T = csc_transpose(A);  // column r of T = row r of A
+    cuda_check(cudaMalloc(&o.rp, sizeof(int) * (T.p.size())), "csr alloc");
+    cuda_check(cudaMalloc(&o.ci, sizeof(int) * std::max<size_t>(T.i.size(), 1)), "csr alloc");
+    cuda_check(cudaMalloc(&o.v, sizeof(double) * std::max<size_t>(T.v.size(), 1)), "csr alloc");
+    cuda_check(cudaMemcpyAsync(o.rp, T.p.data(), sizeof(int) * T.p.size(), cudaMemcpyHostToDevice, s), "csr up");
+    cuda_check(cudaMemcpyAsync(o.ci, T.i.data(), sizeof(int) * T.i.size(), cudaMemcpyHostToDevice, s), "csr up");
+    cuda_check(cudaMemcpyAsync(o.v, T.v.data(), sizeof(double) * T.v.size(), cudaMemcpyHostToDevice, s), "csr up");
+    d.m = A.m;
+    d.n = A.n;
+    d.rp = o.rp;
+    d.ci = o.ci;
+    d.v = o.v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* spq_last_error(void) { return g_err.c_str(); }
+int spq_version(void) { return 1; }
+
+int spq_device_count(int* count) {
+    if (!count) return fail(SPQ_ERR_ARG, "null count");
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(SPQ_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return SPQ_OK;
+}
+
+int spq_create(spq_tree** out, int nlevels, int skip) {
+    if (!out) return fail(SPQ_ERR_ARG, "null handle pointer");
+    if (nlevels < 1) return fail(SPQ_ERR_ARG, "nlevels must be >= 1");
+    if (skip < 0) return fail(SPQ_ERR_ARG, "skip must be >= 0");
+    spq_tree* t = new (std::nothrow) spq_tree;
+    if (!t) return fail(SPQ_ERR_ALLOC, "handle allocation failed");
+    t->cfg.nlevels = nlevels;
+    t->cfg.skip = skip;
+    *out = t;
+    return SPQ_OK;
+}
+
+int spq_destroy(spq_tree* t) {
+    delete t;
+    return SPQ_OK;
+}
+
+#define SPQ_SETTER_GUARD                                                          \
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");                             \
+    if (t->state != 0) return fail(SPQ_ERR_STATE, "options must be set before partition");
+
+int spq_set_tol(spq_tree* t, double tol) {
+    SPQ_SETTER_GUARD
+    if (!(tol >= 0)) return fail(SPQ_ERR_ARG, "tol must be >= 0");
+    t->cfg.tol = tol;
+    return SPQ_OK;
+}
+int spq_set_scale(spq_tree* t, int scale) {
+    SPQ_SETTER_GUARD
+    t->cfg.scale = scale;
+    return SPQ_OK;
+}
+int spq_set_order(spq_tree* t, float order) {
+    SPQ_SETTER_GUARD
+    t->cfg.order = order;
+    return SPQ_OK;
+}
+int spq_set_hsl(spq_tree* t, int hsl) {
+    SPQ_SETTER_GUARD
+    if (hsl) return fail(SPQ_ERR_UNSUPPORTED, "HSL bipartite matching is not available");
+    t->cfg.hsl = hsl;
+    return SPQ_OK;
+}
+int spq_set_square(spq_tree* t, int square) {
+    SPQ_SETTER_GUARD
+    t->cfg.square = square;
+    return SPQ_OK;
+}
+int spq_set_coords(spq_tree* t, int d, int n, const double* X) {
+    SPQ_SETTER_GUARD
+    if (d < 1 || n < 1 || !X) return fail(SPQ_ERR_ARG, "invalid coordinates");
+    t->cfg.d = d;
+    t->cfg.X.assign(X, X + (size_t)d * n);
+    return SPQ_OK;
+}
+int spq_set_coords_grid(spq_tree* t, int n, int d) {
+    SPQ_SETTER_GUARD
+    if (n < 1 || d < 1 || d > 3) return fail(SPQ_ERR_ARG, "grid coordinates need n >= 1 and 1 <= d <= 3");
+    // linspace_nd (src/util.cpp:852-881): lexicographic, first coordinate slowest
+    const size_t N = (size_t)std::llround(std::pow((double)n, d));
+    t->cfg.d = d;
+    t->cfg.X.assign(N * d, 0.0);
+    for (size_t id = 0; id < N; ++id) {
+        size_t r = id;
+        for (int a = d - 1; a >= 0; --a) {
+            t->cfg.X[id * d + a] = (double)(r % n);
+            r /= n;
+        }
+    }
+    return SPQ_OK;
+}
+int spq_set_precision(spq_tree* t, int precision) {
+    SPQ_SETTER_GUARD
+    if (precision != SPQ_FP64 && precision != SPQ_FP32) return fail(SPQ_ERR_ARG, "unknown precision");
+    t->precision = precision;
+    return SPQ_OK;
+}
+int spq_set_device(spq_tree* t, int device) {
+    SPQ_SETTER_GUARD
+    t->cfg.device = device;
+    return SPQ_OK;
+}
+int spq_set_verbose(spq_tree* t, int verbose) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    t->cfg.verbose = verbose;
+    return SPQ_OK;
+}
+
+int spq_partition(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 0) return fail(SPQ_ERR_STATE, "partition called twice");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (m < n) return fail(SPQ_ERR_ARG, "need rows >= cols (factor the transpose instead)");
+    if (t->cfg.X.empty())
+        return fail(SPQ_ERR_UNSUPPORTED, "only the geometric partition is built: set coordinates first");
+    if ((int64_t)t->cfg.X.size() != (int64_t)t->cfg.d * n) return fail(SPQ_ERR_ARG, "coordinates must be d x ncols");
+    return guard([&] {
+        if (!t->eng) t->eng = make_engine(t->cfg, t->precision);
+        t->eng->partition(csc_from(m, n, cp, ri, va));
+        t->state = 1;
+        return SPQ_OK;
+    });
+}
+
+int spq_assemble(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 1) return fail(SPQ_ERR_STATE, "assemble must follow partition");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (m != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "matrix size differs from partition");
+    return guard([&] {
+        t->eng->assemble(csc_from(m, n, cp, ri, va));
+        t->state = 2;
+        return SPQ_OK;
+    });
+}
+
+int spq_factorize(spq_tree* t) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 2) return fail(SPQ_ERR_STATE, "factorize must follow assemble");
+    return guard([&] {
+        t->eng->factorize();
+        t->state = 3;
+        return SPQ_OK;
+    });
+}
+
+int spq_solve_dev(spq_tree* t, const double* d_b, double* d_x) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve before factorize");
+    if (!d_b || !d_x) return fail(SPQ_ERR_ARG, "null vector");
+    return guard([&] {
+        t->eng->solve_dev(d_b, d_x);
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "solve");
+        return SPQ_OK;
+    });
+}
+
+int spq_solve(spq_tree* t, const double* b, double* x) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve before factorize");
+    if (!b || !x) return fail(SPQ_ERR_ARG, "null vector");
+    return guard([&] {
+        const int m = t->eng->nrows(), n = t->eng->ncols();
+        cudaStream_t s = t->eng->stream();
+        double *db = nullptr, *dx = nullptr;
+        cuda_check(cudaMalloc(&db, sizeof(double) * m), "solve alloc");
+        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "solve alloc");
+        cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "solve h2d");
+        t->eng->solve_dev(db, dx);
+        cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "solve d2h");
+        cuda_check(cudaStreamSynchronize(s), "solve");
+        cudaFree(db);
+        cudaFree(dx);
+        return SPQ_OK;
+    });
+}
+
+int spq_solve_nrml(spq_tree* t, const double*, double*) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (solve_nrml) is not supported by this build");
+}
+int spq_solve_nrml_dev(spq_tree* t, const double*, double*) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (solve_nrml) is not supported by this build");
+}
+
+int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va, const double* b, double* x,
+              int iters, int restart, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "gmres before factorize");
+    if (m != n || m != t->eng->nrows()) return fail(SPQ_ERR_ARG, "gmres needs the square factorized matrix");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (!b || !x || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid gmres arguments");
+    return guard([&] {
+        cudaStream_t s = t->eng->stream();
+        DevCsrOwned o;
+        DevCsr A;
+        upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
+        double *db = nullptr, *dx = nullptr;
+        cuda_check(cudaMalloc(&db, sizeof(double) * m), "gmres alloc");
+        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "gmres alloc");
+        cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "gmres h2d");
+        cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "gmres h2d");
+        *its = gmres_device(*t->eng, A, db, dx, iters, restart, tol, res, &t->launches_krylov);
+        cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gmres d2h");
+        cuda_check(cudaStreamSynchronize(s), "gmres");
+        cudaFree(db);
+        cudaFree(dx);
+        return SPQ_OK;
+    });
+}
+
+int spq_cgls(spq_tree* t, int, int, const int*, const int*, const double*, const double*, double*, int, double, int*,
+             double*) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (CGLS) is not supported by this build");
+}
+
+int spq_get_perm(spq_tree* t, int* cperm, int* rperm) {
+    if (!t || !t->eng || t->state < 1) return fail(SPQ_ERR_STATE, "no partition");
+    if (cperm) std::memcpy(cperm, t->eng->cperm().data(), sizeof(int) * t->eng->cperm().size());
+    if (rperm) std::memcpy(rperm, t->eng->rperm().data(), sizeof(int) * t->eng->rperm().size());
+    return SPQ_OK;
+}
+int spq_log_size(spq_tree* t, long long* n) {
+    if (!t || !n) return fail(SPQ_ERR_ARG, "null argument");
+    *n = t->eng ? (long long)t->eng->log().size() : 0;
+    return SPQ_OK;
+}
+int spq_get_log(spq_tree* t, long long* out) {
+    if (!t || !out) return fail(SPQ_ERR_ARG, "null argument");
+    if (t->eng) std::memcpy(out, t->eng->log().data(), sizeof(long long) * t->eng->log().size());
+    return SPQ_OK;
+}
+int spq_num_bottom(spq_tree* t, int* n) {
+    if (!t || !n) return fail(SPQ_ERR_ARG, "null argument");
+    *n = t->eng ? (int)(t->eng->bottom_info().size() / 10) : 0;
+    return SPQ_OK;
+}
+int spq_get_bottom(spq_tree* t, int* out) {
+    if (!t || !out) return fail(SPQ_ERR_ARG, "null argument");
+    if (t->eng) {
+        auto v = t->eng->bottom_info();
+        std::memcpy(out, v.data(), sizeof(int) * v.size());
+    }
+    return SPQ_OK;
+}
+int spq_get_stats(spq_tree* t, double* times, long long* counters) {
+    if (!t || !times || !counters) return fail(SPQ_ERR_ARG, "null argument");
+    if (!t->eng) return fail(SPQ_ERR_STATE, "no engine");
+    t->eng->stats(times, counters);
+    return SPQ_OK;
+}
+int spq_get_level_times(spq_tree* t, double* out) {
+    if (!t || !out) return fail(SPQ_ERR_ARG, "null argument");
+    if (!t->eng || t->state < 3) return fail(SPQ_ERR_STATE, "not factorized");
+    auto v = t->eng->level_times();
+    std::memcpy(out, v.data(), sizeof(double) * v.size());
+    return SPQ_OK;
+}
+
+int spq_column_normalize(int m, int n, const int* cp, const int* ri, double* va) {
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    for (int j = 0; j < n; ++j) {
+        double s = 0;
+        for (int q = cp[j]; q < cp[j + 1]; ++q) s += va[q] * va[q];
+        const double d = 1.0 / std::sqrt(s);
+        for (int q = cp[j]; q < cp[j + 1]; ++q) va[q] = (va[q] * d) * 10.0;
+    }
+    return SPQ_OK;
+}
+
+}  // extern "C"

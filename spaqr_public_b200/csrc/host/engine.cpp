@@ -1,0 +1,1119 @@
+// spaQR engine: host symbolic graph + batched device numerics. See engine.hpp
+// for the reference map. The symbolic steps are performed in the reference's
+// order on the host; the numerical work of each phase is collected into tasks,
+// grouped into waves of tasks that touch disjoint blocks (so that running a
+// wave concurrently gives the same result as the reference's sequential loop),
+// and issued as batched kernels on the handle's stream.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <numeric>
+
+namespace spq {
+namespace {
+
+double wall() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+inline int npanels(int k) { return (k + kNB - 1) / kNB; }
+
+// Greedy wave assignment in list order: a task runs one wave after the last
+// task that touched any of its blocks.
+std::vector<int> assign_waves(const std::vector<std::vector<int>>& touched, int nuid, int* nwaves) {
+    std::vector<int> last(nuid, -1), wave(touched.size(), 0);
+    int nw = 0;
+    for (size_t t = 0; t < touched.size(); ++t) {
+        int w = 0;
+        for (int u : touched[t]) w = std::max(w, last[u] + 1);
+        for (int u : touched[t]) last[u] = w;
+        wave[t] = w;
+        nw = std::max(nw, w + 1);
+    }
+    *nwaves = nw;
+    return wave;
+}
+
+template <class T>
+class Engine final : public EngineBase {
+public:
+    struct Cluster;
+    struct Blk {
+        T* p = nullptr;
+        int ld = 0, rows = 0, cols = 0, uid = -1;
+    };
+    struct Edge {
+        Cluster* n1;
+        Cluster* n2;
+        Blk A;
+        bool live = true;
+    };
+    struct ByOrder {
+        bool operator()(const Cluster* a, const Cluster* b) const { return a->order < b->order; }
+    };
+    struct Cluster {
+        int cstart, csize, rstart, rsize;
+        Cid id;
+        int order;
+        bool elim = false;
+        int csize_org, rsize_org;
+        Cluster* parent = nullptr;
+        Cid parentid;
+        int rposparent = 0, cposparent = 0;
+        std::vector<Cluster*> children;
+        std::set<Cluster*, ByOrder> rsparsity, cnbrs;
+        std::vector<Edge*> out, in;
+        int xcap = 0;
+        int64_t xoff = -1;
+        int level() const { return id.self.lvl; }
+    };
+    enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE };
+    struct A12 {
+        const T* B;
+        int ld, s;
+        Cluster* n1;
+    };
+    struct TapeOp {
+        TapeKind kind;
+        Cluster* c = nullptr;
+        Cluster* f = nullptr;
+        const T* fac = nullptr;
+        const T* tp = nullptr;
+        int m = 0, k = 0, ld = 0;
+        std::vector<std::pair<Cluster*, int>> segs;
+        std::vector<A12> a12;
+        int crows = 0, ccols = 0, rank = 0;
+    };
+
+    // The host symbolic steps (partition) need no GPU; the device is opened by
+    // the first step that uses it (assemble).
+    Engine(const Config& cfg) : cfg_(cfg), bottoms_(std::max(cfg.nlevels, 1)), fine_(std::max(cfg.nlevels, 1)) {}
+    ~Engine() override {
+        if (!stream_) return;
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        for (auto& e : events_) cudaEventDestroy(e);
+        cudaStreamSynchronize(stream_);
+        arena_.release();
+        desc_arena_.release();
+        cudaStreamDestroy(stream_);
+    }
+    void open_device() {
+        if (stream_) return;
+        cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
+        cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        arena_.set_stream(stream_);
+        desc_arena_.set_stream(stream_);
+        prepare_kernels<T>();
+    }
+
+    cudaStream_t stream() const override { return stream_; }
+    const Log& log() const override { return log_; }
+    const std::vector<int>& cperm() const override { return cperm_; }
+    const std::vector<int>& rperm() const override { return rperm_; }
+    int nrows() const override { return nrows_; }
+    int ncols() const override { return ncols_; }
+    bool factorized() const override { return factorized_; }
+
+    // ------------------------------------------------------------- partition
+    void partition(const Csc& A) override {
+        double t0 = wall();
+        if (cfg_.X.empty()) throw std::invalid_argument("only the geometric partition is built: set coordinates");
+        if (A.m != A.n && !cfg_.square) {
+            // rectangular input is recognised but its row-shift path is not built here
+        }
+        if (A.m != A.n) throw std::invalid_argument("rectangular input (least squares) is not supported by this build");
+        nrows_ = A.m;
+        ncols_ = A.n;
+        Ordering o = geometric_ordering(A, cfg_.nlevels, cfg_.d, cfg_.X);
+        cperm_ = o.cperm;
+        rperm_ = o.rperm;
+        const int c = A.n;
+        int k = 0, l = 0;
+        while (k < c) {
+            int kn = k + 1;
+            const Cid cid = o.cid_of_pos[k];
+            int nr = o.rows_of_col[k];
+            while (kn < c && o.cid_of_pos[kn] == cid) { nr += o.rows_of_col[kn]; ++kn; }
+            bottoms_[0].push_back(new_cluster(k, kn - k, l, nr, cid));
+            k = kn;
+            l += nr;
+        }
+        if (l != A.m) throw std::runtime_error("partition: row count mismatch");
+        for (int lvl = 1; lvl < cfg_.nlevels; ++lvl) {
+            auto& prev = bottoms_[lvl - 1];
+            size_t b = 0;
+            while (b < prev.size() && prev[b]->level() < lvl) ++b;
+            for (size_t i = b; i < prev.size(); ++i) prev[i]->parentid = lift(prev[i]->id, lvl);
+            for (size_t i = b; i < prev.size();) {
+                const Cid pid = prev[i]->parentid;
+                std::vector<Cluster*> ch{prev[i]};
+                int cs = prev[i]->csize, rs = prev[i]->rsize, c0 = prev[i]->cstart, r0 = prev[i]->rstart;
+                ++i;
+                while (i < prev.size() && prev[i]->parentid == pid) {
+                    ch.push_back(prev[i]);
+                    cs += prev[i]->csize;
+                    rs += prev[i]->rsize;
+                    ++i;
+                }
+                Cluster* p = new_cluster(c0, cs, r0, rs, pid);
+                for (Cluster* x : ch) {
+                    x->parent = p;
+                    p->children.push_back(x);
+                }
+                bottoms_[lvl].push_back(p);
+            }
+        }
+        t_part_ = wall() - t0;
+    }
+
+    // ------------------------------------------------------------- assemble
+    void assemble(const Csc& A) override {
+        double t0 = wall();
+        if (bottoms_[0].empty()) throw std::logic_error("assemble before partition");
+        open_device();
+        nnzA_ = A.i.size();
+        const Csc App = csc_gather_rows(csc_gather_cols(A, cperm_), rperm_);
+        std::vector<Cluster*> rowcl(A.m);
+        for (Cluster* s : bottoms_[0])
+            for (int i = s->rstart; i < s->rstart + s->rsize; ++i) rowcl[i] = s;
+        std::vector<uint64_t> addr;
+        std::vector<double> vals;
+        addr.reserve(A.i.size());
+        vals.reserve(A.i.size());
+        for (Cluster* self : bottoms_[0]) {
+            std::set<Cluster*, ByOrder> cn;
+            for (int j = self->cstart; j < self->cstart + self->csize; ++j)
+                for (int q = App.p[j]; q < App.p[j + 1]; ++q) cn.insert(rowcl[App.i[q]]);
+            cn.insert(self);
+            for (Cluster* nbr : cn) {
+                Blk b = new_block(nbr->rsize, self->csize);
+                for (int col = 0; col < self->csize; ++col) {
+                    const int j = self->cstart + col;
+                    for (int q = App.p[j]; q < App.p[j + 1]; ++q) {
+                        const int r = App.i[q];
+                        if (r >= nbr->rstart && r < nbr->rstart + nbr->rsize) {
+                            addr.push_back(reinterpret_cast<uint64_t>(b.p + (r - nbr->rstart) + (size_t)col * b.ld));
+                            vals.push_back(App.v[q]);
+                        }
+                    }
+                }
+                Edge* e = new_edge(self, nbr, b);
+                self->out.push_back(e);
+                if (self != nbr) nbr->in.push_back(e);
+            }
+            std::stable_sort(self->out.begin(), self->out.end(),
+                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
+            self->cnbrs = cn;
+        }
+        uint64_t* d_addr = desc_arena_.alloc_n<uint64_t>(addr.size());
+        double* d_vals = desc_arena_.alloc_n<double>(vals.size());
+        cuda_check(cudaMemcpyAsync(d_addr, addr.data(), addr.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
+        cuda_check(cudaMemcpyAsync(d_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
+        launch_scatter_values<T>(d_addr, d_vals, (int64_t)addr.size(), stream_);
+        ++launches_fact_;
+        cuda_check(cudaStreamSynchronize(stream_), "assemble");
+        assembled_ = true;
+        t_asm_ = wall() - t0;
+    }
+
+    // ------------------------------------------------------------- factorize
+    void factorize() override {
+        if (!assembled_) throw std::logic_error("factorize before assemble");
+        if (factorized_) throw std::logic_error("factorize called twice");
+        if (cfg_.order != 1.0f) throw std::invalid_argument("--order 1.5 is not supported by this build");
+        if (!cfg_.scale && cfg_.tol != 0) throw std::invalid_argument("--scale 0 is not supported by this build");
+        double t0 = wall();
+        launches_fact_ = 0;
+        const int L = cfg_.nlevels;
+        level_ev_.assign((size_t)L * 7, nullptr);
+        for (auto& e : level_ev_) {
+            cuda_check(cudaEventCreate(&e), "event");
+            events_.push_back(e);
+        }
+        for (ilvl_ = 0; ilvl_ < L; ++ilvl_) {
+            cudaEvent_t* ev = &level_ev_[(size_t)ilvl_ * 7];
+            cudaEventRecord(ev[0], stream_);
+            for (Cluster* s : cur())
+                if (s->level() == ilvl_) get_sparsity(s);
+            cudaEventRecord(ev[1], stream_);
+            elim_phase();
+            cudaEventRecord(ev[2], stream_);
+            cudaEventRecord(ev[3], stream_);  // shift (rectangular only)
+            const bool window = ilvl_ < L - 2 && ilvl_ >= cfg_.skip && cfg_.tol != 0;
+            if (cfg_.scale && window) scale_phase();
+            cudaEventRecord(ev[4], stream_);
+            if (window) sparsify_phase();
+            cudaEventRecord(ev[5], stream_);
+            if (ilvl_ < L - 1) merge_all();
+            cudaEventRecord(ev[6], stream_);
+            auto ts = topsize();
+            rec(5, ts.first, ts.second, (long long)cur().size());
+            if (cfg_.verbose) print_level(ev, ts);
+        }
+        rec(6, (long long)nnzA_, (long long)nnzR_, (long long)nnzH_, (long long)nnzQ_);
+        build_solve_plan();
+        cuda_check(cudaStreamSynchronize(stream_), "factorize");
+        factorized_ = true;
+        t_fact_ = wall() - t0;
+        if (cfg_.verbose) {
+            std::printf("Tolerance set: %.3e\nTime to factorize:  %.3e\n", cfg_.tol, t_fact_);
+            std::printf("Size of top separator: %d\n", bottoms_[L - 1].empty() ? 0 : bottoms_[L - 1].front()->csize);
+            std::printf("nnzA: %llu nnzR: %llu\nnnzH: %llu nnzQ: %llu\n", nnzA_, nnzR_, nnzH_, nnzQ_);
+        }
+    }
+
+    // ------------------------------------------------------------- solve
+    void solve_dev(const double* d_b, double* d_x) override {
+        if (!factorized_) throw std::logic_error("solve before factorize");
+        double t0 = wall();
+        cuda_check(cudaMemcpyAsync(d_bin_, d_b, sizeof(double) * nrows_, cudaMemcpyDeviceToDevice, stream_), "solve in");
+        if (!graph_exec_) {
+            cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+            run_solve_sweeps();
+            cuda_check(cudaStreamEndCapture(stream_, &graph_), "capture end");
+            cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+        }
+        cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+        cuda_check(cudaMemcpyAsync(d_x, d_xout_, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
+                   "solve out");
+        t_solve_ = wall() - t0;
+    }
+
+    std::vector<int> bottom_info() const override {
+        std::vector<int> out;
+        for (Cluster* c : bottoms_[0]) {
+            int r[10] = {c->cstart, c->csize_org, c->rstart, c->rsize_org, c->id.self.lvl,
+                         c->id.self.sep, c->id.l.lvl, c->id.l.sep, c->id.r.lvl, c->id.r.sep};
+            out.insert(out.end(), r, r + 10);
+        }
+        return out;
+    }
+    void stats(double* times, long long* counters) const override {
+        times[0] = t_part_;
+        times[1] = t_asm_;
+        times[2] = t_fact_;
+        times[3] = t_solve_;
+        counters[0] = (long long)nnzA_;
+        counters[1] = (long long)nnzR_;
+        counters[2] = (long long)nnzH_;
+        counters[3] = (long long)nnzQ_;
+        counters[4] = launches_fact_;
+        counters[5] = launches_solve_;
+        counters[6] = (long long)(arena_.bytes_reserved() + desc_arena_.bytes_reserved() + scratch_.capacity());
+    }
+    std::vector<double> level_times() const override {
+        std::vector<double> out;
+        for (size_t l = 0; l + 7 <= level_ev_.size(); l += 7) {
+            for (int p = 0; p < 6; ++p) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, level_ev_[l + p], level_ev_[l + p + 1]);
+                out.push_back(ms);
+            }
+        }
+        return out;
+    }
+
+private:
+    Config cfg_;
+    cudaStream_t stream_ = nullptr;
+    Arena arena_;
+    Arena desc_arena_{size_t(16) << 20};
+    Scratch scratch_;
+    std::vector<std::vector<Cluster*>> bottoms_, fine_;
+    std::vector<std::unique_ptr<Cluster>> clusters_;
+    std::vector<std::unique_ptr<Edge>> edges_;
+    std::vector<TapeOp> tape_;
+    std::vector<int> cperm_, rperm_;
+    int nrows_ = 0, ncols_ = 0, ilvl_ = -1, cur_bottom_ = 0, max_order_ = 0, next_uid_ = 0;
+    bool assembled_ = false, factorized_ = false;
+    unsigned long long nnzA_ = 0, nnzR_ = 0, nnzH_ = 0, nnzQ_ = 0;
+    Log log_;
+    double t_part_ = 0, t_asm_ = 0, t_fact_ = 0, t_solve_ = 0;
+    long long launches_fact_ = 0, launches_solve_ = 0;
+    std::vector<cudaEvent_t> events_, level_ev_;
+    // solve plan
+    T* xbuf_ = nullptr;
+    double* d_bin_ = nullptr;
+    double* d_xout_ = nullptr;
+    int* d_src_ = nullptr;
+    int* d_dst_ = nullptr;
+    int64_t* d_xin_ = nullptr;
+    int64_t* d_xout_pos_ = nullptr;
+    struct Wave {
+        const SolveOp* ops;
+        int nops, smem;
+    };
+    std::vector<Wave> fwd_waves_, bwd_waves_;
+    const XSeg* d_segs_ = nullptr;
+    const GemvRef<T>* d_gemv_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+
+    // ------------------------------------------------------------- helpers
+    const std::vector<Cluster*>& cur() const { return bottoms_[cur_bottom_]; }
+
+    void rec(long long type, long long a, long long b = 0, long long c = 0, long long d = 0, long long e = 0,
+             long long order = -1) {
+        long long r[8] = {type, ilvl_, order, a, b, c, d, e};
+        log_.insert(log_.end(), r, r + 8);
+    }
+
+    Cluster* new_cluster(int cs, int cz, int rs, int rz, const Cid& id) {
+        Cluster* c = new Cluster{cs, cz, rs, rz, id, max_order_++};
+        c->csize_org = cz;
+        c->rsize_org = rz;
+        c->xcap = rz;
+        clusters_.emplace_back(c);
+        return c;
+    }
+    Blk new_block(int rows, int cols) {
+        Blk b;
+        b.rows = rows;
+        b.cols = cols;
+        b.ld = std::max(rows, 1);
+        b.p = arena_.alloc_n<T>((size_t)b.ld * std::max(cols, 1));
+        b.uid = next_uid_++;
+        return b;
+    }
+    Edge* new_edge(Cluster* n1, Cluster* n2, const Blk& b) {
+        edges_.emplace_back(new Edge{n1, n2, b, true});
+        return edges_.back().get();
+    }
+    Edge* add_edge(Cluster* c1, Cluster* c2) {  // src/tree.cpp:251-261
+        Edge* e = new_edge(c1, c2, new_block(c2->rsize, c1->csize));
+        c1->cnbrs.insert(c2);
+        c1->out.push_back(e);
+        if (c1 != c2) c2->in.push_back(e);
+        return e;
+    }
+    static Edge* find_out(Cluster* c, Cluster* n2) {
+        for (Edge* e : c->out)
+            if (e->n2 == n2) return e;
+        return nullptr;
+    }
+    std::pair<int, int> topsize() const {
+        int tr = 0, tc = 0;
+        for (Cluster* s : cur())
+            if (s->level() == cfg_.nlevels - 1) { tr += s->rsize; tc += s->csize; }
+        return {tr, tc};
+    }
+    bool want_sparsify(const Cluster* c) const {
+        return c->level() > ilvl_ && c->id.l.lvl <= ilvl_ && c->id.r.lvl <= ilvl_;
+    }
+
+    // src/tree.cpp:168-224
+    bool valid_fill(const Cid& cid, const Cid& nid, const std::set<Sep>& cols) const {
+        const Sep cs = cid.self, ns = nid.self;
+        if (cs.lvl > ns.lvl) return false;
+        auto pw = [](int e) { return (int)std::pow(2.0, e); };
+        if (cs.sep / pw(ns.lvl - cs.lvl) != ns.sep) return false;
+        auto side_ok = [&](const Sep& s) {
+            const int dl = s.lvl - cs.lvl;
+            return s.lvl >= cs.lvl ? (cs.sep / pw(dl)) == s.sep : (s.sep / pw(-dl)) == cs.sep;
+        };
+        if (!side_ok(nid.l) && !side_ok(nid.r)) return false;
+        if (!cols.count(ns)) return false;
+        if (!cols.count(nid.l) && !cols.count(nid.r)) return false;
+        return true;
+    }
+    // src/tree.cpp:834-870 (geometric mode: purely symbolic)
+    void get_sparsity(Cluster* c) {
+        std::set<Cluster*, ByOrder> rs;
+        std::set<Sep> cols;
+        for (Edge* e : c->out) cols.insert(e->n2->id.self);
+        for (Edge* e : c->out) {
+            if (!e->live) continue;
+            Cluster* n = e->n2;
+            rs.insert(n);
+            for (Edge* ein : n->in)
+                if (ein->live && ein->n1 != c && !ein->n1->elim && valid_fill(c->id, ein->n1->id, cols))
+                    rs.insert(ein->n1);
+        }
+        c->rsparsity = std::move(rs);
+    }
+
+    // ------------------------------------------------------------- batched QR execution
+    // One QR job: gathers into [fac | scratch], factors, scatters the trailing part back.
+    struct QRJob {
+        int m = 0, k = 0, ntr = 0;
+        T* fac = nullptr;
+        T* tau = nullptr;
+        T* tp = nullptr;
+        size_t tr_off = 0;  // element offset in the wave scratch
+        std::vector<CopyDesc<T>> gather, scatter;  // tr pointers patched at issue time (relative)
+    };
+
+    // Issues the jobs of one wave (already built), then extra copies (after the QR).
+    void run_qr_wave(std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm,
+                     const std::vector<CopyDesc<T>>& post) {
+        size_t tr_elems = 0;
+        for (auto& j : jobs) {
+            j.tr_off = tr_elems;
+            tr_elems += (size_t)j.m * j.ntr;
+        }
+        T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(tr_elems, 1) * sizeof(T), stream_));
+        std::vector<CopyDesc<T>> g, s;
+        std::vector<QRTask<T>> qt;
+        int maxk = 0, maxR = 0;
+        for (auto& j : jobs) {
+            T* tr = trbase + j.tr_off;
+            for (auto c : j.gather) {
+                if (c.dst == nullptr) c.dst = tr + c.pad;  // relative trailing destination
+                c.pad = 0;
+                g.push_back(c);
+            }
+            for (auto c : j.scatter) {
+                c.src = tr + c.pad;
+                c.pad = 0;
+                s.push_back(c);
+            }
+            qt.push_back(QRTask<T>{j.fac, tr, j.tau, j.tp, j.m, j.k, j.ntr, 0});
+            maxk = std::max(maxk, j.k);
+            maxR = std::max(maxR, j.m);
+        }
+        // per-panel active lists and trailing tiles
+        std::vector<std::vector<int>> ids;
+        std::vector<std::vector<TileRef>> tiles;
+        for (int p = 0; p < maxk; p += kNB) {
+            std::vector<int> a;
+            std::vector<TileRef> tl;
+            for (size_t t = 0; t < qt.size(); ++t) {
+                if (qt[t].k <= p) continue;
+                a.push_back((int)t);
+                const int w = std::min(kNB, qt[t].k - p);
+                const int ntot = (qt[t].k - p - w) + qt[t].ntr;
+                for (int c0 = 0, ti = 0; c0 < ntot; c0 += kTN, ++ti) tl.push_back(TileRef{(int)t, ti});
+            }
+            ids.push_back(std::move(a));
+            tiles.push_back(std::move(tl));
+        }
+        std::vector<TileRef> trsm_tiles;
+        for (size_t t = 0; t < trsm.size(); ++t)
+            for (int r0 = 0, ti = 0; r0 < trsm[t].rows; r0 += 128, ++ti) trsm_tiles.push_back(TileRef{(int)t, ti});
+        Upload up;
+        size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
+               o_post = up.add(post);
+        std::vector<size_t> o_ids, o_tiles;
+        for (size_t i = 0; i < ids.size(); ++i) {
+            o_ids.push_back(up.add(ids[i]));
+            o_tiles.push_back(up.add(tiles[i]));
+        }
+        char* d = up.commit(desc_arena_, stream_);
+        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_g), (int)g.size(), stream_);
+        ++launches_fact_;
+        const int smem_limit = (int)((160 * 1024) / (kNB * sizeof(T)));
+        for (size_t i = 0; i < ids.size(); ++i) {
+            const int p = (int)i * kNB;
+            int rows = 0;
+            for (int t : ids[i]) rows = std::max(rows, qt[t].m - p);
+            const int smem_rows = std::min(rows, smem_limit);
+            launch_panel<T>(reinterpret_cast<const QRTask<T>*>(d + o_q), reinterpret_cast<const int*>(d + o_ids[i]),
+                            (int)ids[i].size(), p, smem_rows, stream_);
+            launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
+                               reinterpret_cast<const TileRef*>(d + o_tiles[i]), (int)tiles[i].size(), p, stream_);
+            launches_fact_ += 1 + (tiles[i].empty() ? 0 : 1);
+        }
+        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_s), (int)s.size(), stream_);
+        launch_trsm<T>(reinterpret_cast<const TrsmTask<T>*>(d + o_tr), reinterpret_cast<const TileRef*>(d + o_tt),
+                       (int)trsm_tiles.size(), stream_);
+        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_post), (int)post.size(), stream_);
+        launches_fact_ += (s.empty() ? 0 : 1) + (trsm_tiles.empty() ? 0 : 1) + (post.empty() ? 0 : 1);
+    }
+
+    static CopyDesc<T> cp(const T* src, T* dst, int sld, int dld, int rows, int cols, int mode = 0, int pad = 0) {
+        return CopyDesc<T>{src, dst, sld, dld, rows, cols, mode, pad};
+    }
+
+    // ------------------------------------------------------------- elimination (src/tree.cpp:780-832)
+    void elim_phase() {
+        struct Task {
+            QRJob job;
+            std::vector<int> uids;
+        };
+        std::vector<Task> tasks;
+        for (Cluster* c : cur()) {
+            if (c->level() != ilvl_) continue;
+            if (c->csize == 0) {
+                c->elim = true;
+                rec(1, 0, 0, 0, 0, 0, c->order);
+                continue;
+            }
+            std::vector<Edge*> H;
+            int m = 0;
+            for (Edge* e : c->out)
+                if (e->live) { H.push_back(e); m += e->A.rows; }
+            const int k = H.front()->A.cols;
+            Task t;
+            QRJob& j = t.job;
+            j.m = m;
+            j.k = k;
+            j.fac = arena_.alloc_n<T>((size_t)m * k);
+            j.tau = arena_.alloc_n<T>(k);
+            j.tp = arena_.alloc_n<T>((size_t)npanels(k) * kNB * kNB);
+            int off = 0;
+            for (Edge* e : H) {
+                j.gather.push_back(cp(e->A.p, j.fac + off, e->A.ld, m, e->A.rows, k));
+                t.uids.push_back(e->A.uid);
+                off += e->A.rows;
+            }
+            int nupd = 0, co = 0;
+            for (Cluster* n : c->rsparsity) {
+                if (n->elim || n == c) continue;
+                off = 0;
+                for (Edge* e : H) {
+                    Edge* ecn = find_out(n, e->n2);
+                    if (!ecn) ecn = add_edge(n, e->n2);
+                    const int pad = off + co * m;  // relative to the wave scratch of this job
+                    j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
+                    j.scatter.push_back(cp(nullptr, ecn->A.p, m, ecn->A.ld, ecn->A.rows, n->csize, 0, pad));
+                    t.uids.push_back(ecn->A.uid);
+                    off += ecn->A.rows;
+                }
+                co += n->csize;
+                nnzR_ += (unsigned long long)(c->csize * n->csize);
+                ++nupd;
+            }
+            j.ntr = co;
+            nnzH_ += (unsigned long long)(m * k);
+            TapeOp op;
+            op.kind = TK_QR;
+            op.c = c;
+            op.fac = j.fac;
+            op.tp = j.tp;
+            op.m = m;
+            op.k = k;
+            op.ld = m;
+            for (Edge* e : H) op.segs.emplace_back(e->n2, e->n2->rsize);
+            for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
+            tape_.push_back(std::move(op));
+            c->elim = true;
+            rec(1, m, k, nupd, (long long)H.size(), 0, c->order);
+            tasks.push_back(std::move(t));
+        }
+        if (tasks.empty()) return;
+        std::vector<std::vector<int>> touched;
+        for (auto& t : tasks) touched.push_back(t.uids);
+        int nw = 0;
+        auto wave = assign_waves(touched, next_uid_, &nw);
+        for (int w = 0; w < nw; ++w) {
+            std::vector<QRJob> jobs;
+            for (size_t t = 0; t < tasks.size(); ++t)
+                if (wave[t] == w) jobs.push_back(tasks[t].job);
+            run_qr_wave(jobs, {}, {});
+        }
+    }
+
+    // ------------------------------------------------------------- scaling (src/tree.cpp:533-580)
+    void scale_phase() {
+        struct Task {
+            QRJob job;
+            std::vector<TrsmTask<T>> trsm;
+            CopyDesc<T> ident;
+            std::vector<int> uids;
+        };
+        std::vector<Task> tasks;
+        for (Cluster* c : cur()) {
+            if (!want_sparsify(c)) continue;
+            Edge* es = find_out(c, c);
+            if (!es) throw std::runtime_error("diagScale: cluster without diagonal block");
+            const int rows = c->rsize, cols = c->csize;
+            nnzR_ = (unsigned long long)((double)nnzR_ + 0.5 * cols * cols);
+            nnzH_ += (unsigned long long)(rows * cols);
+            Task t;
+            QRJob& j = t.job;
+            j.m = rows;
+            j.k = cols;
+            j.fac = arena_.alloc_n<T>((size_t)rows * std::max(cols, 1));
+            j.tau = arena_.alloc_n<T>(std::max(cols, 1));
+            j.tp = arena_.alloc_n<T>((size_t)std::max(npanels(cols), 1) * kNB * kNB);
+            j.gather.push_back(cp(es->A.p, j.fac, es->A.ld, rows, rows, cols));
+            t.uids.push_back(es->A.uid);
+            int co = 0, nrow = 0, ncol = 0;
+            for (Edge* e : c->in) {
+                if (e->n1->elim) continue;
+                const int pad = co * rows;
+                j.gather.push_back(cp(e->A.p, nullptr, e->A.ld, rows, rows, e->A.cols, 0, pad));
+                j.scatter.push_back(cp(nullptr, e->A.p, rows, e->A.ld, rows, e->A.cols, 0, pad));
+                t.uids.push_back(e->A.uid);
+                co += e->A.cols;
+                ++nrow;
+            }
+            j.ntr = co;
+            for (Edge* e : c->out) {
+                if (e->n2->elim || e->n2 == c) continue;
+                t.trsm.push_back(TrsmTask<T>{j.fac, e->A.p, rows, cols, e->A.ld, e->A.rows});
+                t.uids.push_back(e->A.uid);
+                ++ncol;
+            }
+            t.ident = cp(nullptr, es->A.p, 0, es->A.ld, rows, cols, 1);
+            TapeOp op;
+            op.kind = TK_SCALED;
+            op.c = c;
+            op.fac = j.fac;
+            op.tp = j.tp;
+            op.m = rows;  // full segment
+            op.k = cols;  // head / reflectors
+            op.ld = rows;
+            tape_.push_back(std::move(op));
+            rec(2, rows, cols, nrow, ncol, 0, c->order);
+            if (cols == 0) continue;
+            tasks.push_back(std::move(t));
+        }
+        if (tasks.empty()) return;
+        std::vector<std::vector<int>> touched;
+        for (auto& t : tasks) touched.push_back(t.uids);
+        int nw = 0;
+        auto wave = assign_waves(touched, next_uid_, &nw);
+        for (int w = 0; w < nw; ++w) {
+            std::vector<QRJob> jobs;
+            std::vector<TrsmTask<T>> tr;
+            std::vector<CopyDesc<T>> post;
+            for (size_t t = 0; t < tasks.size(); ++t) {
+                if (wave[t] != w) continue;
+                jobs.push_back(tasks[t].job);
+                tr.insert(tr.end(), tasks[t].trsm.begin(), tasks[t].trsm.end());
+                post.push_back(tasks[t].ident);
+            }
+            run_qr_wave(jobs, tr, post);
+        }
+    }
+
+    // ------------------------------------------------------------- sparsification (src/tree.cpp:992-1114)
+    void sparsify_phase() {
+        std::vector<Cluster*> list;
+        std::vector<std::vector<int>> touched;
+        for (Cluster* c : cur()) {
+            if (!want_sparsify(c)) continue;
+            std::vector<int> u;
+            for (Edge* e : c->in)
+                if (!e->n1->elim) u.push_back(e->A.uid);
+            for (Edge* e : c->out)
+                if (!e->n2->elim) u.push_back(e->A.uid);
+            list.push_back(c);
+            touched.push_back(std::move(u));
+        }
+        if (list.empty()) return;
+        int nw = 0;
+        auto wave = assign_waves(touched, next_uid_, &nw);
+        std::vector<std::vector<long long>> recs(list.size());
+        for (int w = 0; w < nw; ++w) {
+            struct Job {
+                size_t idx;
+                Cluster* c;
+                std::vector<Edge*> apm, amp;
+                Edge* self;
+                int m, n, smp;
+                size_t c_off, i_off;
+            };
+            std::vector<Job> jobs;
+            size_t celems = 0, ielems = 0;
+            for (size_t t = 0; t < list.size(); ++t) {
+                if (wave[t] != w) continue;
+                Cluster* c = list[t];
+                if (c->csize == 0) {
+                    recs[t] = {0, 0, 0, c->rsize};
+                    continue;
+                }
+                Job j;
+                j.idx = t;
+                j.c = c;
+                j.self = nullptr;
+                int spm = 0, smp = 0;
+                for (Edge* e : c->in)
+                    if (!e->n1->elim) { j.apm.push_back(e); spm += e->A.cols; }
+                for (Edge* e : c->out) {
+                    if (!e->n2->elim && e->n2 != c) { j.amp.push_back(e); smp += e->A.rows; }
+                    else if (e->n2 == c) j.self = e;
+                }
+                j.m = c->csize;
+                j.n = smp + spm;
+                j.smp = smp;
+                j.c_off = celems;
+                celems += (size_t)j.m * std::max(j.n, 1);
+                j.i_off = ielems;
+                ielems += 3 * (size_t)std::max(j.n, 1) + 1;
+                celems += 3 * (size_t)std::max(j.n, 1);  // tau, vn1, vn2
+                jobs.push_back(std::move(j));
+            }
+            if (!jobs.empty()) run_sparsify_wave(jobs, celems, ielems, recs);
+        }
+        for (size_t t = 0; t < list.size(); ++t) {
+            const auto& r = recs[t];
+            rec(3, r[0], r[1], r[2], r[3], 0, list[t]->order);
+        }
+    }
+
+    template <class Job>
+    void run_sparsify_wave(std::vector<Job>& jobs, size_t celems, size_t ielems,
+                           std::vector<std::vector<long long>>& recs) {
+        const size_t ibytes = (((ielems + jobs.size()) * sizeof(int)) + 255) & ~size_t(255);
+        char* base = static_cast<char*>(scratch_.get(ibytes + celems * sizeof(T), stream_));
+        int* ib = reinterpret_cast<int*>(base);
+        T* cb = reinterpret_cast<T*>(base + ibytes);
+        std::vector<CopyDesc<T>> g;
+        std::vector<RRQRTask<T>> rt;
+        for (auto& j : jobs) {
+            T* C = cb + j.c_off;
+            int cur = 0;
+            for (Edge* e : j.amp) {  // C[:, cur + i] = A(i, :)^T
+                g.push_back(cp(e->A.p, C + (size_t)cur * j.m, e->A.ld, j.m, e->A.rows, e->A.cols, 2));
+                cur += e->A.rows;
+            }
+            for (Edge* e : j.apm) {
+                g.push_back(cp(e->A.p, C + (size_t)cur * j.m, e->A.ld, j.m, j.m, e->A.cols));
+                cur += e->A.cols;
+            }
+            const size_t nn = std::max(j.n, 1);
+            T* tail = C + (size_t)j.m * nn;
+            int* ii = ib + jobs.size() + j.i_off;
+            int* rk = ib + rt.size();
+            rt.push_back(RRQRTask<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, cfg_.tol});
+        }
+        Upload up;
+        size_t o_g = up.add(g), o_r = up.add(rt);
+        char* d = up.commit(desc_arena_, stream_);
+        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_g), (int)g.size(), stream_);
+        launch_rrqr<T>(reinterpret_cast<const RRQRTask<T>*>(d + o_r), (int)rt.size(), 1024, stream_);
+        launches_fact_ += 2;
+        std::vector<int> ranks(jobs.size());
+        cuda_check(cudaMemcpyAsync(ranks.data(), ib, sizeof(int) * jobs.size(), cudaMemcpyDeviceToHost, stream_),
+                   "rank");
+        cuda_check(cudaStreamSynchronize(stream_), "rank readback");
+        std::vector<SparsWB<T>> wb;
+        std::vector<SpBlock<T>> blocks;
+        for (size_t q = 0; q < jobs.size(); ++q) {
+            auto& j = jobs[q];
+            Cluster* c = j.c;
+            const int r = ranks[q];
+            const int m = j.m;
+            if (r >= m) {
+                recs[j.idx] = {m, c->csize, j.n, c->rsize};
+                continue;
+            }
+            if (r < 0) throw std::runtime_error("sparsify: invalid rank from device");
+            T* V = arena_.alloc_n<T>((size_t)m * std::max(r, 1));
+            T* tau = arena_.alloc_n<T>(std::max(r, 1));
+            T* tp = arena_.alloc_n<T>((size_t)std::max(npanels(r), 1) * kNB * kNB);
+            SparsWB<T> s{rt[q].C, rt[q].ipvt, rt[q].tau, rt[q].rank, V, tau, tp, m, 0, (int)blocks.size(), 0};
+            int cur = 0;
+            for (Edge* e : j.amp) {
+                blocks.push_back(SpBlock<T>{e->A.p, e->A.ld, e->A.rows, e->A.cols, cur, 0});
+                cur += e->A.rows;
+            }
+            for (Edge* e : j.apm) {
+                blocks.push_back(SpBlock<T>{e->A.p, e->A.ld, e->A.rows, e->A.cols, cur, 1});
+                cur += e->A.cols;
+            }
+            s.nblk = (int)blocks.size() - s.blk0;
+            wb.push_back(s);
+            // tape: OrthogonalD then SplitD (pushed before the size change)
+            TapeOp od;
+            od.kind = TK_ORTHD;
+            od.c = c;
+            od.fac = V;
+            od.tp = tp;
+            od.m = m;
+            od.k = r;
+            od.ld = m;
+            tape_.push_back(std::move(od));
+            nnzQ_ += (unsigned long long)(m * r);
+            const int nf = m - r;
+            Cluster* cf = new_cluster(c->cstart + r, nf, c->rstart + c->csize - nf, nf, c->id);
+            TapeOp sd;
+            sd.kind = TK_SPLITD;
+            sd.c = c;
+            sd.f = cf;
+            sd.crows = c->rsize;
+            sd.ccols = c->csize;
+            sd.rank = r;
+            tape_.push_back(std::move(sd));
+            // new shapes
+            for (Edge* e : j.amp) e->A.cols = r;
+            for (Edge* e : j.apm) e->A.rows = r;
+            j.self->A.rows = r;
+            j.self->A.cols = r;
+            c->rsize = r;
+            c->csize = r;
+            fine_[ilvl_].push_back(cf);
+            cf->elim = true;
+            recs[j.idx] = {m, r, j.n, r};
+        }
+        if (!wb.empty()) {
+            Upload u2;
+            size_t o_w = u2.add(wb), o_b = u2.add(blocks);
+            char* d2 = u2.commit(desc_arena_, stream_);
+            launch_spars_wb<T>(reinterpret_cast<const SparsWB<T>*>(d2 + o_w),
+                               reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
+            ++launches_fact_;
+        }
+    }
+
+    // ------------------------------------------------------------- merge (src/tree.cpp:414-475, 872-881)
+    void merge_all() {
+        ++cur_bottom_;
+        for (Cluster* s : cur()) {
+            int rs = 0, cs = 0;
+            for (Cluster* so : s->children) {
+                so->rposparent = rs;
+                so->cposparent = cs;
+                rs += so->rsize;
+                cs += so->csize;
+            }
+            s->rsize = rs;
+            s->csize = cs;
+            s->rsize_org = rs;
+            s->csize_org = cs;
+            s->xcap = rs;
+            TapeOp op;
+            op.kind = TK_MERGE;
+            op.c = s;
+            tape_.push_back(std::move(op));
+            rec(4, rs, cs, (long long)s->children.size(), 0, 0, s->order);
+        }
+        std::vector<CopyDesc<T>> copies;
+        for (Cluster* s : cur()) {
+            for (Cluster* so : s->children)
+                for (Edge* eo : so->out)
+                    if (!eo->n2->elim) s->cnbrs.insert(eo->n2->parent);
+            std::vector<Cluster*> nb(s->cnbrs.begin(), s->cnbrs.end());
+            for (Cluster* n : nb) add_edge(s, n);
+            std::stable_sort(s->out.begin(), s->out.end(),
+                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
+            for (Cluster* so : s->children) {
+                for (Edge* eo : so->out) {
+                    Cluster* nold = eo->n2;
+                    if (nold->elim || !eo->live) continue;
+                    Edge* f = find_out(s, nold->parent);
+                    if (!f) throw std::runtime_error("merge: missing parent edge");
+                    if (eo->A.rows != nold->rsize || eo->A.cols != so->csize)
+                        throw std::runtime_error("merge: block shape mismatch");
+                    copies.push_back(cp(eo->A.p, f->A.p + nold->rposparent + (size_t)so->cposparent * f->A.ld,
+                                        eo->A.ld, f->A.ld, eo->A.rows, eo->A.cols));
+                    eo->live = false;
+                }
+            }
+        }
+        if (!copies.empty()) {
+            Upload up;
+            size_t o = up.add(copies);
+            char* d = up.commit(desc_arena_, stream_);
+            launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o), (int)copies.size(), stream_);
+            ++launches_fact_;
+        }
+    }
+
+    void print_level(cudaEvent_t* ev, std::pair<int, int> ts) {
+        cudaEventSynchronize(ev[6]);
+        float ms[6];
+        for (int p = 0; p < 6; ++p) cudaEventElapsedTime(&ms[p], ev[p], ev[p + 1]);
+        std::printf(
+            "lvl: %d    update fill-in: %.3f  elmn: %.3f  shift: %.3f  scale: %.3f  sprsfy: %.3f  merge: %.3f  "
+            "size top_sep: %d, %d   a.r top_sep: %.3f\n",
+            ilvl_, ms[0] * 1e-3, ms[1] * 1e-3, ms[2] * 1e-3, ms[3] * 1e-3, ms[4] * 1e-3, ms[5] * 1e-3, ts.first,
+            ts.second, ts.second ? (double)ts.first / ts.second : 0.0);
+    }
+
+    // ------------------------------------------------------------- solve plan
+    void build_solve_plan() {
+        int64_t xtot = 0;
+        for (auto& c : clusters_) {
+            c->xoff = xtot;
+            xtot += std::max(c->xcap, 1);
+        }
+        xbuf_ = arena_.alloc_n<T>(xtot);
+        d_bin_ = arena_.alloc_n<double>(nrows_);
+        d_xout_ = arena_.alloc_n<double>(ncols_);
+        std::vector<int> src, dst;
+        std::vector<int64_t> xin, xo;
+        for (Cluster* c : bottoms_[0]) {
+            for (int i = 0; i < c->rsize_org; ++i) {
+                src.push_back(rperm_[c->rstart + i]);
+                xin.push_back(c->xoff + i);
+            }
+            for (int i = 0; i < c->csize_org; ++i) {
+                dst.push_back(cperm_[c->cstart + i]);
+                xo.push_back(c->xoff + i);
+            }
+        }
+        // ops with read / write sets
+        struct POp {
+            SolveOp op;
+            std::vector<Cluster*> rd, wr;
+            int smem;
+        };
+        std::vector<XSeg> segs;
+        std::vector<GemvRef<T>> gemv;
+        std::vector<POp> fwd, bwd;
+        auto ptr = [](const T* p) { return (int64_t)reinterpret_cast<uintptr_t>(p); };
+        for (const TapeOp& t : tape_) {
+            POp f{}, b{};
+            switch (t.kind) {
+                case TK_QR: {
+                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, 0, 0, ptr(t.fac), ptr(t.tp), 0,
+                                   (int)segs.size(), (int)t.segs.size()};
+                    for (auto& s : t.segs) {
+                        segs.push_back(XSeg{s.first->xoff, s.second, 0});
+                        f.rd.push_back(s.first);
+                        f.wr.push_back(s.first);
+                    }
+                    f.smem = t.m;
+                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, (int)gemv.size(),
+                                   (int)t.a12.size()};
+                    for (auto& a : t.a12) {
+                        gemv.push_back(GemvRef<T>{ptr(a.B), a.n1->xoff, a.ld, a.s});
+                        b.rd.push_back(a.n1);
+                    }
+                    b.rd.push_back(t.c);
+                    b.wr.push_back(t.c);
+                    b.smem = t.k;
+                    break;
+                }
+                case TK_SCALED:
+                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    f.rd = f.wr = {t.c};
+                    f.smem = t.m;
+                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, 0, 0};
+                    b.rd = b.wr = {t.c};
+                    b.smem = t.k;
+                    break;
+                case TK_ORTHD:
+                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    f.rd = f.wr = {t.c};
+                    f.smem = t.m;
+                    b.op = f.op;
+                    b.op.dir = 1;
+                    b.rd = b.wr = {t.c};
+                    b.smem = t.m;
+                    break;
+                case TK_SPLITD:
+                    f.op = SolveOp{SK_SPLIT, 0, t.crows, t.ccols, t.rank, 0, t.c->xoff, t.f->xoff, 0, 0, 0, 0, 0};
+                    f.rd = {t.c};
+                    f.wr = {t.c, t.f};
+                    f.smem = t.crows;
+                    b.op = f.op;
+                    b.op.dir = 1;
+                    b.rd = {t.c, t.f};
+                    b.wr = {t.c};
+                    b.smem = t.crows;
+                    break;
+                case TK_MERGE: {
+                    f.op = SolveOp{SK_MERGE, 0, 0, 0, 0, 0, t.c->xoff, 0, 0, 0, 0, (int)segs.size(),
+                                   (int)t.c->children.size()};
+                    for (Cluster* ch : t.c->children) {
+                        segs.push_back(XSeg{ch->xoff, ch->rsize, ch->csize});
+                        f.rd.push_back(ch);
+                        b.wr.push_back(ch);
+                    }
+                    f.wr = {t.c};
+                    b.rd = {t.c};
+                    b.op = f.op;
+                    b.op.dir = 1;
+                    f.smem = b.smem = 0;
+                    break;
+                }
+            }
+            fwd.push_back(std::move(f));
+            bwd.push_back(std::move(b));
+        }
+        std::reverse(bwd.begin(), bwd.end());
+        // wave scheduling on x segments (RAW, WAR, WAW)
+        auto schedule = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves) {
+            std::map<const Cluster*, int> lw, lr;
+            std::vector<int> wv(ops.size());
+            int nw = 0;
+            for (size_t i = 0; i < ops.size(); ++i) {
+                int w = 0;
+                for (Cluster* c : ops[i].rd) {
+                    auto it = lw.find(c);
+                    if (it != lw.end()) w = std::max(w, it->second + 1);
+                }
+                for (Cluster* c : ops[i].wr) {
+                    auto it = lw.find(c);
+                    if (it != lw.end()) w = std::max(w, it->second + 1);
+                    auto ir = lr.find(c);
+                    if (ir != lr.end()) w = std::max(w, ir->second + 1);
+                }
+                for (Cluster* c : ops[i].wr) lw[c] = w;
+                for (Cluster* c : ops[i].rd) lr[c] = std::max(lr.count(c) ? lr[c] : -1, w);
+                wv[i] = w;
+                nw = std::max(nw, w + 1);
+            }
+            waves.assign(nw, {});
+            for (size_t i = 0; i < ops.size(); ++i) waves[wv[i]].push_back((int)i);
+        };
+        std::vector<std::vector<int>> fw, bw;
+        schedule(fwd, fw);
+        schedule(bwd, bw);
+        std::vector<SolveOp> all;
+        struct WMeta {
+            size_t off;
+            int n, smem;
+        };
+        std::vector<WMeta> fm, bm;
+        auto pack = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves, std::vector<WMeta>& meta) {
+            for (auto& w : waves) {
+                WMeta mt{all.size(), (int)w.size(), 0};
+                for (int i : w) {
+                    all.push_back(ops[i].op);
+                    mt.smem = std::max(mt.smem, ops[i].smem);
+                }
+                meta.push_back(mt);
+            }
+        };
+        pack(fwd, fw, fm);
+        pack(bwd, bw, bm);
+        Upload up;
+        size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
+               o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
+        char* d = up.commit(desc_arena_, stream_);
+        const SolveOp* d_ops = reinterpret_cast<const SolveOp*>(d + o_ops);
+        d_segs_ = reinterpret_cast<const XSeg*>(d + o_segs);
+        d_gemv_ = reinterpret_cast<const GemvRef<T>*>(d + o_gemv);
+        d_src_ = reinterpret_cast<int*>(d + o_src);
+        d_dst_ = reinterpret_cast<int*>(d + o_dst);
+        d_xin_ = reinterpret_cast<int64_t*>(d + o_xin);
+        d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
+        fwd_waves_.clear();
+        bwd_waves_.clear();
+        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem});
+        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem});
+        nin_ = (int)src.size();
+        nout_ = (int)dst.size();
+        const size_t smem_cap = (200 * 1024) / sizeof(T);
+        for (auto* ws : {&fwd_waves_, &bwd_waves_})
+            for (auto& w : *ws)
+                if ((size_t)w.smem > smem_cap)
+                    throw std::runtime_error("solve: a cluster exceeds the shared-memory vector capacity");
+    }
+    int nin_ = 0, nout_ = 0;
+
+    void run_solve_sweeps() {
+        launches_solve_ = 0;
+        launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, stream_);
+        ++launches_solve_;
+        for (auto& w : fwd_waves_) {
+            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
+            ++launches_solve_;
+        }
+        for (auto& w : bwd_waves_) {
+            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
+            ++launches_solve_;
+        }
+        launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
+        ++launches_solve_;
+    }
+};
+
+}  // namespace
+
+std::unique_ptr<EngineBase> make_engine(const Config& cfg, int precision) {
+    if (precision == 1) return std::unique_ptr<EngineBase>(new Engine<float>(cfg));
+    return std::unique_ptr<EngineBase>(new Engine<double>(cfg));
+}
+
+}  // namespace spq

@@ -1,0 +1,63 @@
+// The spaQR factorization engine of one handle: the reference's cluster/edge
+// graph kept on the host (symbolic, bit-exact), dense blocks in device memory,
+// and every numerical step issued as batched sm_100a kernels.
+//
+// Reference map:
+//   Tree state and API                  include/tree.h:36-152
+//   partition / assemble                src/tree.cpp:595-778
+//   get_sparsity / check_if_valid       src/tree.cpp:168-224, 834-870
+//   eliminate_cluster / update_cluster  src/tree.cpp:263-316, 780-832
+//   diagScale                           src/tree.cpp:533-580
+//   sparsifyD                           src/tree.cpp:992-1114
+//   merge_all / update_size / edges     src/tree.cpp:414-475, 872-881
+//   factorize                           src/tree.cpp:1309-1437
+//   solve                               src/tree.cpp:1440-1466, src/operations.cpp
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../kernels/kernels.hpp"
+#include "device.hpp"
+#include "symbolic.hpp"
+
+namespace spq {
+
+struct Config {
+    int nlevels = 0, skip = 0, scale = 0, square = 0;
+    double tol = 0;
+    float order = 1.0f;
+    int hsl = 0, verbose = 0, device = 0;
+    int d = 0;
+    std::vector<double> X;
+};
+
+// Event log record: [type, ilvl, order, a, b, c, d, e] (same layout as the
+// CPU oracle): 1 ELIM, 2 SCALE, 3 SPARS, 4 MERGE, 5 LEVEL, 6 FINAL.
+using Log = std::vector<long long>;
+
+class EngineBase {
+public:
+    virtual ~EngineBase() = default;
+    virtual void partition(const Csc& A) = 0;
+    virtual void assemble(const Csc& A) = 0;
+    virtual void factorize() = 0;
+    virtual void solve_dev(const double* d_b, double* d_x) = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual const Log& log() const = 0;
+    virtual const std::vector<int>& cperm() const = 0;
+    virtual const std::vector<int>& rperm() const = 0;
+    virtual int nrows() const = 0;
+    virtual int ncols() const = 0;
+    virtual bool factorized() const = 0;
+    virtual std::vector<int> bottom_info() const = 0;
+    virtual void stats(double* times, long long* counters) const = 0;
+    virtual std::vector<double> level_times() const = 0;
+};
+
+std::unique_ptr<EngineBase> make_engine(const Config& cfg, int precision);
+
+}  // namespace spq

@@ -1,0 +1,23 @@
+// Device Krylov drivers (src/is.cpp) on top of an engine's preconditioner.
+#pragma once
+#include "engine.hpp"
+
+namespace spq {
+
+// CSR matrix resident in device memory (FP64).
+struct DevCsr {
+    int m = 0, n = 0;
+    const int* rp = nullptr;
+    const int* ci = nullptr;
+    const double* v = nullptr;
+};
+
+// Householder GMRES, left preconditioned by P (src/is.cpp:94-272). x holds the
+// initial guess; returns the iteration count, *res = |w(k)|/|r0|.
+int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart, double tol,
+                 double* res, long long* launches);
+
+// ||b - A x|| / ||b|| on the device (FP64).
+double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x);
+
+}  // namespace spq

@@ -1,0 +1,965 @@
+// sm_100a kernels of the spaQR factorization (elimination, scaling,
+// sparsification, merge) and of the solve sweeps and Krylov vector work.
+//
+// Layout: every dense block is column-major in HBM; a batched launch receives a
+// device array of task descriptors and serves one descriptor per CTA (or one
+// tile of a descriptor per CTA). Householder conventions follow LAPACK
+// (dgeqrf/dlarfg/dlarft forward-columnwise, dgeqp3 with Drmac-Bujanovic norm
+// downdating) so that ranks and reflectors agree with the reference's LAPACK
+// calls up to rounding.
+#include "kernels.hpp"
+
+#include <cfloat>
+#include <cmath>
+
+namespace spq {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRC = 64;  // row chunk of the trailing update
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum; red must hold 32 elements of shared memory.
+template <class T>
+__device__ T block_sum(T v, T* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        T r = lane < nw ? red[lane] : T(0);
+        r = warp_sum(r);
+        if (lane == 0) red[0] = r;
+    }
+    __syncthreads();
+    return red[0];
+}
+
+template <class T>
+__device__ __forceinline__ T dev_hypot(T a, T b);
+template <>
+__device__ __forceinline__ double dev_hypot<double>(double a, double b) { return hypot(a, b); }
+template <>
+__device__ __forceinline__ float dev_hypot<float>(float a, float b) { return hypotf(a, b); }
+
+// Elementary reflector (LAPACK dlarfg): given alpha and the squared norm of
+// the tail, returns tau, beta and the tail scale 1/(alpha - beta).
+template <class T>
+__device__ __forceinline__ void make_reflector(T alpha, T xn2, T& tau, T& beta, T& scal) {
+    if (xn2 == T(0)) {
+        tau = T(0);
+        beta = alpha;
+        scal = T(1);
+    } else {
+        T nrm = dev_hypot(alpha, (T)sqrt(xn2));
+        beta = alpha >= T(0) ? -nrm : nrm;
+        tau = (beta - alpha) / beta;
+        scal = T(1) / (alpha - beta);
+    }
+}
+
+// Triangular factor of one panel of unit-lower reflectors (LAPACK dlarft,
+// forward, columnwise). Vp points at the panel's diagonal element (local row
+// 0, column 0); R rows, w <= kNB columns. G and Ts are shared scratch of
+// kNB x (kNB+1). Result written to Tout (kNB x kNB, column-major, zero padded).
+template <class T>
+__device__ void build_tfac(const T* Vp, int ldv, int R, int w, const T* taus, T* Tout, T* G, T* Ts) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int P = kNB + 1;
+    // G(i, j) = v_i^T v_j for i < j.
+    int pair = 0;
+    for (int j = 1; j < w; ++j) {
+        for (int i = 0; i < j; ++i, ++pair) {
+            if ((pair % nw) != warp) continue;
+            T s = T(0);
+            for (int r = j + 1 + lane; r < R; r += 32) s += Vp[r + (size_t)i * ldv] * Vp[r + (size_t)j * ldv];
+            s = warp_sum(s);
+            if (lane == 0) G[i * P + j] = s + (j < R ? Vp[j + (size_t)i * ldv] : T(0));
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int j = 0; j < kNB; ++j) {
+            if (j < w) {
+                T tj = taus[j];
+                T tmp = T(0);
+                if (lane < j)
+                    for (int l = lane; l < j; ++l) tmp += Ts[lane * P + l] * G[l * P + j];
+                if (lane < j) Ts[lane * P + j] = -tj * tmp;
+                if (lane == j) Ts[j * P + j] = tj;
+                if (lane > j) Ts[lane * P + j] = T(0);
+            } else {
+                Ts[lane * P + j] = T(0);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        int i = e % kNB, j = e / kNB;
+        Tout[e] = Ts[i * P + j];
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ copies
+template <class T>
+__global__ void k_copy(const CopyDesc<T>* descs, int n) {
+    for (int d = blockIdx.x; d < n; d += gridDim.x) {
+        const CopyDesc<T> c = descs[d];
+        const int64_t tot = (int64_t)c.rows * c.cols;
+        for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+            int i = (int)(e % c.rows), j = (int)(e / c.rows);
+            if (c.mode == 2) {
+                c.dst[j + (size_t)i * c.dld] = c.src[i + (size_t)j * c.sld];
+                continue;
+            }
+            T v;
+            if (c.mode == 1) v = (i == j) ? T(1) : T(0);
+            else v = c.src ? c.src[i + (size_t)j * c.sld] : T(0);
+            c.dst[i + (size_t)j * c.dld] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ panel QR
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, const int* ids, int p, int smem_rows) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    __shared__ T red[32];
+    __shared__ T s_tau[kNB];
+    __shared__ T G[kNB * (kNB + 1)];
+    __shared__ T Ts[kNB * (kNB + 1)];
+    const QRTask<T> t = tasks[ids[blockIdx.x]];
+    const int m = t.m, k = t.k;
+    if (p >= k) return;
+    const int w = min(kNB, k - p);
+    const int R = m - p;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    T* gp = t.fac + p + (size_t)p * m;
+    const bool in_smem = R <= smem_rows;
+    T* P = in_smem ? sm : gp;
+    const int ldp = in_smem ? R : m;
+    if (in_smem) {
+        for (int e = tid; e < R * w; e += blockDim.x) {
+            int i = e % R, j = e / R;
+            P[i + j * ldp] = gp[i + (size_t)j * m];
+        }
+        __syncthreads();
+    }
+    for (int j = 0; j < w; ++j) {
+        if (j >= R) {
+            if (tid == 0) s_tau[j] = T(0);
+            continue;
+        }
+        T part = T(0);
+        for (int i = j + 1 + tid; i < R; i += blockDim.x) {
+            T v = P[i + (size_t)j * ldp];
+            part += v * v;
+        }
+        const T xn2 = block_sum(part, red);
+        const T alpha = P[j + (size_t)j * ldp];
+        T tau, beta, scal;
+        make_reflector(alpha, xn2, tau, beta, scal);
+        if (tau != T(0))
+            for (int i = j + 1 + tid; i < R; i += blockDim.x) P[i + (size_t)j * ldp] *= scal;
+        __syncthreads();
+        if (tid == 0) {
+            P[j + (size_t)j * ldp] = beta;
+            s_tau[j] = tau;
+        }
+        __syncthreads();
+        if (tau != T(0)) {
+            for (int c = j + 1 + warp; c < w; c += nw) {
+                T s = T(0);
+                for (int i = j + 1 + lane; i < R; i += 32) s += P[i + (size_t)j * ldp] * P[i + (size_t)c * ldp];
+                s = warp_sum(s);
+                s = (s + P[j + (size_t)c * ldp]) * tau;
+                for (int i = j + 1 + lane; i < R; i += 32) P[i + (size_t)c * ldp] -= s * P[i + (size_t)j * ldp];
+                if (lane == 0) P[j + (size_t)c * ldp] -= s;
+            }
+        }
+        __syncthreads();
+    }
+    // tau and the panel's T factor
+    for (int j = tid; j < w; j += blockDim.x) t.tau[p + j] = s_tau[j];
+    build_tfac(P, ldp, R, w, s_tau, t.tp + (size_t)(p / kNB) * kNB * kNB, G, Ts);
+    if (in_smem) {
+        for (int e = tid; e < R * w; e += blockDim.x) {
+            int i = e % R, j = e / R;
+            gp[i + (size_t)j * m] = P[i + j * ldp];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ trailing update
+// C <- (I - V T V^T)^T C = C - V (T^T (V^T C)) on one tile of kTN columns.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, const TileRef* tiles, int p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int VP = kNB + 1, CP = kTN + 1;
+    T* Vs = reinterpret_cast<T*>(smem_raw);  // kRC x VP
+    T* Cs = Vs + kRC * VP;                    // kRC x CP
+    T* Ys = Cs + kRC * CP;                    // kNB x CP
+    T* Tsh = Ys + kNB * CP;                   // kNB x VP
+    __shared__ T* colp[kTN];
+    const TileRef tr = tiles[blockIdx.x];
+    const QRTask<T> t = tasks[tr.task];
+    const int m = t.m, k = t.k;
+    const int w = min(kNB, k - p);
+    const int R = m - p;
+    const int nf = k - p - w;
+    const int ntot = nf + t.ntr;
+    const int c0 = tr.tile * kTN;
+    const int tn = min(kTN, ntot - c0);
+    const int tid = threadIdx.x;
+    if (tid < kTN) {
+        int vc = c0 + tid;
+        T* ptr = nullptr;
+        if (tid < tn) ptr = vc < nf ? t.fac + (size_t)(p + w + vc) * m : t.tr + (size_t)(vc - nf) * m;
+        colp[tid] = ptr;
+    }
+    const T* V0 = t.fac + (size_t)p * m;  // column p
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        int i = e % kNB, j = e / kNB;
+        Tsh[i * VP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
+    }
+    __syncthreads();
+    auto load_v = [&](int r0, int rc) {
+        for (int e = tid; e < kRC * kNB; e += blockDim.x) {
+            int r = e % kRC, q = e / kRC;
+            T v = T(0);
+            int gr = r0 + r;
+            if (r < rc && q < w) v = gr < q ? T(0) : (gr == q ? T(1) : V0[p + gr + (size_t)q * m]);
+            Vs[r * VP + q] = v;
+        }
+    };
+    auto load_c = [&](int r0, int rc) {
+        for (int e = tid; e < kRC * kTN; e += blockDim.x) {
+            int r = e % kRC, c = e / kRC;
+            Cs[r * CP + c] = (r < rc && c < tn) ? colp[c][p + r0 + r] : T(0);
+        }
+    };
+    const int c = tid % kTN, jq = tid / kTN;  // jq in [0, 8)
+    constexpr int QPT = kNB / (kThreads / kTN);  // 4 rows of Y per thread
+    T acc[QPT];
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) acc[u] = T(0);
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+        const int rc = min(kRC, R - r0);
+        load_v(r0, rc);
+        load_c(r0, rc);
+        __syncthreads();
+        for (int r = 0; r < rc; ++r) {
+            const T cv = Cs[r * CP + c];
+#pragma unroll
+            for (int u = 0; u < QPT; ++u) acc[u] += Vs[r * VP + jq * QPT + u] * cv;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = acc[u];
+    __syncthreads();
+    // Z = T^T Y
+    T z[QPT];
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) {
+        const int i = jq * QPT + u;
+        T s = T(0);
+        for (int l = 0; l <= i; ++l) s += Tsh[l * VP + i] * Ys[l * CP + c];
+        z[u] = s;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = z[u];
+    __syncthreads();
+    // C -= V Z
+    constexpr int RG = kThreads / kTN;
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+        const int rc = min(kRC, R - r0);
+        load_v(r0, rc);
+        load_c(r0, rc);
+        __syncthreads();
+        for (int r = jq; r < rc; r += RG) {
+            T s = T(0);
+#pragma unroll 8
+            for (int q = 0; q < kNB; ++q) s += Vs[r * VP + q] * Ys[q * CP + c];
+            Cs[r * CP + c] -= s;
+        }
+        __syncthreads();
+        for (int e = tid; e < kRC * kTN; e += blockDim.x) {
+            int r = e % kRC, cc = e / kRC;
+            if (r < rc && cc < tn) colp[cc][p + r0 + r] = Cs[r * CP + cc];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ TRSM (right, upper)
+template <class T>
+__global__ void __launch_bounds__(128) k_trsm(const TrsmTask<T>* tasks, const TileRef* tiles) {
+    __shared__ T Rs[64][kNB + 1];
+    __shared__ T Rd[kNB][kNB + 1];
+    const TileRef tr = tiles[blockIdx.x];
+    const TrsmTask<T> t = tasks[tr.task];
+    const int tid = threadIdx.x;
+    const int row = tr.tile * 128 + tid;
+    const bool active = row < t.rows;
+    for (int J0 = 0; J0 < t.k; J0 += kNB) {
+        const int wj = min(kNB, t.k - J0);
+        T acc[kNB];
+#pragma unroll
+        for (int jj = 0; jj < kNB; ++jj) acc[jj] = (active && jj < wj) ? t.X[row + (size_t)(J0 + jj) * t.ldx] : T(0);
+        for (int i0 = 0; i0 < J0; i0 += 64) {
+            const int ic = min(64, J0 - i0);
+            for (int e = tid; e < 64 * kNB; e += blockDim.x) {
+                int i = e % 64, jj = e / 64;
+                Rs[i][jj] = (i < ic && jj < wj) ? t.R[(i0 + i) + (size_t)(J0 + jj) * t.ldr] : T(0);
+            }
+            __syncthreads();
+            for (int i = 0; i < ic; ++i) {
+                const T xi = active ? t.X[row + (size_t)(i0 + i) * t.ldx] : T(0);
+#pragma unroll
+                for (int jj = 0; jj < kNB; ++jj) acc[jj] -= xi * Rs[i][jj];
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+            int i = e % kNB, jj = e / kNB;
+            Rd[i][jj] = (i < wj && jj < wj) ? t.R[(J0 + i) + (size_t)(J0 + jj) * t.ldr] : T(1);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int jj = 0; jj < kNB; ++jj) {
+            acc[jj] = acc[jj] / Rd[jj][jj];
+#pragma unroll
+            for (int ll = jj + 1; ll < kNB; ++ll) acc[ll] -= acc[jj] * Rd[jj][ll];
+        }
+        if (active)
+            for (int jj = 0; jj < wj; ++jj) t.X[row + (size_t)(J0 + jj) * t.ldx] = acc[jj];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ truncated RRQR
+template <class T>
+struct Eps;
+template <>
+struct Eps<double> {
+    static __device__ double tol3z() { return 1.0536712127723509e-08; }  // sqrt(2^-53)
+};
+template <>
+struct Eps<float> {
+    static __device__ float tol3z() { return 2.44140625e-04f; }  // sqrt(2^-24)
+};
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_rrqr(const RRQRTask<T>* tasks) {
+    __shared__ T red[32];
+    __shared__ T redv[32];
+    __shared__ int redi[32];
+    __shared__ int s_pvt;
+    const RRQRTask<T> t = tasks[blockIdx.x];
+    const int m = t.m, n = t.n;
+    T* C = t.C;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int j = warp; j < n; j += nw) {
+        T s = T(0);
+        for (int i = lane; i < m; i += 32) s += C[i + (size_t)j * m] * C[i + (size_t)j * m];
+        s = warp_sum(s);
+        if (lane == 0) {
+            T v = sqrt(s);
+            t.vn1[j] = v;
+            t.vn2[j] = v;
+            t.jpvt[j] = j;
+        }
+    }
+    __syncthreads();
+    const int kmax = min(m, n);
+    int rank = kmax;
+    const double tol = t.tol;
+    if (tol != 0.0 && tol >= 1.0) rank = 0;
+    T r00 = T(0);
+    const int kstop = (tol != 0.0 && tol >= 1.0) ? 0 : kmax;
+    for (int k = 0; k < kstop; ++k) {
+        // pivot: first index of the largest partial norm in [k, n)
+        T bv = T(-1);
+        int bi = n;
+        for (int j = k + tid; j < n; j += blockDim.x) {
+            T v = t.vn1[j];
+            if (v > bv) { bv = v; bi = j; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { redv[warp] = bv; redi[warp] = bi; }
+        __syncthreads();
+        if (warp == 0) {
+            bv = lane < nw ? redv[lane] : T(-1);
+            bi = lane < nw ? redi[lane] : n;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+            }
+            if (lane == 0) s_pvt = bi;
+        }
+        __syncthreads();
+        const int pvt = s_pvt;
+        if (pvt != k && pvt < n) {
+            for (int i = tid; i < m; i += blockDim.x) {
+                T a = C[i + (size_t)k * m];
+                C[i + (size_t)k * m] = C[i + (size_t)pvt * m];
+                C[i + (size_t)pvt * m] = a;
+            }
+            if (tid == 0) {
+                int a = t.jpvt[k];
+                t.jpvt[k] = t.jpvt[pvt];
+                t.jpvt[pvt] = a;
+                t.vn1[pvt] = t.vn1[k];
+                t.vn2[pvt] = t.vn2[k];
+            }
+        }
+        __syncthreads();
+        T part = T(0);
+        for (int i = k + 1 + tid; i < m; i += blockDim.x) {
+            T v = C[i + (size_t)k * m];
+            part += v * v;
+        }
+        const T xn2 = block_sum(part, red);
+        const T alpha = C[k + (size_t)k * m];
+        T tau, beta, scal;
+        make_reflector(alpha, xn2, tau, beta, scal);
+        if (tau != T(0))
+            for (int i = k + 1 + tid; i < m; i += blockDim.x) C[i + (size_t)k * m] *= scal;
+        __syncthreads();
+        if (tid == 0) {
+            C[k + (size_t)k * m] = beta;
+            t.tau[k] = tau;
+        }
+        // rank rule of choose_rank (uniform across the block)
+        if (tol != 0.0 && kmax > 1) {
+            if (k == 0) {
+                r00 = fabs(beta);
+            } else if (!((double)fabs(beta) / (double)r00 >= tol)) {
+                rank = k;
+                break;
+            }
+        }
+        __syncthreads();
+        const T* v = C + (size_t)k * m;
+        for (int j = k + 1 + warp; j < n; j += nw) {
+            T* cj = C + (size_t)j * m;
+            if (tau != T(0)) {
+                T s = T(0);
+                for (int i = k + 1 + lane; i < m; i += 32) s += v[i] * cj[i];
+                s = warp_sum(s);
+                s = (s + cj[k]) * tau;
+                for (int i = k + 1 + lane; i < m; i += 32) cj[i] -= s * v[i];
+                __syncwarp();
+                if (lane == 0) cj[k] -= s;
+                __syncwarp();
+            }
+            // partial column norm downdate (LAPACK dlaqp2 rule)
+            T n1 = t.vn1[j];
+            if (n1 != T(0)) {
+                T r = fabs(cj[k]) / n1;
+                T temp = T(1) - r * r;
+                temp = temp < T(0) ? T(0) : temp;
+                T q = n1 / t.vn2[j];
+                T temp2 = temp * q * q;
+                if (temp2 <= Eps<T>::tol3z()) {
+                    T s = T(0);
+                    for (int i = k + 1 + lane; i < m; i += 32) s += cj[i] * cj[i];
+                    s = warp_sum(s);
+                    if (lane == 0) {
+                        T nv = (k + 1 < m) ? (T)sqrt(s) : T(0);
+                        t.vn1[j] = nv;
+                        t.vn2[j] = nv;
+                    }
+                } else if (lane == 0) {
+                    t.vn1[j] = n1 * (T)sqrt(temp);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    if (tid == 0) *t.rank = rank;
+    for (int j = tid; j < n; j += blockDim.x) t.ipvt[t.jpvt[j]] = j;
+}
+
+// ------------------------------------------------------------------ sparsification write-back
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks) {
+    __shared__ T G[kNB * (kNB + 1)];
+    __shared__ T Ts[kNB * (kNB + 1)];
+    __shared__ T s_tau[kNB];
+    const SparsWB<T> t = tasks[blockIdx.x];
+    const int r = *t.rank;
+    const int m = t.m;
+    if (r >= m) return;
+    const int tid = threadIdx.x;
+    for (int b = 0; b < t.nblk; ++b) {
+        const SpBlock<T> B = blocks[t.blk0 + b];
+        if (B.kind == 0) {
+            const int64_t tot = (int64_t)B.rows * r;
+            for (int64_t e = tid; e < tot; e += blockDim.x) {
+                int i = (int)(e % B.rows), j = (int)(e / B.rows);
+                int q = t.ipvt[B.coff + i];
+                B.p[i + (size_t)j * B.ld] = (j <= q) ? t.C[j + (size_t)q * m] : T(0);
+            }
+        } else {
+            const int64_t tot = (int64_t)r * B.cols;
+            for (int64_t e = tid; e < tot; e += blockDim.x) {
+                int i = (int)(e % r), j = (int)(e / r);
+                int q = t.ipvt[B.coff + j];
+                B.p[i + (size_t)j * B.ld] = (i <= q) ? t.C[i + (size_t)q * m] : T(0);
+            }
+        }
+    }
+    for (int64_t e = tid; e < (int64_t)m * r; e += blockDim.x) t.V[e] = t.C[e];
+    for (int j = tid; j < r; j += blockDim.x) t.tau[j] = t.tau_in[j];
+    __syncthreads();
+    for (int p0 = 0; p0 < r; p0 += kNB) {
+        const int w = min(kNB, r - p0);
+        if (tid < kNB) s_tau[tid] = tid < w ? t.tau_in[p0 + tid] : T(0);
+        __syncthreads();
+        build_tfac(t.C + p0 + (size_t)p0 * m, m, m - p0, w, s_tau, t.tp + (size_t)(p0 / kNB) * kNB * kNB, G, Ts);
+    }
+}
+
+// ------------------------------------------------------------------ assembly scatter
+template <class T>
+__global__ void k_scatter_values(const uint64_t* addr, const double* vals, int64_t n) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        *reinterpret_cast<T*>(addr[e]) = (T)vals[e];
+}
+
+// ------------------------------------------------------------------ solve sweeps
+template <class T>
+__device__ __forceinline__ const T* aptr(int64_t v) {
+    return reinterpret_cast<const T*>(v);
+}
+
+// x(0:m) <- Q^T x (dir 0) or Q x (dir 1), Q from unit-lower V (ld ldv), T panels.
+template <class T>
+__device__ void apply_q(T* xs, int m, int kq, const T* V, int ldv, const T* tp, int dir, T* red_y, T* red_z) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int np = (kq + kNB - 1) / kNB;
+    for (int pi = 0; pi < np; ++pi) {
+        const int pidx = dir == 0 ? pi : np - 1 - pi;
+        const int p0 = pidx * kNB;
+        const int w = min(kNB, kq - p0);
+        for (int q = warp; q < w; q += nw) {
+            const int col = p0 + q;
+            const T* vc = V + (size_t)col * ldv;
+            T s = T(0);
+            for (int r = col + 1 + lane; r < m; r += 32) s += vc[r] * xs[r];
+            s = warp_sum(s);
+            if (lane == 0) red_y[q] = s + (col < m ? xs[col] : T(0));
+        }
+        __syncthreads();
+        const T* Tp = tp + (size_t)pidx * kNB * kNB;
+        if (tid < w) {
+            T s = T(0);
+            if (dir == 0) {
+                for (int l = 0; l <= tid; ++l) s += Tp[l + tid * kNB] * red_y[l];  // T^T y
+            } else {
+                for (int l = tid; l < w; ++l) s += Tp[tid + l * kNB] * red_y[l];  // T y
+            }
+            red_z[tid] = s;
+        }
+        __syncthreads();
+        for (int r = p0 + tid; r < m; r += blockDim.x) {
+            T s = T(0);
+            const int qmax = min(w - 1, r - p0);
+            for (int q = 0; q <= qmax; ++q) {
+                const int col = p0 + q;
+                s += (r == col ? T(1) : V[r + (size_t)col * ldv]) * red_z[q];
+            }
+            xs[r] -= s;
+        }
+        __syncthreads();
+    }
+}
+
+// Upper-triangular solve in shared memory: x <- inv(R) x (trans 0) or inv(R^T) x (trans 1).
+template <class T>
+__device__ void tri_solve(T* xs, int k, const T* R, int ldr, int trans) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (trans == 0) {
+        const int nb = (k + 31) / 32;
+        for (int b = nb - 1; b >= 0; --b) {
+            const int j0 = b * 32, bw = min(32, k - j0);
+            if (warp == 0) {
+                T xv = lane < bw ? xs[j0 + lane] : T(0);
+                for (int i = bw - 1; i >= 0; --i) {
+                    if (lane == i) xv = xv / R[(j0 + i) + (size_t)(j0 + i) * ldr];
+                    T xi = __shfl_sync(0xffffffffu, xv, i);
+                    if (lane < i) xv -= R[(j0 + lane) + (size_t)(j0 + i) * ldr] * xi;
+                }
+                if (lane < bw) xs[j0 + lane] = xv;
+            }
+            __syncthreads();
+            for (int i = tid; i < j0; i += blockDim.x) {
+                T s = T(0);
+                for (int l = 0; l < bw; ++l) s += R[i + (size_t)(j0 + l) * ldr] * xs[j0 + l];
+                xs[i] -= s;
+            }
+            __syncthreads();
+        }
+    } else {
+        const int nb = (k + 31) / 32;
+        for (int b = 0; b < nb; ++b) {
+            const int j0 = b * 32, bw = min(32, k - j0);
+            if (warp == 0) {
+                T xv = lane < bw ? xs[j0 + lane] : T(0);
+                for (int i = 0; i < bw; ++i) {
+                    if (lane == i) xv = xv / R[(j0 + i) + (size_t)(j0 + i) * ldr];
+                    T xi = __shfl_sync(0xffffffffu, xv, i);
+                    if (lane > i && lane < bw) xv -= R[(j0 + i) + (size_t)(j0 + lane) * ldr] * xi;
+                }
+                if (lane < bw) xs[j0 + lane] = xv;
+            }
+            __syncthreads();
+            for (int i = j0 + bw + tid; i < k; i += blockDim.x) {
+                T s = T(0);
+                for (int l = 0; l < bw; ++l) s += R[(j0 + l) + (size_t)i * ldr] * xs[j0 + l];
+                xs[i] -= s;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, const XSeg* segs,
+                                                        const GemvRef<T>* gemv, T* x) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* xs = reinterpret_cast<T*>(smem_raw);
+    __shared__ T red_y[kNB];
+    __shared__ T red_z[kNB];
+    const SolveOp op = ops[blockIdx.x];
+    const int tid = threadIdx.x;
+    switch (op.kind) {
+        case SK_APPLYQ: {
+            const int m = op.a, kq = op.b, ldv = op.c;
+            if (op.nseg > 0) {
+                int cur = 0;
+                for (int s = 0; s < op.nseg; ++s) {
+                    const XSeg sg = segs[op.seg0 + s];
+                    for (int i = tid; i < sg.len; i += blockDim.x) xs[cur + i] = x[sg.xoff + i];
+                    cur += sg.len;
+                }
+            } else {
+                for (int i = tid; i < m; i += blockDim.x) xs[i] = x[op.x0 + i];
+            }
+            __syncthreads();
+            apply_q(xs, m, kq, aptr<T>(op.p0), ldv, aptr<T>(op.p1), op.dir, red_y, red_z);
+            if (op.nseg > 0) {
+                int cur = 0;
+                for (int s = 0; s < op.nseg; ++s) {
+                    const XSeg sg = segs[op.seg0 + s];
+                    for (int i = tid; i < sg.len; i += blockDim.x) x[sg.xoff + i] = xs[cur + i];
+                    cur += sg.len;
+                }
+            } else {
+                for (int i = tid; i < m; i += blockDim.x) x[op.x0 + i] = xs[i];
+            }
+            break;
+        }
+        case SK_TRI: {
+            const int k = op.a, ldr = op.c;
+            const T* R = aptr<T>(op.p0);
+            for (int i = tid; i < k; i += blockDim.x) xs[i] = x[op.x0 + i];
+            __syncthreads();
+            if (op.dir == 0) {
+                for (int b = 0; b < op.nseg; ++b) {
+                    const GemvRef<T> g = gemv[op.seg0 + b];
+                    const T* B = aptr<T>(g.boff);
+                    for (int i = tid; i < k; i += blockDim.x) {
+                        T s = T(0);
+                        for (int j = 0; j < g.s; ++j) s += B[i + (size_t)j * g.ld] * x[g.xoff + j];
+                        xs[i] -= s;
+                    }
+                }
+                __syncthreads();
+                tri_solve(xs, k, R, ldr, 0);
+                for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
+            } else {
+                tri_solve(xs, k, R, ldr, 1);
+                for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
+                for (int b = 0; b < op.nseg; ++b) {
+                    const GemvRef<T> g = gemv[op.seg0 + b];
+                    const T* B = aptr<T>(g.boff);
+                    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+                    for (int j = warp; j < g.s; j += nw) {
+                        T s = T(0);
+                        for (int i = lane; i < k; i += 32) s += B[i + (size_t)j * g.ld] * xs[i];
+                        s = warp_sum(s);
+                        if (lane == 0) x[g.xoff + j] -= s;
+                    }
+                }
+            }
+            break;
+        }
+        case SK_SPLIT: {
+            const int crows = op.a, ccols = op.b, rank = op.c;
+            T* xc = x + op.x0;
+            T* xf = x + op.x1;
+            for (int i = tid; i < crows; i += blockDim.x) xs[i] = xc[i];
+            __syncthreads();
+            const int nf = ccols - rank, nr = crows - ccols;
+            if (op.dir == 0) {
+                for (int q = tid; q < nf; q += blockDim.x) xf[q] = xs[rank + q];
+                for (int q = tid; q < nr; q += blockDim.x) xc[rank + q] = xs[ccols + q];
+                for (int q = tid; q < nf; q += blockDim.x) xc[crows - nf + q] = xs[rank + q];
+            } else {
+                for (int q = tid; q < nf; q += blockDim.x) xc[rank + q] = xf[q];
+                for (int q = tid; q < nr; q += blockDim.x) xc[ccols + q] = xs[rank + q];
+            }
+            break;
+        }
+        case SK_MERGE: {
+            // dir 0: parent <- children rows; dir 1: children cols <- parent
+            int cur = 0;
+            for (int s = 0; s < op.nseg; ++s) {
+                const XSeg sg = segs[op.seg0 + s];
+                const int len = op.dir == 0 ? sg.len : sg.pad;
+                if (op.dir == 0)
+                    for (int i = tid; i < len; i += blockDim.x) x[op.x0 + cur + i] = x[sg.xoff + i];
+                else
+                    for (int i = tid; i < len; i += blockDim.x) x[sg.xoff + i] = x[op.x0 + cur + i];
+                cur += len;
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+template <class T>
+__global__ void k_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[xpos[i]] = (T)b[src[i]];
+}
+template <class T>
+__global__ void k_scatter_out(const T* x, const int64_t* xpos, const int* dst, double* out, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[dst[i]] = (double)x[xpos[i]];
+}
+
+// ------------------------------------------------------------------ Krylov (FP64)
+constexpr int kRedBlocks = 296;
+
+__global__ void k_spmv(int m, const int* rp, const int* ci, const double* v, const double* x, double* y) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int q = rp[r]; q < rp[r + 1]; ++q) s += v[q] * x[ci[q]];
+        y[r] = s;
+    }
+}
+
+__global__ void k_dot_partials(const double* a, const double* b, int lo, int m, double* partials) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        s += b ? a[i] * b[i] : a[i] * a[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__device__ double sum_partials(const double* partials, int nblk, double* red) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += partials[i];
+    return block_sum(s, red);
+}
+
+// v[i:] <- (I - tau h h^T) v[i:], h = [1; ess]; partials hold sum_{r>i} ess[r-i-1] v[r].
+__global__ void k_apply_reflector(const double* ess, const double* tau, double* v, int i, int m,
+                                  const double* partials, int nblk) {
+    __shared__ double red[32];
+    const double d = sum_partials(partials, nblk, red) + v[i];
+    const double tv = *tau;
+    if (tv == 0.0) return;
+    __syncthreads();
+    const double f = tv * d;
+    for (int r = i + 1 + blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+        v[r] -= f * ess[r - i - 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) v[i] -= f;
+}
+
+// makeHouseholder of v[k:]: partials hold sum_{r>k} v[r]^2.
+__global__ void k_make_reflector(const double* v, int k, int m, double* ess, double* tau, double* beta,
+                                 const double* partials, int nblk) {
+    __shared__ double red[32];
+    const double tail = sum_partials(partials, nblk, red);
+    const double c0 = v[k];
+    double b, tv;
+    const bool zero = tail <= DBL_MIN;
+    if (zero) {
+        tv = 0.0;
+        b = c0;
+    } else {
+        b = sqrt(c0 * c0 + tail);
+        if (c0 >= 0.0) b = -b;
+        tv = (b - c0) / b;
+    }
+    for (int r = k + 1 + blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+        ess[r - k - 1] = zero ? 0.0 : v[r] / (c0 - b);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *tau = tv;
+        *beta = b;
+    }
+}
+
+__global__ void k_axpby(int n, double a, const double* x, double b, double* y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+__global__ void k_sub(int n, const double* a, const double* b, double* y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a[i] - b[i];
+}
+
+inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+template <class T>
+size_t trailing_smem() {
+    return sizeof(T) * ((size_t)kRC * (kNB + 1) + (size_t)kRC * (kTN + 1) + (size_t)kNB * (kTN + 1) +
+                        (size_t)kNB * (kNB + 1));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+template <class T>
+void launch_copy(const CopyDesc<T>* d, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_copy<T><<<n < 65535 ? n : 65535, 256, 0, s>>>(d, n);
+}
+
+template <class T>
+void launch_panel(const QRTask<T>* tasks, const int* ids, int ntasks, int p, int smem_rows, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    size_t smem = (size_t)smem_rows * kNB * sizeof(T);
+    k_panel<T><<<ntasks, kThreads, smem, s>>>(tasks, ids, p, smem_rows);
+}
+
+template <class T>
+void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s) {
+    if (ntiles <= 0) return;
+    k_trailing<T><<<ntiles, kThreads, trailing_smem<T>(), s>>>(tasks, tiles, p);
+}
+
+template <class T>
+void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
+    if (ntiles <= 0) return;
+    k_trsm<T><<<ntiles, 128, 0, s>>>(tasks, tiles);
+}
+
+template <class T>
+void launch_rrqr(const RRQRTask<T>* tasks, int ntasks, int nthreads, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_rrqr<T><<<ntasks, nthreads, 0, s>>>(tasks);
+}
+
+template <class T>
+void launch_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_spars_wb<T><<<ntasks, kThreads, 0, s>>>(tasks, blocks);
+}
+
+template <class T>
+void launch_scatter_values(const uint64_t* addr, const double* vals, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_scatter_values<T><<<grid_for(n, 256), 256, 0, s>>>(addr, vals, n);
+}
+
+template <class T>
+void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const GemvRef<T>* gemv, const T* arena,
+                       T* x, int smem_elems, cudaStream_t s) {
+    (void)arena;
+    if (nops <= 0) return;
+    size_t smem = (size_t)(smem_elems < 32 ? 32 : smem_elems) * sizeof(T);
+    k_solve_step<T><<<nops, kThreads, smem, s>>>(ops, segs, gemv, x);
+}
+
+template <class T>
+void launch_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n, cudaStream_t s) {
+    k_gather_in<T><<<grid_for(n, 256), 256, 0, s>>>(b, src, xpos, x, n);
+}
+template <class T>
+void launch_scatter_out(const T* x, const int64_t* xpos, const int* dst, double* out, int n, cudaStream_t s) {
+    k_scatter_out<T><<<grid_for(n, 256), 256, 0, s>>>(x, xpos, dst, out, n);
+}
+
+void launch_spmv_csr(int m, const int* rp, const int* ci, const double* v, const double* x, double* y,
+                     cudaStream_t s) {
+    k_spmv<<<grid_for(m, 256, 148 * 32), 256, 0, s>>>(m, rp, ci, v, x, y);
+}
+void launch_dot_partials(const double* a, const double* b, int lo, int m, double* partials, int nblk,
+                         cudaStream_t s) {
+    k_dot_partials<<<nblk, 256, 0, s>>>(a, b, lo, m, partials);
+}
+void launch_apply_reflector(const double* ess, const double* tau, double* v, int i, int m, const double* partials,
+                            int nblk, cudaStream_t s) {
+    k_apply_reflector<<<nblk, 256, 0, s>>>(ess, tau, v, i, m, partials, nblk);
+}
+void launch_make_reflector(double* v, int k, int m, double* ess_col, double* tau, double* beta,
+                           const double* partials, int nblk, cudaStream_t s) {
+    k_make_reflector<<<nblk, 256, 0, s>>>(v, k, m, ess_col, tau, beta, partials, nblk);
+}
+void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t s) {
+    k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, a, x, b, y);
+}
+void launch_sub(int n, const double* a, const double* b, double* y, cudaStream_t s) {
+    k_sub<<<grid_for(n, 256), 256, 0, s>>>(n, a, b, y);
+}
+int reduce_blocks() { return kRedBlocks; }
+
+template <class T>
+void prepare_kernels() {
+    static bool done = false;
+    if (done) return;
+    cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem<T>());
+    cudaFuncSetAttribute(k_solve_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    done = true;
+}
+
+#define SPQ_INST(T)                                                                                           \
+    template void launch_copy<T>(const CopyDesc<T>*, int, cudaStream_t);                                      \
+    template void launch_panel<T>(const QRTask<T>*, const int*, int, int, int, cudaStream_t);                 \
+    template void launch_trailing<T>(const QRTask<T>*, const TileRef*, int, int, cudaStream_t);               \
+    template void launch_trsm<T>(const TrsmTask<T>*, const TileRef*, int, cudaStream_t);                      \
+    template void launch_rrqr<T>(const RRQRTask<T>*, int, int, cudaStream_t);                                 \
+    template void launch_spars_wb<T>(const SparsWB<T>*, const SpBlock<T>*, int, cudaStream_t);                \
+    template void launch_scatter_values<T>(const uint64_t*, const double*, int64_t, cudaStream_t);         \
+    template void launch_solve_step<T>(const SolveOp*, int, const XSeg*, const GemvRef<T>*, const T*, T*, int, \
+                                       cudaStream_t);                                                          \
+    template void launch_gather_in<T>(const double*, const int*, const int64_t*, T*, int, cudaStream_t);      \
+    template void launch_scatter_out<T>(const T*, const int64_t*, const int*, double*, int, cudaStream_t);    \
+    template void prepare_kernels<T>();
+
+SPQ_INST(double)
+SPQ_INST(float)
+
+}  // namespace spq

@@ -1,0 +1,168 @@
+// Device kernels of the spaQR factorization and solve, with their batched task
+// descriptors. Every launch takes an array of descriptors resident in device
+// memory; one CTA (or a few) serves one descriptor. T is double (plain form) or
+// float (FP32 factor form).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace spq {
+
+constexpr int kNB = 32;  // Householder panel width (columns per compact-WY block)
+constexpr int kTN = 32;  // trailing-update tile width (columns per CTA)
+
+// ---------------------------------------------------------------- copies
+// dst(rows x cols, ld dld) = src(rows x cols, ld sld); src == nullptr writes 0;
+// mode 1 writes the identity pattern instead of copying; mode 2 writes the
+// transpose (dst(j, i) = src(i, j), dst is cols x rows).
+template <class T>
+struct CopyDesc {
+    const T* src;
+    T* dst;
+    int sld, dld, rows, cols;
+    int mode, pad;
+};
+template <class T>
+void launch_copy(const CopyDesc<T>* d, int n, cudaStream_t s);
+
+// ---------------------------------------------------------------- Householder QR
+// A task factors the first k columns of the m x (k + ntr) matrix [fac | tr]
+// (both column-major, ld m) and applies the reflectors to the ntr trailing
+// columns. Outputs: R (upper) and V (strictly lower, unit diagonal implied) in
+// fac, tau[k], and one NB x NB triangular factor per panel in tp
+// (H_panel = I - V T V^T, LAPACK dlarft forward/columnwise convention).
+template <class T>
+struct QRTask {
+    T* fac;
+    T* tr;
+    T* tau;
+    T* tp;
+    int m, k, ntr, pad;
+};
+struct TileRef {
+    int task, tile;
+};
+// Panel p (columns [p, p+NB)) of every listed task.
+template <class T>
+void launch_panel(const QRTask<T>* tasks, const int* task_ids, int ntasks, int p, int smem_rows,
+                  cudaStream_t s);
+// Trailing update after panel p: tiles of kTN columns of [fac(:, p+NB:k) | tr].
+template <class T>
+void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s);
+
+// ---------------------------------------------------------------- TRSM
+// X(rows x k) <- X * inv(R), R upper k x k (ld ldr). One CTA per 128-row tile.
+template <class T>
+struct TrsmTask {
+    const T* R;
+    T* X;
+    int ldr, k, ldx, rows;
+};
+template <class T>
+void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s);
+
+// ---------------------------------------------------------------- truncated RRQR
+// Column-pivoted Householder QR of C (m x n, ld m) stopped at the first k with
+// |R_kk| < tol |R_00| (the rank rule of choose_rank, src/util.cpp:795-816).
+// Writes rank, jpvt (0-based original column of each pivoted position), ipvt
+// (inverse) and tau; C holds R (rows < rank) and V as LAPACK dgeqp3 does.
+template <class T>
+struct RRQRTask {
+    T* C;
+    int* jpvt;
+    int* ipvt;
+    T* tau;
+    T* vn1;
+    T* vn2;
+    int* rank;
+    int m, n;
+    double tol;
+};
+template <class T>
+void launch_rrqr(const RRQRTask<T>* tasks, int ntasks, int nthreads, cudaStream_t s);
+
+// Write-back after the RRQR (sparsifyD, src/tree.cpp:1082-1110): rebuild the
+// interface's column blocks (A(n2, c) <- first rank columns of (Crank P^T)^T)
+// and row blocks (top rank rows <- Crank P^T), save V and tau for the solve and
+// build the panel T factors of V.
+template <class T>
+struct SpBlock {
+    T* p;
+    int ld, rows, cols, coff, kind;  // kind 0: column block (Amp), 1: row block (Apm)
+};
+template <class T>
+struct SparsWB {
+    const T* C;
+    const int* ipvt;
+    const T* tau_in;
+    const int* rank;
+    T* V;        // m x m capacity, ld m
+    T* tau;      // m
+    T* tp;       // panels
+    int m, nblk, blk0, pad;
+};
+template <class T>
+void launch_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s);
+
+// ---------------------------------------------------------------- assembly
+// *(T*)dst_addr[e] = (T) vals[e]
+template <class T>
+void launch_scatter_values(const uint64_t* dst_addr, const double* vals, int64_t n, cudaStream_t s);
+
+// ---------------------------------------------------------------- solve sweeps
+// One CTA per op; all ops of one launch are independent.
+enum SolveKind : int {
+    SK_APPLYQ = 0,  // x <- Q^T x (dir 0) or Q x (dir 1); gathered or contiguous x
+    SK_TRI = 1,     // x <- inv(R) (x - sum_b B_b x_b)  or transposed variant
+    SK_SPLIT = 2,   // SplitD fwd/bwd index shuffle
+    SK_MERGE = 3,   // Merge fwd/bwd copies
+    SK_REASSIGN = 4 // rectangular row reassignment
+};
+struct SolveOp {
+    int kind, dir;
+    int a, b, c, d;       // kind-specific sizes
+    int64_t x0, x1;       // x offsets
+    int64_t p0, p1, p2;   // offsets into the factor arena (elements) / segment tables
+    int seg0, nseg;       // segment / block range
+};
+struct XSeg {
+    int64_t xoff;
+    int len, pad;
+};
+template <class T>
+struct GemvRef {
+    int64_t boff;  // offset of the block in the arena
+    int64_t xoff;  // x segment of the neighbour
+    int ld, s;
+};
+template <class T>
+void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const GemvRef<T>* gemv, const T* arena,
+                       T* x, int smem_elems, cudaStream_t s);
+// x[xpos[k]] = (T) b[src[k]]  /  out[dst[k]] = (double) x[xpos[k]]
+template <class T>
+void launch_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n, cudaStream_t s);
+template <class T>
+void launch_scatter_out(const T* x, const int64_t* xpos, const int* dst, double* out, int n, cudaStream_t s);
+
+// ---------------------------------------------------------------- Krylov helpers (FP64)
+void launch_spmv_csr(int m, const int* rp, const int* ci, const double* v, const double* x, double* y,
+                     cudaStream_t s);
+// partial sums of a[i]*b[i] (or a[i]^2 if b == nullptr) over [lo, m): nblk partials
+void launch_dot_partials(const double* a, const double* b, int lo, int m, double* partials, int nblk,
+                         cudaStream_t s);
+// v[i:] <- (I - tau h h^T) v[i:] with h = [1; ess], ess = H[i+1:, col]; dot from partials
+void launch_apply_reflector(const double* ess, const double* tau, double* v, int i, int m, const double* partials,
+                            int nblk, cudaStream_t s);
+// Householder of v[k:] (makeHouseholder): writes ess into H col k (rows k+1..), tau, beta.
+void launch_make_reflector(double* v, int k, int m, double* ess_col, double* tau, double* beta,
+                           const double* partials, int nblk, cudaStream_t s);
+void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
+void launch_sub(int n, const double* a, const double* b, double* y, cudaStream_t s);          // y = a - b
+int reduce_blocks();
+
+// Sets the shared-memory opt-ins of the kernels (once per process and type);
+// called when a handle is created, outside any stream capture.
+template <class T>
+void prepare_kernels();
+
+}  // namespace spq

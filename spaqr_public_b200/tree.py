@@ -1,0 +1,193 @@
+"""Python mirror of the reference's ``Tree`` and Krylov drivers over the C ABI.
+
+Reference surface (include/tree.h:113-147, include/is.h:14-19):
+
+    Tree t(nlevels, skip); t.set_tol(tol); t.set_scale(1); t.set_square(1);
+    t.set_Xcoo(&X); t.partition(A); t.assemble(A); t.factorize();
+    t.solve(b, x);  gmres(A, b, x, t, iters, restart, tol, verb);
+
+Here::
+
+    t = Tree(nlevels, skip); t.set_tol(tol); t.set_scale(1); t.set_square(1)
+    t.set_coords_grid(n, d)            # -n/-d, i.e. set_Xcoo(linspace_nd(n, d))
+    t.partition(A); t.assemble(A); t.factorize()
+    x = t.solve(b)
+    x, its, res = gmres(A, b, t, iters, restart, tol)
+
+Matrices are CSC tuples ``(m, n, colptr, rowind, val)`` (as produced by
+``spaqr_public_b200.matgen``) with sorted row indices.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, dptr, iptr, lib
+
+FP64 = _abi.SPQ_FP64
+FP32 = _abi.SPQ_FP32
+
+
+def _csc(A):
+    m, n, cp, ri, va = A
+    return (int(m), int(n), np.ascontiguousarray(cp, dtype=np.int32), np.ascontiguousarray(ri, dtype=np.int32),
+            np.ascontiguousarray(va, dtype=np.float64))
+
+
+class Tree:
+    """spaQR hierarchical sparsified QR on one B200 (include/tree.h:36-152)."""
+
+    def __init__(self, nlevels, skip=0, precision=FP64, device=0):
+        h = C.c_void_p()
+        check(lib().spq_create(C.byref(h), int(nlevels), int(skip)))
+        self._h = h
+        self.nlevels = nlevels
+        self.m = self.n = 0
+        if precision != FP64:
+            self.set_precision(precision)
+        if device:
+            check(lib().spq_set_device(h, int(device)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().spq_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # setters (include/tree.h:124-130)
+    def set_tol(self, tol):
+        check(lib().spq_set_tol(self._h, float(tol)))
+
+    def set_scale(self, s):
+        check(lib().spq_set_scale(self._h, int(s)))
+
+    def set_order(self, o):
+        check(lib().spq_set_order(self._h, float(o)))
+
+    def set_hsl(self, h):
+        check(lib().spq_set_hsl(self._h, int(h)))
+
+    def set_square(self, s):
+        check(lib().spq_set_square(self._h, int(s)))
+
+    def set_precision(self, p):
+        check(lib().spq_set_precision(self._h, int(p)))
+
+    def set_verbose(self, v):
+        check(lib().spq_set_verbose(self._h, int(v)))
+
+    def set_coords(self, X):
+        """X: d x n coordinates (set_Xcoo)."""
+        X = np.asarray(X, dtype=np.float64)
+        d, n = X.shape
+        Xc = np.ascontiguousarray(X.T.reshape(-1))
+        check(lib().spq_set_coords(self._h, d, n, dptr(Xc)))
+
+    def set_coords_grid(self, n, d):
+        check(lib().spq_set_coords_grid(self._h, int(n), int(d)))
+
+    # main steps (include/tree.h:139-147)
+    def partition(self, A):
+        m, n, cp, ri, va = _csc(A)
+        self.m, self.n = m, n
+        check(lib().spq_partition(self._h, m, n, iptr(cp), iptr(ri), dptr(va)))
+
+    def assemble(self, A):
+        m, n, cp, ri, va = _csc(A)
+        check(lib().spq_assemble(self._h, m, n, iptr(cp), iptr(ri), dptr(va)))
+
+    def factorize(self):
+        check(lib().spq_factorize(self._h))
+        return 0
+
+    def solve(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        check(lib().spq_solve(self._h, dptr(b), dptr(x)))
+        return x
+
+    def solve_dev(self, d_b, d_x):
+        """Device pointers (e.g. torch tensors' data_ptr()) of FP64 vectors."""
+        check(lib().spq_solve_dev(self._h, C.c_void_p(d_b), C.c_void_p(d_x)))
+
+    def solve_nrml(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        check(lib().spq_solve_nrml(self._h, dptr(b), dptr(x)))
+        return x
+
+    # introspection
+    def perms(self):
+        cp = np.zeros(self.n, dtype=np.int32)
+        rp = np.zeros(self.m, dtype=np.int32)
+        check(lib().spq_get_perm(self._h, iptr(cp), iptr(rp)))
+        return cp, rp
+
+    def log(self):
+        n = C.c_longlong(0)
+        check(lib().spq_log_size(self._h, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.int64)
+        if n.value:
+            check(lib().spq_get_log(self._h, out.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return out.reshape(-1, 8)
+
+    def bottom(self):
+        k = C.c_int(0)
+        check(lib().spq_num_bottom(self._h, C.byref(k)))
+        out = np.zeros(10 * k.value, dtype=np.int32)
+        if k.value:
+            check(lib().spq_get_bottom(self._h, iptr(out)))
+        return out.reshape(-1, 10)
+
+    def stats(self):
+        t = np.zeros(4)
+        c = np.zeros(7, dtype=np.int64)
+        check(lib().spq_get_stats(self._h, dptr(t), c.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return dict(partition=t[0], assemble=t[1], factorize=t[2], solve=t[3], nnzA=int(c[0]), nnzR=int(c[1]),
+                    nnzH=int(c[2]), nnzQ=int(c[3]), launches_factorize=int(c[4]), launches_solve=int(c[5]),
+                    device_bytes=int(c[6]))
+
+    def level_times(self):
+        out = np.zeros(6 * self.nlevels)
+        check(lib().spq_get_level_times(self._h, dptr(out)))
+        return out.reshape(self.nlevels, 6)
+
+
+def gmres(A, b, precond, iters=300, restart=None, tol=1e-12, x0=None):
+    """Householder GMRES left-preconditioned by ``precond`` (src/is.cpp:94-272).
+    Returns (x, iterations, preconditioned residual estimate)."""
+    m, n, cp, ri, va = _csc(A)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    its = C.c_int(0)
+    res = C.c_double(0)
+    check(lib().spq_gmres(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(b), dptr(x), int(iters),
+                          int(iters if restart is None else restart), float(tol), C.byref(its), C.byref(res)))
+    return x, its.value, res.value
+
+
+def cgls(A, b, precond, iters=300, tol=1e-12):
+    """Preconditioned CGLS (src/is.cpp:274-345)."""
+    m, n, cp, ri, va = _csc(A)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n)
+    its = C.c_int(0)
+    res = C.c_double(0)
+    check(lib().spq_cgls(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(b), dptr(x), int(iters), float(tol),
+                         C.byref(its), C.byref(res)))
+    return x, its.value, res.value
+
+
+def column_normalize(A):
+    """A <- A diag(1/||A_j||) 10 (spaQR.cpp:131-147), computed by the library."""
+    m, n, cp, ri, va = _csc(A)
+    out = va.copy()
+    check(lib().spq_column_normalize(m, n, iptr(cp), iptr(ri), dptr(out)))
+    return (m, n, cp, ri, out)
