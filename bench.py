@@ -1,0 +1,410 @@
+"""Benchmark: time to ||Ax-b||/||b|| <= 1e-10 (factor + Krylov) on one B200.
+
+Workload: 3D advection-diffusion on a 64^3 grid (n = 262144, 7-point stencil,
+first-order upwind, seeded Fourier velocity field of magnitude 100), 12 levels,
+tolerance 1e-2, skip 2, column-normalised as spaQR.cpp:131-147, b ~ N(0,1).
+Synthetic, seeded (spaqr_public_b200.matgen.workload("advdiff3d_64")).
+
+One step = factorize + FP64 GMRES iterative refinement until the TRUE relative
+residual is <= 1e-10, with the matrix (CSR), b and x already in HBM and the
+tree partitioned and assembled before the step (setup is not timed). The
+headline `value` is the FP32-factor / FP64-Krylov form; the plain FP64 form is
+timed the same way and reported beside it. Device time: CUDA events on the
+handle's stream around each step, synchronize + barrier on both sides, max
+over ranks. Inputs (~6-12 GB of blocks) are larger than L2, so no flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of the reference algorithm (oracle/,
+LAPACK from OpenBLAS) on the host cores, on a bounded sample (the same
+generator on a smaller cube) scaled to the full workload by the ratio of the
+reference's algorithmic flops (factorization) and factor-words x iterations
+(Krylov).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "advdiff3d_64"
+TARGET = 1e-10
+METRIC = "time to ‖Ax−b‖/‖b‖≤1e-10 (factor+Krylov), FP32-batched vs plain FP64, 1 B200"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, local):
+    import torch
+    import torch.distributed as dist
+    if ws > 1 and not dist.is_initialized():
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist if ws > 1 else None
+
+
+def barrier(d):
+    import torch
+    torch.cuda.synchronize()
+    if d is not None:
+        d.barrier()
+
+
+def max_over_ranks(d, v):
+    if d is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    d.all_reduce(t, op=d.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.path = os.path.join("/tmp", f"spq_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- our arm
+def make_tree(w, A, precision, device):
+    from spaqr_public_b200 import Tree
+    t = Tree(w["levels"], w["skip"], precision=precision, device=device)
+    t.set_tol(w["tol"])
+    t.set_scale(1)
+    t.set_square(1)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    return t
+
+
+def device_csr(A):
+    import torch
+    from spaqr_public_b200 import matgen
+    m, n, rp, ci, va = matgen.to_csr(A)
+    return (torch.tensor(rp, dtype=torch.int32, device="cuda"), torch.tensor(ci, dtype=torch.int32, device="cuda"),
+            torch.tensor(va, dtype=torch.float64, device="cuda"))
+
+
+def timed_step(w, A, csr, d_b, precision, device, profile=False):
+    """Untimed setup (partition + assemble), then factorize + refinement timed
+    with CUDA events on the handle's stream. Returns (seconds, info)."""
+    import torch
+    from spaqr_public_b200 import _abi, launches
+    from spaqr_public_b200._abi import check, lib
+    t = make_tree(w, A, precision, device)
+    if profile:
+        check(lib().spq_set_profile(t._h, 1))
+    sp = C.c_void_p()
+    check(lib().spq_get_stream(t._h, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    x = torch.zeros(A[1], dtype=torch.float64, device="cuda")
+    rp, ci, va = csr
+    inner = TARGET if precision == 0 else 1e-6
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    check(lib().spq_factorize(t._h))
+    its = C.c_int(0)
+    res = C.c_double(0)
+    rc = lib().spq_solve_to_residual_dev(t._h, A[0], C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                                         C.c_void_p(va.data_ptr()), C.c_void_p(d_b.data_ptr()),
+                                         C.c_void_p(x.data_ptr()), TARGET, inner, 8, 300, C.byref(its),
+                                         C.byref(res))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    check(rc)
+    sec = e0.elapsed_time(e1) / 1e3
+    info = dict(its=its.value, res=res.value, launches=launches(t), stats=t.stats())
+    if profile:
+        fams = {}
+        out = np.zeros(4)
+        for i, name in enumerate(_abi.KERNEL_FAMILIES):
+            check(lib().spq_get_kernel_stats(t._h, i, out.ctypes.data_as(C.POINTER(C.c_double))))
+            fams[name] = dict(launches=int(out[0]), ms=float(out[1]), flops=float(out[2]), bytes=float(out[3]))
+        info["kernels"] = fams
+        info["log"] = t.log()
+    t.close()
+    return sec, info
+
+
+def e2e_step(w, A, b, precision, device):
+    """The public host API end to end: create, partition, assemble, factorize and
+    solve_to_residual with host buffers (all copies inside). Wall clock with a
+    device synchronize on both sides."""
+    import torch
+    from spaqr_public_b200 import Tree, solve_to_residual
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    t = Tree(w["levels"], w["skip"], precision=precision, device=device)
+    t.set_tol(w["tol"])
+    t.set_scale(1)
+    t.set_square(1)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    t.factorize()
+    x, its, res = solve_to_residual(A, b, t, target=TARGET, inner_tol=TARGET if precision == 0 else 1e-6)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    t.close()
+    m, n, cp, ri, va = A
+    nnz = len(va)
+    h2d = 16 * nnz + (4 * (m + 1) + 12 * nnz) + 8 * m + 8 * n  # assemble values+addresses, CSR, b, x0
+    d2h = 8 * n
+    return sec, res, h2d, d2h
+
+
+def roofline(info, peaks):
+    """Dominant kernel family of the instrumented step, its algorithmic bytes per
+    launch over its average CUDA-event duration, against the measured HBM copy
+    bandwidth (all families are bandwidth/latency bound here: FP64 and FP32
+    SIMT work with no measured FP64 peak to compare against)."""
+    fams = info["kernels"]
+    dom = max((k for k in fams if k != "precond_apply"), key=lambda k: fams[k]["ms"])
+    f = fams[dom]
+    per_launch_s = f["ms"] / 1e3 / max(f["launches"], 1)
+    bytes_per_launch = f["bytes"] / max(f["launches"], 1)
+    achieved = bytes_per_launch / per_launch_s / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get(dom)
+        except Exception:
+            traffic = None
+    total_ms = sum(v["ms"] for v in fams.values())
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 5), "traffic": traffic,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+            "share_of_kernel_time": round(f["ms"] / total_ms, 3) if total_ms else None,
+            "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": f["ms"] / max(f["launches"], 1),
+            "algorithmic_flops_per_launch": f["flops"] / max(f["launches"], 1),
+            "families": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                             "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None,
+                             "GFLOPs": round(v["flops"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None}
+                         for k, v in fams.items()}}
+
+
+# --------------------------------------------------------------------------- CPU arm
+def cpu_sample(n_side, threads):
+    """Oracle pipeline on the advdiff3d generator at n_side^3; returns timing parts."""
+    from oracle import oracle_py as O
+    from spaqr_public_b200 import matgen, work
+    w = matgen.workload(f"advdiff3d_{n_side}")
+    A = matgen.column_normalize(w["A"])
+    if threads:
+        O.blas_threads(threads)
+    t0 = time.perf_counter()
+    t = O.OracleTree(w["levels"], w["skip"], w["tol"], 1, 1.0, 1)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    t.factorize()
+    t1 = time.perf_counter()
+    x, its, r = t.gmres(A, w["b"], iters=300, tol=TARGET)
+    t2 = time.perf_counter()
+    log = t.log()
+    return dict(n=n_side, factor_s=t1 - t0, krylov_s=t2 - t1, its=its, flops=work.total_flops(log, reference=True),
+                words=work.factor_bytes(log))
+
+
+def cpu_scaled(sample):
+    """Scales a sample's time to the 64^3 workload (reference flops for the
+    factorization, factor words x iterations for the Krylov part)."""
+    full = json.load(open(os.path.join(ROOT, "tests", "golden", "work_advdiff3d_64.json")))
+    fw = full["final"][4] + full["final"][5] + full["final"][6]
+    t_fact = sample["factor_s"] * full["reference_flops"] / sample["flops"]
+    t_kry = sample["krylov_s"] * (fw * full["gmres_its"]) / (sample["words"] * max(sample["its"], 1))
+    return t_fact + t_kry
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    threads = cpu_threads()
+    n_side = 40 if (args.steps + args.warmup) <= 6 else 32
+    for _ in range(args.warmup):
+        cpu_sample(n_side, threads)
+    vals = []
+    for _ in range(args.steps):
+        s = cpu_sample(n_side, threads)
+        vals.append(cpu_scaled(s))
+    v = float(np.mean(vals))
+    sample = (f"advdiff3d_{n_side} ({n_side}^3, same generator and settings) full pipeline, scaled to 64^3 by "
+              f"reference flops (factor) and factor words x iterations (GMRES)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD} (n=262144, 12 levels, tol 1e-2, skip 2, target 1e-10)",
+                       "parallelism": "cpu"},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- main
+def run_ours(args):
+    import torch
+    from spaqr_public_b200 import matgen
+    ws, rank, local = dist_env()
+    d = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    w = matgen.workload(WORKLOAD)
+    A = matgen.column_normalize(w["A"])
+    b = w["b"]
+    csr = device_csr(A)
+    d_b = torch.tensor(b, dtype=torch.float64, device="cuda")
+    result = {}
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        for _ in range(args.warmup):
+            timed_step(w, A, csr, d_b, prec, local)
+        times, infos = [], []
+        barrier(d)
+        with Clocks(local) as clk:
+            for _ in range(args.steps):
+                barrier(d)
+                s, info = timed_step(w, A, csr, d_b, prec, local)
+                barrier(d)
+                times.append(s)
+                infos.append(info)
+        mean = max_over_ranks(d, float(np.mean(times)))
+        result[name] = dict(value=mean, times=times, info=infos[-1], clocks=clk.summary())
+    # instrumented step for the roofline (FP32 form, after the timed steps)
+    _, pinfo = timed_step(w, A, csr, d_b, 1, local, profile=True)
+    rl = roofline(pinfo, peaks)
+    e2e_sec, e2e_res, h2d, d2h = e2e_step(w, A, b, 1, local)
+    e2e_sec = max_over_ranks(d, e2e_sec)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        s = cpu_sample(40, cpu_threads())
+        cpu = {"value": cpu_scaled(s), "unit": "s", "cores": cpu_threads(), "kind": "port",
+               "sample": ("oracle on advdiff3d_40 (40^3) full pipeline "
+                          f"({s['factor_s']:.1f}s factor + {s['krylov_s']:.1f}s GMRES), scaled to 64^3 by "
+                          "reference flops and factor words x iterations")}
+    f32, f64 = result["fp32"], result["fp64"]
+    inf = f32["info"]
+    line = {
+        "metric": METRIC, "value": f32["value"], "unit": "s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": f32["value"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-factor/f64-krylov", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{WORKLOAD} (n=262144, 12 levels, tol 1e-2, skip 2, target 1e-10)",
+                   "step": "factorize + FP64 GMRES refinement to true residual 1e-10 (partition/assemble untimed)",
+                   "l2": "inputs larger than L2 (no flush needed)",
+                   "parallelism": "replicas" if ws > 1 else "single GPU"},
+        "fp64_form": {"value": f64["value"], "unit": "s", "gmres_its": f64["info"]["its"],
+                      "residual": f64["info"]["res"], "speedup_fp32_over_fp64": f64["value"] / f32["value"]},
+        "gmres_its": inf["its"], "residual": inf["res"],
+        "e2e": {"value": e2e_sec, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "residual": e2e_res, "includes": "create+partition+assemble+factorize+refinement, host buffers"},
+        "gpu_launches": inf["launches"]["total"],
+        "roofline": rl,
+        "cpu_baseline": cpu,
+        "clocks": f32["clocks"],
+        "clocks_fp64": f64["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if d is not None:
+        d.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

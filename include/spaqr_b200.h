@@ -91,6 +91,43 @@ int spq_gmres(spq_tree* t, int m, int n, const int* colptr, const int* rowind, c
 int spq_cgls(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
              const double* b, double* x, int iters, double tol, int* its, double* res);
 
+/* Time-to-residual driver (the benchmark's metric): iterative refinement on
+ * the true residual. Each correction solves A d = b - A x (residual in FP64)
+ * with the GMRES above to inner_tol, until ||b - A x|| / ||b|| <= target or
+ * max_outer corrections. With the FP64 form one correction with
+ * inner_tol = target is the reference's own GMRES call; with the FP32 form the
+ * outer loop is the refinement that recovers FP64 accuracy.
+ * *its = total GMRES iterations, *true_res = final relative residual. */
+int spq_solve_to_residual(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
+                          const double* b, double* x, double target, double inner_tol, int max_outer, int iters,
+                          int* its, double* true_res);
+/* Same with device-resident inputs: A as CSR on the device (row pointers,
+ * column indices, values; FP64), b and x device vectors. */
+int spq_solve_to_residual_dev(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
+                              const double* d_b, double* d_x, double target, double inner_tol, int max_outer,
+                              int iters, int* its, double* true_res);
+/* GMRES with device-resident inputs (CSR on the device). */
+int spq_gmres_dev(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
+                  const double* d_b, double* d_x, int iters, int restart, double tol, int* its, double* res);
+/* Kernel launches issued by the last spq_factorize and by Krylov calls since
+ * the handle was created; solve_graph_kernels = kernels in one preconditioner
+ * application (one CUDA graph launch), applications = graph launches so far. */
+int spq_get_launches(spq_tree* t, long long* factorize, long long* krylov, long long* solve_graph_kernels,
+                     long long* applications);
+
+/* Per-kernel timing (off by default): with profile = 1 every launch of the
+ * handle is bracketed by CUDA events on its stream. spq_get_kernel_stats
+ * returns, for kernel family f (0 copy, 1 panel QR, 2 trailing update, 3 trsm,
+ * 4 truncated RRQR, 5 sparsification write-back, 6 assembly scatter,
+ * 7 preconditioner application), out[0..3] = launches, total ms, algorithmic
+ * flops, algorithmic bytes. spq_reset_kernel_stats clears the counters. */
+int spq_set_profile(spq_tree* t, int profile);
+int spq_get_kernel_stats(spq_tree* t, int family, double* out4);
+int spq_reset_kernel_stats(spq_tree* t);
+/* The CUDA stream (cudaStream_t) the handle issues its work on; valid after
+ * spq_assemble. */
+int spq_get_stream(spq_tree* t, void** stream);
+
 /* Introspection: permutations, event log (records of 8 int64, layout documented
  * in the package's host source), nnz counters, per-level phase times. */
 int spq_get_perm(spq_tree* t, int* cperm, int* rperm);
@@ -101,7 +138,7 @@ int spq_get_bottom(spq_tree* t, int* out); /* 10 ints per bottom cluster */
 /* times[0..3] = partition, assemble, factorize, last solve (seconds);
  * counters[0..3] = nnzA, nnzR, nnzH, nnzQ; counters[4] = kernel launches of the
  * last factorize; counters[5] = kernel launches of the last solve;
- * counters[6] = device bytes in use. */
+ * counters[6] = device bytes in use; counters[7] = preconditioner applications. */
 int spq_get_stats(spq_tree* t, double* times, long long* counters);
 /* Per-level factorization phase times in ms (6 per level: fill, elmn, shift,
  * scale, sprsfy, merge), as printed by src/tree.cpp:1417-1426. */

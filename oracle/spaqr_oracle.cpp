@@ -13,7 +13,9 @@
 //
 // Event log: records of 8 long longs [type, ilvl, order, a, b, c, d, e]
 //   1 ELIM   a=stacked rows b=cols c=#updated column clusters d=#stacked blocks
+//            e=total width of the updated columns
 //   2 SCALE  a=rows b=cols c=#row blocks (larfb) d=#column blocks (trsm)
+//            e=100000 * (width of the row blocks) + (height of the column blocks)
 //   3 SPARS  a=cols before b=cols after c=width of C d=rows after
 //   4 MERGE  a=rows b=cols c=#children
 //   5 LEVEL  a=top-separator rows b=top-separator cols c=#clusters in the next bottom
@@ -1010,12 +1012,13 @@ public:
         }
         larft(Q, c->tau, c->T);
         nnzH_ += (unsigned long long)(num_rows * num_cols);
-        int nupd = 0;
+        int nupd = 0, wtr = 0;
         for (Cluster* n : c->rsparsity) {
             if (!n->eliminated && c != n) {
                 update_cluster(c, n, Q);
                 nnzR_ += (unsigned long long)(c->cols() * n->cols());
                 ++nupd;
+                wtr += n->cols();
             }
         }
         if (!square_)
@@ -1024,7 +1027,7 @@ public:
         ops_.emplace_back(new OpQR(c));
         if (!square_) tops_.emplace_back(new TOpQR(c));
         c->eliminated = true;
-        rec(1, num_rows, num_cols, nupd, (long long)H.size(), 0, c->order);
+        rec(1, num_rows, num_cols, nupd, (long long)H.size(), wtr, c->order);
     }
 
     // -------- rectangular row shift (src/tree.cpp:319-411) --------
@@ -1153,12 +1156,20 @@ public:
             for (int i = 0; i < D.rows; ++i) D(i, j) = (i == j) ? 1.0 : 0.0;
         nnzR_ = (unsigned long long)((double)nnzR_ + 0.5 * c->cols() * c->cols());
         nnzH_ += (unsigned long long)(c->rows() * c->cols());
-        int nrow = 0, ncol = 0;
+        int nrow = 0, ncol = 0, wrow = 0, hcol = 0;
         for (Edge* ei : c->edgesIn)
-            if (!ei->n1->eliminated) { larfb_lt(Q, T, ei->A->data(), ei->A->rows, ei->A->cols); ++nrow; }
+            if (!ei->n1->eliminated) {
+                larfb_lt(Q, T, ei->A->data(), ei->A->rows, ei->A->cols);
+                ++nrow;
+                wrow += ei->A->cols;
+            }
         for (Edge* eo : c->edgesOut)
-            if (!eo->n2->eliminated && eo->n2 != c) { trsm_right_upper(R, *eo->A); ++ncol; }
-        rec(2, c->rows(), c->cols(), nrow, ncol, 0, c->order);
+            if (!eo->n2->eliminated && eo->n2 != c) {
+                trsm_right_upper(R, *eo->A);
+                ++ncol;
+                hcol += eo->A->rows;
+            }
+        rec(2, c->rows(), c->cols(), nrow, ncol, (long long)wrow * 100000 + hcol, c->order);
         if (square_) {
             ops_.emplace_back(new OpScaleD(c, std::move(Q), std::move(t), true));
         } else {

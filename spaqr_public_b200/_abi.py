@@ -62,6 +62,21 @@ SIGNATURES = {
     "spq_get_stats": (_i, [_p, _dp, _llp]),
     "spq_get_level_times": (_i, [_p, _dp]),
     "spq_column_normalize": (_i, [_i, _i, _ip, _ip, _dp]),
+    "spq_solve_to_residual": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _d, _d, _i, _i, _ip, _dp]),
+    "spq_solve_to_residual_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _d, _d, _i, _i, _ip, _dp]),
+    "spq_gmres_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _i, _i, _d, _ip, _dp]),
+    "spq_get_launches": (_i, [_p, _llp, _llp, _llp, _llp]),
+    "spq_set_profile": (_i, [_p, _i]),
+    "spq_get_kernel_stats": (_i, [_p, _i, _dp]),
+    "spq_reset_kernel_stats": (_i, [_p]),
+    "spq_get_stream": (_i, [_p, C.POINTER(_p)]),
+}
+
+KERNEL_FAMILIES = ["copy", "panel_qr", "trailing_update", "trsm", "rrqr", "spars_writeback", "assemble_scatter",
+                   "precond_apply"]
+KERNEL_NAMES = {  # device function names as they appear in ncu launch lists
+    "copy": "k_copy", "panel_qr": "k_panel", "trailing_update": "k_trailing", "trsm": "k_trsm", "rrqr": "k_rrqr",
+    "spars_writeback": "k_spars_wb", "assemble_scatter": "k_scatter_values", "precond_apply": "k_solve_step",
 }
 
 _lib = None

@@ -292,13 +292,137 @@ int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const dou
         cuda_check(cudaMalloc(&dx, sizeof(double) * n), "gmres alloc");
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "gmres h2d");
         cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "gmres h2d");
-        *its = gmres_device(*t->eng, A, db, dx, iters, restart, tol, res, &t->launches_krylov);
+        long long l = 0;
+        *its = gmres_device(*t->eng, A, db, dx, iters, restart, tol, res, &l);
+        t->launches_krylov += l;
         cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gmres d2h");
         cuda_check(cudaStreamSynchronize(s), "gmres");
         cudaFree(db);
         cudaFree(dx);
         return SPQ_OK;
     });
+}
+
+int spq_solve_to_residual(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va, const double* b,
+                          double* x, double target, double inner_tol, int max_outer, int iters, int* its,
+                          double* true_res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve_to_residual before factorize");
+    if (m != n || m != t->eng->nrows()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (!b || !x || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
+        return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        cudaStream_t s = t->eng->stream();
+        DevCsrOwned o;
+        DevCsr A;
+        upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
+        double *db = nullptr, *dx = nullptr;
+        cuda_check(cudaMalloc(&db, sizeof(double) * m), "alloc");
+        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "alloc");
+        cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "h2d");
+        cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "h2d");
+        int outer = 0;
+        long long l = 0;
+        *its = refine_device(*t->eng, A, db, dx, target, inner_tol, max_outer, iters, true_res, &outer, &l);
+        t->launches_krylov += l;
+        cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "d2h");
+        cuda_check(cudaStreamSynchronize(s), "solve_to_residual");
+        cudaFree(db);
+        cudaFree(dx);
+        return *true_res <= target ? SPQ_OK : fail(SPQ_ERR_NOCONV, "target residual not reached");
+    });
+}
+
+int spq_solve_to_residual_dev(spq_tree* t, int m, const int* rp, const int* ci, const double* va, const double* d_b,
+                              double* d_x, double target, double inner_tol, int max_outer, int iters, int* its,
+                              double* true_res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve_to_residual before factorize");
+    if (m != t->eng->nrows() || m != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    if (!rp || !ci || !va || !d_b || !d_x || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
+        return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        DevCsr A;
+        A.m = A.n = m;
+        A.rp = rp;
+        A.ci = ci;
+        A.v = va;
+        int outer = 0;
+        long long l = 0;
+        *its = refine_device(*t->eng, A, d_b, d_x, target, inner_tol, max_outer, iters, true_res, &outer, &l);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "solve_to_residual");
+        return *true_res <= target ? SPQ_OK : fail(SPQ_ERR_NOCONV, "target residual not reached");
+    });
+}
+
+int spq_gmres_dev(spq_tree* t, int m, const int* rp, const int* ci, const double* va, const double* d_b, double* d_x,
+                  int iters, int restart, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "gmres before factorize");
+    if (m != t->eng->nrows() || m != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    if (!rp || !ci || !va || !d_b || !d_x || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        DevCsr A;
+        A.m = A.n = m;
+        A.rp = rp;
+        A.ci = ci;
+        A.v = va;
+        long long l = 0;
+        *its = gmres_device(*t->eng, A, d_b, d_x, iters, restart, tol, res, &l);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "gmres");
+        return SPQ_OK;
+    });
+}
+
+int spq_get_launches(spq_tree* t, long long* factorize, long long* krylov, long long* solve_graph_kernels,
+                     long long* applications) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    double times[4];
+    long long c[8] = {0};
+    if (t->eng) t->eng->stats(times, c);
+    if (factorize) *factorize = c[4];
+    if (krylov) *krylov = t->launches_krylov;
+    if (solve_graph_kernels) *solve_graph_kernels = c[5];
+    if (applications) *applications = c[7];
+    return SPQ_OK;
+}
+
+int spq_set_profile(spq_tree* t, int profile) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (!t->eng) return fail(SPQ_ERR_STATE, "profile before partition");
+    t->eng->set_profile(profile != 0);
+    return SPQ_OK;
+}
+int spq_get_kernel_stats(spq_tree* t, int family, double* out4) {
+    if (!t || !out4) return fail(SPQ_ERR_ARG, "null argument");
+    if (!t->eng) return fail(SPQ_ERR_STATE, "no engine");
+    if (family < 0 || family >= kNumFamilies) return fail(SPQ_ERR_ARG, "unknown kernel family");
+    return guard([&] {
+        KernelStat s = t->eng->kernel_stat(family);
+        out4[0] = (double)s.launches;
+        out4[1] = s.ms;
+        out4[2] = s.flops;
+        out4[3] = s.bytes;
+        return SPQ_OK;
+    });
+}
+int spq_reset_kernel_stats(spq_tree* t) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (!t->eng) return SPQ_OK;
+    return guard([&] {
+        t->eng->reset_kernel_stats();
+        return SPQ_OK;
+    });
+}
+int spq_get_stream(spq_tree* t, void** stream) {
+    if (!t || !stream) return fail(SPQ_ERR_ARG, "null argument");
+    if (!t->eng || t->state < 2) return fail(SPQ_ERR_STATE, "no stream before assemble");
+    *stream = (void*)t->eng->stream();
+    return SPQ_OK;
 }
 
 int spq_cgls(spq_tree* t, int, int, const int*, const int*, const double*, const double*, double*, int, double, int*,

@@ -214,7 +214,8 @@ public:
         double* d_vals = desc_arena_.alloc_n<double>(vals.size());
         cuda_check(cudaMemcpyAsync(d_addr, addr.data(), addr.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
         cuda_check(cudaMemcpyAsync(d_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
-        launch_scatter_values<T>(d_addr, d_vals, (int64_t)addr.size(), stream_);
+        timed(KF_ASSEMBLE, 0, (double)addr.size() * (16 + sizeof(T)),
+              [&] { launch_scatter_values<T>(d_addr, d_vals, (int64_t)addr.size(), stream_); });
         ++launches_fact_;
         cuda_check(cudaStreamSynchronize(stream_), "assemble");
         assembled_ = true;
@@ -278,10 +279,11 @@ public:
             cuda_check(cudaStreamEndCapture(stream_, &graph_), "capture end");
             cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
         }
-        cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+        timed(KF_SOLVE, 0, solve_bytes_, [&] { cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch"); });
         cuda_check(cudaMemcpyAsync(d_x, d_xout_, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
                    "solve out");
         t_solve_ = wall() - t0;
+        ++applications_;
     }
 
     std::vector<int> bottom_info() const override {
@@ -305,6 +307,7 @@ public:
         counters[4] = launches_fact_;
         counters[5] = launches_solve_;
         counters[6] = (long long)(arena_.bytes_reserved() + desc_arena_.bytes_reserved() + scratch_.capacity());
+        counters[7] = applications_;
     }
     std::vector<double> level_times() const override {
         std::vector<double> out;
@@ -334,7 +337,7 @@ private:
     unsigned long long nnzA_ = 0, nnzR_ = 0, nnzH_ = 0, nnzQ_ = 0;
     Log log_;
     double t_part_ = 0, t_asm_ = 0, t_fact_ = 0, t_solve_ = 0;
-    long long launches_fact_ = 0, launches_solve_ = 0;
+    long long launches_fact_ = 0, launches_solve_ = 0, applications_ = 0;
     std::vector<cudaEvent_t> events_, level_ev_;
     // solve plan
     T* xbuf_ = nullptr;
@@ -353,7 +356,64 @@ private:
     const GemvRef<T>* d_gemv_ = nullptr;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
+    double solve_bytes_ = 0;  // algorithmic bytes of one preconditioner application
 
+    // ------------------------------------------------------------- kernel timing (optional)
+    // With profiling on, every launch is bracketed by CUDA events on the
+    // handle's stream and charged to its kernel family together with the
+    // algorithmic flops and bytes of the tasks it served.
+    struct Pending {
+        int fam;
+        cudaEvent_t a, b;
+        double flops, bytes;
+    };
+    bool prof_ = false;
+    std::vector<Pending> pend_;
+    KernelStat fam_[kNumFamilies];
+
+    template <class F>
+    size_t timed(int fam, double flops, double bytes, F&& launch) {
+        if (!prof_) {
+            launch();
+            return SIZE_MAX;
+        }
+        cudaEvent_t a, b;
+        cuda_check(cudaEventCreate(&a), "event");
+        cuda_check(cudaEventCreate(&b), "event");
+        cudaEventRecord(a, stream_);
+        launch();
+        cudaEventRecord(b, stream_);
+        pend_.push_back(Pending{fam, a, b, flops, bytes});
+        return pend_.size() - 1;
+    }
+    void flush_prof() {
+        if (pend_.empty()) return;
+        cuda_check(cudaStreamSynchronize(stream_), "profile sync");
+        for (auto& p : pend_) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            fam_[p.fam].launches += 1;
+            fam_[p.fam].ms += ms;
+            fam_[p.fam].flops += p.flops;
+            fam_[p.fam].bytes += p.bytes;
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        pend_.clear();
+    }
+
+public:
+    void set_profile(bool on) override { prof_ = on; }
+    KernelStat kernel_stat(int fam) override {
+        flush_prof();
+        return (fam >= 0 && fam < kNumFamilies) ? fam_[fam] : KernelStat{};
+    }
+    void reset_kernel_stats() override {
+        flush_prof();
+        for (auto& f : fam_) f = KernelStat{};
+    }
+
+private:
     // ------------------------------------------------------------- helpers
     const std::vector<Cluster*>& cur() const { return bottoms_[cur_bottom_]; }
 
@@ -504,25 +564,64 @@ private:
             o_tiles.push_back(up.add(tiles[i]));
         }
         char* d = up.commit(desc_arena_, stream_);
-        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_g), (int)g.size(), stream_);
-        ++launches_fact_;
+        issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
         const int smem_limit = (int)((160 * 1024) / (kNB * sizeof(T)));
         for (size_t i = 0; i < ids.size(); ++i) {
             const int p = (int)i * kNB;
             int rows = 0;
-            for (int t : ids[i]) rows = std::max(rows, qt[t].m - p);
+            double pf = 0, pb = 0, tf = 0, tb = 0;
+            for (int t : ids[i]) {
+                const double R = qt[t].m - p, w = std::min(kNB, qt[t].k - p);
+                rows = std::max(rows, qt[t].m - p);
+                pf += 2 * R * w * w - 2.0 / 3.0 * w * w * w + R * w * w;  // geqrf + larft of the panel
+                pb += 2 * R * w * sizeof(T);
+            }
+            for (const TileRef& tr : tiles[i]) {
+                const QRTask<T>& q = qt[tr.task];
+                const double R = q.m - p, w = std::min(kNB, q.k - p);
+                const int ntot = (q.k - p - (int)w) + q.ntr;
+                const double tn = std::min(kTN, ntot - tr.tile * kTN);
+                tf += 4 * R * tn * w;
+                tb += (2 * R * tn + R * w) * sizeof(T);
+            }
             const int smem_rows = std::min(rows, smem_limit);
-            launch_panel<T>(reinterpret_cast<const QRTask<T>*>(d + o_q), reinterpret_cast<const int*>(d + o_ids[i]),
-                            (int)ids[i].size(), p, smem_rows, stream_);
-            launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
-                               reinterpret_cast<const TileRef*>(d + o_tiles[i]), (int)tiles[i].size(), p, stream_);
-            launches_fact_ += 1 + (tiles[i].empty() ? 0 : 1);
+            timed(KF_PANEL, pf, pb, [&] {
+                launch_panel<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
+                                reinterpret_cast<const int*>(d + o_ids[i]), (int)ids[i].size(), p, smem_rows,
+                                stream_);
+            });
+            ++launches_fact_;
+            if (!tiles[i].empty()) {
+                timed(KF_TRAILING, tf, tb, [&] {
+                    launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
+                                       reinterpret_cast<const TileRef*>(d + o_tiles[i]), (int)tiles[i].size(), p,
+                                       stream_);
+                });
+                ++launches_fact_;
+            }
         }
-        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_s), (int)s.size(), stream_);
-        launch_trsm<T>(reinterpret_cast<const TrsmTask<T>*>(d + o_tr), reinterpret_cast<const TileRef*>(d + o_tt),
-                       (int)trsm_tiles.size(), stream_);
-        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_post), (int)post.size(), stream_);
-        launches_fact_ += (s.empty() ? 0 : 1) + (trsm_tiles.empty() ? 0 : 1) + (post.empty() ? 0 : 1);
+        issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_s), s);
+        if (!trsm_tiles.empty()) {
+            double f = 0, by = 0;
+            for (auto& t : trsm) {
+                f += (double)t.rows * t.k * t.k;
+                by += (2.0 * t.rows * t.k + 0.5 * t.k * t.k) * sizeof(T);
+            }
+            timed(KF_TRSM, f, by, [&] {
+                launch_trsm<T>(reinterpret_cast<const TrsmTask<T>*>(d + o_tr),
+                               reinterpret_cast<const TileRef*>(d + o_tt), (int)trsm_tiles.size(), stream_);
+            });
+            ++launches_fact_;
+        }
+        issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_post), post);
+    }
+
+    void issue_copies(const CopyDesc<T>* d, const std::vector<CopyDesc<T>>& h) {
+        if (h.empty()) return;
+        double by = 0;
+        for (auto& c : h) by += (c.src ? 2.0 : 1.0) * c.rows * c.cols * sizeof(T);
+        timed(KF_COPY, 0, by, [&] { launch_copy<T>(d, (int)h.size(), stream_); });
+        ++launches_fact_;
     }
 
     static CopyDesc<T> cp(const T* src, T* dst, int sld, int dld, int rows, int cols, int mode = 0, int pad = 0) {
@@ -592,7 +691,7 @@ private:
             for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
             tape_.push_back(std::move(op));
             c->elim = true;
-            rec(1, m, k, nupd, (long long)H.size(), 0, c->order);
+            rec(1, m, k, nupd, (long long)H.size(), co, c->order);
             tasks.push_back(std::move(t));
         }
         if (tasks.empty()) return;
@@ -644,11 +743,13 @@ private:
                 ++nrow;
             }
             j.ntr = co;
+            int hcol = 0;
             for (Edge* e : c->out) {
                 if (e->n2->elim || e->n2 == c) continue;
                 t.trsm.push_back(TrsmTask<T>{j.fac, e->A.p, rows, cols, e->A.ld, e->A.rows});
                 t.uids.push_back(e->A.uid);
                 ++ncol;
+                hcol += e->A.rows;
             }
             t.ident = cp(nullptr, es->A.p, 0, es->A.ld, rows, cols, 1);
             TapeOp op;
@@ -660,7 +761,7 @@ private:
             op.k = cols;  // head / reflectors
             op.ld = rows;
             tape_.push_back(std::move(op));
-            rec(2, rows, cols, nrow, ncol, 0, c->order);
+            rec(2, rows, cols, nrow, ncol, (long long)co * 100000 + hcol, c->order);
             if (cols == 0) continue;
             tasks.push_back(std::move(t));
         }
@@ -777,15 +878,29 @@ private:
         Upload up;
         size_t o_g = up.add(g), o_r = up.add(rt);
         char* d = up.commit(desc_arena_, stream_);
-        launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o_g), (int)g.size(), stream_);
-        launch_rrqr<T>(reinterpret_cast<const RRQRTask<T>*>(d + o_r), (int)rt.size(), 1024, stream_);
-        launches_fact_ += 2;
+        issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
+        const size_t rq = timed(KF_RRQR, 0, 0, [&] {
+            launch_rrqr<T>(reinterpret_cast<const RRQRTask<T>*>(d + o_r), (int)rt.size(), 1024, stream_);
+        });
+        ++launches_fact_;
         std::vector<int> ranks(jobs.size());
         cuda_check(cudaMemcpyAsync(ranks.data(), ib, sizeof(int) * jobs.size(), cudaMemcpyDeviceToHost, stream_),
                    "rank");
         cuda_check(cudaStreamSynchronize(stream_), "rank readback");
+        if (rq != SIZE_MAX) {  // algorithmic work of the launch, now that the ranks are known
+            double f = 0, by = 0;
+            for (size_t q = 0; q < jobs.size(); ++q) {
+                const double m = jobs[q].m, n = jobs[q].n;
+                const double r = ranks[q] >= jobs[q].m ? std::min(jobs[q].m, jobs[q].n) : ranks[q];
+                f += 4 * m * n * r - 2 * r * r * (m + n) + 4.0 / 3.0 * r * r * r;
+                by += 2 * m * n * sizeof(T);
+            }
+            pend_[rq].flops = f;
+            pend_[rq].bytes = by;
+        }
         std::vector<SparsWB<T>> wb;
         std::vector<SpBlock<T>> blocks;
+        double wb_bytes = 0;
         for (size_t q = 0; q < jobs.size(); ++q) {
             auto& j = jobs[q];
             Cluster* c = j.c;
@@ -811,6 +926,7 @@ private:
             }
             s.nblk = (int)blocks.size() - s.blk0;
             wb.push_back(s);
+            wb_bytes += ((double)r * j.n + 2.0 * m * r) * sizeof(T);
             // tape: OrthogonalD then SplitD (pushed before the size change)
             TapeOp od;
             od.kind = TK_ORTHD;
@@ -847,8 +963,10 @@ private:
             Upload u2;
             size_t o_w = u2.add(wb), o_b = u2.add(blocks);
             char* d2 = u2.commit(desc_arena_, stream_);
-            launch_spars_wb<T>(reinterpret_cast<const SparsWB<T>*>(d2 + o_w),
-                               reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
+            timed(KF_SPARS_WB, 0, wb_bytes, [&] {
+                launch_spars_wb<T>(reinterpret_cast<const SparsWB<T>*>(d2 + o_w),
+                                   reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
+            });
             ++launches_fact_;
         }
     }
@@ -902,8 +1020,7 @@ private:
             Upload up;
             size_t o = up.add(copies);
             char* d = up.commit(desc_arena_, stream_);
-            launch_copy<T>(reinterpret_cast<const CopyDesc<T>*>(d + o), (int)copies.size(), stream_);
-            ++launches_fact_;
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
         }
     }
 
@@ -1084,6 +1201,9 @@ private:
         for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem});
         nin_ = (int)src.size();
         nout_ = (int)dst.size();
+        // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
+        // right-hand side and solution vectors
+        solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 8.0 * (nrows_ + ncols_);
         const size_t smem_cap = (200 * 1024) / sizeof(T);
         for (auto* ws : {&fwd_waves_, &bwd_waves_})
             for (auto& w : *ws)

@@ -39,9 +39,29 @@ struct Config {
 // CPU oracle): 1 ELIM, 2 SCALE, 3 SPARS, 4 MERGE, 5 LEVEL, 6 FINAL.
 using Log = std::vector<long long>;
 
+// Kernel families timed when profiling is on.
+enum KernelFamily {
+    KF_COPY = 0,      // batched block gather / scatter / merge copies
+    KF_PANEL = 1,     // Householder panel factorization
+    KF_TRAILING = 2,  // compact-WY trailing update
+    KF_TRSM = 3,      // right triangular solve (scaling)
+    KF_RRQR = 4,      // truncated column-pivoted QR (sparsification)
+    KF_SPARS_WB = 5,  // sparsification write-back + T factors
+    KF_ASSEMBLE = 6,  // value scatter into blocks
+    KF_SOLVE = 7,     // one preconditioner application (CUDA graph of sweep waves)
+    kNumFamilies = 8
+};
+struct KernelStat {
+    long long launches = 0;
+    double ms = 0, flops = 0, bytes = 0;  // summed over launches; flops/bytes algorithmic
+};
+
 class EngineBase {
 public:
     virtual ~EngineBase() = default;
+    virtual void set_profile(bool on) = 0;
+    virtual KernelStat kernel_stat(int family) = 0;
+    virtual void reset_kernel_stats() = 0;
     virtual void partition(const Csc& A) = 0;
     virtual void assemble(const Csc& A) = 0;
     virtual void factorize() = 0;

@@ -218,6 +218,35 @@ int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x,
     return it;
 }
 
+int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, double target, double inner_tol,
+                  int max_outer, int iters, double* true_res, int* outer, long long* launches) {
+    cudaStream_t s = P.stream();
+    DevVec r, d;
+    r.alloc(A.m);
+    d.alloc(A.n);
+    int total = 0, k = 0;
+    long long l = 0;
+    double rel = residual_norm(s, A, d_b, d_x);
+    l += 6;
+    while (rel > target && k < max_outer) {
+        launch_spmv_csr(A.m, A.rp, A.ci, A.v, d_x, r.p, s);
+        launch_sub(A.m, d_b, r.p, r.p, s);
+        cuda_check(cudaMemsetAsync(d.p, 0, sizeof(double) * A.n, s), "refine zero");
+        double res = 0;
+        long long gl = 0;
+        total += gmres_device(P, A, r.p, d.p, iters, iters, inner_tol, &res, &gl);
+        launch_axpby(A.n, 1.0, d.p, 1.0, d_x, s);
+        l += gl + 3;
+        ++k;
+        rel = residual_norm(s, A, d_b, d_x);
+        l += 6;
+    }
+    if (true_res) *true_res = rel;
+    if (outer) *outer = k;
+    if (launches) *launches = l;
+    return total;
+}
+
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x) {
     DevVec t, part;
     t.alloc(A.m);

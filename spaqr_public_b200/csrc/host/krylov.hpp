@@ -20,4 +20,11 @@ int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x,
 // ||b - A x|| / ||b|| on the device (FP64).
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x);
 
+// Iterative refinement on the true residual: r = b - A x in FP64, GMRES on
+// A d = r preconditioned by P to inner_tol, x += d, until ||b - A x|| / ||b||
+// <= target or max_outer corrections. Returns the total GMRES iterations;
+// *true_res is the final relative residual, *outer the corrections made.
+int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, double target, double inner_tol,
+                  int max_outer, int iters, double* true_res, int* outer, long long* launches);
+
 }  // namespace spq

@@ -148,7 +148,7 @@ class Tree:
 
     def stats(self):
         t = np.zeros(4)
-        c = np.zeros(7, dtype=np.int64)
+        c = np.zeros(8, dtype=np.int64)
         check(lib().spq_get_stats(self._h, dptr(t), c.ctypes.data_as(C.POINTER(C.c_longlong))))
         return dict(partition=t[0], assemble=t[1], factorize=t[2], solve=t[3], nnzA=int(c[0]), nnzR=int(c[1]),
                     nnzH=int(c[2]), nnzQ=int(c[3]), launches_factorize=int(c[4]), launches_solve=int(c[5]),
@@ -171,6 +171,34 @@ def gmres(A, b, precond, iters=300, restart=None, tol=1e-12, x0=None):
     check(lib().spq_gmres(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(b), dptr(x), int(iters),
                           int(iters if restart is None else restart), float(tol), C.byref(its), C.byref(res)))
     return x, its.value, res.value
+
+
+def solve_to_residual(A, b, precond, target=1e-10, inner_tol=None, max_outer=8, iters=300, x0=None):
+    """Iterative refinement on the true FP64 residual with preconditioned GMRES
+    corrections (the time-to-residual driver). Returns (x, gmres iterations,
+    final ||b - A x|| / ||b||). Raises SpqError(SPQ_ERR_NOCONV) if the target is
+    not reached."""
+    m, n, cp, ri, va = _csc(A)
+    if inner_tol is None:
+        inner_tol = target
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    its = C.c_int(0)
+    res = C.c_double(0)
+    rc = lib().spq_solve_to_residual(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(b), dptr(x),
+                                     float(target), float(inner_tol), int(max_outer), int(iters), C.byref(its),
+                                     C.byref(res))
+    check(rc)
+    return x, its.value, res.value
+
+
+def launches(precond):
+    """Kernel launches: factorize, Krylov vector kernels, kernels per preconditioner
+    application (one CUDA graph) and applications so far."""
+    f, k, s, a = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
+    check(lib().spq_get_launches(precond._h, C.byref(f), C.byref(k), C.byref(s), C.byref(a)))
+    return dict(factorize=f.value, krylov=k.value, solve_graph_kernels=s.value, applications=a.value,
+                total=f.value + k.value + s.value * a.value)
 
 
 def cgls(A, b, precond, iters=300, tol=1e-12):

@@ -1,0 +1,162 @@
+"""GPU parity through the C ABI: the device factorization against the CPU oracle.
+
+Bar (FP64 plain form):
+* event log identical to the oracle's (every elimination shape, scaling,
+  RRQR rank, merge size, nnz counter): integer parity, exact;
+* one-shot preconditioner solve within 1e-10 relative of the oracle's;
+* GMRES iteration count identical, preconditioned residual estimate within
+  1e-6 relative, true residual below the requested tolerance (x 10).
+FP32 form: its factor is not held to FP64 ranks; it must reach the FP64 target
+through the refinement driver.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle_py as O
+from spaqr_public_b200 import FP32, FP64, Tree, gmres, matgen, solve_to_residual
+
+pytestmark = pytest.mark.gpu
+
+
+def build(name, prec=FP64, tol=None, skip=None, levels=None):
+    w = matgen.workload(name)
+    A = matgen.column_normalize(w["A"])
+    lv = levels or w["levels"]
+    tl = w["tol"] if tol is None else tol
+    sk = w["skip"] if skip is None else skip
+    if tl == 0:
+        sk = lv - 1
+    t = Tree(lv, sk, precision=prec)
+    t.set_tol(tl)
+    t.set_scale(1)
+    t.set_square(1)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    t.factorize()
+    return w, A, t, (lv, sk, tl)
+
+
+def oracle(w, A, lv, sk, tl):
+    o = O.OracleTree(lv, sk, tl, 1, 1.0, 1)
+    o.set_coords_grid(w["n"], w["d"])
+    o.partition(A)
+    o.assemble(A)
+    o.factorize()
+    return o
+
+
+CASES = ["advdiff2d_32", "advdiff2d_128", "advdiff3d_16", "advdiff3d_32", "advdiff2d_37"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_factor_log_and_solve_match_oracle(gpu, name):
+    w, A, t, cfg = build(name)
+    o = oracle(w, A, *cfg)
+    assert np.array_equal(t.log(), o.log())
+    b = w["b"]
+    x = t.solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("name", ["advdiff2d_32", "advdiff2d_128", "advdiff3d_32"])
+def test_gmres_iterations_match_oracle(gpu, name):
+    w, A, t, cfg = build(name)
+    o = oracle(w, A, *cfg)
+    b = w["b"]
+    x, its, res = gmres(A, b, t, iters=300, tol=w["res"])
+    xo, itso, reso = o.gmres(A, b, tol=w["res"])
+    assert its == itso
+    assert abs(res - reso) <= 1e-6 * reso
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    assert true <= 10 * w["res"]
+    assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("tol,skip", [(0.0, None), (1e-1, 0), (1e-2, 1)])
+def test_tolerance_and_skip_variants(gpu, tol, skip):
+    w, A, t, cfg = build("advdiff2d_32", tol=tol, skip=skip)
+    o = oracle(w, A, *cfg)
+    assert np.array_equal(t.log(), o.log())
+    x = t.solve(w["b"])
+    if tol == 0:  # exact QR: the preconditioner is A^-1 to rounding
+        r = np.linalg.norm(matgen.spmv(A, x) - w["b"]) / np.linalg.norm(w["b"])
+        assert r < 1e-12
+
+
+@pytest.mark.parametrize("levels", [1, 2, 3])
+def test_few_levels(gpu, levels):
+    w, A, t, cfg = build("advdiff2d_32", levels=levels)
+    o = oracle(w, A, *cfg)
+    assert np.array_equal(t.log(), o.log())
+    x = t.solve(w["b"])
+    xo = o.solve(w["b"])
+    assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
+
+
+def test_high_contrast_parity(gpu):
+    A = matgen.column_normalize(matgen.contrast2d(64, patches=8, seed=5))
+    b = matgen.rhs_normal(A[0], 17)
+    t = Tree(6, 0)
+    t.set_tol(1e-2)
+    t.set_scale(1)
+    t.set_square(1)
+    t.set_coords_grid(64, 2)
+    t.partition(A)
+    t.assemble(A)
+    t.factorize()
+    o = O.OracleTree(6, 0, 1e-2, 1, 1.0, 1)
+    o.set_coords_grid(64, 2)
+    o.partition(A)
+    o.assemble(A)
+    o.factorize()
+    assert np.array_equal(t.log(), o.log())
+    x = t.solve(b)
+    xo = o.solve(b)
+    assert np.linalg.norm(x - xo) <= 1e-10 * np.linalg.norm(xo)
+
+
+def test_repeated_solves_are_deterministic(gpu):
+    w, A, t, _ = build("advdiff2d_128")
+    b = w["b"]
+    x1 = t.solve(b)
+    x2 = t.solve(b)
+    assert np.array_equal(x1, x2)
+
+
+def test_fp32_factor_reaches_fp64_target(gpu):
+    w, A, t, _ = build("advdiff2d_128", prec=FP32)
+    b = w["b"]
+    x, its, res = solve_to_residual(A, b, t, target=1e-10, inner_tol=1e-6)
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    assert res <= 1e-10 and true <= 1e-10
+
+
+def test_fp64_solve_to_residual(gpu):
+    w, A, t, _ = build("advdiff3d_32")
+    b = w["b"]
+    x, its, res = solve_to_residual(A, b, t, target=1e-10)
+    assert res <= 1e-10
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    assert abs(true - res) <= 1e-3 * res + 1e-15
+
+
+def test_device_pointer_solve(gpu):
+    import torch
+    w, A, t, _ = build("advdiff2d_32")
+    b = torch.tensor(w["b"], dtype=torch.float64, device="cuda")
+    x = torch.zeros(A[1], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t.solve_dev(b.data_ptr(), x.data_ptr())
+    xh = t.solve(w["b"])
+    assert np.array_equal(x.cpu().numpy(), xh)
+
+
+def test_device_buffers_loaded(gpu):
+    """The numerical path is the in-tree CUDA library (no CPU fallback)."""
+    import os
+    maps = open("/proc/self/maps").read()
+    assert "libspaqr_b200.so" in maps
+    assert os.path.exists(os.path.join(os.path.dirname(os.path.dirname(__file__)), "spaqr_public_b200", "_build",
+                                       "libspaqr_b200.so"))
