@@ -124,6 +124,10 @@ int spq_get_launches(spq_tree* t, long long* factorize, long long* krylov, long 
 int spq_set_profile(spq_tree* t, int profile);
 int spq_get_kernel_stats(spq_tree* t, int family, double* out4);
 int spq_reset_kernel_stats(spq_tree* t);
+/* Diagnostic: runs one preconditioner application outside its CUDA graph and
+ * times every sweep wave. out (capacity 3 * cap) receives [ms, ops, shared
+ * vector length] per wave (forward then backward); *nwaves = waves. */
+int spq_profile_solve_waves(spq_tree* t, double* out, int cap, int* nwaves);
 /* The CUDA stream (cudaStream_t) the handle issues its work on; valid after
  * spq_assemble. */
 int spq_get_stream(spq_tree* t, void** stream);

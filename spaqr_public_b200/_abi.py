@@ -70,6 +70,7 @@ SIGNATURES = {
     "spq_get_kernel_stats": (_i, [_p, _i, _dp]),
     "spq_reset_kernel_stats": (_i, [_p]),
     "spq_get_stream": (_i, [_p, C.POINTER(_p)]),
+    "spq_profile_solve_waves": (_i, [_p, _dp, _i, _ip]),
 }
 
 KERNEL_FAMILIES = ["copy", "panel_qr", "trailing_update", "trsm", "rrqr", "spars_writeback", "assemble_scatter",

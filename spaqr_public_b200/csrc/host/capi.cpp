@@ -418,6 +418,17 @@ int spq_reset_kernel_stats(spq_tree* t) {
         return SPQ_OK;
     });
 }
+int spq_profile_solve_waves(spq_tree* t, double* out, int cap, int* nwaves) {
+    if (!t || !out || !nwaves) return fail(SPQ_ERR_ARG, "null argument");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "profile before factorize");
+    return guard([&] {
+        auto v = t->eng->profile_solve_waves();
+        *nwaves = (int)(v.size() / 3);
+        std::memcpy(out, v.data(), sizeof(double) * std::min<size_t>(v.size(), (size_t)cap * 3));
+        return SPQ_OK;
+    });
+}
+
 int spq_get_stream(spq_tree* t, void** stream) {
     if (!t || !stream) return fail(SPQ_ERR_ARG, "null argument");
     if (!t->eng || t->state < 2) return fail(SPQ_ERR_STATE, "no stream before assemble");

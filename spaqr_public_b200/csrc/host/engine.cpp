@@ -699,6 +699,7 @@ private:
         for (auto& t : tasks) touched.push_back(t.uids);
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
+        print_waves("elim", wave, nw);
         for (int w = 0; w < nw; ++w) {
             std::vector<QRJob> jobs;
             for (size_t t = 0; t < tasks.size(); ++t)
@@ -770,6 +771,7 @@ private:
         for (auto& t : tasks) touched.push_back(t.uids);
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
+        print_waves("scale", wave, nw);
         for (int w = 0; w < nw; ++w) {
             std::vector<QRJob> jobs;
             std::vector<TrsmTask<T>> tr;
@@ -801,6 +803,7 @@ private:
         if (list.empty()) return;
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
+        print_waves("sparsify", wave, nw);
         std::vector<std::vector<long long>> recs(list.size());
         for (int w = 0; w < nw; ++w) {
             struct Job {
@@ -808,7 +811,7 @@ private:
                 Cluster* c;
                 std::vector<Edge*> apm, amp;
                 Edge* self;
-                int m, n, smp;
+                int m, n, smp, ld;
                 size_t c_off, i_off;
             };
             std::vector<Job> jobs;
@@ -834,14 +837,22 @@ private:
                 j.m = c->csize;
                 j.n = smp + spm;
                 j.smp = smp;
+                j.ld = std::max((j.n + 1) & ~1, 2);  // even row stride
                 j.c_off = celems;
-                celems += (size_t)j.m * std::max(j.n, 1);
+                celems += (size_t)j.m * j.ld;
                 j.i_off = ielems;
                 ielems += 3 * (size_t)std::max(j.n, 1) + 1;
                 celems += 3 * (size_t)std::max(j.n, 1);  // tau, vn1, vn2
                 jobs.push_back(std::move(j));
             }
+            const double tw = wall();
             if (!jobs.empty()) run_sparsify_wave(jobs, celems, ielems, recs);
+            if (cfg_.verbose >= 2 && !jobs.empty()) {
+                int mm = 0, mn = 0;
+                for (auto& j : jobs) { mm = std::max(mm, j.m); mn = std::max(mn, j.n); }
+                std::fprintf(stderr, "    sparsify wave %d: %zu tasks, max m %d, max n %d, %.2f ms\n", w, jobs.size(),
+                             mm, mn, (wall() - tw) * 1e3);
+            }
         }
         for (size_t t = 0; t < list.size(); ++t) {
             const auto& r = recs[t];
@@ -857,39 +868,73 @@ private:
         int* ib = reinterpret_cast<int*>(base);
         T* cb = reinterpret_cast<T*>(base + ibytes);
         std::vector<CopyDesc<T>> g;
-        std::vector<RRQRTask<T>> rt;
+        std::vector<RRQRTaskRM<T>> rt;
         for (auto& j : jobs) {
+            // C is row-major (row stride ld): C(i, cur + r) = A_mp(r, i), C(i, smp + c) = A_pm(i, c)
             T* C = cb + j.c_off;
+            const int ld = j.ld;
             int cur = 0;
-            for (Edge* e : j.amp) {  // C[:, cur + i] = A(i, :)^T
-                g.push_back(cp(e->A.p, C + (size_t)cur * j.m, e->A.ld, j.m, e->A.rows, e->A.cols, 2));
+            for (Edge* e : j.amp) {
+                g.push_back(cp(e->A.p, C + cur, e->A.ld, ld, e->A.rows, e->A.cols));
                 cur += e->A.rows;
             }
             for (Edge* e : j.apm) {
-                g.push_back(cp(e->A.p, C + (size_t)cur * j.m, e->A.ld, j.m, j.m, e->A.cols));
+                g.push_back(cp(e->A.p, C + cur, e->A.ld, ld, j.m, e->A.cols, 2));
                 cur += e->A.cols;
             }
             const size_t nn = std::max(j.n, 1);
-            T* tail = C + (size_t)j.m * nn;
+            T* tail = C + (size_t)j.m * ld;
             int* ii = ib + jobs.size() + j.i_off;
             int* rk = ib + rt.size();
-            rt.push_back(RRQRTask<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, cfg_.tol});
+            rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, ld, 0, cfg_.tol});
         }
+        // one launch per cluster size; larger interfaces get more CTAs
+        auto cluster_of = [](const Job& j) {
+            const double w = (double)j.m * j.n;
+            int c = w <= 32768 ? 1 : w <= 131072 ? 2 : w <= 524288 ? 4 : w <= 2097152 ? 8 : 16;
+            while (c < 16 && (j.n + c - 1) / c > 4096) c *= 2;  // keep each CTA's slab <= 4096 columns
+            return c;
+        };
+        std::map<int, std::vector<int>> groups;
+        for (size_t q = 0; q < jobs.size(); ++q) groups[cluster_of(jobs[q])].push_back((int)q);
         Upload up;
         size_t o_g = up.add(g), o_r = up.add(rt);
+        std::map<int, size_t> o_ids;
+        for (auto& kv : groups) o_ids[kv.first] = up.add(kv.second);
         char* d = up.commit(desc_arena_, stream_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
-        const size_t rq = timed(KF_RRQR, 0, 0, [&] {
-            launch_rrqr<T>(reinterpret_cast<const RRQRTask<T>*>(d + o_r), (int)rt.size(), 1024, stream_);
-        });
-        ++launches_fact_;
+        std::vector<size_t> rqs;
+        for (auto& kv : groups) {
+            int maxm = 0, maxn = 0;
+            for (int q : kv.second) {
+                maxm = std::max(maxm, jobs[q].m);
+                maxn = std::max(maxn, jobs[q].n);
+            }
+            const int cl = kv.first;
+            rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
+                cudaError_t e = launch_rrqr_rm<T>(reinterpret_cast<const RRQRTaskRM<T>*>(d + o_r),
+                                                  reinterpret_cast<const int*>(d + o_ids[cl]), (int)kv.second.size(),
+                                                  cl, maxm, maxn, stream_);
+                if (e != cudaSuccess && cl > 8) {  // 16-CTA clusters are an opt-in; fall back to 8
+                    cudaGetLastError();
+                    e = launch_rrqr_rm<T>(reinterpret_cast<const RRQRTaskRM<T>*>(d + o_r),
+                                          reinterpret_cast<const int*>(d + o_ids[cl]), (int)kv.second.size(), 8,
+                                          maxm, maxn, stream_);
+                }
+                cuda_check(e, "rrqr launch");
+            }));
+            ++launches_fact_;
+        }
         std::vector<int> ranks(jobs.size());
         cuda_check(cudaMemcpyAsync(ranks.data(), ib, sizeof(int) * jobs.size(), cudaMemcpyDeviceToHost, stream_),
                    "rank");
         cuda_check(cudaStreamSynchronize(stream_), "rank readback");
-        if (rq != SIZE_MAX) {  // algorithmic work of the launch, now that the ranks are known
+        size_t gi = 0;
+        for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
+            const size_t rq = rqs[gi++];
+            if (rq == SIZE_MAX) continue;
             double f = 0, by = 0;
-            for (size_t q = 0; q < jobs.size(); ++q) {
+            for (int q : kv.second) {
                 const double m = jobs[q].m, n = jobs[q].n;
                 const double r = ranks[q] >= jobs[q].m ? std::min(jobs[q].m, jobs[q].n) : ranks[q];
                 f += 4 * m * n * r - 2 * r * r * (m + n) + 4.0 / 3.0 * r * r * r;
@@ -898,7 +943,7 @@ private:
             pend_[rq].flops = f;
             pend_[rq].bytes = by;
         }
-        std::vector<SparsWB<T>> wb;
+        std::vector<SparsWBRM<T>> wb;
         std::vector<SpBlock<T>> blocks;
         double wb_bytes = 0;
         for (size_t q = 0; q < jobs.size(); ++q) {
@@ -914,7 +959,8 @@ private:
             T* V = arena_.alloc_n<T>((size_t)m * std::max(r, 1));
             T* tau = arena_.alloc_n<T>(std::max(r, 1));
             T* tp = arena_.alloc_n<T>((size_t)std::max(npanels(r), 1) * kNB * kNB);
-            SparsWB<T> s{rt[q].C, rt[q].ipvt, rt[q].tau, rt[q].rank, V, tau, tp, m, 0, (int)blocks.size(), 0};
+            SparsWBRM<T> s{rt[q].C, rt[q].pos, rt[q].colat, rt[q].tau, V, tau, tp, m, j.ld, r, 0,
+                           (int)blocks.size(), 0};
             int cur = 0;
             for (Edge* e : j.amp) {
                 blocks.push_back(SpBlock<T>{e->A.p, e->A.ld, e->A.rows, e->A.cols, cur, 0});
@@ -964,8 +1010,8 @@ private:
             size_t o_w = u2.add(wb), o_b = u2.add(blocks);
             char* d2 = u2.commit(desc_arena_, stream_);
             timed(KF_SPARS_WB, 0, wb_bytes, [&] {
-                launch_spars_wb<T>(reinterpret_cast<const SparsWB<T>*>(d2 + o_w),
-                                   reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
+                launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
+                                      reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
             });
             ++launches_fact_;
         }
@@ -1022,6 +1068,16 @@ private:
             char* d = up.commit(desc_arena_, stream_);
             issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
         }
+    }
+
+    // Diagnostic (verbose >= 2): tasks and waves of one phase.
+    void print_waves(const char* phase, const std::vector<int>& wave, int nw) {
+        if (cfg_.verbose < 2) return;
+        std::vector<int> cnt(nw, 0);
+        for (int w : wave) cnt[w]++;
+        int mx = 0;
+        for (int c : cnt) mx = std::max(mx, c);
+        std::fprintf(stderr, "[lvl %d] %-8s tasks %zu waves %d max/wave %d\n", ilvl_, phase, wave.size(), nw, mx);
     }
 
     void print_level(cudaEvent_t* ev, std::pair<int, int> ts) {
@@ -1212,6 +1268,39 @@ private:
     }
     int nin_ = 0, nout_ = 0;
 
+public:
+    std::vector<double> profile_solve_waves() override {
+        if (!factorized_) throw std::logic_error("profile before factorize");
+        std::vector<double> out;
+        std::vector<cudaEvent_t> ev;
+        auto rec_ev = [&]() {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreate(&e), "event");
+            cudaEventRecord(e, stream_);
+            ev.push_back(e);
+        };
+        launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, stream_);
+        rec_ev();
+        std::vector<const Wave*> all;
+        for (auto& w : fwd_waves_) all.push_back(&w);
+        for (auto& w : bwd_waves_) all.push_back(&w);
+        for (const Wave* w : all) {
+            launch_solve_step<T>(w->ops, w->nops, d_segs_, d_gemv_, nullptr, xbuf_, w->smem, stream_);
+            rec_ev();
+        }
+        cuda_check(cudaStreamSynchronize(stream_), "profile solve");
+        for (size_t i = 0; i < all.size(); ++i) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            out.push_back(ms);
+            out.push_back(all[i]->nops);
+            out.push_back(all[i]->smem);
+        }
+        for (auto e : ev) cudaEventDestroy(e);
+        return out;
+    }
+
+private:
     void run_solve_sweeps() {
         launches_solve_ = 0;
         launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, stream_);

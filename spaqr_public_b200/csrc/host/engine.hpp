@@ -76,6 +76,10 @@ public:
     virtual std::vector<int> bottom_info() const = 0;
     virtual void stats(double* times, long long* counters) const = 0;
     virtual std::vector<double> level_times() const = 0;
+    // One preconditioner application outside the CUDA graph with every sweep
+    // wave timed: returns [ms, ops, smem elements] per wave (forward waves then
+    // backward waves).
+    virtual std::vector<double> profile_solve_waves() = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(const Config& cfg, int precision);

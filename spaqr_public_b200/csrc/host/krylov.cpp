@@ -64,7 +64,7 @@ public:
         t_.alloc(m_);
         v_.alloc(m_);
         xnew_.alloc(m_);
-        part_.alloc(nblk_);
+        part_.alloc(nblk_ + 1);
         scal_.alloc(2 * (restart + 1) + 4);
         H_.alloc((size_t)m_ * (restart + 1));
         hpart_.resize(nblk_);
@@ -85,7 +85,7 @@ public:
 
     // v[i:] <- H_i v[i:]
     void reflect(int i, double* v) {
-        launch_dot_partials(col(i), v, i + 1, m_, part_.p, nblk_, s_);
+        launch_dot_partials(col(i), v, i + 1, m_, part_.p, nblk_, s_, v + i);
         launch_apply_reflector(col(i) + i + 1, tau(i), v, i, m_, part_.p, nblk_, s_);
         launches_ += 2;
     }

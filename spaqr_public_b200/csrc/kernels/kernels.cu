@@ -131,14 +131,24 @@ __global__ void k_copy(const CopyDesc<T>* descs, int n) {
 }
 
 // ------------------------------------------------------------------ panel QR
+// One CTA factors one panel of <= kNB columns (rows p..m-1) of one task. Each
+// column step is one row-parallel pass: every thread walks its rows and
+// accumulates, in registers, the dot products of the new reflector with all
+// other panel columns (coalesced loads, ~31 independent per row). The products
+// with the later columns drive the rank-1 update; those with the earlier
+// reflectors are the Gram entries v_i^T v_j of the panel's T factor (LAPACK
+// dlarft, forward columnwise), so T needs no extra pass.
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, const int* ids, int p, int smem_rows) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     __shared__ T red[32];
     __shared__ T s_tau[kNB];
+    __shared__ T dots[kNB];
+    __shared__ T wred[(kThreads / 32) * kNB];
     __shared__ T G[kNB * (kNB + 1)];
     __shared__ T Ts[kNB * (kNB + 1)];
+    constexpr int GP = kNB + 1;
     const QRTask<T> t = tasks[ids[blockIdx.x]];
     const int m = t.m, k = t.k;
     if (p >= k) return;
@@ -151,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
     const int ldp = in_smem ? R : m;
     if (in_smem) {
         for (int e = tid; e < R * w; e += blockDim.x) {
-            int i = e % R, j = e / R;
+            const int i = e % R, j = e / R;
             P[i + j * ldp] = gp[i + (size_t)j * m];
         }
         __syncthreads();
@@ -159,43 +169,81 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
     for (int j = 0; j < w; ++j) {
         if (j >= R) {
             if (tid == 0) s_tau[j] = T(0);
+            for (int c = tid; c < j; c += blockDim.x) G[c * GP + j] = T(0);
             continue;
         }
+        T* pj = P + (size_t)j * ldp;
         T part = T(0);
-        for (int i = j + 1 + tid; i < R; i += blockDim.x) {
-            T v = P[i + (size_t)j * ldp];
-            part += v * v;
-        }
+        for (int i = j + 1 + tid; i < R; i += blockDim.x) part += pj[i] * pj[i];
         const T xn2 = block_sum(part, red);
-        const T alpha = P[j + (size_t)j * ldp];
+        const T alpha = pj[j];
         T tau, beta, scal;
         make_reflector(alpha, xn2, tau, beta, scal);
         if (tau != T(0))
-            for (int i = j + 1 + tid; i < R; i += blockDim.x) P[i + (size_t)j * ldp] *= scal;
+            for (int i = j + 1 + tid; i < R; i += blockDim.x) pj[i] *= scal;
         __syncthreads();
         if (tid == 0) {
-            P[j + (size_t)j * ldp] = beta;
+            pj[j] = beta;
             s_tau[j] = tau;
+        }
+        // d[c] = P[j, c] + sum_{r > j} v_j[r] P[r, c] for every panel column c != j
+        T acc[kNB];
+#pragma unroll
+        for (int c = 0; c < kNB; ++c) acc[c] = T(0);
+        for (int r = j + 1 + tid; r < R; r += blockDim.x) {
+            const T vr = pj[r];
+#pragma unroll
+            for (int c = 0; c < kNB; ++c)
+                if (c < w && c != j) acc[c] += vr * P[r + (size_t)c * ldp];
+        }
+#pragma unroll
+        for (int c = 0; c < kNB; ++c) {
+            const T v = warp_sum(acc[c]);
+            if (lane == c) wred[warp * kNB + c] = v;
+        }
+        __syncthreads();
+        if (tid < w && tid != j) {
+            T d = P[j + (size_t)tid * ldp];
+            for (int q = 0; q < nw; ++q) d += wred[q * kNB + tid];
+            dots[tid] = d;
+            if (tid < j) G[tid * GP + j] = d;  // v_tid^T v_j
         }
         __syncthreads();
         if (tau != T(0)) {
-            for (int c = j + 1 + warp; c < w; c += nw) {
-                T s = T(0);
-                for (int i = j + 1 + lane; i < R; i += 32) s += P[i + (size_t)j * ldp] * P[i + (size_t)c * ldp];
-                s = warp_sum(s);
-                s = (s + P[j + (size_t)c * ldp]) * tau;
-                for (int i = j + 1 + lane; i < R; i += 32) P[i + (size_t)c * ldp] -= s * P[i + (size_t)j * ldp];
-                if (lane == 0) P[j + (size_t)c * ldp] -= s;
+            for (int r = j + 1 + tid; r < R; r += blockDim.x) {
+                const T vr = pj[r];
+#pragma unroll
+                for (int c = 0; c < kNB; ++c)
+                    if (c > j && c < w) P[r + (size_t)c * ldp] -= (tau * dots[c]) * vr;
             }
+            if (tid > j && tid < w) P[j + (size_t)tid * ldp] -= tau * dots[tid];
         }
         __syncthreads();
     }
-    // tau and the panel's T factor
     for (int j = tid; j < w; j += blockDim.x) t.tau[p + j] = s_tau[j];
-    build_tfac(P, ldp, R, w, s_tau, t.tp + (size_t)(p / kNB) * kNB * kNB, G, Ts);
+    // T factor from the Gram entries (warp 0): T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j)
+    if (warp == 0) {
+        for (int j = 0; j < kNB; ++j) {
+            if (j < w) {
+                const T tj = s_tau[j];
+                T tmp = T(0);
+                if (lane < j)
+                    for (int l = lane; l < j; ++l) tmp += Ts[lane * GP + l] * G[l * GP + j];
+                if (lane < j) Ts[lane * GP + j] = -tj * tmp;
+                if (lane == j) Ts[j * GP + j] = tj;
+                if (lane > j) Ts[lane * GP + j] = T(0);
+            } else {
+                Ts[lane * GP + j] = T(0);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    T* Tout = t.tp + (size_t)(p / kNB) * kNB * kNB;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) Tout[e] = Ts[(e % kNB) * GP + (e / kNB)];
     if (in_smem) {
         for (int e = tid; e < R * w; e += blockDim.x) {
-            int i = e % R, j = e / R;
+            const int i = e % R, j = e / R;
             gp[i + (size_t)j * m] = P[i + j * ldp];
         }
     }
@@ -347,198 +395,6 @@ __global__ void __launch_bounds__(128) k_trsm(const TrsmTask<T>* tasks, const Ti
         if (active)
             for (int jj = 0; jj < wj; ++jj) t.X[row + (size_t)(J0 + jj) * t.ldx] = acc[jj];
         __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------------ truncated RRQR
-template <class T>
-struct Eps;
-template <>
-struct Eps<double> {
-    static __device__ double tol3z() { return 1.0536712127723509e-08; }  // sqrt(2^-53)
-};
-template <>
-struct Eps<float> {
-    static __device__ float tol3z() { return 2.44140625e-04f; }  // sqrt(2^-24)
-};
-
-template <class T>
-__global__ void __launch_bounds__(1024) k_rrqr(const RRQRTask<T>* tasks) {
-    __shared__ T red[32];
-    __shared__ T redv[32];
-    __shared__ int redi[32];
-    __shared__ int s_pvt;
-    const RRQRTask<T> t = tasks[blockIdx.x];
-    const int m = t.m, n = t.n;
-    T* C = t.C;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int j = warp; j < n; j += nw) {
-        T s = T(0);
-        for (int i = lane; i < m; i += 32) s += C[i + (size_t)j * m] * C[i + (size_t)j * m];
-        s = warp_sum(s);
-        if (lane == 0) {
-            T v = sqrt(s);
-            t.vn1[j] = v;
-            t.vn2[j] = v;
-            t.jpvt[j] = j;
-        }
-    }
-    __syncthreads();
-    const int kmax = min(m, n);
-    int rank = kmax;
-    const double tol = t.tol;
-    if (tol != 0.0 && tol >= 1.0) rank = 0;
-    T r00 = T(0);
-    const int kstop = (tol != 0.0 && tol >= 1.0) ? 0 : kmax;
-    for (int k = 0; k < kstop; ++k) {
-        // pivot: first index of the largest partial norm in [k, n)
-        T bv = T(-1);
-        int bi = n;
-        for (int j = k + tid; j < n; j += blockDim.x) {
-            T v = t.vn1[j];
-            if (v > bv) { bv = v; bi = j; }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            T ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
-        if (lane == 0) { redv[warp] = bv; redi[warp] = bi; }
-        __syncthreads();
-        if (warp == 0) {
-            bv = lane < nw ? redv[lane] : T(-1);
-            bi = lane < nw ? redi[lane] : n;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                T ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-            }
-            if (lane == 0) s_pvt = bi;
-        }
-        __syncthreads();
-        const int pvt = s_pvt;
-        if (pvt != k && pvt < n) {
-            for (int i = tid; i < m; i += blockDim.x) {
-                T a = C[i + (size_t)k * m];
-                C[i + (size_t)k * m] = C[i + (size_t)pvt * m];
-                C[i + (size_t)pvt * m] = a;
-            }
-            if (tid == 0) {
-                int a = t.jpvt[k];
-                t.jpvt[k] = t.jpvt[pvt];
-                t.jpvt[pvt] = a;
-                t.vn1[pvt] = t.vn1[k];
-                t.vn2[pvt] = t.vn2[k];
-            }
-        }
-        __syncthreads();
-        T part = T(0);
-        for (int i = k + 1 + tid; i < m; i += blockDim.x) {
-            T v = C[i + (size_t)k * m];
-            part += v * v;
-        }
-        const T xn2 = block_sum(part, red);
-        const T alpha = C[k + (size_t)k * m];
-        T tau, beta, scal;
-        make_reflector(alpha, xn2, tau, beta, scal);
-        if (tau != T(0))
-            for (int i = k + 1 + tid; i < m; i += blockDim.x) C[i + (size_t)k * m] *= scal;
-        __syncthreads();
-        if (tid == 0) {
-            C[k + (size_t)k * m] = beta;
-            t.tau[k] = tau;
-        }
-        // rank rule of choose_rank (uniform across the block)
-        if (tol != 0.0 && kmax > 1) {
-            if (k == 0) {
-                r00 = fabs(beta);
-            } else if (!((double)fabs(beta) / (double)r00 >= tol)) {
-                rank = k;
-                break;
-            }
-        }
-        __syncthreads();
-        const T* v = C + (size_t)k * m;
-        for (int j = k + 1 + warp; j < n; j += nw) {
-            T* cj = C + (size_t)j * m;
-            if (tau != T(0)) {
-                T s = T(0);
-                for (int i = k + 1 + lane; i < m; i += 32) s += v[i] * cj[i];
-                s = warp_sum(s);
-                s = (s + cj[k]) * tau;
-                for (int i = k + 1 + lane; i < m; i += 32) cj[i] -= s * v[i];
-                __syncwarp();
-                if (lane == 0) cj[k] -= s;
-                __syncwarp();
-            }
-            // partial column norm downdate (LAPACK dlaqp2 rule)
-            T n1 = t.vn1[j];
-            if (n1 != T(0)) {
-                T r = fabs(cj[k]) / n1;
-                T temp = T(1) - r * r;
-                temp = temp < T(0) ? T(0) : temp;
-                T q = n1 / t.vn2[j];
-                T temp2 = temp * q * q;
-                if (temp2 <= Eps<T>::tol3z()) {
-                    T s = T(0);
-                    for (int i = k + 1 + lane; i < m; i += 32) s += cj[i] * cj[i];
-                    s = warp_sum(s);
-                    if (lane == 0) {
-                        T nv = (k + 1 < m) ? (T)sqrt(s) : T(0);
-                        t.vn1[j] = nv;
-                        t.vn2[j] = nv;
-                    }
-                } else if (lane == 0) {
-                    t.vn1[j] = n1 * (T)sqrt(temp);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-    if (tid == 0) *t.rank = rank;
-    for (int j = tid; j < n; j += blockDim.x) t.ipvt[t.jpvt[j]] = j;
-}
-
-// ------------------------------------------------------------------ sparsification write-back
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks) {
-    __shared__ T G[kNB * (kNB + 1)];
-    __shared__ T Ts[kNB * (kNB + 1)];
-    __shared__ T s_tau[kNB];
-    const SparsWB<T> t = tasks[blockIdx.x];
-    const int r = *t.rank;
-    const int m = t.m;
-    if (r >= m) return;
-    const int tid = threadIdx.x;
-    for (int b = 0; b < t.nblk; ++b) {
-        const SpBlock<T> B = blocks[t.blk0 + b];
-        if (B.kind == 0) {
-            const int64_t tot = (int64_t)B.rows * r;
-            for (int64_t e = tid; e < tot; e += blockDim.x) {
-                int i = (int)(e % B.rows), j = (int)(e / B.rows);
-                int q = t.ipvt[B.coff + i];
-                B.p[i + (size_t)j * B.ld] = (j <= q) ? t.C[j + (size_t)q * m] : T(0);
-            }
-        } else {
-            const int64_t tot = (int64_t)r * B.cols;
-            for (int64_t e = tid; e < tot; e += blockDim.x) {
-                int i = (int)(e % r), j = (int)(e / r);
-                int q = t.ipvt[B.coff + j];
-                B.p[i + (size_t)j * B.ld] = (i <= q) ? t.C[i + (size_t)q * m] : T(0);
-            }
-        }
-    }
-    for (int64_t e = tid; e < (int64_t)m * r; e += blockDim.x) t.V[e] = t.C[e];
-    for (int j = tid; j < r; j += blockDim.x) t.tau[j] = t.tau_in[j];
-    __syncthreads();
-    for (int p0 = 0; p0 < r; p0 += kNB) {
-        const int w = min(kNB, r - p0);
-        if (tid < kNB) s_tau[tid] = tid < w ? t.tau_in[p0 + tid] : T(0);
-        __syncthreads();
-        build_tfac(t.C + p0 + (size_t)p0 * m, m, m - p0, w, s_tau, t.tp + (size_t)(p0 / kNB) * kNB * kNB, G, Ts);
     }
 }
 
@@ -774,13 +630,17 @@ __global__ void k_spmv(int m, const int* rp, const int* ci, const double* v, con
     }
 }
 
-__global__ void k_dot_partials(const double* a, const double* b, int lo, int m, double* partials) {
+// partials[b] = block b's share of sum_{i >= lo} a[i] b[i]; if head is given,
+// partials[gridDim.x] = *head (read before any later kernel changes it).
+__global__ void k_dot_partials(const double* a, const double* b, int lo, int m, double* partials,
+                               const double* head) {
     __shared__ double red[32];
     double s = 0.0;
     for (int i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
         s += b ? a[i] * b[i] : a[i] * a[i];
     s = block_sum(s, red);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    if (head && blockIdx.x == 0 && threadIdx.x == 0) partials[gridDim.x] = *head;
 }
 
 __device__ double sum_partials(const double* partials, int nblk, double* red) {
@@ -789,11 +649,13 @@ __device__ double sum_partials(const double* partials, int nblk, double* red) {
     return block_sum(s, red);
 }
 
-// v[i:] <- (I - tau h h^T) v[i:], h = [1; ess]; partials hold sum_{r>i} ess[r-i-1] v[r].
+// v[i:] <- (I - tau h h^T) v[i:], h = [1; ess]; partials hold sum_{r>i} ess[r-i-1] v[r]
+// and, at index nblk, v[i] as it was before this kernel (block 0 rewrites v[i],
+// so no block may read it here).
 __global__ void k_apply_reflector(const double* ess, const double* tau, double* v, int i, int m,
                                   const double* partials, int nblk) {
     __shared__ double red[32];
-    const double d = sum_partials(partials, nblk, red) + v[i];
+    const double d = sum_partials(partials, nblk, red) + partials[nblk];
     const double tv = *tau;
     if (tv == 0.0) return;
     __syncthreads();
@@ -876,18 +738,6 @@ void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cud
 }
 
 template <class T>
-void launch_rrqr(const RRQRTask<T>* tasks, int ntasks, int nthreads, cudaStream_t s) {
-    if (ntasks <= 0) return;
-    k_rrqr<T><<<ntasks, nthreads, 0, s>>>(tasks);
-}
-
-template <class T>
-void launch_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s) {
-    if (ntasks <= 0) return;
-    k_spars_wb<T><<<ntasks, kThreads, 0, s>>>(tasks, blocks);
-}
-
-template <class T>
 void launch_scatter_values(const uint64_t* addr, const double* vals, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
     k_scatter_values<T><<<grid_for(n, 256), 256, 0, s>>>(addr, vals, n);
@@ -916,8 +766,8 @@ void launch_spmv_csr(int m, const int* rp, const int* ci, const double* v, const
     k_spmv<<<grid_for(m, 256, 148 * 32), 256, 0, s>>>(m, rp, ci, v, x, y);
 }
 void launch_dot_partials(const double* a, const double* b, int lo, int m, double* partials, int nblk,
-                         cudaStream_t s) {
-    k_dot_partials<<<nblk, 256, 0, s>>>(a, b, lo, m, partials);
+                         cudaStream_t s, const double* head) {
+    k_dot_partials<<<nblk, 256, 0, s>>>(a, b, lo, m, partials, head);
 }
 void launch_apply_reflector(const double* ess, const double* tau, double* v, int i, int m, const double* partials,
                             int nblk, cudaStream_t s) {
@@ -950,8 +800,6 @@ void prepare_kernels() {
     template void launch_panel<T>(const QRTask<T>*, const int*, int, int, int, cudaStream_t);                 \
     template void launch_trailing<T>(const QRTask<T>*, const TileRef*, int, int, cudaStream_t);               \
     template void launch_trsm<T>(const TrsmTask<T>*, const TileRef*, int, cudaStream_t);                      \
-    template void launch_rrqr<T>(const RRQRTask<T>*, int, int, cudaStream_t);                                 \
-    template void launch_spars_wb<T>(const SparsWB<T>*, const SpBlock<T>*, int, cudaStream_t);                \
     template void launch_scatter_values<T>(const uint64_t*, const double*, int64_t, cudaStream_t);         \
     template void launch_solve_step<T>(const SolveOp*, int, const XSeg*, const GemvRef<T>*, const T*, T*, int, \
                                        cudaStream_t);                                                          \

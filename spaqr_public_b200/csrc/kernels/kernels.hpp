@@ -62,47 +62,48 @@ template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s);
 
 // ---------------------------------------------------------------- truncated RRQR
-// Column-pivoted Householder QR of C (m x n, ld m) stopped at the first k with
-// |R_kk| < tol |R_00| (the rank rule of choose_rank, src/util.cpp:795-816).
-// Writes rank, jpvt (0-based original column of each pivoted position), ipvt
-// (inverse) and tau; C holds R (rows < rank) and V as LAPACK dgeqp3 does.
-template <class T>
-struct RRQRTask {
-    T* C;
-    int* jpvt;
-    int* ipvt;
-    T* tau;
-    T* vn1;
-    T* vn2;
-    int* rank;
-    int m, n;
-    double tol;
-};
-template <class T>
-void launch_rrqr(const RRQRTask<T>* tasks, int ntasks, int nthreads, cudaStream_t s);
-
 // Write-back after the RRQR (sparsifyD, src/tree.cpp:1082-1110): rebuild the
 // interface's column blocks (A(n2, c) <- first rank columns of (Crank P^T)^T)
 // and row blocks (top rank rows <- Crank P^T), save V and tau for the solve and
-// build the panel T factors of V.
+// build the panel T factors of V. Block descriptor:
 template <class T>
 struct SpBlock {
     T* p;
     int ld, rows, cols, coff, kind;  // kind 0: column block (Amp), 1: row block (Apm)
 };
+// Cluster-parallel truncated RRQR on a ROW-major C (row stride ldc). Outputs:
+// rank, tau[0:rank), pos[c] = pivot position of column c (inverse permutation,
+// positions >= rank for the non-pivot columns), colat[q] = column at position
+// q (jpvt). One cluster of `cluster` CTAs per task.
 template <class T>
-struct SparsWB {
-    const T* C;
-    const int* ipvt;
-    const T* tau_in;
-    const int* rank;
-    T* V;        // m x m capacity, ld m
-    T* tau;      // m
-    T* tp;       // panels
-    int m, nblk, blk0, pad;
+struct RRQRTaskRM {
+    T* C;
+    int* pos;
+    int* colat;
+    T* tau;
+    T* vn1;
+    T* vn2;
+    int* rank;
+    int m, n, ldc, pad;
+    double tol;
 };
 template <class T>
-void launch_spars_wb(const SparsWB<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s);
+cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,
+                           int max_n, cudaStream_t s);
+// Write-back after the cluster RRQR, with the rank r known on the host.
+template <class T>
+struct SparsWBRM {
+    const T* C;
+    const int* pos;
+    const int* colat;
+    const T* tau_in;
+    T* V;    // m x r, ld m
+    T* tau;  // r
+    T* tp;   // panel T factors of V
+    int m, ldc, r, nblk, blk0, pad;
+};
+template <class T>
+void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s);
 
 // ---------------------------------------------------------------- assembly
 // *(T*)dst_addr[e] = (T) vals[e]
@@ -147,10 +148,12 @@ void launch_scatter_out(const T* x, const int64_t* xpos, const int* dst, double*
 // ---------------------------------------------------------------- Krylov helpers (FP64)
 void launch_spmv_csr(int m, const int* rp, const int* ci, const double* v, const double* x, double* y,
                      cudaStream_t s);
-// partial sums of a[i]*b[i] (or a[i]^2 if b == nullptr) over [lo, m): nblk partials
+// partial sums of a[i]*b[i] (or a[i]^2 if b == nullptr) over [lo, m): nblk partials,
+// plus partials[nblk] = *head when head is given (the reflector's head element).
 void launch_dot_partials(const double* a, const double* b, int lo, int m, double* partials, int nblk,
-                         cudaStream_t s);
+                         cudaStream_t s, const double* head = nullptr);
 // v[i:] <- (I - tau h h^T) v[i:] with h = [1; ess], ess = H[i+1:, col]; dot from partials
+// (launch_dot_partials with head = v + i)
 void launch_apply_reflector(const double* ess, const double* tau, double* v, int i, int m, const double* partials,
                             int nblk, cudaStream_t s);
 // Householder of v[k:] (makeHouseholder): writes ess into H col k (rows k+1..), tau, beta.

@@ -1,0 +1,470 @@
+// Truncated column-pivoted Householder QR of the sparsification matrices
+// (sparsifyD, src/tree.cpp:1022-1049; dgeqp3 + choose_rank, src/util.cpp:466-477,
+// 795-816), one thread-block cluster per interface.
+//
+// Layout: C (m x n, m = interface columns, n = total neighbour width) is stored
+// ROW-major with row stride ldc, so a thread that owns a column streams it
+// with warp-coalesced accesses. Columns are never moved: the pivot order is
+// kept as pos[column] / colat[position] exactly as LAPACK's swaps would leave
+// it, so ties in the partial norms are broken by the current position (first
+// index of idamax), and the norms travel with their columns.
+//
+// Per pivot step k, with the columns split in contiguous slabs over the CTAs
+// of the cluster:
+//   1. every CTA finds the largest partial norm of its active columns;
+//      cluster barrier; every CTA reduces the candidates through DSMEM;
+//   2. the CTA owning the pivot column builds the reflector (LAPACK dlarfg)
+//      into its shared memory; cluster barrier; the others copy it through
+//      DSMEM and all stop together if |R_kk| < tol |R_00|;
+//   3. every CTA applies the reflector to its active columns and downdates
+//      their norms (LAPACK dlaqp2 rule with recomputation below sqrt(eps)).
+// The loop stops at the rank, so only rank steps of the O(m n r) work run.
+#include <cooperative_groups.h>
+
+#include <cfloat>
+#include <algorithm>
+#include <climits>
+
+#include "kernels.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace spq {
+namespace {
+
+constexpr int kRRThreads = 512;
+constexpr int kU = 4;  // column tiles per lane in the update passes
+
+template <class T>
+__device__ __forceinline__ T wsum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class T>
+__device__ T bsum(T v, T* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = wsum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        T r = lane < nw ? red[lane] : T(0);
+        r = wsum(r);
+        if (lane == 0) red[0] = r;
+    }
+    __syncthreads();
+    return red[0];
+}
+
+template <class T>
+struct Tol3z;
+template <>
+struct Tol3z<double> {
+    static __device__ double v() { return 1.0536712127723509e-08; }  // sqrt(2^-53)
+};
+template <>
+struct Tol3z<float> {
+    static __device__ float v() { return 2.44140625e-04f; }  // sqrt(2^-24)
+};
+
+__device__ __forceinline__ double dhypot(double a, double b) { return hypot(a, b); }
+__device__ __forceinline__ float dhypot(float a, float b) { return hypotf(a, b); }
+
+// (value, position, column): larger value wins, then the smaller position.
+template <class T>
+__device__ __forceinline__ bool better(T v, int p, T bv, int bp) {
+    return v > bv || (v == bv && p < bp);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids,
+                                                         size_t smem_bytes) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* vsh = reinterpret_cast<T*>(smem_raw);
+    __shared__ T red[32];
+    __shared__ T wv[32];
+    __shared__ int wp[32], wc[32];
+    __shared__ T s_val, s_beta, s_tau;
+    __shared__ int s_pos, s_col, s_gp, s_gc;
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int cr = (int)cl.block_rank();
+    const RRQRTaskRM<T> t = tasks[ids[blockIdx.x / CL]];
+    const int m = t.m, n = t.n;
+    const size_t ld = (size_t)t.ldc;
+    T* C = t.C;
+    const int W = (n + CL - 1) / CL;
+    const int j0 = min(n, cr * W), j1 = min(n, j0 + W);
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+    // shared memory: reflector (m) | dot partials (G x Wp) | per-column scale (Wp)
+    const int mpad = (m + 7) & ~7;
+    const int Wp = ((j1 - j0) + 31) & ~31;
+    const int avail = (int)(smem_bytes / sizeof(T)) - mpad - Wp;
+    const int G = max(1, min(16, Wp > 0 ? avail / Wp : 1));
+    T* part = vsh + mpad;
+    T* svec = part + (size_t)G * Wp;
+
+    for (int j = j0 + tid; j < j1; j += nth) {
+        T s = T(0);
+#pragma unroll 8
+        for (int i = 0; i < m; ++i) {
+            const T v = C[i * ld + j];
+            s += v * v;
+        }
+        const T nv = sqrt(s);
+        t.vn1[j] = nv;
+        t.vn2[j] = nv;
+        t.pos[j] = j;
+        t.colat[j] = j;
+    }
+    cl.sync();
+
+    const int kmax = min(m, n);
+    const double tol = t.tol;
+    int rank = kmax;
+    const int ksteps = (tol != 0.0 && tol >= 1.0) ? 0 : kmax;
+    if (ksteps == 0) rank = (tol != 0.0 && tol >= 1.0) ? 0 : kmax;
+    T r00 = T(0);
+    for (int k = 0; k < ksteps; ++k) {
+        // 1. pivot: largest partial norm, ties to the smallest position
+        T bv = T(-1);
+        int bp = INT_MAX, bc = -1;
+        for (int j = j0 + tid; j < j1; j += nth) {
+            const int p = t.pos[j];
+            if (p < k) continue;
+            const T v = t.vn1[j];
+            if (better(v, p, bv, bp)) { bv = v; bp = p; bc = j; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+            const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+            if (better(ov, op, bv, bp)) { bv = ov; bp = op; bc = oc; }
+        }
+        if (lane == 0) { wv[warp] = bv; wp[warp] = bp; wc[warp] = bc; }
+        __syncthreads();
+        if (warp == 0) {
+            bv = lane < nw ? wv[lane] : T(-1);
+            bp = lane < nw ? wp[lane] : INT_MAX;
+            bc = lane < nw ? wc[lane] : -1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+                const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+                if (better(ov, op, bv, bp)) { bv = ov; bp = op; bc = oc; }
+            }
+            if (lane == 0) { s_val = bv; s_pos = bp; s_col = bc; }
+        }
+        cl.sync();
+        // every CTA reduces the cluster's candidates in parallel (lane r reads CTA r)
+        if (warp == 0) {
+            T v = T(-1);
+            int p = INT_MAX, c = -1;
+            if (lane < CL) {
+                c = *cl.map_shared_rank(&s_col, lane);
+                if (c >= 0) {
+                    v = *cl.map_shared_rank(&s_val, lane);
+                    p = *cl.map_shared_rank(&s_pos, lane);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int op = __shfl_xor_sync(0xffffffffu, p, o);
+                const int oc = __shfl_xor_sync(0xffffffffu, c, o);
+                if (better(ov, op, v, p)) { v = ov; p = op; c = oc; }
+            }
+            if (lane == 0) { s_gp = p; s_gc = c; }
+        }
+        __syncthreads();
+        const int gp = s_gp, gc = s_gc;
+        const int pc = gc;
+        const int owner = pc / W;
+        // 2. reflector of the pivot column (rows k..m-1) by its owner
+        if (cr == owner) {
+            T acc = T(0);
+            for (int i = k + 1 + tid; i < m; i += nth) {
+                const T v = C[i * ld + pc];
+                acc += v * v;
+            }
+            const T xn2 = bsum(acc, red);
+            const T alpha = C[k * ld + pc];
+            T tau, beta, scal;
+            if (xn2 == T(0)) {
+                tau = T(0);
+                beta = alpha;
+                scal = T(1);
+            } else {
+                const T nrm = dhypot(alpha, (T)sqrt(xn2));
+                beta = alpha >= T(0) ? -nrm : nrm;
+                tau = (beta - alpha) / beta;
+                scal = T(1) / (alpha - beta);
+            }
+            for (int i = k + 1 + tid; i < m; i += nth) {
+                T v = C[i * ld + pc];
+                if (tau != T(0)) {
+                    v *= scal;
+                    C[i * ld + pc] = v;
+                }
+                vsh[i] = v;
+            }
+            if (tid == 0) {
+                vsh[k] = T(1);
+                s_beta = beta;
+                s_tau = tau;
+                C[k * ld + pc] = beta;
+                t.tau[k] = tau;
+            }
+        }
+        cl.sync();
+        const T beta = *cl.map_shared_rank(&s_beta, owner);
+        const T tau = *cl.map_shared_rank(&s_tau, owner);
+        if (cr != owner) {
+            const T* ov = cl.map_shared_rank(vsh, owner);
+            for (int i = k + tid; i < m; i += nth) vsh[i] = ov[i];
+        }
+        if (tol != 0.0 && kmax > 1) {
+            if (k == 0) {
+                r00 = fabs(beta);
+            } else if (!((double)fabs(beta) / (double)r00 >= tol)) {
+                rank = k;
+                break;  // uniform over the cluster: every CTA read the same beta
+            }
+        }
+        if (cr == 0 && tid == 0) {  // LAPACK's column swap, as positions
+            const int pvt = gp;
+            const int c0 = t.colat[k];
+            t.colat[pvt] = c0;
+            t.pos[c0] = pvt;
+            t.colat[k] = pc;
+            t.pos[pc] = k;
+        }
+        __syncthreads();
+        // 3. apply H_k to the active columns and downdate their norms. The slab
+        //    is cut in 32-column tiles (lane = column: coalesced rows) and the
+        //    rows below k in G chunks; warps take (chunk, tile) items so that no
+        //    thread walks a whole column, and the chunk partials of each dot
+        //    product meet in shared memory.
+        const int Wc = j1 - j0;
+        const int ntile = (Wc + 31) / 32;
+        const int ntg = (ntile + kU - 1) / kU;  // groups of kU tiles handled together by one lane
+        const int Gs = max(1, min(G, (m - k - 1 + 31) / 32));  // >= 32 rows per chunk
+        const int Lr = (m - k - 1 + Gs - 1) / Gs;
+        if (tau != T(0)) {
+            for (int item = warp; item < Gs * ntg; item += nw) {
+                const int g = item % Gs, tg = item / Gs;
+                const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
+                T s[kU];
+                const T* cp[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    s[u] = T(0);
+                    const int jl = (tg * kU + u) * 32 + lane;
+                    cp[u] = jl < Wc ? C + (j0 + jl) : nullptr;
+                }
+#pragma unroll 4
+                for (int i = i0; i < i1; ++i) {
+                    const T vi = vsh[i];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u)
+                        if (cp[u]) s[u] += vi * cp[u][i * ld];
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int jl = (tg * kU + u) * 32 + lane;
+                    if (jl < Wp) part[g * Wp + jl] = s[u];
+                }
+            }
+        }
+        __syncthreads();
+        for (int jl = tid; jl < Wc; jl += nth) {
+            const int j = j0 + jl;
+            T s = T(0);
+            if (tau != T(0) && j != pc && t.pos[j] >= k) {
+                s = C[k * ld + j];
+                for (int g = 0; g < Gs; ++g) s += part[g * Wp + jl];
+                s *= tau;
+                C[k * ld + j] -= s;
+            }
+            svec[jl] = s;
+        }
+        __syncthreads();
+        if (tau != T(0)) {
+            for (int item = warp; item < Gs * ntg; item += nw) {
+                const int g = item % Gs, tg = item / Gs;
+                const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
+                T sc[kU];
+                T* cp[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int jl = (tg * kU + u) * 32 + lane;
+                    sc[u] = jl < Wc ? svec[jl] : T(0);
+                    cp[u] = (jl < Wc && sc[u] != T(0)) ? C + (j0 + jl) : nullptr;
+                }
+#pragma unroll 4
+                for (int i = i0; i < i1; ++i) {
+                    const T vi = vsh[i];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u)
+                        if (cp[u]) cp[u][i * ld] -= sc[u] * vi;
+                }
+            }
+        }
+        __syncthreads();
+        for (int j = j0 + tid; j < j1; j += nth) {
+            if (j == pc || t.pos[j] < k) continue;
+            T* cj = C + j;
+            const T n1 = t.vn1[j];
+            if (n1 != T(0)) {
+                const T rk = fabs(cj[k * ld]) / n1;
+                T temp = T(1) - rk * rk;
+                temp = temp < T(0) ? T(0) : temp;
+                const T q = n1 / t.vn2[j];
+                const T temp2 = temp * q * q;
+                if (temp2 <= Tol3z<T>::v()) {
+                    T ss = T(0);
+                    for (int i = k + 1; i < m; ++i) ss += cj[i * ld] * cj[i * ld];
+                    const T nv = (k + 1 < m) ? (T)sqrt(ss) : T(0);
+                    t.vn1[j] = nv;
+                    t.vn2[j] = nv;
+                } else {
+                    t.vn1[j] = n1 * (T)sqrt(temp);
+                }
+            }
+        }
+        cl.sync();  // positions of step k visible to every CTA before the next pivot search
+    }
+    // No CTA may exit while another still reads its shared memory (the early
+    // exit at the rank leaves right after the DSMEM reads of that step).
+    cl.sync();
+    if (cr == 0 && tid == 0) *t.rank = rank;
+}
+
+// Write-back of a sparsified interface (sparsifyD, src/tree.cpp:1082-1110):
+// Crank = R(0:r, :) un-permuted: Crank(i, c) = C(i, c) if i <= pos[c] else 0.
+template <class T>
+__global__ void __launch_bounds__(256) k_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks) {
+    __shared__ T G[kNB * (kNB + 1)];
+    __shared__ T Ts[kNB * (kNB + 1)];
+    __shared__ T s_tau[kNB];
+    const SparsWBRM<T> t = tasks[blockIdx.x];
+    const int r = t.r, m = t.m;
+    const size_t ld = (size_t)t.ldc;
+    const int tid = threadIdx.x;
+    for (int b = 0; b < t.nblk; ++b) {
+        const SpBlock<T> B = blocks[t.blk0 + b];
+        if (B.kind == 0) {  // column block A(n2, c): rows x r
+            const int64_t tot = (int64_t)B.rows * r;
+            for (int64_t e = tid; e < tot; e += blockDim.x) {
+                const int i = (int)(e % B.rows), j = (int)(e / B.rows);
+                const int c = B.coff + i;
+                B.p[i + (size_t)j * B.ld] = (j <= t.pos[c]) ? t.C[j * ld + c] : T(0);
+            }
+        } else {  // row block A(c, n1): r x cols
+            const int64_t tot = (int64_t)r * B.cols;
+            for (int64_t e = tid; e < tot; e += blockDim.x) {
+                const int j = (int)(e % B.cols), i = (int)(e / B.cols);
+                const int c = B.coff + j;
+                B.p[i + (size_t)j * B.ld] = (i <= t.pos[c]) ? t.C[i * ld + c] : T(0);
+            }
+        }
+    }
+    // V(:, q) = column colat[q] (reflector below the diagonal), tau
+    for (int64_t e = tid; e < (int64_t)m * r; e += blockDim.x) {
+        const int i = (int)(e % m), q = (int)(e / m);
+        t.V[e] = t.C[i * ld + t.colat[q]];
+    }
+    for (int q = tid; q < r; q += blockDim.x) t.tau[q] = t.tau_in[q];
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    constexpr int P = kNB + 1;
+    for (int p0 = 0; p0 < r; p0 += kNB) {
+        const int w = min(kNB, r - p0);
+        const T* Vp = t.V + p0 + (size_t)p0 * m;
+        const int R = m - p0;
+        if (tid < kNB) s_tau[tid] = tid < w ? t.tau_in[p0 + tid] : T(0);
+        int pair = 0;
+        for (int j = 1; j < w; ++j)
+            for (int i = 0; i < j; ++i, ++pair) {
+                if ((pair % nw) != warp) continue;
+                T s = T(0);
+                for (int rr = j + 1 + lane; rr < R; rr += 32) s += Vp[rr + (size_t)i * m] * Vp[rr + (size_t)j * m];
+                s = wsum(s);
+                if (lane == 0) G[i * P + j] = s + (j < R ? Vp[j + (size_t)i * m] : T(0));
+            }
+        __syncthreads();
+        if (warp == 0) {
+            for (int j = 0; j < kNB; ++j) {
+                if (j < w) {
+                    const T tj = s_tau[j];
+                    T tmp = T(0);
+                    if (lane < j)
+                        for (int l = lane; l < j; ++l) tmp += Ts[lane * P + l] * G[l * P + j];
+                    if (lane < j) Ts[lane * P + j] = -tj * tmp;
+                    if (lane == j) Ts[j * P + j] = tj;
+                    if (lane > j) Ts[lane * P + j] = T(0);
+                } else {
+                    Ts[lane * P + j] = T(0);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        T* Tout = t.tp + (size_t)(p0 / kNB) * kNB * kNB;
+        for (int e = tid; e < kNB * kNB; e += blockDim.x) Tout[e] = Ts[(e % kNB) * P + (e / kNB)];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+template <class T>
+cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,
+                           int max_n, cudaStream_t s) {
+    if (ntasks <= 0) return cudaSuccess;
+    // reflector + up to 16 row-chunk partials of the widest slab + per-column scales
+    const size_t mpad = (size_t)((max_m + 7) & ~7);
+    const size_t wp = (size_t)(((max_n + cluster - 1) / cluster + 31) & ~31);
+    size_t smem_bytes = (mpad + 17 * wp) * sizeof(T);
+    const size_t cap = 160 * 1024;
+    if (smem_bytes > cap) smem_bytes = std::max(cap, (mpad + 2 * wp) * sizeof(T));
+    if (smem_bytes > 200 * 1024) return cudaErrorInvalidValue;  // interface too wide for this launch shape
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_rrqr_rm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_rrqr_rm<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        attr = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(ntasks * cluster), 1, 1);
+    cfg.blockDim = dim3(kRRThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_rrqr_rm<T>, tasks, ids, smem_bytes);
+}
+
+template <class T>
+void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_spars_wb_rm<T><<<ntasks, 256, 0, s>>>(tasks, blocks);
+}
+
+template cudaError_t launch_rrqr_rm<double>(const RRQRTaskRM<double>*, const int*, int, int, int, int,
+                                            cudaStream_t);
+template cudaError_t launch_rrqr_rm<float>(const RRQRTaskRM<float>*, const int*, int, int, int, int, cudaStream_t);
+template void launch_spars_wb_rm<double>(const SparsWBRM<double>*, const SpBlock<double>*, int, cudaStream_t);
+template void launch_spars_wb_rm<float>(const SparsWBRM<float>*, const SpBlock<float>*, int, cudaStream_t);
+
+}  // namespace spq
