@@ -109,6 +109,22 @@ int spq_solve_to_residual_dev(spq_tree* t, int m, const int* d_rowptr, const int
 /* GMRES with device-resident inputs (CSR on the device). */
 int spq_gmres_dev(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
                   const double* d_b, double* d_x, int iters, int restart, double tol, int* its, double* res);
+/* GMRES with device-resident inputs that allocates no device memory. No
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * once they run (e.g. a service that reserves its GPU memory at start-up, or a
+ * real-time loop that must not enter the allocator). Same arguments and result
+ * as spq_gmres_dev; its Krylov workspace, gmres workspace = m * (restart + 1)
+ * + 5 m + a few hundred doubles, comes from one fixed 32 MiB device array
+ * (4 Mi doubles) that every GPU loading this library holds until the process
+ * exits; larger requests return SPQ_ERR_ARG with the sizes. Preconditions: the
+ * handle is factorized and its preconditioner has been applied at least once
+ * (spq_solve, spq_solve_dev or spq_gmres_dev build the solve graph), else
+ * SPQ_ERR_STATE. The first call on a device looks up the array's device
+ * address, so make that first call before any stream capture. All calls share
+ * the one array: calls that overlap on the GPU (several handles, streams or
+ * threads at once) race on it. The workspace is re-initialised by every call. */
+int spq_gmres_dev_noalloc(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
+                          const double* d_b, double* d_x, int iters, int restart, double tol, int* its, double* res);
 /* Kernel launches issued by the last spq_factorize and by Krylov calls since
  * the handle was created; solve_graph_kernels = kernels in one preconditioner
  * application (one CUDA graph launch), applications = graph launches so far. */

@@ -14,6 +14,10 @@
 
 using namespace spq;
 
+namespace spq {
+cudaError_t noalloc_scratch(double** ptr, size_t* elems);  // noalloc_scratch.cu
+}
+
 struct spq_tree {
     Config cfg;
     int precision = SPQ_FP64;
@@ -372,6 +376,39 @@ int spq_gmres_dev(spq_tree* t, int m, const int* rp, const int* ci, const double
         A.v = va;
         long long l = 0;
         *its = gmres_device(*t->eng, A, d_b, d_x, iters, restart, tol, res, &l);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "gmres");
+        return SPQ_OK;
+    });
+}
+
+int spq_gmres_dev_noalloc(spq_tree* t, int m, const int* rp, const int* ci, const double* va, const double* d_b,
+                          double* d_x, int iters, int restart, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "gmres before factorize");
+    if (m != t->eng->nrows() || m != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    if (!rp || !ci || !va || !d_b || !d_x || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid arguments");
+    if (!t->eng->solve_ready())
+        return fail(SPQ_ERR_STATE,
+                    "apply the preconditioner once (spq_solve, spq_solve_dev or spq_gmres_dev) before the "
+                    "no-allocation GMRES: the first application builds its solve graph");
+    return guard([&]() -> int {
+        cuda_check(cudaSetDevice(t->cfg.device), "cudaSetDevice");
+        double* ws = nullptr;
+        size_t cap = 0;
+        cuda_check(noalloc_scratch(&ws, &cap), "no-allocation workspace address");
+        const size_t need = gmres_workspace_elems(m, restart);
+        if (need > cap)
+            return fail(SPQ_ERR_ARG, "no-allocation GMRES needs " + std::to_string(need) +
+                                         " doubles of workspace (m * (restart + 1) + 5 m + ...) but the fixed "
+                                         "workspace holds " + std::to_string(cap) + "; lower restart or use spq_gmres_dev");
+        DevCsr A;
+        A.m = A.n = m;
+        A.rp = rp;
+        A.ci = ci;
+        A.v = va;
+        long long l = 0;
+        *its = gmres_device_ws(*t->eng, A, d_b, d_x, iters, restart, tol, res, &l, ws);
         t->launches_krylov += l;
         cuda_check(cudaStreamSynchronize(t->eng->stream()), "gmres");
         return SPQ_OK;

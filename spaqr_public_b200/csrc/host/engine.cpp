@@ -1269,6 +1269,8 @@ private:
     int nin_ = 0, nout_ = 0;
 
 public:
+    bool solve_ready() const override { return graph_exec_ != nullptr; }
+
     std::vector<double> profile_solve_waves() override {
         if (!factorized_) throw std::logic_error("profile before factorize");
         std::vector<double> out;

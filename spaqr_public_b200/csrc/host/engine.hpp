@@ -80,6 +80,9 @@ public:
     // wave timed: returns [ms, ops, smem elements] per wave (forward waves then
     // backward waves).
     virtual std::vector<double> profile_solve_waves() = 0;
+    // True once the preconditioner's solve graph exists (built by the first
+    // application); from then on an application allocates nothing.
+    virtual bool solve_ready() const = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(const Config& cfg, int precision);

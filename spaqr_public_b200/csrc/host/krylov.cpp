@@ -19,12 +19,19 @@ namespace {
 
 struct DevVec {
     double* p = nullptr;
+    bool owned = false;
     ~DevVec() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
     }
     void alloc(size_t n) {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         cuda_check(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)), "krylov cudaMalloc");
+        owned = true;
+    }
+    // Points at caller-provided device memory (never freed here).
+    void borrow(double* q) {
+        p = q;
+        owned = false;
     }
 };
 
@@ -68,6 +75,30 @@ public:
         scal_.alloc(2 * (restart + 1) + 4);
         H_.alloc((size_t)m_ * (restart + 1));
         hpart_.resize(nblk_);
+    }
+    // Same driver on a caller-provided workspace of workspace_elems(m, restart)
+    // doubles; nothing is allocated on the device.
+    Gmres(EngineBase& P, const DevCsr& A, int restart, double* ws) : P_(P), A_(A), m_(A.m), restart_(restart) {
+        s_ = P.stream();
+        nblk_ = reduce_blocks();
+        double* q = ws;
+        auto take = [&q](DevVec& v, size_t n) {
+            v.borrow(q);
+            q += (std::max<size_t>(n, 1) + 31) & ~size_t(31);  // 256-byte steps
+        };
+        take(p0_, m_);
+        take(r0_, m_);
+        take(t_, m_);
+        take(v_, m_);
+        take(xnew_, m_);
+        take(part_, nblk_ + 1);
+        take(scal_, 2 * (restart + 1) + 4);
+        take(H_, (size_t)m_ * (restart + 1));
+        hpart_.resize(nblk_);
+    }
+    static size_t workspace_elems(int m, int restart) {
+        auto r = [](size_t n) { return (std::max<size_t>(n, 1) + 31) & ~size_t(31); };
+        return 5 * r(m) + r(reduce_blocks() + 1) + r(2 * (restart + 1) + 4) + r((size_t)m * (restart + 1));
     }
 
     // Sum of a reduction's partials on the host, in fixed order.
@@ -213,6 +244,17 @@ int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x,
                  double* res, long long* launches) {
     if (restart < 1) restart = 1;
     Gmres g(P, A, restart);
+    int it = g.run(d_b, d_x, iters, tol, res);
+    if (launches) *launches = g.launches_;
+    return it;
+}
+
+size_t gmres_workspace_elems(int m, int restart) { return Gmres::workspace_elems(m, restart < 1 ? 1 : restart); }
+
+int gmres_device_ws(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart,
+                    double tol, double* res, long long* launches, double* workspace) {
+    if (restart < 1) restart = 1;
+    Gmres g(P, A, restart, workspace);
     int it = g.run(d_b, d_x, iters, tol, res);
     if (launches) *launches = g.launches_;
     return it;

@@ -17,6 +17,12 @@ struct DevCsr {
 int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart, double tol,
                  double* res, long long* launches);
 
+// The same GMRES on a caller-provided device workspace of
+// gmres_workspace_elems(m, restart) doubles; allocates no device memory.
+size_t gmres_workspace_elems(int m, int restart);
+int gmres_device_ws(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart,
+                    double tol, double* res, long long* launches, double* workspace);
+
 // ||b - A x|| / ||b|| on the device (FP64).
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x);
 
