@@ -837,12 +837,13 @@ private:
                 j.m = c->csize;
                 j.n = smp + spm;
                 j.smp = smp;
-                j.ld = std::max((j.n + 1) & ~1, 2);  // even row stride
+                j.ld = std::max((j.n + 3) & ~3, 4);  // row stride: 16-byte rows for column vectors
                 j.c_off = celems;
                 celems += (size_t)j.m * j.ld;
                 j.i_off = ielems;
                 ielems += 3 * (size_t)std::max(j.n, 1) + 1;
                 celems += 3 * (size_t)std::max(j.n, 1);  // tau, vn1, vn2
+                celems = (celems + 31) & ~size_t(31);     // next C starts 128-byte aligned (vector loads)
                 jobs.push_back(std::move(j));
             }
             const double tw = wall();

@@ -72,6 +72,20 @@ struct Tol3z<float> {
 __device__ __forceinline__ double dhypot(double a, double b) { return hypot(a, b); }
 __device__ __forceinline__ float dhypot(float a, float b) { return hypotf(a, b); }
 
+// 16-byte vector of adjacent row elements (columns of C).
+template <class T>
+struct Vec;
+template <>
+struct Vec<float> {
+    using type = float4;
+    static constexpr int n = 4;
+};
+template <>
+struct Vec<double> {
+    using type = double2;
+    static constexpr int n = 2;
+};
+
 // (value, position, column): larger value wins, then the smaller position.
 template <class T>
 __device__ __forceinline__ bool better(T v, int p, T bv, int bp) {
@@ -96,12 +110,14 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
     const int m = t.m, n = t.n;
     const size_t ld = (size_t)t.ldc;
     T* C = t.C;
-    const int W = (n + CL - 1) / CL;
+    // slabs start on 32-column boundaries, so 16-byte column vectors never
+    // straddle two CTAs (the row stride ldc is a multiple of 4)
+    const int W = (((n + CL - 1) / CL) + 31) & ~31;
     const int j0 = min(n, cr * W), j1 = min(n, j0 + W);
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
     // shared memory: reflector (m) | dot partials (G x Wp) | per-column scale (Wp)
     const int mpad = (m + 7) & ~7;
-    const int Wp = ((j1 - j0) + 31) & ~31;
+    const int Wp = ((j1 - j0) + 32 * Vec<T>::n - 1) / (32 * Vec<T>::n) * (32 * Vec<T>::n);
     const int avail = (int)(smem_bytes / sizeof(T)) - mpad - Wp;
     const int G = max(1, min(16, Wp > 0 ? avail / Wp : 1));
     T* part = vsh + mpad;
@@ -250,34 +266,49 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
         //    rows below k in G chunks; warps take (chunk, tile) items so that no
         //    thread walks a whole column, and the chunk partials of each dot
         //    product meet in shared memory.
+        // 3. apply H_k to the active columns and downdate their norms. Lanes own
+        //    16-byte vectors of VEC adjacent columns (coalesced row segments),
+        //    kU vectors per lane at once; the rows below k are cut into Gs chunks
+        //    handled by different warps, whose dot partials meet in shared memory.
+        constexpr int VEC = Vec<T>::n;
+        using VT = typename Vec<T>::type;
         const int Wc = j1 - j0;
-        const int ntile = (Wc + 31) / 32;
-        const int ntg = (ntile + kU - 1) / kU;  // groups of kU tiles handled together by one lane
+        const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);  // 32-vector tiles in the slab
+        const int ntg = (nvt + kU - 1) / kU;                 // groups of kU tiles per lane
         const int Gs = max(1, min(G, (m - k - 1 + 31) / 32));  // >= 32 rows per chunk
         const int Lr = (m - k - 1 + Gs - 1) / Gs;
         if (tau != T(0)) {
             for (int item = warp; item < Gs * ntg; item += nw) {
                 const int g = item % Gs, tg = item / Gs;
                 const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
-                T s[kU];
+                T s[kU][VEC];
                 const T* cp[kU];
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    s[u] = T(0);
-                    const int jl = (tg * kU + u) * 32 + lane;
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) s[u][q] = T(0);
+                    const int jl = ((tg * kU + u) * 32 + lane) * VEC;
                     cp[u] = jl < Wc ? C + (j0 + jl) : nullptr;
                 }
-#pragma unroll 4
+#pragma unroll 2
                 for (int i = i0; i < i1; ++i) {
                     const T vi = vsh[i];
 #pragma unroll
-                    for (int u = 0; u < kU; ++u)
-                        if (cp[u]) s[u] += vi * cp[u][i * ld];
+                    for (int u = 0; u < kU; ++u) {
+                        if (!cp[u]) continue;
+                        const VT x = *reinterpret_cast<const VT*>(cp[u] + i * ld);
+                        const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) s[u][q] += vi * xs[q];
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    const int jl = (tg * kU + u) * 32 + lane;
-                    if (jl < Wp) part[g * Wp + jl] = s[u];
+                    const int jl = ((tg * kU + u) * 32 + lane) * VEC;
+                    if (jl < Wp) {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) part[g * Wp + jl + q] = s[u][q];
+                    }
                 }
             }
         }
@@ -293,25 +324,38 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
             }
             svec[jl] = s;
         }
+        for (int jl = Wc + tid; jl < Wp; jl += nth) svec[jl] = T(0);  // vector tail past the slab
         __syncthreads();
         if (tau != T(0)) {
             for (int item = warp; item < Gs * ntg; item += nw) {
                 const int g = item % Gs, tg = item / Gs;
                 const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
-                T sc[kU];
+                T sc[kU][VEC];
                 T* cp[kU];
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    const int jl = (tg * kU + u) * 32 + lane;
-                    sc[u] = jl < Wc ? svec[jl] : T(0);
-                    cp[u] = (jl < Wc && sc[u] != T(0)) ? C + (j0 + jl) : nullptr;
+                    const int jl = ((tg * kU + u) * 32 + lane) * VEC;
+                    bool any = false;
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        sc[u][q] = jl < Wc ? svec[jl + q] : T(0);
+                        any = any || sc[u][q] != T(0);
+                    }
+                    cp[u] = (jl < Wc && any) ? C + (j0 + jl) : nullptr;
                 }
-#pragma unroll 4
+#pragma unroll 2
                 for (int i = i0; i < i1; ++i) {
                     const T vi = vsh[i];
 #pragma unroll
-                    for (int u = 0; u < kU; ++u)
-                        if (cp[u]) cp[u][i * ld] -= sc[u] * vi;
+                    for (int u = 0; u < kU; ++u) {
+                        if (!cp[u]) continue;
+                        VT* px = reinterpret_cast<VT*>(cp[u] + i * ld);
+                        VT x = *px;
+                        T* xs = reinterpret_cast<T*>(&x);
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) xs[q] -= sc[u][q] * vi;
+                        *px = x;
+                    }
                 }
             }
         }
@@ -429,7 +473,7 @@ cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntask
     if (ntasks <= 0) return cudaSuccess;
     // reflector + up to 16 row-chunk partials of the widest slab + per-column scales
     const size_t mpad = (size_t)((max_m + 7) & ~7);
-    const size_t wp = (size_t)(((max_n + cluster - 1) / cluster + 31) & ~31);
+    const size_t wp = (size_t)(((max_n + cluster - 1) / cluster + 127) & ~127);
     size_t smem_bytes = (mpad + 17 * wp) * sizeof(T);
     const size_t cap = 160 * 1024;
     if (smem_bytes > cap) smem_bytes = std::max(cap, (mpad + 2 * wp) * sizeof(T));
