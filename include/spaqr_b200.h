@@ -141,8 +141,10 @@ int spq_set_profile(spq_tree* t, int profile);
 int spq_get_kernel_stats(spq_tree* t, int family, double* out4);
 int spq_reset_kernel_stats(spq_tree* t);
 /* Diagnostic: runs one preconditioner application outside its CUDA graph and
- * times every sweep wave. out (capacity 3 * cap) receives [ms, ops, shared
- * vector length] per wave (forward then backward); *nwaves = waves. */
+ * times every sweep wave. out (capacity 7 * cap) receives, per wave (forward
+ * then backward): [ms, ops, shared vector length, factor words read, kind of
+ * the largest op (0 Q apply, 1 triangular), its rows, its columns (Q apply)
+ * or neighbour blocks (triangular)]; *nwaves = waves. */
 int spq_profile_solve_waves(spq_tree* t, double* out, int cap, int* nwaves);
 /* The CUDA stream (cudaStream_t) the handle issues its work on; valid after
  * spq_assemble. */

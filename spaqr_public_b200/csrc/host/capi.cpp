@@ -460,8 +460,8 @@ int spq_profile_solve_waves(spq_tree* t, double* out, int cap, int* nwaves) {
     if (t->state != 3) return fail(SPQ_ERR_STATE, "profile before factorize");
     return guard([&] {
         auto v = t->eng->profile_solve_waves();
-        *nwaves = (int)(v.size() / 3);
-        std::memcpy(out, v.data(), sizeof(double) * std::min<size_t>(v.size(), (size_t)cap * 3));
+        *nwaves = (int)(v.size() / 7);
+        std::memcpy(out, v.data(), sizeof(double) * std::min<size_t>(v.size(), (size_t)cap * 7));
         return SPQ_OK;
     });
 }

@@ -350,6 +350,8 @@ private:
     struct Wave {
         const SolveOp* ops;
         int nops, smem;
+        double words;        // factor words the wave reads
+        int hkind, ha, hb;   // kind and sizes of its largest op
     };
     std::vector<Wave> fwd_waves_, bwd_waves_;
     const XSeg* d_segs_ = nullptr;
@@ -1227,14 +1229,32 @@ private:
         struct WMeta {
             size_t off;
             int n, smem;
+            double words;
+            int hkind, ha, hb;
         };
         std::vector<WMeta> fm, bm;
+        auto op_words = [&](const SolveOp& o) -> double {
+            if (o.kind == SK_APPLYQ) return (double)o.a * o.b - 0.5 * (double)o.b * (o.b - 1);
+            if (o.kind != SK_TRI) return 0.0;
+            double w = 0.5 * (double)o.a * (o.a + 1);
+            for (int q = 0; q < o.nseg; ++q) w += (double)o.a * gemv[o.seg0 + q].s;
+            return w;
+        };
         auto pack = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves, std::vector<WMeta>& meta) {
             for (auto& w : waves) {
-                WMeta mt{all.size(), (int)w.size(), 0};
+                WMeta mt{all.size(), (int)w.size(), 0, 0.0, -1, 0, 0};
+                double hw = -1;
                 for (int i : w) {
                     all.push_back(ops[i].op);
                     mt.smem = std::max(mt.smem, ops[i].smem);
+                    const double ow = op_words(ops[i].op);
+                    mt.words += ow;
+                    if (ow > hw) {
+                        hw = ow;
+                        mt.hkind = ops[i].op.kind;
+                        mt.ha = ops[i].op.a;
+                        mt.hb = ops[i].op.kind == SK_TRI ? ops[i].op.nseg : ops[i].op.b;
+                    }
                 }
                 meta.push_back(mt);
             }
@@ -1254,8 +1274,8 @@ private:
         d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
         fwd_waves_.clear();
         bwd_waves_.clear();
-        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem});
-        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem});
+        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
         nin_ = (int)src.size();
         nout_ = (int)dst.size();
         // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
@@ -1298,6 +1318,10 @@ public:
             out.push_back(ms);
             out.push_back(all[i]->nops);
             out.push_back(all[i]->smem);
+            out.push_back(all[i]->words);
+            out.push_back(all[i]->hkind);
+            out.push_back(all[i]->ha);
+            out.push_back(all[i]->hb);
         }
         for (auto e : ev) cudaEventDestroy(e);
         return out;

@@ -187,14 +187,19 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
             s_tau[j] = tau;
         }
         // d[c] = P[j, c] + sum_{r > j} v_j[r] P[r, c] for every panel column c != j
+        // (loads issued unconditionally from columns clamped to the panel, so
+        // that a row's kNB loads are in flight together; masked by selects)
+        const int wl = w - 1;
         T acc[kNB];
 #pragma unroll
         for (int c = 0; c < kNB; ++c) acc[c] = T(0);
         for (int r = j + 1 + tid; r < R; r += blockDim.x) {
             const T vr = pj[r];
+            T pv[kNB];
 #pragma unroll
-            for (int c = 0; c < kNB; ++c)
-                if (c < w && c != j) acc[c] += vr * P[r + (size_t)c * ldp];
+            for (int c = 0; c < kNB; ++c) pv[c] = P[r + (size_t)min(c, wl) * ldp];
+#pragma unroll
+            for (int c = 0; c < kNB; ++c) acc[c] += (c < w && c != j) ? vr * pv[c] : T(0);
         }
 #pragma unroll
         for (int c = 0; c < kNB; ++c) {
@@ -212,9 +217,12 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
         if (tau != T(0)) {
             for (int r = j + 1 + tid; r < R; r += blockDim.x) {
                 const T vr = pj[r];
+                T pv[kNB];
+#pragma unroll
+                for (int c = 0; c < kNB; ++c) pv[c] = P[r + (size_t)min(c, wl) * ldp];
 #pragma unroll
                 for (int c = 0; c < kNB; ++c)
-                    if (c > j && c < w) P[r + (size_t)c * ldp] -= (tau * dots[c]) * vr;
+                    if (c > j && c < w) P[r + (size_t)c * ldp] = pv[c] - (tau * dots[c]) * vr;
             }
             if (tid > j && tid < w) P[j + (size_t)tid * ldp] -= tau * dots[tid];
         }
@@ -411,90 +419,221 @@ __device__ __forceinline__ const T* aptr(int64_t v) {
     return reinterpret_cast<const T*>(v);
 }
 
-// x(0:m) <- Q^T x (dir 0) or Q x (dir 1), Q from unit-lower V (ld ldv), T panels.
+// Warp transpose-sum: lane q returns sum over the 32 lanes of a[q] (31
+// shuffles, recursive halving of the index range).
 template <class T>
-__device__ void apply_q(T* xs, int m, int kq, const T* V, int ldv, const T* tp, int dir, T* red_y, T* red_z) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+__device__ __forceinline__ T warp_transpose_sum(T (&a)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int q = 0; q < s; ++q) {
+            const T send = upper ? a[q] : a[q + s];
+            const T keep = upper ? a[q + s] : a[q];
+            a[q] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    return a[0];
+}
+
+// Scratch of the solve-step CTA (static shared memory).
+template <class T>
+struct SolveShared {
+    T wred[(kThreads / 32) * kNB];  // per-warp partials
+    T y[kNB], z[kNB];
+    T tsh[kNB * (kNB + 1)];         // panel T factor / diagonal block of R
+};
+
+// x(0:m) <- Q^T x (dir 0) or Q x (dir 1), Q from unit-lower V (ld ldv) with
+// one kNB x kNB T factor per panel (H_panel = I - V T V^T). Per panel, each
+// thread walks its rows once for the kNB products V^T x and once for the
+// update x -= V z. Every row issues its kNB loads unconditionally (columns
+// past the panel's width are clamped to its last column and weighted by zero)
+// so that they are all in flight together.
+template <class T>
+__device__ void apply_q(T* xs, int m, int kq, const T* V, int ldv, const T* tp, int dir, SolveShared<T>& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5, nth = blockDim.x;
+    constexpr int TP = kNB + 1;
     const int np = (kq + kNB - 1) / kNB;
     for (int pi = 0; pi < np; ++pi) {
         const int pidx = dir == 0 ? pi : np - 1 - pi;
         const int p0 = pidx * kNB;
         const int w = min(kNB, kq - p0);
-        for (int q = warp; q < w; q += nw) {
-            const int col = p0 + q;
-            const T* vc = V + (size_t)col * ldv;
-            T s = T(0);
-            for (int r = col + 1 + lane; r < m; r += 32) s += vc[r] * xs[r];
-            s = warp_sum(s);
-            if (lane == 0) red_y[q] = s + (col < m ? xs[col] : T(0));
-        }
-        __syncthreads();
+        const int wl = w - 1;
+        const T* Vp = V + (size_t)p0 * ldv;
         const T* Tp = tp + (size_t)pidx * kNB * kNB;
-        if (tid < w) {
-            T s = T(0);
-            if (dir == 0) {
-                for (int l = 0; l <= tid; ++l) s += Tp[l + tid * kNB] * red_y[l];  // T^T y
-            } else {
-                for (int l = tid; l < w; ++l) s += Tp[tid + l * kNB] * red_y[l];  // T y
+        for (int e = tid; e < kNB * kNB; e += nth) sh.tsh[(e % kNB) * TP + e / kNB] = Tp[e];
+        T acc[kNB];
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) acc[q] = T(0);
+        for (int r = p0 + tid; r < m; r += nth) {
+            const T xr = xs[r];
+            const int rr = r - p0;
+            const T* vr = Vp + r;
+            T v[kNB];
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) v[q] = vr[(size_t)min(q, wl) * ldv];
+            if (rr < kNB) {  // unit diagonal, zeros above it
+#pragma unroll
+                for (int q = 0; q < kNB; ++q) v[q] = q < rr ? v[q] : (q == rr ? T(1) : T(0));
             }
-            red_z[tid] = s;
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) acc[q] += v[q] * xr;
+        }
+        const T part = warp_transpose_sum(acc);
+        sh.wred[warp * kNB + lane] = part;
+        __syncthreads();
+        if (tid < kNB) {
+            T y = T(0);
+            for (int q = 0; q < nw; ++q) y += sh.wred[q * kNB + tid];
+            sh.y[tid] = y;
         }
         __syncthreads();
-        for (int r = p0 + tid; r < m; r += blockDim.x) {
+        if (tid < kNB) {  // z = T^T y (dir 0) or T y (dir 1); T upper triangular; z = 0 past w
             T s = T(0);
-            const int qmax = min(w - 1, r - p0);
-            for (int q = 0; q <= qmax; ++q) {
-                const int col = p0 + q;
-                s += (r == col ? T(1) : V[r + (size_t)col * ldv]) * red_z[q];
+            if (tid < w) {
+                if (dir == 0) {
+                    for (int l = 0; l <= tid; ++l) s += sh.tsh[l * TP + tid] * sh.y[l];
+                } else {
+                    for (int l = tid; l < w; ++l) s += sh.tsh[tid * TP + l] * sh.y[l];
+                }
             }
+            sh.z[tid] = s;
+        }
+        __syncthreads();
+        for (int r = p0 + tid; r < m; r += nth) {
+            const int rr = r - p0;
+            const T* vr = Vp + r;
+            T v[kNB];
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) v[q] = vr[(size_t)min(q, wl) * ldv];
+            if (rr < kNB) {
+#pragma unroll
+                for (int q = 0; q < kNB; ++q) v[q] = q < rr ? v[q] : (q == rr ? T(1) : T(0));
+            }
+            T s = T(0);
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) s += v[q] * sh.z[q];
             xs[r] -= s;
         }
         __syncthreads();
     }
 }
 
-// Upper-triangular solve in shared memory: x <- inv(R) x (trans 0) or inv(R^T) x (trans 1).
+// Upper-triangular solve in shared memory: x <- inv(R) x (trans 0) or
+// inv(R^T) x (trans 1), in 32-row blocks. Warp 0 holds the diagonal block in
+// registers (lane l: row l for trans 0, column l for trans 1) and solves it
+// with shuffles; all threads then update the remaining rows, each issuing its
+// 32 loads unconditionally (clamped to the block, weighted by zero past it).
 template <class T>
-__device__ void tri_solve(T* xs, int k, const T* R, int ldr, int trans) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (trans == 0) {
-        const int nb = (k + 31) / 32;
-        for (int b = nb - 1; b >= 0; --b) {
-            const int j0 = b * 32, bw = min(32, k - j0);
-            if (warp == 0) {
-                T xv = lane < bw ? xs[j0 + lane] : T(0);
-                for (int i = bw - 1; i >= 0; --i) {
-                    if (lane == i) xv = xv / R[(j0 + i) + (size_t)(j0 + i) * ldr];
-                    T xi = __shfl_sync(0xffffffffu, xv, i);
-                    if (lane < i) xv -= R[(j0 + lane) + (size_t)(j0 + i) * ldr] * xi;
-                }
-                if (lane < bw) xs[j0 + lane] = xv;
+__device__ void tri_solve(T* xs, int k, const T* R, int ldr, int trans, SolveShared<T>& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nth = blockDim.x;
+    const int nb = (k + 31) / 32;
+    for (int bi = 0; bi < nb; ++bi) {
+        const int b = trans == 0 ? nb - 1 - bi : bi;
+        const int j0 = b * 32, bw = min(32, k - j0);
+        const int bl = bw - 1;
+        if (warp == 0) {
+            T rd[32];
+            const int ll = min(lane, bl);
+            if (trans == 0) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) rd[i] = R[(j0 + ll) + (size_t)(j0 + min(i, bl)) * ldr];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) rd[i] = R[(j0 + min(i, bl)) + (size_t)(j0 + ll) * ldr];
             }
-            __syncthreads();
-            for (int i = tid; i < j0; i += blockDim.x) {
+            T xv = lane < bw ? xs[j0 + lane] : T(0);
+            if (trans == 0) {
+#pragma unroll
+                for (int i = 31; i >= 0; --i) {
+                    if (i < bw) {
+                        if (lane == i) xv = xv / rd[i];
+                        const T xi = __shfl_sync(0xffffffffu, xv, i);
+                        if (lane < i) xv -= rd[i] * xi;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    if (i < bw) {
+                        if (lane == i) xv = xv / rd[i];
+                        const T xi = __shfl_sync(0xffffffffu, xv, i);
+                        if (lane > i) xv -= rd[i] * xi;
+                    }
+                }
+            }
+            if (lane < bw) xs[j0 + lane] = xv;
+            sh.y[lane] = lane < bw ? xv : T(0);
+        }
+        __syncthreads();
+        if (trans == 0) {
+            for (int i = tid; i < j0; i += nth) {
+                T rv[32];
+#pragma unroll
+                for (int l = 0; l < 32; ++l) rv[l] = R[i + (size_t)(j0 + min(l, bl)) * ldr];
                 T s = T(0);
-                for (int l = 0; l < bw; ++l) s += R[i + (size_t)(j0 + l) * ldr] * xs[j0 + l];
+#pragma unroll
+                for (int l = 0; l < 32; ++l) s += rv[l] * sh.y[l];
                 xs[i] -= s;
             }
-            __syncthreads();
-        }
-    } else {
-        const int nb = (k + 31) / 32;
-        for (int b = 0; b < nb; ++b) {
-            const int j0 = b * 32, bw = min(32, k - j0);
-            if (warp == 0) {
-                T xv = lane < bw ? xs[j0 + lane] : T(0);
-                for (int i = 0; i < bw; ++i) {
-                    if (lane == i) xv = xv / R[(j0 + i) + (size_t)(j0 + i) * ldr];
-                    T xi = __shfl_sync(0xffffffffu, xv, i);
-                    if (lane > i && lane < bw) xv -= R[(j0 + i) + (size_t)(j0 + lane) * ldr] * xi;
-                }
-                if (lane < bw) xs[j0 + lane] = xv;
-            }
-            __syncthreads();
-            for (int i = j0 + bw + tid; i < k; i += blockDim.x) {
+        } else {
+            for (int i = j0 + bw + tid; i < k; i += nth) {
+                T rv[32];
+#pragma unroll
+                for (int l = 0; l < 32; ++l) rv[l] = R[(j0 + min(l, bl)) + (size_t)i * ldr];
                 T s = T(0);
-                for (int l = 0; l < bw; ++l) s += R[(j0 + l) + (size_t)i * ldr] * xs[j0 + l];
+#pragma unroll
+                for (int l = 0; l < 32; ++l) s += rv[l] * sh.y[l];
+                xs[i] -= s;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// xs(0:k) -= sum_b B_b x_b over the neighbour blocks of a triangular op (B_b:
+// k x s_b, ld). Threads form G column groups of RT row threads; each thread
+// keeps eight loads in flight and the groups meet in shared memory.
+template <class T>
+__device__ void gemv_sub(T* xs, int k, const GemvRef<T>* gv, int nb, const T* x, SolveShared<T>& sh) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int RT = min(nth, (k + 31) & ~31);
+    const int G = nth / RT;
+    const int ri = tid % RT, g = tid / RT;
+    for (int i0 = 0; i0 < k; i0 += RT) {
+        const int i = i0 + ri;
+        T a[4] = {T(0), T(0), T(0), T(0)};
+        if (g < G && i < k) {
+            for (int bb = 0; bb < nb; ++bb) {
+                const GemvRef<T> r = gv[bb];
+                const T* B = aptr<T>(r.boff) + i;
+                const T* xn = x + r.xoff;
+                const size_t ld = (size_t)r.ld;
+                int j = g;
+                for (; j + 7 * G < r.s; j += 8 * G) {
+                    T bv[8], xv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        bv[u] = B[(size_t)(j + u * G) * ld];
+                        xv[u] = xn[j + u * G];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) a[u & 3] += bv[u] * xv[u];
+                }
+                for (; j < r.s; j += G) a[0] += B[(size_t)j * ld] * xn[j];
+            }
+        }
+        const T part = (a[0] + a[1]) + (a[2] + a[3]);
+        if (G == 1) {
+            if (i < k) xs[i] -= part;
+        } else {
+            sh.wred[tid] = part;
+            __syncthreads();
+            if (g == 0 && i < k) {
+                T s = T(0);
+                for (int q = 0; q < G; ++q) s += sh.wred[q * RT + ri];
                 xs[i] -= s;
             }
             __syncthreads();
@@ -507,8 +646,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
                                                         const GemvRef<T>* gemv, T* x) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* xs = reinterpret_cast<T*>(smem_raw);
-    __shared__ T red_y[kNB];
-    __shared__ T red_z[kNB];
+    __shared__ SolveShared<T> sh;
     const SolveOp op = ops[blockIdx.x];
     const int tid = threadIdx.x;
     switch (op.kind) {
@@ -525,7 +663,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
                 for (int i = tid; i < m; i += blockDim.x) xs[i] = x[op.x0 + i];
             }
             __syncthreads();
-            apply_q(xs, m, kq, aptr<T>(op.p0), ldv, aptr<T>(op.p1), op.dir, red_y, red_z);
+            apply_q(xs, m, kq, aptr<T>(op.p0), ldv, aptr<T>(op.p1), op.dir, sh);
             if (op.nseg > 0) {
                 int cur = 0;
                 for (int s = 0; s < op.nseg; ++s) {
@@ -544,20 +682,12 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
             for (int i = tid; i < k; i += blockDim.x) xs[i] = x[op.x0 + i];
             __syncthreads();
             if (op.dir == 0) {
-                for (int b = 0; b < op.nseg; ++b) {
-                    const GemvRef<T> g = gemv[op.seg0 + b];
-                    const T* B = aptr<T>(g.boff);
-                    for (int i = tid; i < k; i += blockDim.x) {
-                        T s = T(0);
-                        for (int j = 0; j < g.s; ++j) s += B[i + (size_t)j * g.ld] * x[g.xoff + j];
-                        xs[i] -= s;
-                    }
-                }
+                gemv_sub(xs, k, gemv + op.seg0, op.nseg, x, sh);
                 __syncthreads();
-                tri_solve(xs, k, R, ldr, 0);
+                tri_solve(xs, k, R, ldr, 0, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
             } else {
-                tri_solve(xs, k, R, ldr, 1);
+                tri_solve(xs, k, R, ldr, 1, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
                 for (int b = 0; b < op.nseg; ++b) {
                     const GemvRef<T> g = gemv[op.seg0 + b];
@@ -565,6 +695,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
                     const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
                     for (int j = warp; j < g.s; j += nw) {
                         T s = T(0);
+#pragma unroll 4
                         for (int i = lane; i < k; i += 32) s += B[i + (size_t)j * g.ld] * xs[i];
                         s = warp_sum(s);
                         if (lane == 0) x[g.xoff + j] -= s;
