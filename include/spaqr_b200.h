@@ -165,6 +165,14 @@ int spq_get_stats(spq_tree* t, double* times, long long* counters);
 /* Per-level factorization phase times in ms (6 per level: fill, elmn, shift,
  * scale, sprsfy, merge), as printed by src/tree.cpp:1417-1426. */
 int spq_get_level_times(spq_tree* t, double* out);
+/* Host side of the last factorize in seconds: out5 = [wall time, waits for the
+ * per-wave rank readbacks, device allocations of the arenas, scratch growth,
+ * solve-plan build]. */
+int spq_get_host_times(spq_tree* t, double* out5);
+/* Device memory of destroyed handles stays cached in a per-device pool for the
+ * next handle (no allocation cost on refactorization); this returns the
+ * cached, unused part to the device. */
+int spq_trim_memory(void);
 
 /* A <- A * diag(1/||A_j||) * 10, in place on val (spaQR.cpp:131-147). */
 int spq_column_normalize(int m, int n, const int* colptr, const int* rowind, double* val);

@@ -61,6 +61,8 @@ SIGNATURES = {
     "spq_get_bottom": (_i, [_p, _ip]),
     "spq_get_stats": (_i, [_p, _dp, _llp]),
     "spq_get_level_times": (_i, [_p, _dp]),
+    "spq_get_host_times": (_i, [_p, _dp]),
+    "spq_trim_memory": (_i, []),
     "spq_column_normalize": (_i, [_i, _i, _ip, _ip, _dp]),
     "spq_solve_to_residual": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _d, _d, _i, _i, _ip, _dp]),
     "spq_solve_to_residual_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _d, _d, _i, _i, _ip, _dp]),

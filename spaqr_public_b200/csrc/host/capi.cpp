@@ -514,6 +514,19 @@ int spq_get_stats(spq_tree* t, double* times, long long* counters) {
     t->eng->stats(times, counters);
     return SPQ_OK;
 }
+int spq_trim_memory(void) {
+    return guard([&] {
+        trim_device_pools();
+        return SPQ_OK;
+    });
+}
+int spq_get_host_times(spq_tree* t, double* out5) {
+    if (!t || !out5) return fail(SPQ_ERR_ARG, "null argument");
+    if (!t->eng || t->state < 3) return fail(SPQ_ERR_STATE, "not factorized");
+    auto v = t->eng->host_times();
+    std::memcpy(out5, v.data(), sizeof(double) * 5);
+    return SPQ_OK;
+}
 int spq_get_level_times(spq_tree* t, double* out) {
     if (!t || !out) return fail(SPQ_ERR_ARG, "null argument");
     if (!t->eng || t->state < 3) return fail(SPQ_ERR_STATE, "not factorized");

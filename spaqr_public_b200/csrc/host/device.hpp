@@ -4,8 +4,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -20,6 +23,50 @@ inline void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+inline double wall_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Process-wide stream-ordered memory pool of one device, shared by every
+// handle on it. Freed memory stays in the pool (unlimited release threshold),
+// so a later factorization is served without new device allocations and a
+// growing scratch buffer needs no stream synchronisation. trim_device_pools()
+// returns the cached memory to the device.
+inline std::mutex& pool_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+inline std::map<int, cudaMemPool_t>& pool_table() {
+    static std::map<int, cudaMemPool_t> pools;
+    return pools;
+}
+inline cudaMemPool_t device_pool(int dev) {
+    std::lock_guard<std::mutex> g(pool_mutex());
+    auto& pools = pool_table();
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    cuda_check(cudaMemPoolCreate(&p, &props), "cudaMemPoolCreate");
+    uint64_t thr = UINT64_MAX;
+    cuda_check(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr), "pool release threshold");
+    pools[dev] = p;
+    return p;
+}
+inline void trim_device_pools() {
+    std::lock_guard<std::mutex> g(pool_mutex());
+    for (auto& kv : pool_table()) cudaMemPoolTrimTo(kv.second, 0);
+}
+inline void* pool_alloc(cudaMemPool_t pool, size_t bytes, cudaStream_t s, const char* what) {
+    void* p = nullptr;
+    cuda_check(cudaMallocFromPoolAsync(&p, bytes, pool, s), what);
+    return p;
+}
+
 // Chunked bump allocator. Every chunk is zeroed when it is allocated and memory
 // is never reused, so a fresh allocation always reads as zeros (the reference
 // allocates fill-in and merged blocks with setZero).
@@ -30,19 +77,23 @@ public:
     Arena(const Arena&) = delete;
     Arena& operator=(const Arena&) = delete;
 
-    void set_stream(cudaStream_t s) { stream_ = s; }
+    void set_stream(cudaStream_t s, cudaMemPool_t pool) {
+        stream_ = s;
+        pool_ = pool;
+    }
     void* alloc(size_t bytes) {
         bytes = (bytes + 127) & ~size_t(127);
         if (bytes == 0) bytes = 128;
         if (chunks_.empty() || used_ + bytes > cap_) {
+            const double t0 = wall_seconds();
             size_t sz = bytes > chunk_ ? bytes : chunk_;
-            void* p = nullptr;
-            cuda_check(cudaMalloc(&p, sz), "arena cudaMalloc");
+            void* p = pool_alloc(pool_, sz, stream_, "arena allocation");
             cuda_check(cudaMemsetAsync(p, 0, sz, stream_), "arena memset");
             chunks_.push_back(p);
             cap_ = sz;
             used_ = 0;
             total_ += sz;
+            alloc_seconds_ += wall_seconds() - t0;
         }
         char* p = static_cast<char*>(chunks_.back()) + used_;
         used_ += bytes;
@@ -53,8 +104,11 @@ public:
         return static_cast<U*>(alloc(n * sizeof(U)));
     }
     size_t bytes_reserved() const { return total_; }
+    double alloc_seconds() const { return alloc_seconds_; }
+    // Returns the chunks to the pool in stream order (call before the stream
+    // is destroyed).
     void release() {
-        for (void* p : chunks_) cudaFree(p);
+        for (void* p : chunks_) cudaFreeAsync(p, stream_);
         chunks_.clear();
         cap_ = used_ = total_ = 0;
     }
@@ -62,33 +116,82 @@ public:
 private:
     size_t chunk_;
     cudaStream_t stream_ = nullptr;
+    cudaMemPool_t pool_ = nullptr;
     std::vector<void*> chunks_;
     size_t cap_ = 0, used_ = 0, total_ = 0;
+    double alloc_seconds_ = 0;
 };
 
-// Reusable device scratch. grow() waits for the stream before replacing the
-// buffer, so work queued on the old buffer is finished.
+// Reusable device scratch on one stream. Growing frees the old buffer and
+// allocates the new one in stream order, so work already queued on the old
+// buffer finishes first without a host wait.
 class Scratch {
 public:
-    ~Scratch() {
-        if (p_) cudaFree(p_);
-    }
+    void set_pool(cudaMemPool_t pool) { pool_ = pool; }
     void* get(size_t bytes, cudaStream_t s) {
         if (bytes > cap_) {
-            cuda_check(cudaStreamSynchronize(s), "scratch sync");
-            if (p_) cudaFree(p_);
+            const double t0 = wall_seconds();
+            if (p_) cudaFreeAsync(p_, s);
             p_ = nullptr;
-            size_t nc = bytes + bytes / 4 + (size_t(1) << 20);
-            cuda_check(cudaMalloc(&p_, nc), "scratch cudaMalloc");
+            cap_ = 0;
+            const size_t nc = bytes + bytes / 4 + (size_t(1) << 20);
+            p_ = pool_alloc(pool_, nc, s, "scratch allocation");
             cap_ = nc;
+            grow_seconds_ += wall_seconds() - t0;
         }
         return p_;
     }
+    void release(cudaStream_t s) {
+        if (p_) cudaFreeAsync(p_, s);
+        p_ = nullptr;
+        cap_ = 0;
+    }
     size_t capacity() const { return cap_; }
+    double grow_seconds() const { return grow_seconds_; }
 
 private:
+    cudaMemPool_t pool_ = nullptr;
     void* p_ = nullptr;
     size_t cap_ = 0;
+    double grow_seconds_ = 0;
+};
+
+// Pinned host staging for descriptor uploads. A cudaMemcpyAsync from pageable
+// memory may wait for the stream before staging the bytes; from pinned memory
+// it returns at once, so the host builds the next wave while the device runs
+// the current one. Bump allocation in pinned chunks; reset() is legal only
+// when the stream has drained every copy issued from the stage.
+class PinnedStage {
+public:
+    ~PinnedStage() {
+        for (auto& c : chunks_) cudaFreeHost(c.first);
+    }
+    char* get(size_t bytes) {
+        bytes = (bytes + 15) & ~size_t(15);
+        while (ci_ < chunks_.size() && used_ + bytes > chunks_[ci_].second) {
+            ++ci_;
+            used_ = 0;
+        }
+        if (ci_ == chunks_.size()) {
+            const size_t sz = bytes > kChunk ? bytes : kChunk;
+            void* p = nullptr;
+            cuda_check(cudaHostAlloc(&p, sz, cudaHostAllocDefault), "pinned staging");
+            chunks_.emplace_back(static_cast<char*>(p), sz);
+            used_ = 0;
+        }
+        char* p = chunks_[ci_].first + used_;
+        used_ += bytes;
+        return p;
+    }
+    void reset() {
+        ci_ = 0;
+        used_ = 0;
+    }
+
+private:
+    static constexpr size_t kChunk = size_t(8) << 20;
+    std::vector<std::pair<char*, size_t>> chunks_;
+    size_t ci_ = 0, used_ = 0;
 };
 
 // Host staging of one batch of heterogeneous descriptor arrays, uploaded with
@@ -102,12 +205,14 @@ public:
         if (!v.empty()) std::memcpy(buf_.data() + off, v.data(), v.size() * sizeof(U));
         return off;
     }
-    // Returns the device base; element arrays are at base + offset.
-    char* commit(Arena& arena, cudaStream_t s) {
+    // Returns the device base; element arrays are at base + offset. The bytes
+    // go through the pinned stage, so the copy does not wait for the stream.
+    char* commit(Arena& arena, cudaStream_t s, PinnedStage& stage) {
         if (buf_.empty()) return nullptr;
         char* d = static_cast<char*>(arena.alloc(buf_.size()));
-        cuda_check(cudaMemcpyAsync(d, buf_.data(), buf_.size(), cudaMemcpyHostToDevice, s), "descriptor upload");
-        // pageable source: the copy is staged before return, buf_ may be reused
+        char* h = stage.get(buf_.size());
+        std::memcpy(h, buf_.data(), buf_.size());
+        cuda_check(cudaMemcpyAsync(d, h, buf_.size(), cudaMemcpyHostToDevice, s), "descriptor upload");
         return d;
     }
     void clear() { buf_.clear(); }

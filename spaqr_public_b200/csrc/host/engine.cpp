@@ -100,14 +100,18 @@ public:
         cudaStreamSynchronize(stream_);
         arena_.release();
         desc_arena_.release();
+        scratch_.release(stream_);
+        cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
     }
     void open_device() {
         if (stream_) return;
         cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-        arena_.set_stream(stream_);
-        desc_arena_.set_stream(stream_);
+        cudaMemPool_t pool = device_pool(cfg_.device);
+        arena_.set_stream(stream_, pool);
+        desc_arena_.set_stream(stream_, pool);
+        scratch_.set_pool(pool);
         prepare_kernels<T>();
     }
 
@@ -230,6 +234,9 @@ public:
         if (!cfg_.scale && cfg_.tol != 0) throw std::invalid_argument("--scale 0 is not supported by this build");
         double t0 = wall();
         launches_fact_ = 0;
+        t_rank_wait_ = 0;
+        alloc0_ = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
+        grow0_ = scratch_.grow_seconds();
         const int L = cfg_.nlevels;
         level_ev_.assign((size_t)L * 7, nullptr);
         for (auto& e : level_ev_) {
@@ -257,8 +264,11 @@ public:
             if (cfg_.verbose) print_level(ev, ts);
         }
         rec(6, (long long)nnzA_, (long long)nnzR_, (long long)nnzH_, (long long)nnzQ_);
+        const double tp0 = wall();
         build_solve_plan();
+        t_plan_ = wall() - tp0;
         cuda_check(cudaStreamSynchronize(stream_), "factorize");
+        pinned_.reset();
         factorized_ = true;
         t_fact_ = wall() - t0;
         if (cfg_.verbose) {
@@ -309,6 +319,10 @@ public:
         counters[6] = (long long)(arena_.bytes_reserved() + desc_arena_.bytes_reserved() + scratch_.capacity());
         counters[7] = applications_;
     }
+    std::vector<double> host_times() const override {
+        return {t_fact_, t_rank_wait_, arena_.alloc_seconds() + desc_arena_.alloc_seconds() - alloc0_,
+                scratch_.grow_seconds() - grow0_, t_plan_};
+    }
     std::vector<double> level_times() const override {
         std::vector<double> out;
         for (size_t l = 0; l + 7 <= level_ev_.size(); l += 7) {
@@ -327,6 +341,8 @@ private:
     Arena arena_;
     Arena desc_arena_{size_t(16) << 20};
     Scratch scratch_;
+    PinnedStage pinned_;
+    double t_rank_wait_ = 0, t_plan_ = 0, alloc0_ = 0, grow0_ = 0;
     std::vector<std::vector<Cluster*>> bottoms_, fine_;
     std::vector<std::unique_ptr<Cluster>> clusters_;
     std::vector<std::unique_ptr<Edge>> edges_;
@@ -565,7 +581,7 @@ private:
             o_ids.push_back(up.add(ids[i]));
             o_tiles.push_back(up.add(tiles[i]));
         }
-        char* d = up.commit(desc_arena_, stream_);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
         const int smem_limit = (int)((160 * 1024) / (kNB * sizeof(T)));
         for (size_t i = 0; i < ids.size(); ++i) {
@@ -904,7 +920,7 @@ private:
         size_t o_g = up.add(g), o_r = up.add(rt);
         std::map<int, size_t> o_ids;
         for (auto& kv : groups) o_ids[kv.first] = up.add(kv.second);
-        char* d = up.commit(desc_arena_, stream_);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
         std::vector<size_t> rqs;
         for (auto& kv : groups) {
@@ -931,7 +947,10 @@ private:
         std::vector<int> ranks(jobs.size());
         cuda_check(cudaMemcpyAsync(ranks.data(), ib, sizeof(int) * jobs.size(), cudaMemcpyDeviceToHost, stream_),
                    "rank");
+        const double tw0 = wall();
         cuda_check(cudaStreamSynchronize(stream_), "rank readback");
+        t_rank_wait_ += wall() - tw0;
+        pinned_.reset();  // every staged upload before the readback has landed
         size_t gi = 0;
         for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
             const size_t rq = rqs[gi++];
@@ -1011,7 +1030,7 @@ private:
         if (!wb.empty()) {
             Upload u2;
             size_t o_w = u2.add(wb), o_b = u2.add(blocks);
-            char* d2 = u2.commit(desc_arena_, stream_);
+            char* d2 = u2.commit(desc_arena_, stream_, pinned_);
             timed(KF_SPARS_WB, 0, wb_bytes, [&] {
                 launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
                                       reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
@@ -1068,7 +1087,7 @@ private:
         if (!copies.empty()) {
             Upload up;
             size_t o = up.add(copies);
-            char* d = up.commit(desc_arena_, stream_);
+            char* d = up.commit(desc_arena_, stream_, pinned_);
             issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
         }
     }
@@ -1264,7 +1283,7 @@ private:
         Upload up;
         size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
                o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
-        char* d = up.commit(desc_arena_, stream_);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
         const SolveOp* d_ops = reinterpret_cast<const SolveOp*>(d + o_ops);
         d_segs_ = reinterpret_cast<const XSeg*>(d + o_segs);
         d_gemv_ = reinterpret_cast<const GemvRef<T>*>(d + o_gemv);

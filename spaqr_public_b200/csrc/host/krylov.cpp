@@ -17,15 +17,22 @@
 namespace spq {
 namespace {
 
+// Device vector from the device's retained memory pool, allocated and freed
+// in the order of the handle's stream.
 struct DevVec {
     double* p = nullptr;
     bool owned = false;
+    cudaStream_t s = nullptr;
     ~DevVec() {
-        if (p && owned) cudaFree(p);
+        if (p && owned) cudaFreeAsync(p, s);
     }
-    void alloc(size_t n) {
-        if (p && owned) cudaFree(p);
-        cuda_check(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)), "krylov cudaMalloc");
+    void alloc(size_t n, cudaStream_t st) {
+        if (p && owned) cudaFreeAsync(p, s);
+        s = st;
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        p = static_cast<double*>(
+            pool_alloc(device_pool(dev), std::max<size_t>(n, 1) * sizeof(double), st, "krylov allocation"));
         owned = true;
     }
     // Points at caller-provided device memory (never freed here).
@@ -66,14 +73,14 @@ public:
     Gmres(EngineBase& P, const DevCsr& A, int restart) : P_(P), A_(A), m_(A.m), restart_(restart) {
         s_ = P.stream();
         nblk_ = reduce_blocks();
-        p0_.alloc(m_);
-        r0_.alloc(m_);
-        t_.alloc(m_);
-        v_.alloc(m_);
-        xnew_.alloc(m_);
-        part_.alloc(nblk_ + 1);
-        scal_.alloc(2 * (restart + 1) + 4);
-        H_.alloc((size_t)m_ * (restart + 1));
+        p0_.alloc(m_, s_);
+        r0_.alloc(m_, s_);
+        t_.alloc(m_, s_);
+        v_.alloc(m_, s_);
+        xnew_.alloc(m_, s_);
+        part_.alloc(nblk_ + 1, s_);
+        scal_.alloc(2 * (restart + 1) + 4, s_);
+        H_.alloc((size_t)m_ * (restart + 1), s_);
         hpart_.resize(nblk_);
     }
     // Same driver on a caller-provided workspace of workspace_elems(m, restart)
@@ -264,8 +271,8 @@ int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x
                   int max_outer, int iters, double* true_res, int* outer, long long* launches) {
     cudaStream_t s = P.stream();
     DevVec r, d;
-    r.alloc(A.m);
-    d.alloc(A.n);
+    r.alloc(A.m, s);
+    d.alloc(A.n, s);
     int total = 0, k = 0;
     long long l = 0;
     double rel = residual_norm(s, A, d_b, d_x);
@@ -291,9 +298,9 @@ int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x
 
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x) {
     DevVec t, part;
-    t.alloc(A.m);
+    t.alloc(A.m, s);
     const int nblk = reduce_blocks();
-    part.alloc(nblk);
+    part.alloc(nblk, s);
     std::vector<double> h(nblk);
     auto sum = [&]() {
         cuda_check(cudaMemcpyAsync(h.data(), part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, s), "res");

@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
         //    kU vectors per lane at once; the rows below k are cut into Gs chunks
         //    handled by different warps, whose dot partials meet in shared memory.
         constexpr int VEC = Vec<T>::n;
+        constexpr int kRowUnroll = sizeof(T) == 4 ? 4 : 2;  // rows in flight per lane (registers)
         using VT = typename Vec<T>::type;
         const int Wc = j1 - j0;
         const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);  // 32-vector tiles in the slab
@@ -281,6 +282,9 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
             for (int item = warp; item < Gs * ntg; item += nw) {
                 const int g = item % Gs, tg = item / Gs;
                 const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
+                // vectors past the slab read its first vector instead (loads stay
+                // unconditional, so all of a row's loads are in flight together);
+                // their sums land in the unused tail of the partials
                 T s[kU][VEC];
                 const T* cp[kU];
 #pragma unroll
@@ -288,16 +292,17 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
 #pragma unroll
                     for (int q = 0; q < VEC; ++q) s[u][q] = T(0);
                     const int jl = ((tg * kU + u) * 32 + lane) * VEC;
-                    cp[u] = jl < Wc ? C + (j0 + jl) : nullptr;
+                    cp[u] = C + j0 + (jl < Wc ? jl : 0);
                 }
-#pragma unroll 2
+#pragma unroll kRowUnroll
                 for (int i = i0; i < i1; ++i) {
                     const T vi = vsh[i];
+                    VT x[kU];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) x[u] = *reinterpret_cast<const VT*>(cp[u] + i * ld);
 #pragma unroll
                     for (int u = 0; u < kU; ++u) {
-                        if (!cp[u]) continue;
-                        const VT x = *reinterpret_cast<const VT*>(cp[u] + i * ld);
-                        const T* xs = reinterpret_cast<const T*>(&x);
+                        const T* xs = reinterpret_cast<const T*>(&x[u]);
 #pragma unroll
                         for (int q = 0; q < VEC; ++q) s[u][q] += vi * xs[q];
                     }
@@ -332,6 +337,7 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
                 const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
                 T sc[kU][VEC];
                 T* cp[kU];
+                bool st[kU];  // vector inside the slab with a nonzero scale: store it
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     const int jl = ((tg * kU + u) * 32 + lane) * VEC;
@@ -341,20 +347,21 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
                         sc[u][q] = jl < Wc ? svec[jl + q] : T(0);
                         any = any || sc[u][q] != T(0);
                     }
-                    cp[u] = (jl < Wc && any) ? C + (j0 + jl) : nullptr;
+                    st[u] = jl < Wc && any;
+                    cp[u] = C + j0 + (jl < Wc ? jl : 0);
                 }
-#pragma unroll 2
+#pragma unroll kRowUnroll
                 for (int i = i0; i < i1; ++i) {
                     const T vi = vsh[i];
+                    VT x[kU];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) x[u] = *reinterpret_cast<const VT*>(cp[u] + i * ld);
 #pragma unroll
                     for (int u = 0; u < kU; ++u) {
-                        if (!cp[u]) continue;
-                        VT* px = reinterpret_cast<VT*>(cp[u] + i * ld);
-                        VT x = *px;
-                        T* xs = reinterpret_cast<T*>(&x);
+                        T* xs = reinterpret_cast<T*>(&x[u]);
 #pragma unroll
                         for (int q = 0; q < VEC; ++q) xs[q] -= sc[u][q] * vi;
-                        *px = x;
+                        if (st[u]) *reinterpret_cast<VT*>(cp[u] + i * ld) = x[u];
                     }
                 }
             }
