@@ -390,6 +390,21 @@ def run_ours(args):
         d.destroy_process_group()
 
 
+def run_single(args):
+    """One FP32-form step (setup untimed) of the named workload and nothing else:
+    the command the kernel profiler wraps (launch list and kernel captures)."""
+    import torch
+    from spaqr_public_b200 import matgen
+    torch.cuda.set_device(0)
+    w = matgen.workload(args.workload)
+    A = matgen.column_normalize(w["A"])
+    csr = device_csr(A)
+    d_b = torch.tensor(w["b"], dtype=torch.float64, device="cuda")
+    sec, info = timed_step(w, A, csr, d_b, 1, 0)
+    print(json.dumps({"workload": args.workload, "seconds": sec, "gmres_its": info["its"], "residual": info["res"],
+                      "gpu_launches": info["launches"]["total"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -397,7 +412,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--single-step", action="store_true",
+                    help="one FP32-form step of --workload only (for kernel profilers)")
+    ap.add_argument("--workload", default=WORKLOAD, help="workload of --single-step")
     args = ap.parse_args()
+    if args.single_step:
+        run_single(args)
+        return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
