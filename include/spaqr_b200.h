@@ -125,6 +125,33 @@ int spq_gmres_dev(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, 
  * threads at once) race on it. The workspace is re-initialised by every call. */
 int spq_gmres_dev_noalloc(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
                           const double* d_b, double* d_x, int iters, int restart, double tol, int* its, double* res);
+/* Adjoint (transposed) solves for differentiation: no counterpart in the
+ * reference, whose Tree only applies M ~ A^{-1}. For a loss L(x) with A x = b,
+ * lambda = A^{-T} dL/dx gives dL/db = lambda and dL/dA_ij = -lambda_i x_j on the
+ * pattern of A.
+ * spq_solve_adjoint applies y = M^T g with the same factors (R^T solves
+ * first, then Q: the solve sweeps transposed and in reverse order); g has
+ * length n, y length m. */
+int spq_solve_adjoint(spq_tree* t, const double* g, double* y);
+int spq_solve_adjoint_dev(spq_tree* t, const double* d_g, double* d_y);
+/* GMRES on A^T lambda = g preconditioned by M^T (the GMRES of spq_gmres run on
+ * the transpose). A is the factorized matrix as host CSC (which is A^T as CSR);
+ * lambda holds the initial guess on entry. */
+int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
+                      const double* g, double* lambda, int iters, int restart, double tol, int* its, double* res);
+/* Same on device buffers; d_rowptr_t / d_colind_t / d_val_t are the CSR of A^T
+ * (equivalently the CSC of A). */
+int spq_gmres_adjoint_dev(spq_tree* t, int n, const int* d_rowptr_t, const int* d_colind_t, const double* d_val_t,
+                          const double* d_g, double* d_lambda, int iters, int restart, double tol, int* its,
+                          double* res);
+
+/* Time-to-residual driver of the adjoint: iterative refinement on the true
+ * residual g - A^T lambda with adjoint GMRES corrections (the transposed
+ * spq_solve_to_residual_dev); CSR of A^T on the device. */
+int spq_solve_to_residual_adjoint_dev(spq_tree* t, int n, const int* d_rowptr_t, const int* d_colind_t,
+                                      const double* d_val_t, const double* d_g, double* d_lambda, double target,
+                                      double inner_tol, int max_outer, int iters, int* its, double* true_res);
+
 /* Kernel launches issued by the last spq_factorize and by Krylov calls since
  * the handle was created; solve_graph_kernels = kernels in one preconditioner
  * application (one CUDA graph launch), applications = graph launches so far. */

@@ -68,6 +68,11 @@ SIGNATURES = {
     "spq_solve_to_residual_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _d, _d, _i, _i, _ip, _dp]),
     "spq_gmres_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _i, _i, _d, _ip, _dp]),
     "spq_gmres_dev_noalloc": (_i, [_p, _i, _p, _p, _p, _p, _p, _i, _i, _d, _ip, _dp]),
+    "spq_solve_adjoint": (_i, [_p, _dp, _dp]),
+    "spq_solve_adjoint_dev": (_i, [_p, _p, _p]),
+    "spq_gmres_adjoint": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _i, _i, _d, _ip, _dp]),
+    "spq_gmres_adjoint_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _i, _i, _d, _ip, _dp]),
+    "spq_solve_to_residual_adjoint_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _d, _d, _i, _i, _ip, _dp]),
     "spq_get_launches": (_i, [_p, _llp, _llp, _llp, _llp]),
     "spq_set_profile": (_i, [_p, _i]),
     "spq_get_kernel_stats": (_i, [_p, _i, _dp]),

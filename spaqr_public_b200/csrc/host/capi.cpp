@@ -269,6 +269,121 @@ int spq_solve(spq_tree* t, const double* b, double* x) {
     });
 }
 
+int spq_solve_adjoint_dev(spq_tree* t, const double* d_g, double* d_y) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint solve before factorize");
+    if (!d_g || !d_y) return fail(SPQ_ERR_ARG, "null vector");
+    return guard([&] {
+        t->eng->solve_adjoint_dev(d_g, d_y);
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "adjoint solve");
+        return SPQ_OK;
+    });
+}
+
+int spq_solve_adjoint(spq_tree* t, const double* g, double* y) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint solve before factorize");
+    if (!g || !y) return fail(SPQ_ERR_ARG, "null vector");
+    return guard([&] {
+        const int m = t->eng->nrows(), n = t->eng->ncols();
+        cudaStream_t s = t->eng->stream();
+        double *dg = nullptr, *dy = nullptr;
+        cuda_check(cudaMalloc(&dg, sizeof(double) * n), "adjoint alloc");
+        cuda_check(cudaMalloc(&dy, sizeof(double) * m), "adjoint alloc");
+        cuda_check(cudaMemcpyAsync(dg, g, sizeof(double) * n, cudaMemcpyHostToDevice, s), "adjoint h2d");
+        t->eng->solve_adjoint_dev(dg, dy);
+        cuda_check(cudaMemcpyAsync(y, dy, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "adjoint d2h");
+        cuda_check(cudaStreamSynchronize(s), "adjoint solve");
+        cudaFree(dg);
+        cudaFree(dy);
+        return SPQ_OK;
+    });
+}
+
+int spq_gmres_adjoint_dev(spq_tree* t, int n, const int* rp, const int* ci, const double* va, const double* d_g,
+                          double* d_l, int iters, int restart, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint gmres before factorize");
+    if (n != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    if (!rp || !ci || !va || !d_g || !d_l || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        DevCsr At;
+        At.m = At.n = n;
+        At.rp = rp;
+        At.ci = ci;
+        At.v = va;
+        long long l = 0;
+        *its = gmres_device(*t->eng, At, d_g, d_l, iters, restart, tol, res, &l, true);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "adjoint gmres");
+        return SPQ_OK;
+    });
+}
+
+int spq_solve_to_residual_adjoint_dev(spq_tree* t, int n, const int* rp, const int* ci, const double* va,
+                                      const double* d_g, double* d_l, double target, double inner_tol, int max_outer,
+                                      int iters, int* its, double* true_res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint solve before factorize");
+    if (n != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
+    if (!rp || !ci || !va || !d_g || !d_l || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
+        return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        DevCsr At;
+        At.m = At.n = n;
+        At.rp = rp;
+        At.ci = ci;
+        At.v = va;
+        int outer = 0;
+        long long l = 0;
+        *its = refine_device(*t->eng, At, d_g, d_l, target, inner_tol, max_outer, iters, true_res, &outer, &l, true);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "adjoint solve_to_residual");
+        return *true_res <= target ? SPQ_OK : fail(SPQ_ERR_NOCONV, "target residual not reached");
+    });
+}
+
+int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va, const double* g,
+                      double* lam, int iters, int restart, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint gmres before factorize");
+    if (m != n || m != t->eng->nrows()) return fail(SPQ_ERR_ARG, "adjoint gmres needs the square factorized matrix");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (!g || !lam || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid adjoint gmres arguments");
+    return guard([&] {
+        cudaStream_t s = t->eng->stream();
+        // the CSC arrays of A are the CSR arrays of A^T
+        DevCsrOwned o;
+        const size_t nnz = (size_t)cp[n];
+        cuda_check(cudaMalloc(&o.rp, sizeof(int) * (n + 1)), "csr alloc");
+        cuda_check(cudaMalloc(&o.ci, sizeof(int) * std::max<size_t>(nnz, 1)), "csr alloc");
+        cuda_check(cudaMalloc(&o.v, sizeof(double) * std::max<size_t>(nnz, 1)), "csr alloc");
+        cuda_check(cudaMemcpyAsync(o.rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(o.ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(o.v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        DevCsr At;
+        At.m = n;
+        At.n = m;
+        At.rp = o.rp;
+        At.ci = o.ci;
+        At.v = o.v;
+        double *dg = nullptr, *dl = nullptr;
+        cuda_check(cudaMalloc(&dg, sizeof(double) * n), "adjoint alloc");
+        cuda_check(cudaMalloc(&dl, sizeof(double) * m), "adjoint alloc");
+        cuda_check(cudaMemcpyAsync(dg, g, sizeof(double) * n, cudaMemcpyHostToDevice, s), "adjoint h2d");
+        cuda_check(cudaMemcpyAsync(dl, lam, sizeof(double) * m, cudaMemcpyHostToDevice, s), "adjoint h2d");
+        long long l = 0;
+        *its = gmres_device(*t->eng, At, dg, dl, iters, restart, tol, res, &l, true);
+        t->launches_krylov += l;
+        cuda_check(cudaMemcpyAsync(lam, dl, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "adjoint d2h");
+        cuda_check(cudaStreamSynchronize(s), "adjoint gmres");
+        cudaFree(dg);
+        cudaFree(dl);
+        return SPQ_OK;
+    });
+}
+
 int spq_solve_nrml(spq_tree* t, const double*, double*) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     return fail(SPQ_ERR_UNSUPPORTED, "least-squares (solve_nrml) is not supported by this build");

@@ -96,6 +96,8 @@ public:
         if (!stream_) return;
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (graph_) cudaGraphDestroy(graph_);
+        if (adj_exec_) cudaGraphExecDestroy(adj_exec_);
+        if (adj_graph_) cudaGraphDestroy(adj_graph_);
         for (auto& e : events_) cudaEventDestroy(e);
         cudaStreamSynchronize(stream_);
         arena_.release();
@@ -296,6 +298,25 @@ public:
         ++applications_;
     }
 
+    // y = M^T g: the factors applied transposed (adjoint sweeps, own graph).
+    void solve_adjoint_dev(const double* d_g, double* d_y) override {
+        if (!factorized_) throw std::logic_error("adjoint solve before factorize");
+        double t0 = wall();
+        cuda_check(cudaMemcpyAsync(d_adj_in_, d_g, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
+                   "adjoint in");
+        if (!adj_exec_) {
+            cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+            run_adjoint_sweeps();
+            cuda_check(cudaStreamEndCapture(stream_, &adj_graph_), "capture end");
+            cuda_check(cudaGraphInstantiate(&adj_exec_, adj_graph_, 0), "graph instantiate");
+        }
+        timed(KF_SOLVE, 0, solve_bytes_, [&] { cuda_check(cudaGraphLaunch(adj_exec_, stream_), "graph launch"); });
+        cuda_check(cudaMemcpyAsync(d_y, d_adj_out_, sizeof(double) * nrows_, cudaMemcpyDeviceToDevice, stream_),
+                   "adjoint out");
+        t_solve_ = wall() - t0;
+        ++applications_;
+    }
+
     std::vector<int> bottom_info() const override {
         std::vector<int> out;
         for (Cluster* c : bottoms_[0]) {
@@ -369,7 +390,12 @@ private:
         double words;        // factor words the wave reads
         int hkind, ha, hb;   // kind and sizes of its largest op
     };
-    std::vector<Wave> fwd_waves_, bwd_waves_;
+    std::vector<Wave> fwd_waves_, bwd_waves_, adj_waves_;
+    int64_t xtot_ = 0;
+    double* d_adj_in_ = nullptr;
+    double* d_adj_out_ = nullptr;
+    cudaGraph_t adj_graph_ = nullptr;
+    cudaGraphExec_t adj_exec_ = nullptr;
     const XSeg* d_segs_ = nullptr;
     const GemvRef<T>* d_gemv_ = nullptr;
     cudaGraph_t graph_ = nullptr;
@@ -1121,8 +1147,11 @@ private:
             xtot += std::max(c->xcap, 1);
         }
         xbuf_ = arena_.alloc_n<T>(xtot);
+        xtot_ = xtot;
         d_bin_ = arena_.alloc_n<double>(nrows_);
         d_xout_ = arena_.alloc_n<double>(ncols_);
+        d_adj_in_ = arena_.alloc_n<double>(ncols_);
+        d_adj_out_ = arena_.alloc_n<double>(nrows_);
         std::vector<int> src, dst;
         std::vector<int64_t> xin, xo;
         for (Cluster* c : bottoms_[0]) {
@@ -1216,6 +1245,39 @@ private:
             bwd.push_back(std::move(b));
         }
         std::reverse(bwd.begin(), bwd.end());
+        // Adjoint sweeps. One application is M = B_0 ... B_{n-1} F_{n-1} ... F_0
+        // (F forward ops in tape order, then the backward ops in reverse), so
+        // M^T applies B_0^T ... B_{n-1}^T and then F_{n-1}^T ... F_0^T: Q^T and
+        // Q swap, R^{-1} (x - A12 x_n) becomes R^{-T} with x_n -= A12^T z, and
+        // the index maps of SplitD and Merge become their transposes. Every
+        // transposed op reads and writes all the segments it touches.
+        auto transpose_op = [](const POp& o) {
+            POp t = o;
+            std::vector<Cluster*> touch = o.rd;
+            touch.insert(touch.end(), o.wr.begin(), o.wr.end());
+            std::sort(touch.begin(), touch.end(), ByOrder());
+            touch.erase(std::unique(touch.begin(), touch.end()), touch.end());
+            switch (o.op.kind) {
+                case SK_APPLYQ:
+                case SK_TRI:
+                    t.op.dir ^= 1;
+                    break;
+                case SK_SPLIT:
+                    t.op.kind = SK_SPLIT_T;
+                    break;
+                case SK_MERGE:
+                    t.op.kind = SK_MERGE_T;
+                    break;
+                default:
+                    throw std::logic_error("adjoint: op without a transpose");
+            }
+            t.rd = touch;
+            t.wr = touch;
+            return t;
+        };
+        std::vector<POp> adj;
+        for (auto it = bwd.rbegin(); it != bwd.rend(); ++it) adj.push_back(transpose_op(*it));
+        for (auto it = fwd.rbegin(); it != fwd.rend(); ++it) adj.push_back(transpose_op(*it));
         // wave scheduling on x segments (RAW, WAR, WAW)
         auto schedule = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves) {
             std::map<const Cluster*, int> lw, lr;
@@ -1241,9 +1303,10 @@ private:
             waves.assign(nw, {});
             for (size_t i = 0; i < ops.size(); ++i) waves[wv[i]].push_back((int)i);
         };
-        std::vector<std::vector<int>> fw, bw;
+        std::vector<std::vector<int>> fw, bw, aw;
         schedule(fwd, fw);
         schedule(bwd, bw);
+        schedule(adj, aw);
         std::vector<SolveOp> all;
         struct WMeta {
             size_t off;
@@ -1251,7 +1314,7 @@ private:
             double words;
             int hkind, ha, hb;
         };
-        std::vector<WMeta> fm, bm;
+        std::vector<WMeta> fm, bm, am;
         auto op_words = [&](const SolveOp& o) -> double {
             if (o.kind == SK_APPLYQ) return (double)o.a * o.b - 0.5 * (double)o.b * (o.b - 1);
             if (o.kind != SK_TRI) return 0.0;
@@ -1280,6 +1343,7 @@ private:
         };
         pack(fwd, fw, fm);
         pack(bwd, bw, bm);
+        pack(adj, aw, am);
         Upload up;
         size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
                o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
@@ -1295,13 +1359,15 @@ private:
         bwd_waves_.clear();
         for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
         for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        adj_waves_.clear();
+        for (auto& mt : am) adj_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
         nin_ = (int)src.size();
         nout_ = (int)dst.size();
         // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
         // right-hand side and solution vectors
         solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 8.0 * (nrows_ + ncols_);
         const size_t smem_cap = (200 * 1024) / sizeof(T);
-        for (auto* ws : {&fwd_waves_, &bwd_waves_})
+        for (auto* ws : {&fwd_waves_, &bwd_waves_, &adj_waves_})
             for (auto& w : *ws)
                 if ((size_t)w.smem > smem_cap)
                     throw std::runtime_error("solve: a cluster exceeds the shared-memory vector capacity");
@@ -1361,6 +1427,15 @@ private:
         }
         launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
         ++launches_solve_;
+    }
+    // M^T = G_in^T (sweeps)^T S_out^T: start from zero, place g where the solve
+    // reads x out, run the transposed waves, read y where the solve puts b in.
+    void run_adjoint_sweeps() {
+        cuda_check(cudaMemsetAsync(xbuf_, 0, sizeof(T) * (size_t)xtot_, stream_), "adjoint zero");
+        launch_gather_in<T>(d_adj_in_, d_dst_, d_xout_pos_, xbuf_, nout_, stream_);
+        for (auto& w : adj_waves_)
+            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
+        launch_scatter_out<T>(xbuf_, d_xin_, d_src_, d_adj_out_, nin_, stream_);
     }
 };
 

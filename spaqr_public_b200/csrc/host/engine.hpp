@@ -66,6 +66,8 @@ public:
     virtual void assemble(const Csc& A) = 0;
     virtual void factorize() = 0;
     virtual void solve_dev(const double* d_b, double* d_x) = 0;
+    // y = M^T g with M the preconditioner of solve_dev (adjoint sweeps)
+    virtual void solve_adjoint_dev(const double* d_g, double* d_y) = 0;
     virtual cudaStream_t stream() const = 0;
     virtual const Log& log() const = 0;
     virtual const std::vector<int>& cperm() const = 0;

@@ -155,7 +155,7 @@ public:
         const int maxIters = iters;
         int it = 0;
         residual(b, x, p0_.p);
-        P_.solve_dev(p0_.p, r0_.p);
+        precond(p0_.p, r0_.p);
         launch_dot_partials(r0_.p, nullptr, 0, m, part_.p, nblk_, s_);
         ++launches_;
         const double r0Norm = std::sqrt(host_sum());
@@ -178,7 +178,7 @@ public:
             for (int i = k - 1; i >= 0; --i) reflect(i, v_.p);
             launch_spmv_csr(m, A_.rp, A_.ci, A_.v, v_.p, t_.p, s_);
             ++launches_;
-            P_.solve_dev(t_.p, v_.p);
+            precond(t_.p, v_.p);
             for (int i = 0; i < k; ++i) reflect(i, v_.p);
             if (k < m) {
                 launch_dot_partials(v_.p, nullptr, k, m, part_.p, nblk_, s_);
@@ -223,7 +223,7 @@ public:
                 }
                 k = 0;
                 residual(b, x, p0_.p);
-                P_.solve_dev(p0_.p, r0_.p);
+                precond(p0_.p, r0_.p);
                 cuda_check(cudaMemsetAsync(H_.p, 0, sizeof(double) * (size_t)m * (restart + 1), s_), "H zero");
                 cuda_check(cudaMemsetAsync(scal_.p, 0, sizeof(double) * (2 * (restart + 1) + 4), s_), "tau");
                 std::fill(w.begin(), w.end(), 0.0);
@@ -235,8 +235,17 @@ public:
         return it;
     }
     long long launches_ = 0;
+    bool adjoint_ = false;  // A is A^T and the preconditioner is applied transposed
 
 private:
+    // M r, or M^T r in an adjoint solve
+    void precond(const double* in, double* out) {
+        if (adjoint_)
+            P_.solve_adjoint_dev(in, out);
+        else
+            P_.solve_dev(in, out);
+    }
+
     EngineBase& P_;
     DevCsr A_;
     int m_, restart_, nblk_;
@@ -248,9 +257,10 @@ private:
 }  // namespace
 
 int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart, double tol,
-                 double* res, long long* launches) {
+                 double* res, long long* launches, bool adjoint) {
     if (restart < 1) restart = 1;
     Gmres g(P, A, restart);
+    g.adjoint_ = adjoint;
     int it = g.run(d_b, d_x, iters, tol, res);
     if (launches) *launches = g.launches_;
     return it;
@@ -268,7 +278,7 @@ int gmres_device_ws(EngineBase& P, const DevCsr& A, const double* d_b, double* d
 }
 
 int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, double target, double inner_tol,
-                  int max_outer, int iters, double* true_res, int* outer, long long* launches) {
+                  int max_outer, int iters, double* true_res, int* outer, long long* launches, bool adjoint) {
     cudaStream_t s = P.stream();
     DevVec r, d;
     r.alloc(A.m, s);
@@ -283,7 +293,7 @@ int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x
         cuda_check(cudaMemsetAsync(d.p, 0, sizeof(double) * A.n, s), "refine zero");
         double res = 0;
         long long gl = 0;
-        total += gmres_device(P, A, r.p, d.p, iters, iters, inner_tol, &res, &gl);
+        total += gmres_device(P, A, r.p, d.p, iters, iters, inner_tol, &res, &gl, adjoint);
         launch_axpby(A.n, 1.0, d.p, 1.0, d_x, s);
         l += gl + 3;
         ++k;

@@ -13,9 +13,11 @@ struct DevCsr {
 };
 
 // Householder GMRES, left preconditioned by P (src/is.cpp:94-272). x holds the
-// initial guess; returns the iteration count, *res = |w(k)|/|r0|.
+// initial guess; returns the iteration count, *res = |w(k)|/|r0|. With
+// adjoint set, A is A^T (the caller passes the CSR of A^T) and the
+// preconditioner is applied transposed (M^T).
 int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart, double tol,
-                 double* res, long long* launches);
+                 double* res, long long* launches, bool adjoint = false);
 
 // The same GMRES on a caller-provided device workspace of
 // gmres_workspace_elems(m, restart) doubles; allocates no device memory.
@@ -30,7 +32,8 @@ double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const d
 // A d = r preconditioned by P to inner_tol, x += d, until ||b - A x|| / ||b||
 // <= target or max_outer corrections. Returns the total GMRES iterations;
 // *true_res is the final relative residual, *outer the corrections made.
+// With adjoint set, A is A^T and the corrections use the adjoint GMRES.
 int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, double target, double inner_tol,
-                  int max_outer, int iters, double* true_res, int* outer, long long* launches);
+                  int max_outer, int iters, double* true_res, int* outer, long long* launches, bool adjoint = false);
 
 }  // namespace spq

@@ -735,6 +735,54 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
             }
             break;
         }
+        case SK_SPLIT_T: {
+            // Transposes of the SplitD index maps (adjoint sweeps): dir 0 undoes
+            // the forward split (the fine part's adjoint folds back into c and
+            // f's adjoint is consumed), dir 1 the backward split.
+            const int crows = op.a, ccols = op.b, rank = op.c;
+            T* yc = x + op.x0;
+            T* yf = x + op.x1;
+            for (int i = tid; i < crows; i += blockDim.x) xs[i] = yc[i];
+            __syncthreads();
+            const int nf = ccols - rank, nr = crows - ccols;
+            if (op.dir == 0) {
+                for (int q = tid; q < nf; q += blockDim.x) {
+                    yc[rank + q] = xs[crows - nf + q] + yf[q];
+                    yf[q] = T(0);
+                }
+                for (int q = tid; q < nr; q += blockDim.x) yc[ccols + q] = xs[rank + q];
+            } else {
+                for (int q = tid; q < nf; q += blockDim.x) yf[q] += xs[rank + q];
+                for (int q = tid; q < nr; q += blockDim.x) yc[rank + q] = xs[ccols + q];
+                for (int q = tid; q < nf; q += blockDim.x) yc[rank + nr + q] = T(0);
+            }
+            break;
+        }
+        case SK_MERGE_T: {
+            // dir 0 (transpose of parent <- children rows): children += parent
+            // pieces, parent pieces zeroed; dir 1 (transpose of children cols <-
+            // parent): parent pieces += children, children zeroed.
+            int cur = 0;
+            for (int s = 0; s < op.nseg; ++s) {
+                const XSeg sg = segs[op.seg0 + s];
+                const int len = op.dir == 0 ? sg.len : sg.pad;
+                T* yp = x + op.x0 + cur;
+                T* ych = x + sg.xoff;
+                if (op.dir == 0) {
+                    for (int i = tid; i < len; i += blockDim.x) {
+                        ych[i] += yp[i];
+                        yp[i] = T(0);
+                    }
+                } else {
+                    for (int i = tid; i < len; i += blockDim.x) {
+                        yp[i] += ych[i];
+                        ych[i] = T(0);
+                    }
+                }
+                cur += len;
+            }
+            break;
+        }
         default:
             break;
     }

@@ -117,7 +117,9 @@ enum SolveKind : int {
     SK_TRI = 1,     // x <- inv(R) (x - sum_b B_b x_b)  or transposed variant
     SK_SPLIT = 2,   // SplitD fwd/bwd index shuffle
     SK_MERGE = 3,   // Merge fwd/bwd copies
-    SK_REASSIGN = 4 // rectangular row reassignment
+    SK_REASSIGN = 4, // rectangular row reassignment
+    SK_SPLIT_T = 5, // transpose of SK_SPLIT (same dir)
+    SK_MERGE_T = 6  // transpose of SK_MERGE (same dir): add into the source, zero the target
 };
 struct SolveOp {
     int kind, dir;

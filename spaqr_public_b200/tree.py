@@ -117,6 +117,16 @@ class Tree:
         """Device pointers (e.g. torch tensors' data_ptr()) of FP64 vectors."""
         check(lib().spq_solve_dev(self._h, C.c_void_p(d_b), C.c_void_p(d_x)))
 
+    def solve_adjoint(self, g):
+        """y = M^T g: the preconditioner's transpose (factors applied transposed)."""
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        y = np.zeros(self.m)
+        check(lib().spq_solve_adjoint(self._h, dptr(g), dptr(y)))
+        return y
+
+    def solve_adjoint_dev(self, d_g, d_y):
+        check(lib().spq_solve_adjoint_dev(self._h, C.c_void_p(d_g), C.c_void_p(d_y)))
+
     def solve_nrml(self, b):
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n)
@@ -171,6 +181,20 @@ def gmres(A, b, precond, iters=300, restart=None, tol=1e-12, x0=None):
     check(lib().spq_gmres(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(b), dptr(x), int(iters),
                           int(iters if restart is None else restart), float(tol), C.byref(its), C.byref(res)))
     return x, its.value, res.value
+
+
+def gmres_adjoint(A, g, precond, iters=300, restart=None, tol=1e-12, lam0=None):
+    """GMRES on A^T lambda = g preconditioned by M^T (the adjoint of ``gmres``).
+    A is the factorized matrix (CSC). Returns (lambda, iterations, residual estimate)."""
+    m, n, cp, ri, va = _csc(A)
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    lam = np.zeros(m) if lam0 is None else np.array(lam0, dtype=np.float64)
+    its = C.c_int(0)
+    res = C.c_double(0)
+    check(lib().spq_gmres_adjoint(precond._h, m, n, iptr(cp), iptr(ri), dptr(va), dptr(g), dptr(lam), int(iters),
+                                  int(iters if restart is None else restart), float(tol), C.byref(its),
+                                  C.byref(res)))
+    return lam, its.value, res.value
 
 
 def solve_to_residual(A, b, precond, target=1e-10, inner_tol=None, max_outer=8, iters=300, x0=None):
