@@ -405,6 +405,83 @@ def run_single(args):
                       "gpu_launches": info["launches"]["total"]}), flush=True)
 
 
+def run_diff_batch(args):
+    """The differentiation batch: 32 independent 2D advection-diffusion systems
+    (sides 96..256), FP32 factors, loss 1/2 ||x - x*||^2, gradients dL/db and
+    dL/dA by the adjoint solve. Times (wall clock, device synchronised) the
+    batched path (spq_factorize_batch + concurrent forward and adjoint solves)
+    against the same work one system after another."""
+    import torch
+    from spaqr_public_b200 import FP32, factorize_batch, matgen
+    from spaqr_public_b200.autograd import SparsePattern, spaqr_solve, spaqr_solve_batch
+    torch.cuda.set_device(0)
+    ws = matgen.diff_batch(32)
+    As = [matgen.column_normalize(w["A"]) for w in ws]
+    pats = [SparsePattern(A) for A in As]
+    xst = [torch.tensor(w["xstar"], dtype=torch.float64, device="cuda") for w in ws]
+
+    def setup():
+        return [make_tree(w, A, FP32, 0) for w, A in zip(ws, As)]
+
+    def tensors():
+        vals = [torch.tensor(A[4], dtype=torch.float64, device="cuda", requires_grad=True) for A in As]
+        bs = [torch.tensor(w["b"], dtype=torch.float64, device="cuda", requires_grad=True) for w in ws]
+        return vals, bs
+
+    def batched():
+        trees = setup()
+        vals, bs = tensors()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        factorize_batch(trees)
+        t1 = time.perf_counter()
+        xs = spaqr_solve_batch(vals, bs, trees, pats, target=1e-10, inner_tol=1e-6)
+        L = sum(0.5 * ((x - s) ** 2).sum() for x, s in zip(xs, xst))
+        L.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        for t in trees:
+            t.close()
+        return t1 - t0, t2 - t1
+
+    def sequential():
+        trees = setup()
+        vals, bs = tensors()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for t in trees:
+            t.factorize()
+        t1 = time.perf_counter()
+        for i in range(len(trees)):
+            x = spaqr_solve(vals[i], bs[i], trees[i], pats[i], target=1e-10, inner_tol=1e-6)
+            (0.5 * ((x - xst[i]) ** 2).sum()).backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        for t in trees:
+            t.close()
+        return t1 - t0, t2 - t1
+
+    for _ in range(max(1, args.warmup)):
+        batched()
+        sequential()
+    bf, bsv, sf, ssv = [], [], [], []
+    for _ in range(args.steps):
+        a, b = batched()
+        bf.append(a)
+        bsv.append(b)
+        a, b = sequential()
+        sf.append(a)
+        ssv.append(b)
+    med = statistics.median
+    print(json.dumps({
+        "workload": "diff_batch: 32 x advdiff2d, sides 96..256 (seeded), FP32 factors, FP64 GMRES to 1e-10, "
+                    "loss 1/2||x - x*||^2, forward + adjoint solve",
+        "unknowns": int(sum(w["n"] ** 2 for w in ws)),
+        "batched": {"factor_s": med(bf), "solve_fwd_adj_s": med(bsv), "total_s": med(bf) + med(bsv)},
+        "sequential": {"factor_s": med(sf), "solve_fwd_adj_s": med(ssv), "total_s": med(sf) + med(ssv)},
+        "speedup": (med(sf) + med(ssv)) / (med(bf) + med(bsv)), "steps": args.steps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,9 +492,14 @@ def main():
     ap.add_argument("--single-step", action="store_true",
                     help="one FP32-form step of --workload only (for kernel profilers)")
     ap.add_argument("--workload", default=WORKLOAD, help="workload of --single-step")
+    ap.add_argument("--diff-batch", action="store_true",
+                    help="time the 32-system differentiation batch (batched vs one after another)")
     args = ap.parse_args()
     if args.single_step:
         run_single(args)
+        return
+    if args.diff_batch:
+        run_diff_batch(args)
         return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -73,6 +73,14 @@ int spq_partition(spq_tree* t, int m, int n, const int* colptr, const int* rowin
 int spq_assemble(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val);
 int spq_factorize(spq_tree* t);
 
+/* Batched factorization of n independent handles (each partitioned and
+ * assembled, on any devices). Every handle has its own CUDA stream; the
+ * handles run on up to nthreads host threads (<= 0: one per handle, at most
+ * 32), so the small per-wave launches of different systems share the GPU.
+ * Returns the first failure (SPQ_ERR_* with the handle's index in the
+ * message); the other handles are factorized regardless. */
+int spq_factorize_batch(spq_tree* const* ts, int n, int nthreads);
+
 /* Preconditioner applies on HOST buffers (b of length m for solve, n for
  * solve_nrml; x of length n). */
 int spq_solve(spq_tree* t, const double* b, double* x);

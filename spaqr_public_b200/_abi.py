@@ -48,6 +48,7 @@ SIGNATURES = {
     "spq_partition": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "spq_assemble": (_i, [_p, _i, _i, _ip, _ip, _dp]),
     "spq_factorize": (_i, [_p]),
+    "spq_factorize_batch": (_i, [C.POINTER(_p), _i, _i]),
     "spq_solve": (_i, [_p, _dp, _dp]),
     "spq_solve_nrml": (_i, [_p, _dp, _dp]),
     "spq_solve_dev": (_i, [_p, _p, _p]),

@@ -62,24 +62,53 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
-def _solve(tree, pat, values, rhs, target, inner_tol, adjoint):
+def _prepare(pat, values, rhs, adjoint):
+    """Device buffers of one solve (torch's stream): values in the CSR order the
+    solve needs and a zero initial guess."""
     import torch
     out = torch.zeros(pat.n if not adjoint else pat.m, dtype=torch.float64, device=rhs.device)
+    vals = values.contiguous() if adjoint else values[pat.perm].contiguous()
+    return vals, rhs.contiguous(), out
+
+
+def _call(tree, pat, vals, rhs, out, target, inner_tol, adjoint):
+    """The library solve on the handle's own stream (returns when it is done)."""
     its = C.c_int(0)
     res = C.c_double(0)
-    torch.cuda.current_stream().synchronize()  # the library runs on the handle's own stream
     if adjoint:
-        vals = values.contiguous()
         rc = lib().spq_solve_to_residual_adjoint_dev(tree._h, pat.n, _ptr(pat.rp_t), _ptr(pat.ci_t), _ptr(vals),
                                                      _ptr(rhs), _ptr(out), float(target), float(inner_tol), 8, 300,
                                                      C.byref(its), C.byref(res))
     else:
-        vals = values[pat.perm].contiguous()
         rc = lib().spq_solve_to_residual_dev(tree._h, pat.m, _ptr(pat.rp), _ptr(pat.ci), _ptr(vals), _ptr(rhs),
                                              _ptr(out), float(target), float(inner_tol), 8, 300, C.byref(its),
                                              C.byref(res))
     check(rc)
-    return out, its.value, res.value
+    return its.value, res.value
+
+
+def _solve(tree, pat, values, rhs, target, inner_tol, adjoint):
+    import torch
+    vals, rhs, out = _prepare(pat, values, rhs, adjoint)
+    torch.cuda.current_stream().synchronize()  # the library runs on the handle's own stream
+    its, res = _call(tree, pat, vals, rhs, out, target, inner_tol, adjoint)
+    return out, its, res
+
+
+def _solve_many(trees, pats, values, rhss, target, inner_tol, adjoint, nthreads):
+    """Independent solves of a batch, one host thread per handle (each handle
+    has its own CUDA stream, so the solves share the GPU)."""
+    import concurrent.futures as cf
+
+    import torch
+    bufs = [_prepare(p, v, r, adjoint) for p, v, r in zip(pats, values, rhss)]
+    torch.cuda.current_stream().synchronize()
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(nthreads, len(trees)))) as ex:
+        futs = [ex.submit(_call, t, p, b[0], b[1], b[2], target, inner_tol, adjoint)
+                for t, p, b in zip(trees, pats, bufs)]
+        for f in futs:
+            f.result()
+    return [b[2] for b in bufs]
 
 
 def _make_function():
@@ -112,7 +141,52 @@ def _make_function():
     return SpaqrSolve
 
 
+def _make_batch_function():
+    import torch
+
+    class SpaqrSolveBatch(torch.autograd.Function):
+        """x_i = A_i^{-1} b_i for a batch of independent systems; forward and
+        adjoint solves of the batch run concurrently (one stream each)."""
+
+        @staticmethod
+        def forward(ctx, trees, patterns, target, inner_tol, nthreads, *tensors):
+            n = len(trees)
+            values = [v.detach().to(torch.float64).contiguous() for v in tensors[:n]]
+            bs = [b.detach().to(torch.float64).contiguous() for b in tensors[n:]]
+            xs = _solve_many(trees, patterns, values, bs, target, inner_tol, False, nthreads)
+            ctx.save_for_backward(*values, *xs)
+            ctx.trees, ctx.patterns, ctx.target, ctx.inner_tol, ctx.nthreads = trees, patterns, target, inner_tol, \
+                nthreads
+            return tuple(xs)
+
+        @staticmethod
+        def backward(ctx, *gxs):
+            n = len(ctx.trees)
+            saved = ctx.saved_tensors
+            values, xs = saved[:n], saved[n:]
+            gxs = [g.detach().to(torch.float64).contiguous() for g in gxs]
+            lams = _solve_many(ctx.trees, ctx.patterns, values, gxs, ctx.target, ctx.inner_tol, True, ctx.nthreads)
+            gvals = [-lam[p.rows] * x[p.cols] for lam, x, p in zip(lams, xs, ctx.patterns)]
+            return (None, None, None, None, None, *gvals, *lams)
+
+    return SpaqrSolveBatch
+
+
 _FN = None
+_FNB = None
+
+
+def spaqr_solve_batch(values, bs, trees, patterns, target=1e-12, inner_tol=None, nthreads=32):
+    """Batched :func:`spaqr_solve`: lists of values, right-hand sides, factorized
+    trees and patterns of independent systems; returns the list of solutions.
+    Forward and backward solves of the batch run concurrently."""
+    global _FNB
+    if _FNB is None:
+        _FNB = _make_batch_function()
+    if inner_tol is None:
+        inner_tol = target
+    return list(_FNB.apply(list(trees), list(patterns), target, inner_tol, nthreads, *values, *bs))
+
 
 
 def spaqr_solve(values, b, tree, pattern, target=1e-12, inner_tol=None):
@@ -131,4 +205,4 @@ def spaqr_solve(values, b, tree, pattern, target=1e-12, inner_tol=None):
     return _FN.apply(values, b, tree, pattern, target, inner_tol)
 
 
-__all__ = ["SparsePattern", "spaqr_solve", "SpqError"]
+__all__ = ["SparsePattern", "spaqr_solve", "spaqr_solve_batch", "SpqError"]

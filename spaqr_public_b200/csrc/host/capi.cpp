@@ -1,8 +1,11 @@
 // C ABI of spaQR-B200 (declared in include/spaqr_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <memory>
 #include <new>
 #include <string>
@@ -50,6 +53,18 @@ int guard(F&& f) {
     } catch (const std::exception& e) {
         return fail(SPQ_ERR_NUMERIC, e.what());
     }
+}
+
+// guard() for calls on a handle whose device is open: the calling thread's
+// current device becomes the handle's, so a handle may be used from any
+// thread (batches run one handle per thread).
+template <class F>
+int guard_on(spq_tree* t, F&& f) {
+    if (t && t->eng && t->state >= 2) {
+        cudaError_t e = cudaSetDevice(t->cfg.device);
+        if (e != cudaSuccess) return fail(SPQ_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    return guard(std::forward<F>(f));
 }
 
 int check_csc(int m, int n, const int* cp, const int* ri, const double* va) {
@@ -221,7 +236,7 @@ int spq_assemble(spq_tree* t, int m, int n, const int* cp, const int* ri, const 
     int rc = check_csc(m, n, cp, ri, va);
     if (rc) return rc;
     if (m != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "matrix size differs from partition");
-    return guard([&] {
+    return guard_on(t, [&] {
         t->eng->assemble(csc_from(m, n, cp, ri, va));
         t->state = 2;
         return SPQ_OK;
@@ -231,7 +246,7 @@ int spq_assemble(spq_tree* t, int m, int n, const int* cp, const int* ri, const 
 int spq_factorize(spq_tree* t) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (t->state != 2) return fail(SPQ_ERR_STATE, "factorize must follow assemble");
-    return guard([&] {
+    return guard_on(t, [&] {
         t->eng->factorize();
         t->state = 3;
         return SPQ_OK;
@@ -242,7 +257,7 @@ int spq_solve_dev(spq_tree* t, const double* d_b, double* d_x) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (t->state != 3) return fail(SPQ_ERR_STATE, "solve before factorize");
     if (!d_b || !d_x) return fail(SPQ_ERR_ARG, "null vector");
-    return guard([&] {
+    return guard_on(t, [&] {
         t->eng->solve_dev(d_b, d_x);
         cuda_check(cudaStreamSynchronize(t->eng->stream()), "solve");
         return SPQ_OK;
@@ -253,7 +268,7 @@ int spq_solve(spq_tree* t, const double* b, double* x) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (t->state != 3) return fail(SPQ_ERR_STATE, "solve before factorize");
     if (!b || !x) return fail(SPQ_ERR_ARG, "null vector");
-    return guard([&] {
+    return guard_on(t, [&] {
         const int m = t->eng->nrows(), n = t->eng->ncols();
         cudaStream_t s = t->eng->stream();
         double *db = nullptr, *dx = nullptr;
@@ -273,7 +288,7 @@ int spq_solve_adjoint_dev(spq_tree* t, const double* d_g, double* d_y) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint solve before factorize");
     if (!d_g || !d_y) return fail(SPQ_ERR_ARG, "null vector");
-    return guard([&] {
+    return guard_on(t, [&] {
         t->eng->solve_adjoint_dev(d_g, d_y);
         cuda_check(cudaStreamSynchronize(t->eng->stream()), "adjoint solve");
         return SPQ_OK;
@@ -284,7 +299,7 @@ int spq_solve_adjoint(spq_tree* t, const double* g, double* y) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint solve before factorize");
     if (!g || !y) return fail(SPQ_ERR_ARG, "null vector");
-    return guard([&] {
+    return guard_on(t, [&] {
         const int m = t->eng->nrows(), n = t->eng->ncols();
         cudaStream_t s = t->eng->stream();
         double *dg = nullptr, *dy = nullptr;
@@ -306,7 +321,7 @@ int spq_gmres_adjoint_dev(spq_tree* t, int n, const int* rp, const int* ci, cons
     if (t->state != 3) return fail(SPQ_ERR_STATE, "adjoint gmres before factorize");
     if (n != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
     if (!rp || !ci || !va || !d_g || !d_l || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         DevCsr At;
         At.m = At.n = n;
         At.rp = rp;
@@ -328,7 +343,7 @@ int spq_solve_to_residual_adjoint_dev(spq_tree* t, int n, const int* rp, const i
     if (n != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
     if (!rp || !ci || !va || !d_g || !d_l || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
         return fail(SPQ_ERR_ARG, "invalid arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         DevCsr At;
         At.m = At.n = n;
         At.rp = rp;
@@ -351,7 +366,7 @@ int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* cp, const int* ri, c
     int rc = check_csc(m, n, cp, ri, va);
     if (rc) return rc;
     if (!g || !lam || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid adjoint gmres arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         cudaStream_t s = t->eng->stream();
         // the CSC arrays of A are the CSR arrays of A^T
         DevCsrOwned o;
@@ -401,7 +416,7 @@ int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const dou
     int rc = check_csc(m, n, cp, ri, va);
     if (rc) return rc;
     if (!b || !x || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid gmres arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         cudaStream_t s = t->eng->stream();
         DevCsrOwned o;
         DevCsr A;
@@ -432,7 +447,7 @@ int spq_solve_to_residual(spq_tree* t, int m, int n, const int* cp, const int* r
     if (rc) return rc;
     if (!b || !x || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
         return fail(SPQ_ERR_ARG, "invalid arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         cudaStream_t s = t->eng->stream();
         DevCsrOwned o;
         DevCsr A;
@@ -462,7 +477,7 @@ int spq_solve_to_residual_dev(spq_tree* t, int m, const int* rp, const int* ci, 
     if (m != t->eng->nrows() || m != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
     if (!rp || !ci || !va || !d_b || !d_x || !its || !true_res || iters < 1 || max_outer < 1 || !(target > 0))
         return fail(SPQ_ERR_ARG, "invalid arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         DevCsr A;
         A.m = A.n = m;
         A.rp = rp;
@@ -483,7 +498,7 @@ int spq_gmres_dev(spq_tree* t, int m, const int* rp, const int* ci, const double
     if (t->state != 3) return fail(SPQ_ERR_STATE, "gmres before factorize");
     if (m != t->eng->nrows() || m != t->eng->ncols()) return fail(SPQ_ERR_ARG, "needs the square factorized matrix");
     if (!rp || !ci || !va || !d_b || !d_x || !its || !res || iters < 1) return fail(SPQ_ERR_ARG, "invalid arguments");
-    return guard([&] {
+    return guard_on(t, [&] {
         DevCsr A;
         A.m = A.n = m;
         A.rp = rp;
@@ -507,7 +522,7 @@ int spq_gmres_dev_noalloc(spq_tree* t, int m, const int* rp, const int* ci, cons
         return fail(SPQ_ERR_STATE,
                     "apply the preconditioner once (spq_solve, spq_solve_dev or spq_gmres_dev) before the "
                     "no-allocation GMRES: the first application builds its solve graph");
-    return guard([&]() -> int {
+    return guard_on(t, [&]() -> int {
         cuda_check(cudaSetDevice(t->cfg.device), "cudaSetDevice");
         double* ws = nullptr;
         size_t cap = 0;
@@ -553,7 +568,7 @@ int spq_get_kernel_stats(spq_tree* t, int family, double* out4) {
     if (!t || !out4) return fail(SPQ_ERR_ARG, "null argument");
     if (!t->eng) return fail(SPQ_ERR_STATE, "no engine");
     if (family < 0 || family >= kNumFamilies) return fail(SPQ_ERR_ARG, "unknown kernel family");
-    return guard([&] {
+    return guard_on(t, [&] {
         KernelStat s = t->eng->kernel_stat(family);
         out4[0] = (double)s.launches;
         out4[1] = s.ms;
@@ -565,7 +580,7 @@ int spq_get_kernel_stats(spq_tree* t, int family, double* out4) {
 int spq_reset_kernel_stats(spq_tree* t) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (!t->eng) return SPQ_OK;
-    return guard([&] {
+    return guard_on(t, [&] {
         t->eng->reset_kernel_stats();
         return SPQ_OK;
     });
@@ -573,7 +588,7 @@ int spq_reset_kernel_stats(spq_tree* t) {
 int spq_profile_solve_waves(spq_tree* t, double* out, int cap, int* nwaves) {
     if (!t || !out || !nwaves) return fail(SPQ_ERR_ARG, "null argument");
     if (t->state != 3) return fail(SPQ_ERR_STATE, "profile before factorize");
-    return guard([&] {
+    return guard_on(t, [&] {
         auto v = t->eng->profile_solve_waves();
         *nwaves = (int)(v.size() / 7);
         std::memcpy(out, v.data(), sizeof(double) * std::min<size_t>(v.size(), (size_t)cap * 7));
@@ -629,6 +644,35 @@ int spq_get_stats(spq_tree* t, double* times, long long* counters) {
     t->eng->stats(times, counters);
     return SPQ_OK;
 }
+int spq_factorize_batch(spq_tree* const* ts, int n, int nthreads) {
+    if (n < 0 || (n > 0 && !ts)) return fail(SPQ_ERR_ARG, "invalid batch");
+    for (int i = 0; i < n; ++i) {
+        if (!ts[i]) return fail(SPQ_ERR_ARG, "null handle in batch at " + std::to_string(i));
+        if (ts[i]->state != 2) return fail(SPQ_ERR_STATE, "batch handle " + std::to_string(i) + " is not assembled");
+        for (int j = 0; j < i; ++j)
+            if (ts[j] == ts[i]) return fail(SPQ_ERR_ARG, "a handle appears twice in the batch");
+    }
+    if (n == 0) return SPQ_OK;
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min(n, nthreads > 0 ? nthreads : std::min(hw, 32)));
+    std::atomic<int> next{0};
+    std::vector<int> rc(n, SPQ_OK);
+    std::vector<std::string> err(n);
+    auto work = [&] {
+        for (int i = next++; i < n; i = next++) {
+            rc[i] = spq_factorize(ts[i]);
+            if (rc[i] != SPQ_OK) err[i] = g_err;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int q = 1; q < nt; ++q) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    for (int i = 0; i < n; ++i)
+        if (rc[i] != SPQ_OK) return fail(rc[i], "batch handle " + std::to_string(i) + ": " + err[i]);
+    return SPQ_OK;
+}
+
 int spq_trim_memory(void) {
     return guard([&] {
         trim_device_pools();

@@ -94,6 +94,7 @@ public:
     Engine(const Config& cfg) : cfg_(cfg), bottoms_(std::max(cfg.nlevels, 1)), fine_(std::max(cfg.nlevels, 1)) {}
     ~Engine() override {
         if (!stream_) return;
+        cudaSetDevice(cfg_.device);
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (graph_) cudaGraphDestroy(graph_);
         if (adj_exec_) cudaGraphExecDestroy(adj_exec_);

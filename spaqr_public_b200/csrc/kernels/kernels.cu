@@ -11,6 +11,9 @@
 
 #include <cfloat>
 #include <cmath>
+#include <mutex>
+#include <set>
+#include <utility>
 
 namespace spq {
 
@@ -964,14 +967,24 @@ void launch_sub(int n, const double* a, const double* b, double* y, cudaStream_t
 }
 int reduce_blocks() { return kRedBlocks; }
 
+void once_per_device(const void* key, void (*setup)()) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> seen;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);  // held while setup runs: no launch sees a half-done setup
+    if (seen.insert({key, dev}).second) setup();
+}
+
+// Function attributes belong to the device's context: set once per device
+// (thread-safe; handles on several threads or devices share them).
 template <class T>
 void prepare_kernels() {
-    static bool done = false;
-    if (done) return;
-    cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem<T>());
-    cudaFuncSetAttribute(k_solve_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    done = true;
+    once_per_device(reinterpret_cast<const void*>(&k_panel<T>), [] {
+        cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        cudaFuncSetAttribute(k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem<T>());
+        cudaFuncSetAttribute(k_solve_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
 }
 
 #define SPQ_INST(T)                                                                                           \

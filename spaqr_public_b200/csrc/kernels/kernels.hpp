@@ -22,6 +22,11 @@ struct CopyDesc {
     int sld, dld, rows, cols;
     int mode, pad;
 };
+// Runs setup the first time it is called for this key on the current device
+// (thread-safe; callers wait until it has run): per-device one-time setup
+// such as function attributes.
+void once_per_device(const void* key, void (*setup)());
+
 template <class T>
 void launch_copy(const CopyDesc<T>* d, int n, cudaStream_t s);
 

@@ -485,12 +485,10 @@ cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntask
     const size_t cap = 160 * 1024;
     if (smem_bytes > cap) smem_bytes = std::max(cap, (mpad + 2 * wp) * sizeof(T));
     if (smem_bytes > 200 * 1024) return cudaErrorInvalidValue;  // interface too wide for this launch shape
-    static bool attr = false;
-    if (!attr) {
+    once_per_device(reinterpret_cast<const void*>(&k_rrqr_rm<T>), [] {
         cudaFuncSetAttribute(k_rrqr_rm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         cudaFuncSetAttribute(k_rrqr_rm<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        attr = true;
-    }
+    });
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(ntasks * cluster), 1, 1);
     cfg.blockDim = dim3(kRRThreads, 1, 1);

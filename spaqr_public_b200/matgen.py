@@ -252,6 +252,23 @@ def workload(name):
     raise KeyError(name)
 
 
+def diff_batch(count=32, lo=96, hi=256, seed=1004):
+    """The differentiation batch: ``count`` independent 2D advection-diffusion
+    systems built like advdiff2d_128 (|v| = 1000, 8 seeded Fourier modes) with
+    seeded uneven sides in [lo, hi]; system i uses generator seed seed + 7 i,
+    right-hand side N(0, 1) and target x* ~ N(0, 1). Returns a list of dicts
+    as :func:`workload` plus ``xstar``."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(lo, hi + 1, size=count)
+    out = []
+    for i, n in enumerate(sides):
+        n = int(n)
+        A = advdiff2d(n, seed=seed + 7 * i)
+        out.append(dict(A=A, b=rhs_normal(A[0], seed + 7 * i + 1), xstar=rhs_normal(n * n, seed + 7 * i + 2), n=n,
+                        d=2, levels=default_levels(n * n), tol=1e-3, skip=0, res=1e-12))
+    return out
+
+
 def write_mm(path, A):
     m, n, cp, ri, va = A
     nnz = len(va)

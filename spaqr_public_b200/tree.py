@@ -183,6 +183,13 @@ def gmres(A, b, precond, iters=300, restart=None, tol=1e-12, x0=None):
     return x, its.value, res.value
 
 
+def factorize_batch(trees, nthreads=0):
+    """Factorizes independent assembled trees together (spq_factorize_batch):
+    one host thread and CUDA stream per tree, so their launches share the GPU."""
+    arr = (C.c_void_p * len(trees))(*[t._h.value for t in trees])
+    check(lib().spq_factorize_batch(arr, len(trees), int(nthreads)))
+
+
 def gmres_adjoint(A, g, precond, iters=300, restart=None, tol=1e-12, lam0=None):
     """GMRES on A^T lambda = g preconditioned by M^T (the adjoint of ``gmres``).
     A is the factorized matrix (CSC). Returns (lambda, iterations, residual estimate)."""

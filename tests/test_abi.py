@@ -99,3 +99,15 @@ def test_coords_grid_is_linspace_nd():
     from oracle.oracle_py import linspace_nd
     X = linspace_nd(3, 2).reshape(-1, 2)
     assert X[:4].tolist() == [[0, 0], [0, 1], [0, 2], [1, 0]]
+
+
+def test_factorize_batch_argument_checks():
+    L = _abi.lib()
+    h = C.c_void_p()
+    assert L.spq_create(C.byref(h), 4, 0) == 0
+    arr = (C.c_void_p * 2)(h.value, h.value)
+    assert L.spq_factorize_batch(arr, 2, 0) == 2  # not assembled
+    assert b"not assembled" in L.spq_last_error()
+    assert L.spq_factorize_batch(None, 1, 0) == 1
+    assert L.spq_factorize_batch(arr, 0, 0) == 0
+    assert L.spq_destroy(h) == 0
