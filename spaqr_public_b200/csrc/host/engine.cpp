@@ -306,6 +306,7 @@ public:
         cuda_check(cudaMemcpyAsync(d_adj_in_, d_g, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
                    "adjoint in");
         if (!adj_exec_) {
+            if (adj_waves_.empty()) build_adjoint_plan();
             cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
             run_adjoint_sweeps();
             cuda_check(cudaStreamEndCapture(stream_, &adj_graph_), "capture end");
@@ -385,6 +386,20 @@ private:
     int* d_dst_ = nullptr;
     int64_t* d_xin_ = nullptr;
     int64_t* d_xout_pos_ = nullptr;
+    // a sweep op with the x segments it reads and writes (wave scheduling)
+    struct POp {
+        SolveOp op;
+        std::vector<Cluster*> rd, wr;
+        int smem;
+    };
+    struct WMeta {
+        size_t off;
+        int n, smem;
+        double words;
+        int hkind, ha, hb;
+    };
+    std::vector<POp> plan_fwd_, plan_bwd_;  // host copies, kept for the adjoint plan
+    std::vector<int> gemv_cols_;            // columns of every neighbour block (work counts)
     struct Wave {
         const SolveOp* ops;
         int nops, smem;
@@ -664,8 +679,12 @@ private:
     void issue_copies(const CopyDesc<T>* d, const std::vector<CopyDesc<T>>& h) {
         if (h.empty()) return;
         double by = 0;
-        for (auto& c : h) by += (c.src ? 2.0 : 1.0) * c.rows * c.cols * sizeof(T);
-        timed(KF_COPY, 0, by, [&] { launch_copy<T>(d, (int)h.size(), stream_); });
+        int maxc = 0;
+        for (auto& c : h) {
+            by += (c.src ? 2.0 : 1.0) * c.rows * c.cols * sizeof(T);
+            maxc = std::max(maxc, c.cols);
+        }
+        timed(KF_COPY, 0, by, [&] { launch_copy<T>(d, (int)h.size(), maxc, stream_); });
         ++launches_fact_;
     }
 
@@ -1058,9 +1077,12 @@ private:
             Upload u2;
             size_t o_w = u2.add(wb), o_b = u2.add(blocks);
             char* d2 = u2.commit(desc_arena_, stream_, pinned_);
+            int parts = 1;  // CTAs per task: enough for its blocks and its 32-reflector panels
+            for (const auto& x : wb) parts = std::max(parts, std::max(x.nblk, (x.r + kNB - 1) / kNB));
             timed(KF_SPARS_WB, 0, wb_bytes, [&] {
                 launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
-                                      reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), stream_);
+                                      reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), parts,
+                                      stream_);
             });
             ++launches_fact_;
         }
@@ -1165,12 +1187,6 @@ private:
                 xo.push_back(c->xoff + i);
             }
         }
-        // ops with read / write sets
-        struct POp {
-            SolveOp op;
-            std::vector<Cluster*> rd, wr;
-            int smem;
-        };
         std::vector<XSeg> segs;
         std::vector<GemvRef<T>> gemv;
         std::vector<POp> fwd, bwd;
@@ -1246,12 +1262,100 @@ private:
             bwd.push_back(std::move(b));
         }
         std::reverse(bwd.begin(), bwd.end());
-        // Adjoint sweeps. One application is M = B_0 ... B_{n-1} F_{n-1} ... F_0
-        // (F forward ops in tape order, then the backward ops in reverse), so
-        // M^T applies B_0^T ... B_{n-1}^T and then F_{n-1}^T ... F_0^T: Q^T and
-        // Q swap, R^{-1} (x - A12 x_n) becomes R^{-T} with x_n -= A12^T z, and
-        // the index maps of SplitD and Merge become their transposes. Every
-        // transposed op reads and writes all the segments it touches.
+        gemv_cols_.clear();
+        for (auto& g : gemv) gemv_cols_.push_back(g.s);
+        std::vector<std::vector<int>> fw, bw;
+        schedule_ops(fwd, fw);
+        schedule_ops(bwd, bw);
+        std::vector<SolveOp> all;
+        std::vector<WMeta> fm, bm;
+        pack_waves(fwd, fw, all, fm);
+        pack_waves(bwd, bw, all, bm);
+        Upload up;
+        size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
+               o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
+        const SolveOp* d_ops = reinterpret_cast<const SolveOp*>(d + o_ops);
+        d_segs_ = reinterpret_cast<const XSeg*>(d + o_segs);
+        d_gemv_ = reinterpret_cast<const GemvRef<T>*>(d + o_gemv);
+        d_src_ = reinterpret_cast<int*>(d + o_src);
+        d_dst_ = reinterpret_cast<int*>(d + o_dst);
+        d_xin_ = reinterpret_cast<int64_t*>(d + o_xin);
+        d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
+        fwd_waves_.clear();
+        bwd_waves_.clear();
+        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        adj_waves_.clear();  // built on the first adjoint solve
+        plan_fwd_ = std::move(fwd);
+        plan_bwd_ = std::move(bwd);
+        nin_ = (int)src.size();
+        nout_ = (int)dst.size();
+        // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
+        // right-hand side and solution vectors
+        solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 8.0 * (nrows_ + ncols_);
+        const size_t smem_cap = (200 * 1024) / sizeof(T);
+        for (auto* ws : {&fwd_waves_, &bwd_waves_})
+            for (auto& w : *ws)
+                if ((size_t)w.smem > smem_cap)
+                    throw std::runtime_error("solve: a cluster exceeds the shared-memory vector capacity");
+    }
+    int nin_ = 0, nout_ = 0;
+
+    // Wave scheduling on x segments (RAW, WAR, WAW): an op runs one wave after
+    // the last op that wrote a segment it touches, or read one it writes.
+    void schedule_ops(const std::vector<POp>& ops, std::vector<std::vector<int>>& waves) const {
+        std::vector<int> lw(max_order_, -1), lr(max_order_, -1);  // by cluster order
+        std::vector<int> wv(ops.size());
+        int nw = 0;
+        for (size_t i = 0; i < ops.size(); ++i) {
+            int w = 0;
+            for (Cluster* c : ops[i].rd) w = std::max(w, lw[c->order] + 1);
+            for (Cluster* c : ops[i].wr) w = std::max(w, std::max(lw[c->order], lr[c->order]) + 1);
+            for (Cluster* c : ops[i].wr) lw[c->order] = w;
+            for (Cluster* c : ops[i].rd) lr[c->order] = std::max(lr[c->order], w);
+            wv[i] = w;
+            nw = std::max(nw, w + 1);
+        }
+        waves.assign(nw, {});
+        for (size_t i = 0; i < ops.size(); ++i) waves[wv[i]].push_back((int)i);
+    }
+    double op_words(const SolveOp& o) const {
+        if (o.kind == SK_APPLYQ) return (double)o.a * o.b - 0.5 * (double)o.b * (o.b - 1);
+        if (o.kind != SK_TRI) return 0.0;
+        double w = 0.5 * (double)o.a * (o.a + 1);
+        for (int q = 0; q < o.nseg; ++q) w += (double)o.a * gemv_cols_[o.seg0 + q];
+        return w;
+    }
+    void pack_waves(const std::vector<POp>& ops, const std::vector<std::vector<int>>& waves,
+                    std::vector<SolveOp>& all, std::vector<WMeta>& meta) const {
+        for (auto& w : waves) {
+            WMeta mt{all.size(), (int)w.size(), 0, 0.0, -1, 0, 0};
+            double hw = -1;
+            for (int i : w) {
+                all.push_back(ops[i].op);
+                mt.smem = std::max(mt.smem, ops[i].smem);
+                const double ow = op_words(ops[i].op);
+                mt.words += ow;
+                if (ow > hw) {
+                    hw = ow;
+                    mt.hkind = ops[i].op.kind;
+                    mt.ha = ops[i].op.a;
+                    mt.hb = ops[i].op.kind == SK_TRI ? ops[i].op.nseg : ops[i].op.b;
+                }
+            }
+            meta.push_back(mt);
+        }
+    }
+
+    // Adjoint sweeps, built on the first adjoint solve. One application is
+    // M = B_0 ... B_{n-1} F_{n-1} ... F_0 (F forward ops in tape order, then the
+    // backward ops in reverse), so M^T applies B_0^T ... B_{n-1}^T and then
+    // F_{n-1}^T ... F_0^T: Q^T and Q swap, R^{-1} (x - A12 x_n) becomes R^{-T}
+    // with x_n -= A12^T z, and the index maps of SplitD and Merge become their
+    // transposes. Every transposed op reads and writes all the segments it
+    // touches.
+    void build_adjoint_plan() {
         auto transpose_op = [](const POp& o) {
             POp t = o;
             std::vector<Cluster*> touch = o.rd;
@@ -1277,103 +1381,28 @@ private:
             return t;
         };
         std::vector<POp> adj;
-        for (auto it = bwd.rbegin(); it != bwd.rend(); ++it) adj.push_back(transpose_op(*it));
-        for (auto it = fwd.rbegin(); it != fwd.rend(); ++it) adj.push_back(transpose_op(*it));
-        // wave scheduling on x segments (RAW, WAR, WAW)
-        auto schedule = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves) {
-            std::map<const Cluster*, int> lw, lr;
-            std::vector<int> wv(ops.size());
-            int nw = 0;
-            for (size_t i = 0; i < ops.size(); ++i) {
-                int w = 0;
-                for (Cluster* c : ops[i].rd) {
-                    auto it = lw.find(c);
-                    if (it != lw.end()) w = std::max(w, it->second + 1);
-                }
-                for (Cluster* c : ops[i].wr) {
-                    auto it = lw.find(c);
-                    if (it != lw.end()) w = std::max(w, it->second + 1);
-                    auto ir = lr.find(c);
-                    if (ir != lr.end()) w = std::max(w, ir->second + 1);
-                }
-                for (Cluster* c : ops[i].wr) lw[c] = w;
-                for (Cluster* c : ops[i].rd) lr[c] = std::max(lr.count(c) ? lr[c] : -1, w);
-                wv[i] = w;
-                nw = std::max(nw, w + 1);
-            }
-            waves.assign(nw, {});
-            for (size_t i = 0; i < ops.size(); ++i) waves[wv[i]].push_back((int)i);
-        };
-        std::vector<std::vector<int>> fw, bw, aw;
-        schedule(fwd, fw);
-        schedule(bwd, bw);
-        schedule(adj, aw);
+        adj.reserve(plan_fwd_.size() + plan_bwd_.size());
+        for (auto it = plan_bwd_.rbegin(); it != plan_bwd_.rend(); ++it) adj.push_back(transpose_op(*it));
+        for (auto it = plan_fwd_.rbegin(); it != plan_fwd_.rend(); ++it) adj.push_back(transpose_op(*it));
+        std::vector<std::vector<int>> aw;
+        schedule_ops(adj, aw);
         std::vector<SolveOp> all;
-        struct WMeta {
-            size_t off;
-            int n, smem;
-            double words;
-            int hkind, ha, hb;
-        };
-        std::vector<WMeta> fm, bm, am;
-        auto op_words = [&](const SolveOp& o) -> double {
-            if (o.kind == SK_APPLYQ) return (double)o.a * o.b - 0.5 * (double)o.b * (o.b - 1);
-            if (o.kind != SK_TRI) return 0.0;
-            double w = 0.5 * (double)o.a * (o.a + 1);
-            for (int q = 0; q < o.nseg; ++q) w += (double)o.a * gemv[o.seg0 + q].s;
-            return w;
-        };
-        auto pack = [&](std::vector<POp>& ops, std::vector<std::vector<int>>& waves, std::vector<WMeta>& meta) {
-            for (auto& w : waves) {
-                WMeta mt{all.size(), (int)w.size(), 0, 0.0, -1, 0, 0};
-                double hw = -1;
-                for (int i : w) {
-                    all.push_back(ops[i].op);
-                    mt.smem = std::max(mt.smem, ops[i].smem);
-                    const double ow = op_words(ops[i].op);
-                    mt.words += ow;
-                    if (ow > hw) {
-                        hw = ow;
-                        mt.hkind = ops[i].op.kind;
-                        mt.ha = ops[i].op.a;
-                        mt.hb = ops[i].op.kind == SK_TRI ? ops[i].op.nseg : ops[i].op.b;
-                    }
-                }
-                meta.push_back(mt);
-            }
-        };
-        pack(fwd, fw, fm);
-        pack(bwd, bw, bm);
-        pack(adj, aw, am);
+        std::vector<WMeta> am;
+        pack_waves(adj, aw, all, am);
         Upload up;
-        size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
-               o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
+        const size_t o_ops = up.add(all);
         char* d = up.commit(desc_arena_, stream_, pinned_);
         const SolveOp* d_ops = reinterpret_cast<const SolveOp*>(d + o_ops);
-        d_segs_ = reinterpret_cast<const XSeg*>(d + o_segs);
-        d_gemv_ = reinterpret_cast<const GemvRef<T>*>(d + o_gemv);
-        d_src_ = reinterpret_cast<int*>(d + o_src);
-        d_dst_ = reinterpret_cast<int*>(d + o_dst);
-        d_xin_ = reinterpret_cast<int64_t*>(d + o_xin);
-        d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
-        fwd_waves_.clear();
-        bwd_waves_.clear();
-        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
-        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
         adj_waves_.clear();
-        for (auto& mt : am) adj_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
-        nin_ = (int)src.size();
-        nout_ = (int)dst.size();
-        // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
-        // right-hand side and solution vectors
-        solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 8.0 * (nrows_ + ncols_);
         const size_t smem_cap = (200 * 1024) / sizeof(T);
-        for (auto* ws : {&fwd_waves_, &bwd_waves_, &adj_waves_})
-            for (auto& w : *ws)
-                if ((size_t)w.smem > smem_cap)
-                    throw std::runtime_error("solve: a cluster exceeds the shared-memory vector capacity");
+        for (auto& mt : am) {
+            if ((size_t)mt.smem > smem_cap)
+                throw std::runtime_error("adjoint solve: a cluster exceeds the shared-memory vector capacity");
+            adj_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        }
+        cuda_check(cudaStreamSynchronize(stream_), "adjoint plan upload");
+        pinned_.reset();
     }
-    int nin_ = 0, nout_ = 0;
 
 public:
     bool solve_ready() const override { return graph_exec_ != nullptr; }

@@ -9,6 +9,7 @@
 // calls up to rounding.
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <mutex>
@@ -114,21 +115,58 @@ __device__ void build_tfac(const T* Vp, int ldv, int R, int w, const T* taus, T*
 }
 
 // ------------------------------------------------------------------ copies
+// CTA (d, y) copies 32-column chunks y, y + gridDim.y, ... of descriptor d.
+// Modes 0/1 (plain / identity): each warp owns columns of the chunk, lanes
+// walk the rows (coalesced on both sides). Mode 2 (dst = src^T): 32 x 32
+// tiles through shared memory, so reads run along src columns and writes
+// along dst columns.
 template <class T>
-__global__ void k_copy(const CopyDesc<T>* descs, int n) {
+__global__ void __launch_bounds__(256) k_copy(const CopyDesc<T>* descs, int n) {
+    __shared__ T tile[32][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int d = blockIdx.x; d < n; d += gridDim.x) {
         const CopyDesc<T> c = descs[d];
-        const int64_t tot = (int64_t)c.rows * c.cols;
-        for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
-            int i = (int)(e % c.rows), j = (int)(e / c.rows);
+        for (int j0 = blockIdx.y * 32; j0 < c.cols; j0 += gridDim.y * 32) {
             if (c.mode == 2) {
-                c.dst[j + (size_t)i * c.dld] = c.src[i + (size_t)j * c.sld];
+                for (int i0 = 0; i0 < c.rows; i0 += 32) {
+                    const int i = i0 + lane;
+#pragma unroll
+                    for (int jj = warp; jj < 32; jj += 8) {
+                        const int j = j0 + jj;
+                        tile[jj][lane] = (i < c.rows && j < c.cols) ? c.src[i + (size_t)j * c.sld] : T(0);
+                    }
+                    __syncthreads();
+                    const int j = j0 + lane;
+#pragma unroll
+                    for (int ii = warp; ii < 32; ii += 8) {
+                        const int r = i0 + ii;
+                        if (r < c.rows && j < c.cols) c.dst[j + (size_t)r * c.dld] = tile[lane][ii];
+                    }
+                    __syncthreads();
+                }
                 continue;
             }
-            T v;
-            if (c.mode == 1) v = (i == j) ? T(1) : T(0);
-            else v = c.src ? c.src[i + (size_t)j * c.sld] : T(0);
-            c.dst[i + (size_t)j * c.dld] = v;
+            for (int jj = warp; jj < 32; jj += 8) {
+                const int j = j0 + jj;
+                if (j >= c.cols) break;
+                T* dcol = c.dst + (size_t)j * c.dld;
+                if (c.mode == 1) {
+                    for (int i = lane; i < c.rows; i += 32) dcol[i] = (i == j) ? T(1) : T(0);
+                } else if (!c.src) {
+                    for (int i = lane; i < c.rows; i += 32) dcol[i] = T(0);
+                } else {
+                    const T* scol = c.src + (size_t)j * c.sld;
+                    int i = lane;
+                    for (; i + 96 < c.rows; i += 128) {
+                        const T a = scol[i], b = scol[i + 32], e = scol[i + 64], f = scol[i + 96];
+                        dcol[i] = a;
+                        dcol[i + 32] = b;
+                        dcol[i + 64] = e;
+                        dcol[i + 96] = f;
+                    }
+                    for (; i < c.rows; i += 32) dcol[i] = scol[i];
+                }
+            }
         }
     }
 }
@@ -895,9 +933,10 @@ size_t trailing_smem() {
 
 // ------------------------------------------------------------------ launchers
 template <class T>
-void launch_copy(const CopyDesc<T>* d, int n, cudaStream_t s) {
+void launch_copy(const CopyDesc<T>* d, int n, int max_cols, cudaStream_t s) {
     if (n <= 0) return;
-    k_copy<T><<<n < 65535 ? n : 65535, 256, 0, s>>>(d, n);
+    const int chunks = std::max(1, std::min(32, (max_cols + 31) / 32));
+    k_copy<T><<<dim3(n < 65535 ? n : 65535, chunks), 256, 0, s>>>(d, n);
 }
 
 template <class T>
@@ -988,7 +1027,7 @@ void prepare_kernels() {
 }
 
 #define SPQ_INST(T)                                                                                           \
-    template void launch_copy<T>(const CopyDesc<T>*, int, cudaStream_t);                                      \
+    template void launch_copy<T>(const CopyDesc<T>*, int, int, cudaStream_t);                                 \
     template void launch_panel<T>(const QRTask<T>*, const int*, int, int, int, cudaStream_t);                 \
     template void launch_trailing<T>(const QRTask<T>*, const TileRef*, int, int, cudaStream_t);               \
     template void launch_trsm<T>(const TrsmTask<T>*, const TileRef*, int, cudaStream_t);                      \

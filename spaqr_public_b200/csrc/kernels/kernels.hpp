@@ -27,8 +27,9 @@ struct CopyDesc {
 // such as function attributes.
 void once_per_device(const void* key, void (*setup)());
 
+// Batched copies; max_cols = the widest descriptor (sets the column-chunk grid).
 template <class T>
-void launch_copy(const CopyDesc<T>* d, int n, cudaStream_t s);
+void launch_copy(const CopyDesc<T>* d, int n, int max_cols, cudaStream_t s);
 
 // ---------------------------------------------------------------- Householder QR
 // A task factors the first k columns of the m x (k + ntr) matrix [fac | tr]
@@ -107,8 +108,9 @@ struct SparsWBRM {
     T* tp;   // panel T factors of V
     int m, ldc, r, nblk, blk0, pad;
 };
+// parts: CTAs per task (blocks, V column groups and T panels are spread over them)
 template <class T>
-void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s);
+void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, int parts, cudaStream_t s);
 
 // ---------------------------------------------------------------- assembly
 // *(T*)dst_addr[e] = (T) vals[e]

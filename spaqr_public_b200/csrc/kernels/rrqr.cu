@@ -398,56 +398,100 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
 
 // Write-back of a sparsified interface (sparsifyD, src/tree.cpp:1082-1110):
 // Crank = R(0:r, :) un-permuted: Crank(i, c) = C(i, c) if i <= pos[c] else 0.
+// CTA (task, y) of a (tasks x ny) grid takes the blocks b = y mod ny, the
+// 32-column groups of V and the T panels with index = y mod ny. Row-major C
+// is transposed into column-major blocks and V through 32 x 32 shared tiles;
+// each panel's Gram matrix V_p^T V_p is accumulated over staged row tiles and
+// turned into the panel's T factor (LAPACK dlarft, forward, columnwise).
 template <class T>
 __global__ void __launch_bounds__(256) k_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks) {
-    __shared__ T G[kNB * (kNB + 1)];
-    __shared__ T Ts[kNB * (kNB + 1)];
+    constexpr int P = kNB + 1;
+    __shared__ T G[kNB * P];
+    __shared__ T Ts[kNB * P];
+    __shared__ T tile[32][33];
     __shared__ T s_tau[kNB];
+    __shared__ int s_col[32];
     const SparsWBRM<T> t = tasks[blockIdx.x];
-    const int r = t.r, m = t.m;
+    const int r = t.r, m = t.m, ny = gridDim.y, y = blockIdx.y;
     const size_t ld = (size_t)t.ldc;
-    const int tid = threadIdx.x;
-    for (int b = 0; b < t.nblk; ++b) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    // 1. interface blocks
+    for (int b = y; b < t.nblk; b += ny) {
         const SpBlock<T> B = blocks[t.blk0 + b];
-        if (B.kind == 0) {  // column block A(n2, c): rows x r
-            const int64_t tot = (int64_t)B.rows * r;
-            for (int64_t e = tid; e < tot; e += blockDim.x) {
-                const int i = (int)(e % B.rows), j = (int)(e / B.rows);
-                const int c = B.coff + i;
-                B.p[i + (size_t)j * B.ld] = (j <= t.pos[c]) ? t.C[j * ld + c] : T(0);
+        if (B.kind == 0) {  // column block A(n2, c): rows x r, element (i, j) = Crank(j, coff + i)
+            for (int j = warp; j < r; j += nw) {
+                T* dcol = B.p + (size_t)j * B.ld;
+                const T* crow = t.C + (size_t)j * ld + B.coff;
+                for (int i = lane; i < B.rows; i += 32) dcol[i] = (j <= t.pos[B.coff + i]) ? crow[i] : T(0);
             }
-        } else {  // row block A(c, n1): r x cols
-            const int64_t tot = (int64_t)r * B.cols;
-            for (int64_t e = tid; e < tot; e += blockDim.x) {
-                const int j = (int)(e % B.cols), i = (int)(e / B.cols);
-                const int c = B.coff + j;
-                B.p[i + (size_t)j * B.ld] = (i <= t.pos[c]) ? t.C[i * ld + c] : T(0);
+        } else {  // row block A(c, n1): r x cols, element (i, j) = Crank(i, coff + j)
+            for (int j0 = 0; j0 < B.cols; j0 += 32) {
+                for (int i0 = 0; i0 < r; i0 += 32) {
+                    const int j = j0 + lane;
+                    const int pc = j < B.cols ? t.pos[B.coff + j] : -1;
+                    for (int ii = warp; ii < 32; ii += nw) {
+                        const int i = i0 + ii;
+                        tile[ii][lane] = (i < r && i <= pc) ? t.C[(size_t)i * ld + B.coff + j] : T(0);
+                    }
+                    __syncthreads();
+                    for (int jj = warp; jj < 32; jj += nw) {
+                        const int jc = j0 + jj, i = i0 + lane;
+                        if (jc < B.cols && i < r) B.p[i + (size_t)jc * B.ld] = tile[lane][jj];
+                    }
+                    __syncthreads();
+                }
             }
         }
     }
-    // V(:, q) = column colat[q] (reflector below the diagonal), tau
-    for (int64_t e = tid; e < (int64_t)m * r; e += blockDim.x) {
-        const int i = (int)(e % m), q = (int)(e / m);
-        t.V[e] = t.C[i * ld + t.colat[q]];
-    }
-    for (int q = tid; q < r; q += blockDim.x) t.tau[q] = t.tau_in[q];
-    __syncthreads();
-    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    constexpr int P = kNB + 1;
-    for (int p0 = 0; p0 < r; p0 += kNB) {
-        const int w = min(kNB, r - p0);
-        const T* Vp = t.V + p0 + (size_t)p0 * m;
-        const int R = m - p0;
-        if (tid < kNB) s_tau[tid] = tid < w ? t.tau_in[p0 + tid] : T(0);
-        int pair = 0;
-        for (int j = 1; j < w; ++j)
-            for (int i = 0; i < j; ++i, ++pair) {
-                if ((pair % nw) != warp) continue;
-                T s = T(0);
-                for (int rr = j + 1 + lane; rr < R; rr += 32) s += Vp[rr + (size_t)i * m] * Vp[rr + (size_t)j * m];
-                s = wsum(s);
-                if (lane == 0) G[i * P + j] = s + (j < R ? Vp[j + (size_t)i * m] : T(0));
+    // 2. V(:, q) = column colat[q] of C (reflector below the diagonal), tau
+    for (int q0 = y * 32; q0 < r; q0 += ny * 32) {
+        if (tid < 32) s_col[tid] = (q0 + tid < r) ? t.colat[q0 + tid] : 0;
+        __syncthreads();
+        for (int i0 = 0; i0 < m; i0 += 32) {
+            for (int ii = warp; ii < 32; ii += nw) {
+                const int i = i0 + ii;
+                tile[ii][lane] = (i < m && q0 + lane < r) ? t.C[(size_t)i * ld + s_col[lane]] : T(0);
             }
+            __syncthreads();
+            for (int qq = warp; qq < 32; qq += nw) {
+                const int q = q0 + qq, i = i0 + lane;
+                if (q < r && i < m) t.V[i + (size_t)q * m] = tile[lane][qq];
+            }
+            __syncthreads();
+        }
+    }
+    if (y == 0)
+        for (int q = tid; q < r; q += blockDim.x) t.tau[q] = t.tau_in[q];
+    // 3. T factor of each 32-reflector panel
+    const int gi = tid & 31, gj = tid >> 5;  // G rows gi, columns gj + 8k
+    for (int pi = y; pi * kNB < r; pi += ny) {
+        const int p0 = pi * kNB;
+        const int w = min(kNB, r - p0);
+        const int R = m - p0;
+        if (tid < kNB) {
+            s_col[tid] = t.colat[p0 + (tid < w ? tid : 0)];
+            s_tau[tid] = tid < w ? t.tau_in[p0 + tid] : T(0);
+        }
+        __syncthreads();
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+        for (int r0 = 0; r0 < R; r0 += 32) {
+            for (int ii = warp; ii < 32; ii += nw) {
+                const int rr = r0 + ii;  // row p0 + rr of the panel; v_q: 1 at rr == q, 0 above
+                T v = T(0);
+                if (rr < R && lane < w) v = rr > lane ? t.C[(size_t)(p0 + rr) * ld + s_col[lane]] : (rr == lane ? T(1) : T(0));
+                tile[ii][lane] = v;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int ii = 0; ii < 32; ++ii) {
+                const T a = tile[ii][gi];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[k] += a * tile[ii][gj + 8 * k];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) G[gi * P + gj + 8 * k] = acc[k];
         __syncthreads();
         if (warp == 0) {
             for (int j = 0; j < kNB; ++j) {
@@ -466,7 +510,7 @@ __global__ void __launch_bounds__(256) k_spars_wb_rm(const SparsWBRM<T>* tasks, 
             }
         }
         __syncthreads();
-        T* Tout = t.tp + (size_t)(p0 / kNB) * kNB * kNB;
+        T* Tout = t.tp + (size_t)pi * kNB * kNB;
         for (int e = tid; e < kNB * kNB; e += blockDim.x) Tout[e] = Ts[(e % kNB) * P + (e / kNB)];
         __syncthreads();
     }
@@ -505,15 +549,17 @@ cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntask
 }
 
 template <class T>
-void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, cudaStream_t s) {
+void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, int parts, cudaStream_t s) {
     if (ntasks <= 0) return;
-    k_spars_wb_rm<T><<<ntasks, 256, 0, s>>>(tasks, blocks);
+    const int ny = parts < 1 ? 1 : (parts > 32 ? 32 : parts);
+    k_spars_wb_rm<T><<<dim3(ntasks, ny), 256, 0, s>>>(tasks, blocks);
 }
 
 template cudaError_t launch_rrqr_rm<double>(const RRQRTaskRM<double>*, const int*, int, int, int, int,
                                             cudaStream_t);
 template cudaError_t launch_rrqr_rm<float>(const RRQRTaskRM<float>*, const int*, int, int, int, int, cudaStream_t);
-template void launch_spars_wb_rm<double>(const SparsWBRM<double>*, const SpBlock<double>*, int, cudaStream_t);
-template void launch_spars_wb_rm<float>(const SparsWBRM<float>*, const SpBlock<float>*, int, cudaStream_t);
+template void launch_spars_wb_rm<double>(const SparsWBRM<double>*, const SpBlock<double>*, int, int,
+                                          cudaStream_t);
+template void launch_spars_wb_rm<float>(const SparsWBRM<float>*, const SpBlock<float>*, int, int, cudaStream_t);
 
 }  // namespace spq
