@@ -82,7 +82,9 @@ int spq_factorize(spq_tree* t);
 int spq_factorize_batch(spq_tree* const* ts, int n, int nthreads);
 
 /* Preconditioner applies on HOST buffers (b of length m for solve, n for
- * solve_nrml; x of length n). */
+ * solve_nrml; x of length n). spq_solve needs a square factorization
+ * (spq_set_square(t, 1)); spq_solve_nrml, M_n ~ (A^T A)^{-1}, a least-squares
+ * one (square matching off; include/tree.h:147). */
 int spq_solve(spq_tree* t, const double* b, double* x);
 int spq_solve_nrml(spq_tree* t, const double* b, double* x);
 /* Same on DEVICE buffers (FP64, on the handle's device). */
@@ -95,9 +97,17 @@ int spq_solve_nrml_dev(spq_tree* t, const double* d_b, double* d_x);
  * *res = last preconditioned residual estimate |w(k)|/|r0|. */
 int spq_gmres(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
               const double* b, double* x, int iters, int restart, double tol, int* its, double* res);
-/* Preconditioned CGLS on the normal equations (src/is.cpp:274-345). */
+/* Preconditioned CGLS on the normal equations (src/is.cpp:274-345) for a
+ * least-squares factorization (square matching off, m >= n): preconditioner
+ * spq_solve_nrml. x holds the initial guess; *its = iterations, *res =
+ * ||A^T (b - A x)|| / ||A^T b||. */
 int spq_cgls(spq_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val,
              const double* b, double* x, int iters, double tol, int* its, double* res);
+/* Same with device inputs: A as device CSR (m rows) and A^T as device CSR (n
+ * rows; the CSC arrays of A), b (m) and x (n) device vectors. */
+int spq_cgls_dev(spq_tree* t, int m, int n, const int* d_rowptr, const int* d_colind, const double* d_val,
+                 const int* d_rowptr_t, const int* d_colind_t, const double* d_val_t, const double* d_b, double* d_x,
+                 int iters, double tol, int* its, double* res);
 
 /* Time-to-residual driver (the benchmark's metric): iterative refinement on
  * the true residual. Each correction solves A d = b - A x (residual in FP64)

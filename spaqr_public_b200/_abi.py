@@ -55,6 +55,7 @@ SIGNATURES = {
     "spq_solve_nrml_dev": (_i, [_p, _p, _p]),
     "spq_gmres": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _i, _i, _d, _ip, _dp]),
     "spq_cgls": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _i, _d, _ip, _dp]),
+    "spq_cgls_dev": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _d, _ip, _dp]),
     "spq_get_perm": (_i, [_p, _ip, _ip]),
     "spq_log_size": (_i, [_p, _llp]),
     "spq_get_log": (_i, [_p, _llp]),

@@ -399,13 +399,34 @@ int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* cp, const int* ri, c
     });
 }
 
-int spq_solve_nrml(spq_tree* t, const double*, double*) {
+int spq_solve_nrml_dev(spq_tree* t, const double* d_b, double* d_x) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
-    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (solve_nrml) is not supported by this build");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve_nrml before factorize");
+    if (!d_b || !d_x) return fail(SPQ_ERR_ARG, "null vector");
+    return guard_on(t, [&] {
+        t->eng->solve_nrml_dev(d_b, d_x);
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "solve_nrml");
+        return SPQ_OK;
+    });
 }
-int spq_solve_nrml_dev(spq_tree* t, const double*, double*) {
+int spq_solve_nrml(spq_tree* t, const double* b, double* x) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
-    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (solve_nrml) is not supported by this build");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "solve_nrml before factorize");
+    if (!b || !x) return fail(SPQ_ERR_ARG, "null vector");
+    return guard_on(t, [&] {
+        const int n = t->eng->ncols();
+        cudaStream_t s = t->eng->stream();
+        double *db = nullptr, *dx = nullptr;
+        cuda_check(cudaMalloc(&db, sizeof(double) * n), "solve_nrml alloc");
+        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "solve_nrml alloc");
+        cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s), "solve_nrml h2d");
+        t->eng->solve_nrml_dev(db, dx);
+        cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "solve_nrml d2h");
+        cuda_check(cudaStreamSynchronize(s), "solve_nrml");
+        cudaFree(db);
+        cudaFree(dx);
+        return SPQ_OK;
+    });
 }
 
 int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va, const double* b, double* x,
@@ -603,10 +624,73 @@ int spq_get_stream(spq_tree* t, void** stream) {
     return SPQ_OK;
 }
 
-int spq_cgls(spq_tree* t, int, int, const int*, const int*, const double*, const double*, double*, int, double, int*,
-             double*) {
+int spq_cgls_dev(spq_tree* t, int m, int n, const int* rp, const int* ci, const double* va, const int* rp_t,
+                 const int* ci_t, const double* va_t, const double* d_b, double* d_x, int iters, double tol, int* its,
+                 double* res) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
-    return fail(SPQ_ERR_UNSUPPORTED, "least-squares (CGLS) is not supported by this build");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "cgls before factorize");
+    if (!t->eng->least_squares())
+        return fail(SPQ_ERR_STATE, "cgls needs a least-squares factorization (square matching off)");
+    if (m != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "cgls needs the factorized matrix");
+    if (!rp || !ci || !va || !rp_t || !ci_t || !va_t || !d_b || !d_x || !its || !res || iters < 0)
+        return fail(SPQ_ERR_ARG, "invalid cgls arguments");
+    return guard_on(t, [&] {
+        DevCsr A, At;
+        A.m = m;
+        A.n = n;
+        A.rp = rp;
+        A.ci = ci;
+        A.v = va;
+        At.m = n;
+        At.n = m;
+        At.rp = rp_t;
+        At.ci = ci_t;
+        At.v = va_t;
+        long long l = 0;
+        *its = cgls_device(*t->eng, A, At, d_b, d_x, iters, tol, res, &l);
+        t->launches_krylov += l;
+        cuda_check(cudaStreamSynchronize(t->eng->stream()), "cgls");
+        return SPQ_OK;
+    });
+}
+
+int spq_cgls(spq_tree* t, int m, int n, const int* cp, const int* ri, const double* va, const double* b, double* x,
+             int iters, double tol, int* its, double* res) {
+    if (!t) return fail(SPQ_ERR_ARG, "null handle");
+    if (t->state != 3) return fail(SPQ_ERR_STATE, "cgls before factorize");
+    if (m != t->eng->nrows() || n != t->eng->ncols()) return fail(SPQ_ERR_ARG, "cgls needs the factorized matrix");
+    int rc = check_csc(m, n, cp, ri, va);
+    if (rc) return rc;
+    if (!b || !x || !its || !res || iters < 0) return fail(SPQ_ERR_ARG, "invalid cgls arguments");
+    if (!t->eng->least_squares())
+        return fail(SPQ_ERR_STATE, "cgls needs a least-squares factorization (square matching off)");
+    return guard_on(t, [&]() -> int {
+        cudaStream_t s = t->eng->stream();
+        DevCsrOwned o, ot;
+        DevCsr A;
+        upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
+        // the CSC arrays of A are the CSR arrays of A^T
+        const size_t nnz = (size_t)cp[n];
+        cuda_check(cudaMalloc(&ot.rp, sizeof(int) * (n + 1)), "csr alloc");
+        cuda_check(cudaMalloc(&ot.ci, sizeof(int) * std::max<size_t>(nnz, 1)), "csr alloc");
+        cuda_check(cudaMalloc(&ot.v, sizeof(double) * std::max<size_t>(nnz, 1)), "csr alloc");
+        cuda_check(cudaMemcpyAsync(ot.rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(ot.ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(ot.v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        double *db = nullptr, *dx = nullptr;
+        cuda_check(cudaMalloc(&db, sizeof(double) * m), "cgls alloc");
+        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "cgls alloc");
+        cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "cgls h2d");
+        cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "cgls h2d");
+        const int r2 = spq_cgls_dev(t, m, n, A.rp, A.ci, A.v, ot.rp, ot.ci, ot.v, db, dx, iters, tol, its, res);
+        if (r2 == SPQ_OK) {
+            cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "cgls d2h");
+            cuda_check(cudaStreamSynchronize(s), "cgls");
+        }
+        cudaFree(db);
+        cudaFree(dx);
+        return r2;
+    });
 }
 
 int spq_get_perm(spq_tree* t, int* cperm, int* rperm) {

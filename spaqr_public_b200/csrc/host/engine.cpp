@@ -71,7 +71,7 @@ public:
         int64_t xoff = -1;
         int level() const { return id.self.lvl; }
     };
-    enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE };
+    enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE, TK_REASSIGN };
     struct A12 {
         const T* B;
         int ld, s;
@@ -87,6 +87,7 @@ public:
         std::vector<std::pair<Cluster*, int>> segs;
         std::vector<A12> a12;
         int crows = 0, ccols = 0, rank = 0;
+        std::vector<int> idx;  // TK_REASSIGN: positions in c's segment; f = destination, m = its start
     };
 
     // The host symbolic steps (partition) need no GPU; the device is opened by
@@ -99,6 +100,8 @@ public:
         if (graph_) cudaGraphDestroy(graph_);
         if (adj_exec_) cudaGraphExecDestroy(adj_exec_);
         if (adj_graph_) cudaGraphDestroy(adj_graph_);
+        if (nrml_exec_) cudaGraphExecDestroy(nrml_exec_);
+        if (nrml_graph_) cudaGraphDestroy(nrml_graph_);
         for (auto& e : events_) cudaEventDestroy(e);
         cudaStreamSynchronize(stream_);
         arena_.release();
@@ -130,13 +133,12 @@ public:
     void partition(const Csc& A) override {
         double t0 = wall();
         if (cfg_.X.empty()) throw std::invalid_argument("only the geometric partition is built: set coordinates");
-        if (A.m != A.n && !cfg_.square) {
-            // rectangular input is recognised but its row-shift path is not built here
-        }
-        if (A.m != A.n) throw std::invalid_argument("rectangular input (least squares) is not supported by this build");
+        if (A.m < A.n) throw std::invalid_argument("need rows >= cols");
+        if (cfg_.square && A.m != A.n) throw std::invalid_argument("square (identity matching) needs m == n");
         nrows_ = A.m;
         ncols_ = A.n;
-        Ordering o = geometric_ordering(A, cfg_.nlevels, cfg_.d, cfg_.X);
+        rect_ = !cfg_.square;
+        Ordering o = geometric_ordering(A, cfg_.nlevels, cfg_.d, cfg_.X, cfg_.square != 0);
         cperm_ = o.cperm;
         rperm_ = o.rperm;
         const int c = A.n;
@@ -254,10 +256,12 @@ public:
             cudaEventRecord(ev[1], stream_);
             elim_phase();
             cudaEventRecord(ev[2], stream_);
+            if (rect_ && ilvl_ < L - 1) reassign_phase();
             cudaEventRecord(ev[3], stream_);  // shift (rectangular only)
             const bool window = ilvl_ < L - 2 && ilvl_ >= cfg_.skip && cfg_.tol != 0;
             if (cfg_.scale && window) scale_phase();
             cudaEventRecord(ev[4], stream_);
+            if (rect_ && cfg_.scale && window) extra_phase();
             if (window) sparsify_phase();
             cudaEventRecord(ev[5], stream_);
             if (ilvl_ < L - 1) merge_all();
@@ -284,6 +288,7 @@ public:
     // ------------------------------------------------------------- solve
     void solve_dev(const double* d_b, double* d_x) override {
         if (!factorized_) throw std::logic_error("solve before factorize");
+        if (rect_) throw std::invalid_argument("least-squares factorization: use solve_nrml / cgls");
         double t0 = wall();
         cuda_check(cudaMemcpyAsync(d_bin_, d_b, sizeof(double) * nrows_, cudaMemcpyDeviceToDevice, stream_), "solve in");
         if (!graph_exec_) {
@@ -302,6 +307,7 @@ public:
     // y = M^T g: the factors applied transposed (adjoint sweeps, own graph).
     void solve_adjoint_dev(const double* d_g, double* d_y) override {
         if (!factorized_) throw std::logic_error("adjoint solve before factorize");
+        if (rect_) throw std::invalid_argument("least-squares factorization: the adjoint solve needs a square one");
         double t0 = wall();
         cuda_check(cudaMemcpyAsync(d_adj_in_, d_g, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
                    "adjoint in");
@@ -371,6 +377,7 @@ private:
     std::vector<std::unique_ptr<Edge>> edges_;
     std::vector<TapeOp> tape_;
     std::vector<int> cperm_, rperm_;
+    bool rect_ = false;  // least squares (no identity row matching): rows move, R^T R solves
     int nrows_ = 0, ncols_ = 0, ilvl_ = -1, cur_bottom_ = 0, max_order_ = 0, next_uid_ = 0;
     bool assembled_ = false, factorized_ = false;
     unsigned long long nnzA_ = 0, nnzR_ = 0, nnzH_ = 0, nnzQ_ = 0;
@@ -755,6 +762,14 @@ private:
             for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
             tape_.push_back(std::move(op));
             c->elim = true;
+            if (rect_) {  // least squares keeps R only: the self block shrinks to k rows, the rest goes
+                for (Edge* e : c->out) {
+                    if (e->n2 == c)
+                        e->A.rows = std::min(e->A.rows, k);
+                    else
+                        e->live = false;
+                }
+            }
             rec(1, m, k, nupd, (long long)H.size(), co, c->order);
             tasks.push_back(std::move(t));
         }
@@ -925,35 +940,30 @@ private:
         }
     }
 
-    template <class Job>
-    void run_sparsify_wave(std::vector<Job>& jobs, size_t celems, size_t ielems,
-                           std::vector<std::vector<long long>>& recs) {
+    // Gathers every job's interface into a row-major C in the wave scratch (row
+    // stride j.ld, rows j.m, columns j.n; gather(job, C, descriptors) lists the
+    // copies), runs the cluster RRQR on all of them (one launch per cluster
+    // size; larger interfaces get more CTAs) and reads the ranks back. rt
+    // receives the device task descriptors (C, positions, tau) for the
+    // write-back.
+    template <class Job, class Gather>
+    std::vector<int> rrqr_batch(std::vector<Job>& jobs, size_t celems, size_t ielems, std::vector<RRQRTaskRM<T>>& rt,
+                                Gather&& gather) {
         const size_t ibytes = (((ielems + jobs.size()) * sizeof(int)) + 255) & ~size_t(255);
         char* base = static_cast<char*>(scratch_.get(ibytes + celems * sizeof(T), stream_));
         int* ib = reinterpret_cast<int*>(base);
         T* cb = reinterpret_cast<T*>(base + ibytes);
         std::vector<CopyDesc<T>> g;
-        std::vector<RRQRTaskRM<T>> rt;
+        rt.clear();
         for (auto& j : jobs) {
-            // C is row-major (row stride ld): C(i, cur + r) = A_mp(r, i), C(i, smp + c) = A_pm(i, c)
             T* C = cb + j.c_off;
-            const int ld = j.ld;
-            int cur = 0;
-            for (Edge* e : j.amp) {
-                g.push_back(cp(e->A.p, C + cur, e->A.ld, ld, e->A.rows, e->A.cols));
-                cur += e->A.rows;
-            }
-            for (Edge* e : j.apm) {
-                g.push_back(cp(e->A.p, C + cur, e->A.ld, ld, j.m, e->A.cols, 2));
-                cur += e->A.cols;
-            }
+            gather(j, C, g);
             const size_t nn = std::max(j.n, 1);
-            T* tail = C + (size_t)j.m * ld;
+            T* tail = C + (size_t)j.m * j.ld;
             int* ii = ib + jobs.size() + j.i_off;
             int* rk = ib + rt.size();
-            rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, ld, 0, cfg_.tol});
+            rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, j.ld, 0, cfg_.tol});
         }
-        // one launch per cluster size; larger interfaces get more CTAs
         auto cluster_of = [](const Job& j) {
             const double w = (double)j.m * j.n;
             int c = w <= 32768 ? 1 : w <= 131072 ? 2 : w <= 524288 ? 4 : w <= 2097152 ? 8 : 16;
@@ -1011,14 +1021,36 @@ private:
             pend_[rq].flops = f;
             pend_[rq].bytes = by;
         }
+        return ranks;
+    }
+
+    template <class Job>
+    void run_sparsify_wave(std::vector<Job>& jobs, size_t celems, size_t ielems,
+                           std::vector<std::vector<long long>>& recs) {
+        std::vector<RRQRTaskRM<T>> rt;
+        const std::vector<int> ranks = rrqr_batch(jobs, celems, ielems, rt, [&](const Job& j, T* C,
+                                                                                 std::vector<CopyDesc<T>>& g) {
+            // C(i, cur + r) = A_mp(r, i), C(i, smp + c) = A_pm(i, c) (top csize rows of A_pm)
+            int cur = 0;
+            for (Edge* e : j.amp) {
+                g.push_back(cp(e->A.p, C + cur, e->A.ld, j.ld, e->A.rows, e->A.cols));
+                cur += e->A.rows;
+            }
+            for (Edge* e : j.apm) {
+                g.push_back(cp(e->A.p, C + cur, e->A.ld, j.ld, j.m, e->A.cols, 2));
+                cur += e->A.cols;
+            }
+        });
         std::vector<SparsWBRM<T>> wb;
         std::vector<SpBlock<T>> blocks;
+        std::vector<CopyDesc<T>> pre, post;  // least squares: extra rows of A_pm move up under the new top
         double wb_bytes = 0;
         for (size_t q = 0; q < jobs.size(); ++q) {
             auto& j = jobs[q];
             Cluster* c = j.c;
             const int r = ranks[q];
             const int m = j.m;
+            const int nr = c->rsize - c->csize;  // rows beyond the columns (0 for square problems)
             if (r >= m) {
                 recs[j.idx] = {m, c->csize, j.n, c->rsize};
                 continue;
@@ -1062,16 +1094,32 @@ private:
             sd.ccols = c->csize;
             sd.rank = r;
             tape_.push_back(std::move(sd));
+            if (nr > 0) {
+                // rows [m, m + nr) of every A_pm block become rows [r, r + nr) (through a
+                // staging copy: the ranges overlap); the diagonal block's rows [r, r + nr) are zero
+                for (Edge* e : j.apm) {
+                    T* st = arena_.alloc_n<T>((size_t)nr * std::max(e->A.cols, 1));
+                    pre.push_back(cp(e->A.p + m, st, e->A.ld, nr, nr, e->A.cols));
+                    post.push_back(cp(st, e->A.p + r, nr, e->A.ld, nr, e->A.cols));
+                }
+                pre.push_back(cp(nullptr, j.self->A.p + r, 0, j.self->A.ld, nr, r));
+            }
             // new shapes
             for (Edge* e : j.amp) e->A.cols = r;
-            for (Edge* e : j.apm) e->A.rows = r;
-            j.self->A.rows = r;
+            for (Edge* e : j.apm) e->A.rows = r + nr;
+            j.self->A.rows = r + nr;
             j.self->A.cols = r;
-            c->rsize = r;
+            c->rsize = r + nr;
             c->csize = r;
             fine_[ilvl_].push_back(cf);
             cf->elim = true;
-            recs[j.idx] = {m, r, j.n, r};
+            recs[j.idx] = {m, r, j.n, r + nr};
+        }
+        if (!pre.empty()) {
+            Upload u1;
+            const size_t o = u1.add(pre);
+            char* d1 = u1.commit(desc_arena_, stream_, pinned_);
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d1 + o), pre);
         }
         if (!wb.empty()) {
             Upload u2;
@@ -1083,6 +1131,258 @@ private:
                 launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
                                       reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), parts,
                                       stream_);
+            });
+            ++launches_fact_;
+        }
+        if (!post.empty()) {
+            Upload u3;
+            const size_t o = u3.add(post);
+            char* d3 = u3.commit(desc_arena_, stream_, pinned_);
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d3 + o), post);
+        }
+    }
+
+    // ------------------------------------------------------------- rectangular row shift (src/tree.cpp:319-411)
+    // The rows of every cluster eliminated at this level beyond its columns move
+    // to the neighbour whose block carries the largest row norm. The norms come
+    // from one batched kernel and one readback; the moves are replayed on the
+    // host in the reference's order, and every block that grows is rebuilt
+    // once (old rows, appended rows, zero padding) by one batched copy.
+    void reassign_phase() {
+        struct Item {
+            Cluster* c;
+            std::vector<std::pair<Edge*, int64_t>> normed;  // in-edge, offset of its row norms
+        };
+        std::vector<Item> items;
+        std::vector<RowNormTask<T>> tasks;
+        int64_t tot = 0;
+        for (Cluster* c : cur()) {
+            if (!c->elim || c->rsize == c->csize) continue;
+            if (c->rsize < c->csize) throw std::runtime_error("reassign_rows: fewer rows than columns");
+            Item it{c, {}};
+            const int rs = c->rsize - c->csize;
+            for (Edge* e : c->in) {
+                if (!find_out(c, e->n1)) continue;  // only column neighbours vote
+                tasks.push_back(RowNormTask<T>{e->A.p, e->A.ld, c->csize, rs, e->A.cols, tot});
+                it.normed.emplace_back(e, tot);
+                tot += rs;
+            }
+            items.push_back(std::move(it));
+        }
+        if (items.empty()) return;
+        std::vector<double> norms((size_t)std::max<int64_t>(tot, 1), 0.0);
+        if (tot > 0) {
+            double* d_norms = static_cast<double*>(scratch_.get(sizeof(double) * (size_t)tot, stream_));
+            Upload up;
+            const size_t o_t = up.add(tasks);
+            char* d = up.commit(desc_arena_, stream_, pinned_);
+            launch_row_norms<T>(reinterpret_cast<const RowNormTask<T>*>(d + o_t), (int)tasks.size(), (int)tot, d_norms,
+                                stream_);
+            ++launches_fact_;
+            cuda_check(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * (size_t)tot, cudaMemcpyDeviceToHost,
+                                       stream_),
+                       "row norms");
+            const double tw0 = wall();
+            cuda_check(cudaStreamSynchronize(stream_), "row norm readback");
+            t_rank_wait_ += wall() - tw0;
+            pinned_.reset();
+        }
+        // host replay; blocks that change are described as row segments of their final layout
+        struct Seg {
+            const T* src;  // null: zeros
+            int ld, rows;
+        };
+        std::map<Edge*, std::vector<Seg>> plan;
+        std::set<Edge*> fresh;
+        auto segs_of = [&](Edge* e) -> std::vector<Seg>& {
+            auto f = plan.find(e);
+            if (f == plan.end()) {
+                std::vector<Seg> v;
+                v.push_back(Seg{fresh.count(e) ? nullptr : e->A.p, e->A.ld, e->A.rows});
+                f = plan.emplace(e, std::move(v)).first;
+            }
+            return f->second;
+        };
+        for (Item& it : items) {
+            Cluster* c = it.c;
+            const int rs = c->rsize - c->csize;
+            std::vector<std::pair<Cluster*, double>> r2c(rs, {c, 0.0});
+            for (auto& ne : it.normed)
+                for (int i = 0; i < rs; ++i) {
+                    const double v = norms[ne.second + i];
+                    if (v > r2c[i].second) r2c[i] = {ne.first->n1, v};
+                }
+            std::vector<int> perm(rs);
+            std::iota(perm.begin(), perm.end(), 0);
+            std::stable_sort(perm.begin(), perm.end(),
+                             [&](int a, int b) { return r2c[a].first->order < r2c[b].first->order; });
+            for (Edge* e : c->in) {
+                Cluster* nold = e->n1;
+                const T* extra = e->A.p + c->csize;  // extra row q of this block: extra + q (ld e->A.ld)
+                for (int i = 0; i < rs;) {
+                    Cluster* nnew = r2c[perm[i]].first;
+                    int inext = i + 1;
+                    while (inext < rs && r2c[perm[inext]].first == nnew) ++inext;
+                    const int rinc = inext - i;
+                    Edge* te = find_out(nold, nnew);
+                    if (nold == nnew) {
+                        if (!te) throw std::runtime_error("reassign_rows: missing self edge");
+                    } else if (!te) {
+                        te = add_edge(nold, nnew);
+                        fresh.insert(te);
+                    }
+                    // rows that stay with the eliminated c only extend its own in-block,
+                    // of which later steps read the top c->csize rows: not materialised
+                    if (nnew != c) {
+                        auto& sg = segs_of(te);
+                        for (int q = i; q < inext; ++q) sg.push_back(Seg{extra + perm[q], e->A.ld, 1});
+                        te->A.rows += rinc;
+                    }
+                    if (nold == nnew) {
+                        TapeOp op;
+                        op.kind = TK_REASSIGN;
+                        op.c = c;
+                        op.f = nnew;
+                        op.m = nnew->rsize;  // first new row of nnew's segment
+                        op.k = rinc;
+                        for (int q = i; q < inext; ++q) op.idx.push_back(c->csize + perm[q]);
+                        tape_.push_back(std::move(op));
+                        nnew->xcap += rinc;
+                    }
+                    i = inext;
+                }
+            }
+            for (Edge* eo : c->out) {  // neighbours take their diagonal block's rows; pad their row blocks
+                if (eo->n2 == c) continue;
+                Cluster* n = eo->n2;
+                Edge* fs = find_out(n, n);
+                if (!fs) throw std::runtime_error("reassign_rows: neighbour without diagonal block");
+                n->rsize = fs->A.rows;
+                n->csize = fs->A.cols;
+                for (Edge* ei : n->in) {
+                    if (ei->n1->elim || !ei->live || ei->A.rows == n->rsize) continue;
+                    if (ei->A.rows > n->rsize) throw std::runtime_error("reassign_rows: block taller than its cluster");
+                    auto& sg = segs_of(ei);
+                    sg.push_back(Seg{nullptr, 0, n->rsize - ei->A.rows});
+                    ei->A.rows = n->rsize;
+                }
+            }
+            rec(7, rs, 0, 0, 0, 0, c->order);
+        }
+        // rebuild every changed block once (fresh storage reads as zeros)
+        std::vector<CopyDesc<T>> copies;
+        std::map<const T*, Blk> moved;
+        for (auto& kv : plan) {
+            Edge* e = kv.first;
+            const int uid = e->A.uid;
+            Blk nb = new_block(e->A.rows, e->A.cols);
+            nb.uid = uid;
+            moved[e->A.p] = nb;
+            int r0 = 0;
+            for (const Seg& sg : kv.second) {
+                if (sg.src && sg.rows > 0 && e->A.cols > 0)
+                    copies.push_back(cp(sg.src, nb.p + r0, sg.ld, nb.ld, sg.rows, e->A.cols));
+                r0 += sg.rows;
+            }
+            if (r0 != e->A.rows) throw std::runtime_error("reassign_rows: row plan mismatch");
+            e->A = nb;
+        }
+        for (TapeOp& t : tape_)  // back-substitutions recorded earlier read the rebuilt blocks
+            for (A12& a : t.a12) {
+                auto f = moved.find(a.B);
+                if (f != moved.end()) {
+                    a.B = f->second.p;
+                    a.ld = f->second.ld;
+                }
+            }
+        if (!copies.empty()) {
+            Upload up;
+            const size_t o = up.add(copies);
+            char* d = up.commit(desc_arena_, stream_, pinned_);
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
+        }
+    }
+
+    // ------------------------------------------------------------- sparsify_extra (src/tree.cpp:1260-1307)
+    // The rows of an interface beyond its columns are compressed by a truncated
+    // column-pivoted QR of [A_pm extra rows] (rank by the same rule as
+    // sparsifyD); only upper(R) P^T is kept, no op. The interfaces' blocks are
+    // disjoint, so all compressions of a level run as one batch.
+    void extra_phase() {
+        struct Job {
+            size_t idx;
+            Cluster* c;
+            std::vector<Edge*> apm;
+            int m, n, ld, csize;
+            size_t c_off, i_off;
+        };
+        std::vector<Job> jobs;
+        size_t celems = 0, ielems = 0;
+        for (Cluster* c : cur()) {
+            if (!want_sparsify(c) || c->csize == 0 || c->rsize <= c->csize) continue;
+            Job j;
+            j.idx = jobs.size();
+            j.c = c;
+            j.csize = c->csize;
+            int spm = 0;
+            for (Edge* e : c->in)
+                if (!e->n1->elim) { j.apm.push_back(e); spm += e->A.cols; }
+            j.m = c->rsize - c->csize;
+            j.n = spm;
+            j.ld = std::max((j.n + 3) & ~3, 4);
+            j.c_off = celems;
+            celems += (size_t)j.m * j.ld + 3 * (size_t)std::max(j.n, 1);
+            celems = (celems + 31) & ~size_t(31);
+            j.i_off = ielems;
+            ielems += 3 * (size_t)std::max(j.n, 1) + 1;
+            jobs.push_back(std::move(j));
+        }
+        if (jobs.empty()) return;
+        std::vector<RRQRTaskRM<T>> rt;
+        const std::vector<int> ranks = rrqr_batch(jobs, celems, ielems, rt, [&](const Job& j, T* C, std::vector<CopyDesc<T>>& g) {
+            int cur = 0;
+            for (Edge* e : j.apm) {  // C(i, cur + c) = A_pm(csize + i, c)
+                g.push_back(cp(e->A.p + j.csize, C + cur, e->A.ld, j.ld, j.m, e->A.cols, 2));
+                cur += e->A.cols;
+            }
+        });
+        std::vector<SparsWBRM<T>> wb;
+        std::vector<SpBlock<T>> blocks;
+        for (size_t q = 0; q < jobs.size(); ++q) {
+            Job& j = jobs[q];
+            Cluster* c = j.c;
+            const int kmax = std::min(j.m, j.n);
+            const int r = std::min(ranks[q], kmax);
+            if (r < 0) throw std::runtime_error("sparsify_extra: invalid rank from device");
+            const int rows_before = c->rsize;
+            if (r > 0) {
+                SparsWBRM<T> w{rt[q].C, rt[q].pos, rt[q].colat, rt[q].tau, nullptr, nullptr, nullptr, j.m, j.ld, r, 0,
+                               (int)blocks.size(), 0};
+                int cur = 0;
+                for (Edge* e : j.apm) {
+                    blocks.push_back(SpBlock<T>{e->A.p + j.csize, e->A.ld, r, e->A.cols, cur, 1});
+                    cur += e->A.cols;
+                }
+                w.nblk = (int)blocks.size() - w.blk0;
+                wb.push_back(w);
+            }
+            const int rows_after = j.csize + r;
+            for (Edge* e : j.apm) e->A.rows = rows_after;
+            Edge* es = find_out(c, c);
+            if (!es) throw std::runtime_error("sparsify_extra: cluster without diagonal block");
+            es->A.rows = rows_after;
+            c->rsize = rows_after;
+            rec(8, rows_before, rows_after, 0, 0, 0, c->order);
+        }
+        if (!wb.empty()) {
+            Upload u2;
+            const size_t o_w = u2.add(wb), o_b = u2.add(blocks);
+            char* d2 = u2.commit(desc_arena_, stream_, pinned_);
+            int parts = 1;
+            for (const auto& x : wb) parts = std::max(parts, x.nblk);
+            timed(KF_SPARS_WB, 0, 0, [&] {
+                launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
+                                      reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), parts, stream_);
             });
             ++launches_fact_;
         }
@@ -1164,6 +1464,10 @@ private:
 
     // ------------------------------------------------------------- solve plan
     void build_solve_plan() {
+        if (rect_) {
+            build_nrml_plan();
+            return;
+        }
         int64_t xtot = 0;
         for (auto& c : clusters_) {
             c->xoff = xtot;
@@ -1301,6 +1605,241 @@ private:
                     throw std::runtime_error("solve: a cluster exceeds the shared-memory vector capacity");
     }
     int nin_ = 0, nout_ = 0;
+
+    // Least-squares preconditioner (Tree::solve_nrml, src/tree.cpp:1471-1517):
+    // x = M_n b with M_n ~ (A^T A)^{-1}, applied as four sweeps of the tape:
+    // (A) the transposed ops forward on xt (R^T solves with x_n -= A12^T z,
+    // Q^T of the sparsifications, transposed merges and splits), (B) the
+    // transposed ops backward without QR / ScaleD / OrthogonalD (reassignments,
+    // merges, splits), then xt -> x on the leaves, (C) the ops forward without
+    // QR / ScaleD / OrthogonalD, and (D) the ops backward (R solves, Q of the
+    // sparsifications, merges, splits). One CUDA graph.
+    void build_nrml_plan() {
+        int64_t xtot = 0;
+        for (auto& c : clusters_) {
+            c->xoff = xtot;
+            xtot += std::max(c->xcap, 1);
+        }
+        xtot_ = xtot;
+        xbuf_ = arena_.alloc_n<T>(xtot);
+        xtbuf_ = arena_.alloc_n<T>(xtot);
+        d_bin_ = arena_.alloc_n<double>(ncols_);
+        d_xout_ = arena_.alloc_n<double>(ncols_);
+        std::vector<int> src, dst;
+        std::vector<int64_t> xin, xo, leaf;
+        for (Cluster* c : bottoms_[0]) {
+            for (int i = 0; i < c->csize_org; ++i) {
+                src.push_back(cperm_[c->cstart + i]);  // b (length n) enters xt
+                xin.push_back(c->xoff + i);
+                dst.push_back(cperm_[c->cstart + i]);
+                xo.push_back(c->xoff + i);
+            }
+            for (int i = 0; i < c->rsize_org; ++i) leaf.push_back(c->xoff + i);
+        }
+        // reassignment index lists first (the ops carry their device addresses)
+        std::vector<int> idx;
+        std::vector<size_t> idx_off(tape_.size(), 0);
+        for (size_t q = 0; q < tape_.size(); ++q)
+            if (tape_[q].kind == TK_REASSIGN) {
+                idx_off[q] = idx.size();
+                idx.insert(idx.end(), tape_[q].idx.begin(), tape_[q].idx.end());
+            }
+        const int* d_idx = nullptr;
+        if (!idx.empty()) {
+            Upload ui;
+            const size_t o = ui.add(idx);
+            d_idx = reinterpret_cast<const int*>(ui.commit(desc_arena_, stream_, pinned_) + o);
+        }
+        auto ptr = [](const void* p) { return (int64_t)reinterpret_cast<uintptr_t>(p); };
+        std::vector<XSeg> segs;
+        std::vector<GemvRef<T>> gemv;
+        std::vector<POp> sa, sb, sc, sd;
+        auto merge_segs = [&](Cluster* c, bool transposed) {
+            const int s0 = (int)segs.size();
+            for (Cluster* ch : c->children)
+                segs.push_back(transposed ? XSeg{ch->xoff, ch->csize, ch->rsize} : XSeg{ch->xoff, ch->rsize, ch->csize});
+            return s0;
+        };
+        for (size_t q = 0; q < tape_.size(); ++q) {
+            const TapeOp& t = tape_[q];
+            switch (t.kind) {
+                case TK_QR: {
+                    POp a{};
+                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, (int)gemv.size(),
+                                   (int)t.a12.size()};
+                    for (auto& e : t.a12) {
+                        gemv.push_back(GemvRef<T>{ptr(e.B), e.n1->xoff, e.ld, e.s});
+                        a.rd.push_back(e.n1);
+                    }
+                    a.rd.push_back(t.c);
+                    a.wr = a.rd;
+                    a.smem = t.k;
+                    POp d = a;
+                    d.op.dir = 0;
+                    d.wr = {t.c};
+                    sa.push_back(a);
+                    sd.push_back(d);
+                    break;
+                }
+                case TK_SCALED: {
+                    POp a{};
+                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, 0, 0};
+                    a.rd = a.wr = {t.c};
+                    a.smem = t.k;
+                    POp d = a;
+                    d.op.dir = 0;
+                    sa.push_back(a);
+                    sd.push_back(d);
+                    break;
+                }
+                case TK_ORTHD: {
+                    POp a{};
+                    a.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    a.rd = a.wr = {t.c};
+                    a.smem = t.m;
+                    POp d = a;
+                    d.op.dir = 1;
+                    sa.push_back(a);
+                    sd.push_back(d);
+                    break;
+                }
+                case TK_SPLITD: {
+                    POp f{};
+                    f.op = SolveOp{SK_SPLIT, 0, t.crows, t.ccols, t.rank, 0, t.c->xoff, t.f->xoff, 0, 0, 0, 0, 0};
+                    f.rd = f.wr = {t.c, t.f};
+                    f.smem = t.crows;
+                    POp b = f;
+                    b.op.dir = 1;
+                    sa.push_back(f);
+                    sb.push_back(b);
+                    sc.push_back(f);
+                    sd.push_back(b);
+                    break;
+                }
+                case TK_MERGE: {
+                    POp tf{}, tb{}, f{}, b{};
+                    std::vector<Cluster*> all{t.c};
+                    all.insert(all.end(), t.c->children.begin(), t.c->children.end());
+                    tf.op = SolveOp{SK_MERGE, 0, 0, 0, 0, 0, t.c->xoff, 0, 0, 0, 0, merge_segs(t.c, true),
+                                    (int)t.c->children.size()};
+                    tb.op = tf.op;
+                    tb.op.dir = 1;
+                    f.op = SolveOp{SK_MERGE, 0, 0, 0, 0, 0, t.c->xoff, 0, 0, 0, 0, merge_segs(t.c, false),
+                                   (int)t.c->children.size()};
+                    b.op = f.op;
+                    b.op.dir = 1;
+                    for (POp* o : {&tf, &tb, &f, &b}) {
+                        o->rd = o->wr = all;
+                        o->smem = 0;
+                    }
+                    sa.push_back(tf);
+                    sb.push_back(tb);
+                    sc.push_back(f);
+                    sd.push_back(b);
+                    break;
+                }
+                case TK_REASSIGN: {
+                    POp f{};
+                    f.op = SolveOp{SK_REASSIGN, 0, t.k, 0, 0, 0, t.c->xoff, t.f->xoff + t.m, ptr(d_idx + idx_off[q]), 0,
+                                   0, 0, 0};
+                    f.rd = f.wr = {t.c, t.f};
+                    f.smem = 0;
+                    POp b = f;
+                    b.op.dir = 1;
+                    sb.push_back(b);
+                    sc.push_back(f);
+                    break;
+                }
+            }
+        }
+        std::reverse(sb.begin(), sb.end());
+        std::reverse(sd.begin(), sd.end());
+        gemv_cols_.clear();
+        for (auto& g : gemv) gemv_cols_.push_back(g.s);
+        std::vector<SolveOp> all;
+        std::vector<WMeta> meta[4];
+        std::vector<POp>* lists[4] = {&sa, &sb, &sc, &sd};
+        for (int L = 0; L < 4; ++L) {
+            std::vector<std::vector<int>> w;
+            schedule_ops(*lists[L], w);
+            pack_waves(*lists[L], w, all, meta[L]);
+        }
+        Upload up;
+        size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
+               o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo), o_leaf = up.add(leaf);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
+        const SolveOp* d_ops = reinterpret_cast<const SolveOp*>(d + o_ops);
+        d_segs_ = reinterpret_cast<const XSeg*>(d + o_segs);
+        d_gemv_ = reinterpret_cast<const GemvRef<T>*>(d + o_gemv);
+        d_src_ = reinterpret_cast<int*>(d + o_src);
+        d_dst_ = reinterpret_cast<int*>(d + o_dst);
+        d_xin_ = reinterpret_cast<int64_t*>(d + o_xin);
+        d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
+        d_leaf_ = reinterpret_cast<int64_t*>(d + o_leaf);
+        const size_t smem_cap = (200 * 1024) / sizeof(T);
+        for (int L = 0; L < 4; ++L) {
+            nrml_waves_[L].clear();
+            for (auto& mt : meta[L]) {
+                if ((size_t)mt.smem > smem_cap)
+                    throw std::runtime_error("solve_nrml: a cluster exceeds the shared-memory vector capacity");
+                nrml_waves_[L].push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+            }
+        }
+        nin_ = (int)src.size();
+        nout_ = (int)dst.size();
+        nleaf_ = (int)leaf.size();
+        solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 16.0 * ncols_;
+    }
+    std::vector<Wave> nrml_waves_[4];
+    T* xtbuf_ = nullptr;
+    int64_t* d_leaf_ = nullptr;
+    int nleaf_ = 0;
+    cudaGraph_t nrml_graph_ = nullptr;
+    cudaGraphExec_t nrml_exec_ = nullptr;
+
+    void run_nrml_sweeps() {
+        launches_solve_ = 0;
+        cuda_check(cudaMemsetAsync(xtbuf_, 0, sizeof(T) * (size_t)xtot_, stream_), "nrml zero");
+        cuda_check(cudaMemsetAsync(xbuf_, 0, sizeof(T) * (size_t)xtot_, stream_), "nrml zero");
+        launch_gather_in<T>(d_bin_, d_src_, d_xin_, xtbuf_, nin_, stream_);
+        ++launches_solve_;
+        for (int L = 0; L < 4; ++L) {
+            if (L == 2) {
+                launch_seg_copy<T>(xtbuf_, xbuf_, d_leaf_, nleaf_, stream_);
+                ++launches_solve_;
+            }
+            T* xb = L < 2 ? xtbuf_ : xbuf_;
+            for (auto& w : nrml_waves_[L]) {
+                launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, stream_);
+                ++launches_solve_;
+            }
+        }
+        launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
+        ++launches_solve_;
+    }
+
+public:
+    void solve_nrml_dev(const double* d_b, double* d_x) override {
+        if (!factorized_) throw std::logic_error("solve_nrml before factorize");
+        if (!rect_) throw std::invalid_argument("solve_nrml needs a least-squares factorization (square matching off)");
+        double t0 = wall();
+        cuda_check(cudaMemcpyAsync(d_bin_, d_b, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
+                   "nrml in");
+        if (!nrml_exec_) {
+            cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+            run_nrml_sweeps();
+            cuda_check(cudaStreamEndCapture(stream_, &nrml_graph_), "capture end");
+            cuda_check(cudaGraphInstantiate(&nrml_exec_, nrml_graph_, 0), "graph instantiate");
+        }
+        timed(KF_SOLVE, 0, solve_bytes_, [&] { cuda_check(cudaGraphLaunch(nrml_exec_, stream_), "graph launch"); });
+        cuda_check(cudaMemcpyAsync(d_x, d_xout_, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
+                   "nrml out");
+        t_solve_ = wall() - t0;
+        ++applications_;
+    }
+    bool least_squares() const override { return rect_; }
+
+private:
 
     // Wave scheduling on x segments (RAW, WAR, WAW): an op runs one wave after
     // the last op that wrote a segment it touches, or read one it writes.

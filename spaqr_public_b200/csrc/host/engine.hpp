@@ -68,6 +68,9 @@ public:
     virtual void solve_dev(const double* d_b, double* d_x) = 0;
     // y = M^T g with M the preconditioner of solve_dev (adjoint sweeps)
     virtual void solve_adjoint_dev(const double* d_g, double* d_y) = 0;
+    // x = M_n b, M_n ~ (A^T A)^{-1} of a least-squares factorization (b, x of length n)
+    virtual void solve_nrml_dev(const double* d_b, double* d_x) = 0;
+    virtual bool least_squares() const = 0;
     virtual cudaStream_t stream() const = 0;
     virtual const Log& log() const = 0;
     virtual const std::vector<int>& cperm() const = 0;

@@ -306,6 +306,79 @@ int refine_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x
     return total;
 }
 
+int cgls_device(EngineBase& P, const DevCsr& A, const DevCsr& At, const double* d_b, double* d_x, int iters,
+                double tol, double* res, long long* launches) {
+    cudaStream_t s = P.stream();
+    const int m = A.m, n = A.n;
+    const int nblk = reduce_blocks();
+    DevVec residual, nr, tmp, p, z, atb, part;
+    residual.alloc(m, s);
+    nr.alloc(n, s);
+    tmp.alloc(m, s);
+    p.alloc(n, s);
+    z.alloc(n, s);
+    atb.alloc(n, s);
+    part.alloc(nblk, s);
+    std::vector<double> h(nblk);
+    long long l = 0;
+    // deterministic inner product: fixed block partials summed in order on the host
+    auto dot = [&](const double* a, const double* b, int len) {
+        launch_dot_partials(a, b, 0, len, part.p, nblk, s, nullptr);
+        ++l;
+        cuda_check(cudaMemcpyAsync(h.data(), part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, s), "cgls dot");
+        cuda_check(cudaStreamSynchronize(s), "cgls dot");
+        double acc = 0;
+        for (double v : h) acc += v;
+        return acc;
+    };
+    auto spmv = [&](const DevCsr& M, const double* x, double* y) {
+        launch_spmv_csr(M.m, M.rp, M.ci, M.v, x, y, s);
+        ++l;
+    };
+    spmv(A, d_x, tmp.p);
+    launch_sub(m, d_b, tmp.p, residual.p, s);
+    spmv(At, residual.p, nr.p);
+    spmv(At, d_b, atb.p);
+    l += 1;
+    const double rhs2 = dot(atb.p, atb.p, n);
+    if (rhs2 == 0) {
+        cuda_check(cudaMemsetAsync(d_x, 0, sizeof(double) * n, s), "cgls zero");
+        *res = 0;
+        if (launches) *launches = l;
+        return 0;
+    }
+    const double threshold = tol * tol * rhs2;
+    double rn2 = dot(nr.p, nr.p, n);
+    if (rn2 < threshold) {
+        *res = std::sqrt(rn2 / rhs2);
+        if (launches) *launches = l;
+        return 0;
+    }
+    P.solve_nrml_dev(nr.p, p.p);
+    double abs_new = dot(nr.p, p.p, n);
+    int i = 0;
+    while (i < iters) {
+        spmv(A, p.p, tmp.p);
+        const double alpha = abs_new / dot(tmp.p, tmp.p, m);
+        launch_axpby(n, alpha, p.p, 1.0, d_x, s);
+        launch_axpby(m, -alpha, tmp.p, 1.0, residual.p, s);
+        l += 2;
+        spmv(At, residual.p, nr.p);
+        rn2 = dot(nr.p, nr.p, n);
+        if (rn2 < threshold) break;
+        P.solve_nrml_dev(nr.p, z.p);
+        const double abs_old = abs_new;
+        abs_new = dot(nr.p, z.p, n);
+        const double beta = abs_new / abs_old;
+        launch_axpby(n, 1.0, z.p, beta, p.p, s);
+        ++l;
+        ++i;
+    }
+    *res = std::sqrt(rn2 / rhs2);
+    if (launches) *launches = l;
+    return i;
+}
+
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x) {
     DevVec t, part;
     t.alloc(A.m, s);

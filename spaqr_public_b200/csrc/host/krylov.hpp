@@ -25,6 +25,13 @@ size_t gmres_workspace_elems(int m, int restart);
 int gmres_device_ws(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart,
                     double tol, double* res, long long* launches, double* workspace);
 
+// Preconditioned CGLS on the normal equations (src/is.cpp:274-345), with the
+// least-squares preconditioner P.solve_nrml_dev. A (m x n) and At (its
+// transpose, n x m) as device CSR; x holds the initial guess. Returns the
+// iteration count, *res = ||A^T (b - A x)|| / ||A^T b||.
+int cgls_device(EngineBase& P, const DevCsr& A, const DevCsr& At, const double* d_b, double* d_x, int iters,
+                double tol, double* res, long long* launches);
+
 // ||b - A x|| / ||b|| on the device (FP64).
 double residual_norm(cudaStream_t s, const DevCsr& A, const double* d_b, const double* d_x);
 

@@ -188,7 +188,7 @@ void rows_by_norm(const Csc& At_perm, const std::vector<Cid>& cid_of_pos, std::v
 
 }  // namespace
 
-Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X) {
+Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X, bool square) {
     if (nlevels < 1) throw std::invalid_argument("nlevels must be >= 1");
     if ((int64_t)X.size() != (int64_t)d * A.n) throw std::invalid_argument("coordinates must be d x ncols");
     const int n = A.n, m = A.m;
@@ -287,7 +287,8 @@ Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<
     o.cid_of_pos.resize(n);
     for (int k = 0; k < n; ++k) o.cid_of_pos[k] = rmap[o.cperm[k]];
 
-    if (m == n) {
+    if (square) {
+        if (m != n) throw std::invalid_argument("identity row matching needs a square matrix");
         o.rperm = o.cperm;
         o.rows_of_col.assign(n, 1);
     } else {

@@ -60,7 +60,9 @@ struct Ordering {
 
 // Geometric nested dissection on A^T A followed by the interface inference on A
 // and the hierarchical column sort. X is d x n column-major (column j = the
-// coordinates of unknown j).
-Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X);
+// coordinates of unknown j). With square set (identity row matching, m == n)
+// the rows follow the columns; otherwise every row joins the first column of
+// its largest-norm run of equal cluster ids (src/tree.cpp:100-163).
+Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X, bool square = true);
 
 }  // namespace spq

@@ -776,6 +776,22 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
             }
             break;
         }
+        case SK_REASSIGN: {
+            // Reassign (src/operations.cpp:60-69, src/toperations.cpp:62-70): dir 0
+            // moves x(c)[idx[i]] to x(n)[nstart + i]; dir 1 (transposed tape) moves
+            // them back. idx holds positions inside c's segment.
+            const int nr = op.a;
+            const int* idx = reinterpret_cast<const int*>(op.p0);
+            T* xc = x + op.x0;
+            T* xn = x + op.x1;
+            for (int i = tid; i < nr; i += blockDim.x) {
+                if (op.dir == 0)
+                    xn[i] = xc[idx[i]];
+                else
+                    xc[idx[i]] = xn[i];
+            }
+            break;
+        }
         case SK_SPLIT_T: {
             // Transposes of the SplitD index maps (adjoint sweeps): dir 0 undoes
             // the forward split (the fine part's adjoint folds back into c and
@@ -826,6 +842,31 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
         }
         default:
             break;
+    }
+}
+
+template <class T>
+__global__ void k_seg_copy(const T* src, T* dst, const int64_t* pos, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[pos[i]] = src[pos[i]];
+}
+
+// out[t][i] = || row (row0 + i) of block t || (FP64 sums), one warp per row.
+template <class T>
+__global__ void k_row_norms(const RowNormTask<T>* tasks, int ntasks, double* out) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = 0; t < ntasks; ++t) {
+        const RowNormTask<T> k = tasks[t];
+        for (int i = gw; i < k.rows; i += nwarps) {
+            const T* row = k.p + k.row0 + i;
+            double s = 0.0;
+            for (int j = lane; j < k.cols; j += 32) {
+                const double v = (double)row[(size_t)j * k.ld];
+                s += v * v;
+            }
+            s = warp_sum(s);
+            if (lane == 0) out[k.out + i] = sqrt(s);
+        }
     }
 }
 
@@ -974,6 +1015,17 @@ void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const Gem
 }
 
 template <class T>
+void launch_seg_copy(const T* src, T* dst, const int64_t* pos, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_seg_copy<T><<<grid_for(n, 256), 256, 0, s>>>(src, dst, pos, n);
+}
+template <class T>
+void launch_row_norms(const RowNormTask<T>* tasks, int ntasks, int total_rows, double* out, cudaStream_t s) {
+    if (ntasks <= 0 || total_rows <= 0) return;
+    k_row_norms<T><<<grid_for((int64_t)total_rows * 32, 256, 148 * 8), 256, 0, s>>>(tasks, ntasks, out);
+}
+
+template <class T>
 void launch_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n, cudaStream_t s) {
     k_gather_in<T><<<grid_for(n, 256), 256, 0, s>>>(b, src, xpos, x, n);
 }
@@ -1035,6 +1087,8 @@ void prepare_kernels() {
     template void launch_solve_step<T>(const SolveOp*, int, const XSeg*, const GemvRef<T>*, const T*, T*, int, \
                                        cudaStream_t);                                                          \
     template void launch_gather_in<T>(const double*, const int*, const int64_t*, T*, int, cudaStream_t);      \
+    template void launch_seg_copy<T>(const T*, T*, const int64_t*, int, cudaStream_t);                         \
+    template void launch_row_norms<T>(const RowNormTask<T>*, int, int, double*, cudaStream_t);                \
     template void launch_scatter_out<T>(const T*, const int64_t*, const int*, double*, int, cudaStream_t);    \
     template void prepare_kernels<T>();
 

@@ -103,7 +103,7 @@ struct SparsWBRM {
     const int* pos;
     const int* colat;
     const T* tau_in;
-    T* V;    // m x r, ld m
+    T* V;    // m x r, ld m (null: rebuild the blocks only)
     T* tau;  // r
     T* tp;   // panel T factors of V
     int m, ldc, r, nblk, blk0, pad;
@@ -124,7 +124,7 @@ enum SolveKind : int {
     SK_TRI = 1,     // x <- inv(R) (x - sum_b B_b x_b)  or transposed variant
     SK_SPLIT = 2,   // SplitD fwd/bwd index shuffle
     SK_MERGE = 3,   // Merge fwd/bwd copies
-    SK_REASSIGN = 4, // rectangular row reassignment
+    SK_REASSIGN = 4, // rectangular row reassignment: dir 0 x(n)[nstart + i] = x(c)[idx[i]], dir 1 back
     SK_SPLIT_T = 5, // transpose of SK_SPLIT (same dir)
     SK_MERGE_T = 6  // transpose of SK_MERGE (same dir): add into the source, zero the target
 };
@@ -148,6 +148,19 @@ struct GemvRef {
 template <class T>
 void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const GemvRef<T>* gemv, const T* arena,
                        T* x, int smem_elems, cudaStream_t s);
+// dst[pos[k]] = src[pos[k]] (one x buffer into the other at the given positions)
+template <class T>
+void launch_seg_copy(const T* src, T* dst, const int64_t* pos, int n, cudaStream_t s);
+// Norms of rows row0 .. row0 + rows - 1 of a column-major block (rectangular
+// row reassignment, src/tree.cpp:319-345); results at out[out_off + i].
+template <class T>
+struct RowNormTask {
+    const T* p;
+    int ld, row0, rows, cols;
+    int64_t out;
+};
+template <class T>
+void launch_row_norms(const RowNormTask<T>* tasks, int ntasks, int total_rows, double* out, cudaStream_t s);
 // x[xpos[k]] = (T) b[src[k]]  /  out[dst[k]] = (double) x[xpos[k]]
 template <class T>
 void launch_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n, cudaStream_t s);

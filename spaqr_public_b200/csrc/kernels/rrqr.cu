@@ -443,6 +443,8 @@ __global__ void __launch_bounds__(256) k_spars_wb_rm(const SparsWBRM<T>* tasks, 
             }
         }
     }
+    // the compression of extra rows (sparsify_extra) keeps no reflectors
+    if (t.V == nullptr) return;
     // 2. V(:, q) = column colat[q] of C (reflector below the diagonal), tau
     for (int q0 = y * 32; q0 < r; q0 += ny * 32) {
         if (tid < 32) s_col[tid] = (q0 + tid < r) ? t.colat[q0 + tid] : 0;

@@ -71,13 +71,20 @@ def test_invalid_csc_rejected():
         t.partition((m, n, cp, bad, va))
 
 
-def test_rectangular_is_reported_unsupported():
+def test_rectangular_needs_square_matching_off():
     A, b, _ = matgen.lsq2d(16, seed=1)
     t = Tree(4, 0)
+    t.set_square(1)
     t.set_coords_grid(16, 2)
-    with pytest.raises(_abi.SpqError) as e:
+    with pytest.raises(_abi.SpqError) as e:  # identity matching of a 300 x 256 matrix
         t.partition(A)
     assert e.value.code == 6
+    t = Tree(4, 0)
+    t.set_coords_grid(16, 2)
+    t.partition(A)  # least squares: partitions on the host
+    with pytest.raises(_abi.SpqError) as e:
+        t.solve_nrml(np.zeros(A[1]))
+    assert e.value.code == 2
 
 
 def test_setters_after_partition_rejected():

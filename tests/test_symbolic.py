@@ -8,14 +8,14 @@ from oracle import oracle_py as O
 from spaqr_public_b200 import Tree, matgen
 
 
-def _compare(A, n, d, levels):
+def _compare(A, n, d, levels, square=1):
     t = Tree(levels, 0)
     t.set_tol(1e-2)
     t.set_scale(1)
-    t.set_square(1)
+    t.set_square(square)
     t.set_coords_grid(n, d)
     t.partition(A)
-    o = O.OracleTree(levels, 0, 1e-2, 1, 1.0, 1)
+    o = O.OracleTree(levels, 0, 1e-2, 1, 1.0, square)
     o.set_coords_grid(n, d)
     o.partition(A)
     cp, rp = t.perms()
@@ -67,3 +67,12 @@ def test_column_normalize_matches_reference_formula():
     m, n, cp, ri, va = B
     for j in range(n):
         assert abs(np.linalg.norm(va[cp[j]:cp[j + 1]]) - 10.0) < 1e-12
+
+
+@pytest.mark.parametrize("n,levels", [(16, 4), (24, 5), (32, 5)])
+def test_partition_least_squares(n, levels):
+    # rectangular [L; 10 S]: rows join the first column of their largest-norm cluster run
+    A, _, _ = matgen.lsq2d(n, seed=5 + n)
+    t = _compare(A, n, 2, levels, square=0)
+    b = t.bottom()
+    assert b[:, 3].sum() == A[0] and b[:, 1].sum() == A[1]
