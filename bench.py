@@ -405,6 +405,153 @@ def run_single(args):
                       "gpu_launches": info["launches"]["total"]}), flush=True)
 
 
+def _tree_for(w, A, precision, square=1):
+    from spaqr_public_b200 import Tree
+    t = Tree(w["levels"], w["skip"], precision=precision)
+    t.set_tol(w["tol"])
+    t.set_scale(1)
+    t.set_square(square)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    return t
+
+
+def _gpu_square(w, A, precision, target, inner):
+    """factorize + refinement to the true residual target (CUDA events)."""
+    import torch
+    from spaqr_public_b200._abi import check, lib
+    rp, ci, va = device_csr(A)
+    d_b = torch.tensor(w["b"], dtype=torch.float64, device="cuda")
+    x = torch.zeros(A[1], dtype=torch.float64, device="cuda")
+    t = _tree_for(w, A, precision)
+    sp = C.c_void_p()
+    check(lib().spq_get_stream(t._h, C.byref(sp)))
+    st = torch.cuda.ExternalStream(sp.value)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    check(lib().spq_factorize(t._h))
+    e_f = torch.cuda.Event(enable_timing=True)
+    e_f.record(st)
+    its, res = C.c_int(0), C.c_double(0)
+    rc = lib().spq_solve_to_residual_dev(t._h, A[0], C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                                         C.c_void_p(va.data_ptr()), C.c_void_p(d_b.data_ptr()),
+                                         C.c_void_p(x.data_ptr()), target, inner, 20, 300, C.byref(its), C.byref(res))
+    e1.record(st)
+    torch.cuda.synchronize()
+    if rc not in (0, 7):  # 7: target not reached within 20 corrections (reported, not raised)
+        check(rc)
+    out = dict(total_s=e0.elapsed_time(e1) / 1e3, factor_s=e0.elapsed_time(e_f) / 1e3, its=its.value,
+               true_residual=res.value, converged=rc == 0)
+    t.close()
+    return out, x.cpu().numpy()
+
+
+def _gpu_lsq(w, A, precision, tol):
+    """factorize + CGLS to ||A^T r|| / ||A^T b|| <= tol (CUDA events)."""
+    import torch
+    from spaqr_public_b200 import matgen
+    from spaqr_public_b200._abi import check, lib
+    m, n, cp, ri, va = A
+    rp, ci, vr = device_csr(A)
+    rp_t = torch.tensor(np.asarray(cp), dtype=torch.int32, device="cuda")
+    ci_t = torch.tensor(np.asarray(ri), dtype=torch.int32, device="cuda")
+    va_t = torch.tensor(np.asarray(va), dtype=torch.float64, device="cuda")
+    d_b = torch.tensor(w["b"], dtype=torch.float64, device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    t = _tree_for(w, A, precision, square=0)
+    sp = C.c_void_p()
+    check(lib().spq_get_stream(t._h, C.byref(sp)))
+    st = torch.cuda.ExternalStream(sp.value)
+    e0, e_f, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    e0.record(st)
+    check(lib().spq_factorize(t._h))
+    e_f.record(st)
+    its, res = C.c_int(0), C.c_double(0)
+    rc = lib().spq_cgls_dev(t._h, m, n, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                            C.c_void_p(vr.data_ptr()), C.c_void_p(rp_t.data_ptr()), C.c_void_p(ci_t.data_ptr()),
+                            C.c_void_p(va_t.data_ptr()), C.c_void_p(d_b.data_ptr()), C.c_void_p(x.data_ptr()), 300,
+                            tol, C.byref(its), C.byref(res))
+    e1.record(st)
+    torch.cuda.synchronize()
+    check(rc)
+    out = dict(total_s=e0.elapsed_time(e1) / 1e3, factor_s=e0.elapsed_time(e_f) / 1e3, its=its.value,
+               normal_residual=res.value)
+    t.close()
+    return out, x.cpu().numpy()
+
+
+def run_configs(args):
+    """The reference configurations other than the headline: advdiff2d_128 (plain
+    FP64, GMRES to 1e-12), contrast2d_512 (FP32 factor, tolerance sweep, FP64
+    refinement to 1e-10, error against the FP64 form) and lsq2d_256 (FP32 and
+    FP64 factors, CGLS to 1e-10), with the oracle's CPU time where it runs in
+    seconds. One JSON line per configuration; the second of two runs is kept
+    (the first warms the memory pool)."""
+    import torch
+    from oracle import oracle_py as O
+    from spaqr_public_b200 import FP32, FP64, matgen
+    torch.cuda.set_device(0)
+    threads = cpu_threads()
+    O.blas_threads(threads)
+    # config 0
+    w = matgen.workload("advdiff2d_128")
+    A = matgen.column_normalize(w["A"])
+    for _ in range(2):
+        g64, _ = _gpu_square(w, A, FP64, w["res"], w["res"])
+    t0 = time.perf_counter()
+    o = O.OracleTree(w["levels"], w["skip"], w["tol"], 1, 1.0, 1)
+    o.set_coords_grid(w["n"], w["d"])
+    o.partition(A)
+    o.assemble(A)
+    t1 = time.perf_counter()
+    o.factorize()
+    _, ito, reso = o.gmres(A, w["b"], iters=300, tol=w["res"])
+    t2 = time.perf_counter()
+    print(json.dumps({"config": "advdiff2d_128 (128^2, 8 levels, tol 1e-3, skip 0), plain FP64, GMRES to 1e-12",
+                      "gpu": g64, "oracle_cpu": {"factor_plus_gmres_s": t2 - t1, "gmres_its": ito, "cores": threads},
+                      "speedup": (t2 - t1) / g64["total_s"]}), flush=True)
+    # config 2: tolerance sweep
+    w = matgen.workload("contrast2d_512")
+    A = matgen.column_normalize(w["A"])
+    for _ in range(2):
+        ref64, x64 = _gpu_square(w, A, FP64, 1e-10, 1e-10)
+    rows = []
+    for tol in (1e-1, 1e-2, 1e-3):
+        w2 = dict(w, tol=tol)
+        for _ in range(2):
+            g32, x32 = _gpu_square(w2, A, FP32, 1e-10, 1e-6)
+        g64t, _ = _gpu_square(w2, A, FP64, 1e-10, 1e-10)
+        rows.append({"tol": tol, "fp32": g32, "fp64": g64t,
+                     "rel_error_vs_fp64_tol1e-2": float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))})
+    print(json.dumps({"config": "contrast2d_512 (512^2, 16x16 log-uniform patches in [1e-3, 1e3], 12 levels), FP32 "
+                                "factor + FP64 refinement to 1e-10, tolerance sweep", "sweep": rows}), flush=True)
+    # config 3: least squares
+    w = matgen.workload("lsq2d_256")
+    A = matgen.column_normalize(w["A"])
+    for _ in range(2):
+        l32, x32 = _gpu_lsq(w, A, FP32, 1e-10)
+    for _ in range(2):
+        l64, x64 = _gpu_lsq(w, A, FP64, 1e-10)
+    t0 = time.perf_counter()
+    o = O.OracleTree(w["levels"], w["skip"], w["tol"], 1, 1.0, 0)
+    o.set_coords_grid(w["n"], w["d"])
+    o.partition(A)
+    o.assemble(A)
+    t1 = time.perf_counter()
+    o.factorize()
+    xo, ito, reso = o.cgls(A, w["b"], iters=300, tol=1e-10)
+    t2 = time.perf_counter()
+    print(json.dumps({"config": "lsq2d_256 ([L; 10 S], 72090 x 65536, 10 levels, tol 1e-2), CGLS to 1e-10",
+                      "gpu_fp32": l32, "gpu_fp64": l64,
+                      "rel_error_fp32_vs_oracle": float(np.linalg.norm(x32 - xo) / np.linalg.norm(xo)),
+                      "rel_error_fp64_vs_oracle": float(np.linalg.norm(x64 - xo) / np.linalg.norm(xo)),
+                      "oracle_cpu": {"factor_plus_cgls_s": t2 - t1, "cgls_its": ito, "cores": threads},
+                      "speedup_fp32": (t2 - t1) / l32["total_s"]}), flush=True)
+
+
 def run_diff_batch(args):
     """The differentiation batch: 32 independent 2D advection-diffusion systems
     (sides 96..256), FP32 factors, loss 1/2 ||x - x*||^2, gradients dL/db and
@@ -494,7 +641,12 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD, help="workload of --single-step")
     ap.add_argument("--diff-batch", action="store_true",
                     help="time the 32-system differentiation batch (batched vs one after another)")
+    ap.add_argument("--configs", action="store_true",
+                    help="time the other reference configurations (2D plain FP64, contrast sweep, least squares)")
     args = ap.parse_args()
+    if args.configs:
+        run_configs(args)
+        return
     if args.single_step:
         run_single(args)
         return
