@@ -88,4 +88,31 @@ inline int gmres(const CscView& A, const std::vector<double>& b, std::vector<dou
     return its;
 }
 
+// cgls(A, b, x, precond, iters, tol, verb) -> iterations (src/is.cpp:274-345) for a
+// least-squares Tree (square matching off). x holds the initial guess; tol is
+// updated to ||A^T (b - A x)|| / ||A^T b||.
+inline int cgls(const CscView& A, const std::vector<double>& b, std::vector<double>& x, const Tree& precond,
+                int iters, double& tol) {
+    x.resize(A.n, 0.0);
+    int its = 0;
+    double res = 0;
+    check(spq_cgls(precond.handle(), A.m, A.n, A.colptr, A.rowind, A.val, b.data(), x.data(), iters, tol, &its, &res));
+    tol = res;
+    return its;
+}
+
+// Adjoint solve for differentiation: lambda = A^{-T} g by GMRES on A^T with the
+// factors applied transposed. With x = A^{-1} b and a loss L(x): g = dL/dx,
+// dL/db = lambda, dL/dA_ij = -lambda_i x_j.
+inline int gmres_adjoint(const CscView& A, const std::vector<double>& g, std::vector<double>& lambda,
+                         const Tree& precond, int iters, int restart, double& tol) {
+    lambda.resize(A.m, 0.0);
+    int its = 0;
+    double res = 0;
+    check(spq_gmres_adjoint(precond.handle(), A.m, A.n, A.colptr, A.rowind, A.val, g.data(), lambda.data(), iters,
+                            restart, tol, &its, &res));
+    tol = res;
+    return its;
+}
+
 }  // namespace spq
