@@ -210,10 +210,12 @@ int spq_get_stats(spq_tree* t, double* times, long long* counters);
 /* Per-level factorization phase times in ms (6 per level: fill, elmn, shift,
  * scale, sprsfy, merge), as printed by src/tree.cpp:1417-1426. */
 int spq_get_level_times(spq_tree* t, double* out);
-/* Host side of the last factorize in seconds: out5 = [wall time, waits for the
- * per-wave rank readbacks, device allocations of the arenas, scratch growth,
- * solve-plan build]. */
-int spq_get_host_times(spq_tree* t, double* out5);
+/* Host side of the last factorize in seconds: out11 = [wall time, waits for
+ * the device readbacks (ranks, row norms), device allocations of the arenas,
+ * scratch growth, solve-plan build, then the host time of each level phase
+ * summed over the levels: fill, elimination, row shift, scaling,
+ * sparsification, merge (waits and allocations included)]. */
+int spq_get_host_times(spq_tree* t, double* out11);
 /* Device memory of destroyed handles stays cached in a per-device pool for the
  * next handle (no allocation cost on refactorization); this returns the
  * cached, unused part to the device. */

@@ -763,11 +763,11 @@ int spq_trim_memory(void) {
         return SPQ_OK;
     });
 }
-int spq_get_host_times(spq_tree* t, double* out5) {
-    if (!t || !out5) return fail(SPQ_ERR_ARG, "null argument");
+int spq_get_host_times(spq_tree* t, double* out11) {
+    if (!t || !out11) return fail(SPQ_ERR_ARG, "null argument");
     if (!t->eng || t->state < 3) return fail(SPQ_ERR_STATE, "not factorized");
     auto v = t->eng->host_times();
-    std::memcpy(out5, v.data(), sizeof(double) * 5);
+    std::memcpy(out11, v.data(), sizeof(double) * 11);
     return SPQ_OK;
 }
 int spq_get_level_times(spq_tree* t, double* out) {

@@ -240,6 +240,7 @@ public:
         double t0 = wall();
         launches_fact_ = 0;
         t_rank_wait_ = 0;
+        for (double& x : t_phase_) x = 0;
         alloc0_ = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
         grow0_ = scratch_.grow_seconds();
         const int L = cfg_.nlevels;
@@ -251,20 +252,32 @@ public:
         for (ilvl_ = 0; ilvl_ < L; ++ilvl_) {
             cudaEvent_t* ev = &level_ev_[(size_t)ilvl_ * 7];
             cudaEventRecord(ev[0], stream_);
+            double th = wall();
+            auto lap = [&](int k) {
+                const double now = wall();
+                t_phase_[k] += now - th;
+                th = now;
+            };
             for (Cluster* s : cur())
                 if (s->level() == ilvl_) get_sparsity(s);
+            lap(0);
             cudaEventRecord(ev[1], stream_);
             elim_phase();
+            lap(1);
             cudaEventRecord(ev[2], stream_);
             if (rect_ && ilvl_ < L - 1) reassign_phase();
+            lap(2);
             cudaEventRecord(ev[3], stream_);  // shift (rectangular only)
             const bool window = ilvl_ < L - 2 && ilvl_ >= cfg_.skip && cfg_.tol != 0;
             if (cfg_.scale && window) scale_phase();
+            lap(3);
             cudaEventRecord(ev[4], stream_);
             if (rect_ && cfg_.scale && window) extra_phase();
             if (window) sparsify_phase();
+            lap(4);
             cudaEventRecord(ev[5], stream_);
             if (ilvl_ < L - 1) merge_all();
+            lap(5);
             cudaEventRecord(ev[6], stream_);
             auto ts = topsize();
             rec(5, ts.first, ts.second, (long long)cur().size());
@@ -349,8 +362,9 @@ public:
         counters[7] = applications_;
     }
     std::vector<double> host_times() const override {
-        return {t_fact_, t_rank_wait_, arena_.alloc_seconds() + desc_arena_.alloc_seconds() - alloc0_,
-                scratch_.grow_seconds() - grow0_, t_plan_};
+        return {t_fact_,     t_rank_wait_, arena_.alloc_seconds() + desc_arena_.alloc_seconds() - alloc0_,
+                scratch_.grow_seconds() - grow0_, t_plan_, t_phase_[0], t_phase_[1], t_phase_[2], t_phase_[3],
+                t_phase_[4], t_phase_[5]};
     }
     std::vector<double> level_times() const override {
         std::vector<double> out;
@@ -372,6 +386,7 @@ private:
     Scratch scratch_;
     PinnedStage pinned_;
     double t_rank_wait_ = 0, t_plan_ = 0, alloc0_ = 0, grow0_ = 0;
+    double t_phase_[6] = {0, 0, 0, 0, 0, 0};  // host time per phase: fill, elim, shift, scale, sparsify, merge
     std::vector<std::vector<Cluster*>> bottoms_, fine_;
     std::vector<std::unique_ptr<Cluster>> clusters_;
     std::vector<std::unique_ptr<Edge>> edges_;
@@ -622,13 +637,26 @@ private:
         std::vector<TileRef> trsm_tiles;
         for (size_t t = 0; t < trsm.size(); ++t)
             for (int r0 = 0, ti = 0; r0 < trsm[t].rows; r0 += 128, ++ti) trsm_tiles.push_back(TileRef{(int)t, ti});
+        // panel groups: cluster size by panel height (row slabs of about 256 rows, at
+        // least 32), 0 = single-CTA kernel for panels beyond the clusters' shared memory
+        auto panel_cluster = [](int R) {
+            int c = std::max(1, std::min(16, (R + 255) / 256));
+            while (c > 1 && R < 32 * c) --c;
+            while (c < 16 && (size_t)R > panel_cl_max_rows<T>(c)) ++c;
+            return (size_t)R > panel_cl_max_rows<T>(c) ? 0 : c;
+        };
+        std::vector<std::map<int, std::vector<int>>> pgroups(ids.size());
+        for (size_t i = 0; i < ids.size(); ++i)
+            for (int t : ids[i]) pgroups[i][panel_cluster(qt[t].m - (int)i * kNB)].push_back(t);
         Upload up;
         size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
                o_post = up.add(post);
         std::vector<size_t> o_ids, o_tiles;
+        std::vector<std::map<int, size_t>> o_pg(ids.size());
         for (size_t i = 0; i < ids.size(); ++i) {
             o_ids.push_back(up.add(ids[i]));
             o_tiles.push_back(up.add(tiles[i]));
+            for (auto& kv : pgroups[i]) o_pg[i][kv.first] = up.add(kv.second);
         }
         char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
@@ -653,11 +681,20 @@ private:
             }
             const int smem_rows = std::min(rows, smem_limit);
             timed(KF_PANEL, pf, pb, [&] {
-                launch_panel<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
-                                reinterpret_cast<const int*>(d + o_ids[i]), (int)ids[i].size(), p, smem_rows,
-                                stream_);
+                for (auto& kv : pgroups[i]) {
+                    const int* gids = reinterpret_cast<const int*>(d + o_pg[i][kv.first]);
+                    const QRTask<T>* dq = reinterpret_cast<const QRTask<T>*>(d + o_q);
+                    if (kv.first == 0) {
+                        launch_panel<T>(dq, gids, (int)kv.second.size(), p, smem_rows, stream_);
+                    } else {
+                        int maxr = 0;
+                        for (int t : kv.second) maxr = std::max(maxr, qt[t].m - p);
+                        cuda_check(launch_panel_cl<T>(dq, gids, (int)kv.second.size(), kv.first, maxr, p, stream_),
+                                   "panel launch");
+                    }
+                    ++launches_fact_;
+                }
             });
-            ++launches_fact_;
             if (!tiles[i].empty()) {
                 timed(KF_TRAILING, tf, tb, [&] {
                     launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
@@ -959,7 +996,7 @@ private:
             T* C = cb + j.c_off;
             gather(j, C, g);
             const size_t nn = std::max(j.n, 1);
-            T* tail = C + (size_t)j.m * j.ld;
+            T* tail = C + (size_t)j.m * j.ld;  // tau, vn1, vn2
             int* ii = ib + jobs.size() + j.i_off;
             int* rk = ib + rt.size();
             rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, j.ld, 0, cfg_.tol});
@@ -1001,9 +1038,9 @@ private:
             ++launches_fact_;
         }
         std::vector<int> ranks(jobs.size());
+        const double tw0 = wall();
         cuda_check(cudaMemcpyAsync(ranks.data(), ib, sizeof(int) * jobs.size(), cudaMemcpyDeviceToHost, stream_),
                    "rank");
-        const double tw0 = wall();
         cuda_check(cudaStreamSynchronize(stream_), "rank readback");
         t_rank_wait_ += wall() - tw0;
         pinned_.reset();  // every staged upload before the readback has landed
@@ -1179,10 +1216,10 @@ private:
             launch_row_norms<T>(reinterpret_cast<const RowNormTask<T>*>(d + o_t), (int)tasks.size(), (int)tot, d_norms,
                                 stream_);
             ++launches_fact_;
+            const double tw0 = wall();
             cuda_check(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * (size_t)tot, cudaMemcpyDeviceToHost,
                                        stream_),
                        "row norms");
-            const double tw0 = wall();
             cuda_check(cudaStreamSynchronize(stream_), "row norm readback");
             t_rank_wait_ += wall() - tw0;
             pinned_.reset();

@@ -81,9 +81,11 @@ public:
     virtual std::vector<int> bottom_info() const = 0;
     virtual void stats(double* times, long long* counters) const = 0;
     virtual std::vector<double> level_times() const = 0;
-    // Host side of the last factorize, seconds: [wall, waits for the rank
-    // readbacks, device allocations of the arenas, scratch growth (with its
-    // stream wait), solve-plan build]
+    // Host side of the last factorize, seconds: [wall, waits for the device
+    // readbacks (ranks, row norms), device allocations of the arenas, scratch
+    // growth, solve-plan build, then the host time of each level phase summed
+    // over levels: fill, elimination, row shift, scaling, sparsification,
+    // merge] (waits and allocations are part of the phase times)
     virtual std::vector<double> host_times() const = 0;
     // One preconditioner application outside the CUDA graph with every sweep
     // wave timed: returns [ms, ops, smem elements] per wave (forward waves then

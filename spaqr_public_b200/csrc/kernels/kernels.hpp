@@ -52,6 +52,15 @@ struct TileRef {
 template <class T>
 void launch_panel(const QRTask<T>* tasks, const int* task_ids, int ntasks, int p, int smem_rows,
                   cudaStream_t s);
+// Panel p of every listed task on a thread-block cluster of `cluster` CTAs
+// (row slabs in shared memory, one DSMEM reduction per column). Every task's
+// panel height m - p must be at least 32 * cluster when cluster > 1 and at
+// most panel_cl_max_rows(cluster); max_rows = the largest height in the list.
+template <class T>
+cudaError_t launch_panel_cl(const QRTask<T>* tasks, const int* task_ids, int ntasks, int cluster, int max_rows, int p,
+                            cudaStream_t s);
+template <class T>
+size_t panel_cl_max_rows(int cluster);
 // Trailing update after panel p: tiles of kTN columns of [fac(:, p+NB:k) | tr].
 template <class T>
 void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s);

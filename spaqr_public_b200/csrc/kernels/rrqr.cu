@@ -200,6 +200,10 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
         __syncthreads();
         const int gp = s_gp, gc = s_gc;
         const int pc = gc;
+        if (pc < 0) {  // no finite partial norm left (NaN input): stop here, uniformly over the cluster
+            rank = k;
+            break;
+        }
         const int owner = pc / W;
         // 2. reflector of the pivot column (rows k..m-1) by its owner
         if (cr == owner) {
