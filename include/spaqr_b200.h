@@ -221,6 +221,22 @@ int spq_get_host_times(spq_tree* t, double* out11);
  * cached, unused part to the device. */
 int spq_trim_memory(void);
 
+/* Autotuner of launch shapes that do not change results (today the cluster
+ * size of the blocked RRQR of sparsifyD, src/tree.cpp:1022-1049, whose output
+ * is bitwise the same for every size). No counterpart in the reference, which
+ * has no launch shapes. Process-wide, shared by all handles.
+ *   mode 0: off, the built-in default shape;
+ *   mode 1: online (default), each fitting shape is timed twice per size
+ *           bucket as factorizations run, then the fastest is used;
+ *   mode 2: frozen, only the table (e.g. loaded from a file) is used.
+ * save/load write/read a text table (one line per bucket and shape); load
+ * merges into the current table. */
+int spq_autotune_set_mode(int mode);
+int spq_autotune_get(int* mode, int* entries);
+int spq_autotune_reset(void);
+int spq_autotune_save(const char* path);
+int spq_autotune_load(const char* path);
+
 /* A <- A * diag(1/||A_j||) * 10, in place on val (spaQR.cpp:131-147). */
 int spq_column_normalize(int m, int n, const int* colptr, const int* rowind, double* val);
 

@@ -5,8 +5,8 @@ C ABI in ``include/spaqr_b200.h``); this package is its Python mirror of the
 reference's ``Tree`` / ``gmres`` / ``cgls`` surface plus the seeded workload
 generators.
 """
-from .tree import (FP32, FP64, Tree, cgls, column_normalize, factorize_batch, gmres, gmres_adjoint,  # noqa: F401
-                   launches, solve_to_residual)
+from .tree import (FP32, FP64, Tree, autotune, cgls, column_normalize, factorize_batch, gmres,  # noqa: F401
+                   gmres_adjoint, launches, solve_to_residual)
 
 __all__ = ["Tree", "gmres", "gmres_adjoint", "cgls", "solve_to_residual", "launches", "column_normalize",
-           "factorize_batch", "FP32", "FP64"]
+           "factorize_batch", "autotune", "FP32", "FP64"]

@@ -65,6 +65,11 @@ SIGNATURES = {
     "spq_get_level_times": (_i, [_p, _dp]),
     "spq_get_host_times": (_i, [_p, _dp]),
     "spq_trim_memory": (_i, []),
+    "spq_autotune_set_mode": (_i, [_i]),
+    "spq_autotune_get": (_i, [_ip, _ip]),
+    "spq_autotune_reset": (_i, []),
+    "spq_autotune_save": (_i, [C.c_char_p]),
+    "spq_autotune_load": (_i, [C.c_char_p]),
     "spq_column_normalize": (_i, [_i, _i, _ip, _ip, _dp]),
     "spq_solve_to_residual": (_i, [_p, _i, _i, _ip, _ip, _dp, _dp, _dp, _d, _d, _i, _i, _ip, _dp]),
     "spq_solve_to_residual_dev": (_i, [_p, _i, _p, _p, _p, _p, _p, _d, _d, _i, _i, _ip, _dp]),

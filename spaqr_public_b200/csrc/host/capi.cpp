@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../../include/spaqr_b200.h"
+#include "autotune.hpp"
 #include "engine.hpp"
 #include "krylov.hpp"
 
@@ -762,6 +763,30 @@ int spq_trim_memory(void) {
         trim_device_pools();
         return SPQ_OK;
     });
+}
+int spq_autotune_set_mode(int mode) {
+    if (mode < 0 || mode > 2) return fail(SPQ_ERR_ARG, "autotune mode must be 0 (off), 1 (online) or 2 (frozen)");
+    spq::Autotuner::get().set_mode(mode);
+    return SPQ_OK;
+}
+int spq_autotune_get(int* mode, int* entries) {
+    if (!mode && !entries) return fail(SPQ_ERR_ARG, "null arguments");
+    if (mode) *mode = spq::Autotuner::get().mode();
+    if (entries) *entries = spq::Autotuner::get().entries();
+    return SPQ_OK;
+}
+int spq_autotune_reset(void) {
+    spq::Autotuner::get().reset();
+    return SPQ_OK;
+}
+int spq_autotune_save(const char* path) {
+    if (!path) return fail(SPQ_ERR_ARG, "null path");
+    return spq::Autotuner::get().save(path) ? SPQ_OK : fail(SPQ_ERR_ARG, std::string("cannot write ") + path);
+}
+int spq_autotune_load(const char* path) {
+    if (!path) return fail(SPQ_ERR_ARG, "null path");
+    return spq::Autotuner::get().load(path) ? SPQ_OK
+                                            : fail(SPQ_ERR_ARG, std::string("cannot read a tuning table from ") + path);
 }
 int spq_get_host_times(spq_tree* t, double* out11) {
     if (!t || !out11) return fail(SPQ_ERR_ARG, "null argument");

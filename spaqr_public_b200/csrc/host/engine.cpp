@@ -6,6 +6,8 @@
 // and issued as batched kernels on the handle's stream.
 #include "engine.hpp"
 
+#include "autotune.hpp"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -1007,14 +1009,32 @@ private:
             while (c < 16 && (j.n + c - 1) / c > 4096) c *= 2;  // keep each CTA's slab <= 4096 columns
             return c;
         };
-        std::map<int, std::vector<int>> groups;
-        for (size_t q = 0; q < jobs.size(); ++q) groups[cluster_of(jobs[q])].push_back((int)q);
+        // Interfaces that fit a 16-CTA cluster take the blocked kernel (its result
+        // is the same for every cluster size, so the size is the autotuner's
+        // choice); wider ones the unblocked kernel with the cluster size above.
+        // Groups: (blocked, size class).
+        std::map<std::pair<int, int>, std::vector<int>> groups;
+        for (size_t q = 0; q < jobs.size(); ++q) {
+            const int blk = rrqr_blk_fits<T>(jobs[q].m, jobs[q].n, 16) ? 1 : 0;
+            groups[{blk, cluster_of(jobs[q])}].push_back((int)q);
+        }
         Upload up;
         size_t o_g = up.add(g), o_r = up.add(rt);
-        std::map<int, size_t> o_ids;
+        std::map<std::pair<int, int>, size_t> o_ids;
         for (auto& kv : groups) o_ids[kv.first] = up.add(kv.second);
         char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
+        Autotuner& tuner = Autotuner::get();
+        const bool tuning = tuner.mode() == 1;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        struct Tuned {
+            TuneKey key;
+            int cluster;
+            cudaEvent_t a, b;
+            const std::vector<int>* q;
+        };
+        std::vector<Tuned> tuned;
         std::vector<size_t> rqs;
         for (auto& kv : groups) {
             int maxm = 0, maxn = 0;
@@ -1022,19 +1042,54 @@ private:
                 maxm = std::max(maxm, jobs[q].m);
                 maxn = std::max(maxn, jobs[q].n);
             }
-            const int cl = kv.first;
-            rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
-                cudaError_t e = launch_rrqr_rm<T>(reinterpret_cast<const RRQRTaskRM<T>*>(d + o_r),
-                                                  reinterpret_cast<const int*>(d + o_ids[cl]), (int)kv.second.size(),
-                                                  cl, maxm, maxn, stream_);
-                if (e != cudaSuccess && cl > 8) {  // 16-CTA clusters are an opt-in; fall back to 8
-                    cudaGetLastError();
-                    e = launch_rrqr_rm<T>(reinterpret_cast<const RRQRTaskRM<T>*>(d + o_r),
-                                          reinterpret_cast<const int*>(d + o_ids[cl]), (int)kv.second.size(), 8,
-                                          maxm, maxn, stream_);
+            const int nt = (int)kv.second.size();
+            const RRQRTaskRM<T>* dt = reinterpret_cast<const RRQRTaskRM<T>*>(d + o_r);
+            const int* di = reinterpret_cast<const int*>(d + o_ids[kv.first]);
+            if (kv.first.first == 1) {
+                // candidates: every cluster size whose slab fits; default: the smallest
+                // that puts at least one CTA on every SM, else the largest
+                std::vector<int> cands;
+                for (int c = 1; c <= 16; c *= 2)
+                    if (rrqr_blk_fits<T>(maxm, maxn, c)) cands.push_back(c);
+                int dflt = cands.back();
+                for (int c : cands)
+                    if ((long long)c * nt >= 148) {
+                        dflt = c;
+                        break;
+                    }
+                const TuneKey key{0, dev, (int)sizeof(T), Autotuner::bucket(maxm), Autotuner::bucket(maxn),
+                                  Autotuner::bucket(nt)};
+                int cl = tuner.choose(key, cands, dflt);
+                cudaEvent_t ea = nullptr, eb = nullptr;
+                if (tuning) {
+                    cuda_check(cudaEventCreate(&ea), "event");
+                    cuda_check(cudaEventCreate(&eb), "event");
+                    cudaEventRecord(ea, stream_);
                 }
-                cuda_check(e, "rrqr launch");
-            }));
+                rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
+                    cudaError_t e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                    while (e != cudaSuccess && cl > 1 && rrqr_blk_fits<T>(maxm, maxn, cl / 2)) {
+                        cudaGetLastError();  // a cluster this large did not launch here: halve it
+                        cl /= 2;
+                        e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                    }
+                    cuda_check(e, "rrqr launch");
+                }));
+                if (tuning) {
+                    cudaEventRecord(eb, stream_);
+                    tuned.push_back(Tuned{key, cl, ea, eb, &kv.second});
+                }
+            } else {
+                const int cl = kv.first.second;
+                rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
+                    cudaError_t e = launch_rrqr_rm<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                    if (e != cudaSuccess && cl > 8) {  // 16-CTA clusters are an opt-in; fall back to 8
+                        cudaGetLastError();
+                        e = launch_rrqr_rm<T>(dt, di, nt, 8, maxm, maxn, stream_);
+                    }
+                    cuda_check(e, "rrqr launch");
+                }));
+            }
             ++launches_fact_;
         }
         std::vector<int> ranks(jobs.size());
@@ -1044,6 +1099,19 @@ private:
         cuda_check(cudaStreamSynchronize(stream_), "rank readback");
         t_rank_wait_ += wall() - tw0;
         pinned_.reset();  // every staged upload before the readback has landed
+        for (auto& tu : tuned) {  // device time per unit of work (m n (r + 1)) of each tuned launch
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, tu.a, tu.b) == cudaSuccess) {
+                double work = 0;
+                for (int q : *tu.q) {
+                    const double r = std::min(std::max(ranks[q], 0), std::min(jobs[q].m, jobs[q].n));
+                    work += (double)jobs[q].m * jobs[q].n * (r + 1);
+                }
+                if (work > 0) tuner.record(tu.key, tu.cluster, ms / work);
+            }
+            cudaEventDestroy(tu.a);
+            cudaEventDestroy(tu.b);
+        }
         size_t gi = 0;
         for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
             const size_t rq = rqs[gi++];

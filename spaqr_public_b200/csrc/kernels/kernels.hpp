@@ -105,6 +105,17 @@ struct RRQRTaskRM {
 template <class T>
 cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,
                            int max_n, cudaStream_t s);
+// Blocked form of the same factorization (LAPACK dlaqps: the update of the
+// rows below a block of pivot steps is deferred to one rank-NB update, NB = 32
+// in FP32 and 16 in FP64). Each CTA keeps the F factor of its slab and a copy
+// of the block's reflectors in shared memory; rrqr_blk_fits tells whether a
+// launch shape fits (else launch_rrqr_blk returns cudaErrorInvalidValue
+// without a launch). The result does not depend on the cluster size.
+template <class T>
+bool rrqr_blk_fits(int max_m, int max_n, int cluster);
+template <class T>
+cudaError_t launch_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,
+                            int max_n, cudaStream_t s);
 // Write-back after the cluster RRQR, with the rank r known on the host.
 template <class T>
 struct SparsWBRM {

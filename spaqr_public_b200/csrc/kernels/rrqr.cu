@@ -26,6 +26,7 @@
 #include <climits>
 
 #include "kernels.hpp"
+#include "rrqr_common.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -35,62 +36,7 @@ namespace {
 constexpr int kRRThreads = 512;
 constexpr int kU = 4;  // column tiles per lane in the update passes
 
-template <class T>
-__device__ __forceinline__ T wsum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-template <class T>
-__device__ T bsum(T v, T* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    v = wsum(v);
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        T r = lane < nw ? red[lane] : T(0);
-        r = wsum(r);
-        if (lane == 0) red[0] = r;
-    }
-    __syncthreads();
-    return red[0];
-}
-
-template <class T>
-struct Tol3z;
-template <>
-struct Tol3z<double> {
-    static __device__ double v() { return 1.0536712127723509e-08; }  // sqrt(2^-53)
-};
-template <>
-struct Tol3z<float> {
-    static __device__ float v() { return 2.44140625e-04f; }  // sqrt(2^-24)
-};
-
-__device__ __forceinline__ double dhypot(double a, double b) { return hypot(a, b); }
-__device__ __forceinline__ float dhypot(float a, float b) { return hypotf(a, b); }
-
-// 16-byte vector of adjacent row elements (columns of C).
-template <class T>
-struct Vec;
-template <>
-struct Vec<float> {
-    using type = float4;
-    static constexpr int n = 4;
-};
-template <>
-struct Vec<double> {
-    using type = double2;
-    static constexpr int n = 2;
-};
-
-// (value, position, column): larger value wins, then the smaller position.
-template <class T>
-__device__ __forceinline__ bool better(T v, int p, T bv, int bp) {
-    return v > bv || (v == bv && p < bp);
-}
+using namespace rrqr;
 
 template <class T>
 __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids,

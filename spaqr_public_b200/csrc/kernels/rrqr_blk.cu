@@ -1,0 +1,519 @@
+// Blocked truncated column-pivoted Householder QR of the sparsification
+// matrices (sparsifyD, src/tree.cpp:1022-1049; dgeqp3 + choose_rank,
+// src/util.cpp:466-477, 795-816), one thread-block cluster per interface.
+//
+// dgeqp3 factors in blocks of NB pivot steps (LAPACK dlaqps): inside a block
+// only the pivot column and the pivot row of each step are brought up to date;
+// the rest of the matrix waits for one rank-NB update at the end of the block,
+// C(k:m, :) -= V_b F^T, with
+//     V_b  the block's reflectors (m x NB),
+//     F    (n x NB), F(c, j) = tau_j v_j^T C_j(:, c), C_j = C as left by reflectors < j,
+// built column by column from the block-start matrix C_bs:
+//     F(:, j) = tau_j (C_bs(k:m, :)^T v_j - F(:, 0:j) (V_b(k:m, 0:j)^T v_j)).
+// A pivot step therefore reads C once (the product C_bs^T v_j) instead of
+// twice plus a write (the reflector applied at once), which is what bounds
+// the unblocked kernel on the many-interface levels.
+//
+// Layout as in the unblocked kernel: C (m x n) row-major with stride ldc, the
+// columns split in contiguous 32-aligned slabs over the CTAs of the cluster;
+// pivoting is kept as positions (pos / colat), so ties break on the current
+// position exactly as LAPACK's swaps would. Each CTA keeps F of its slab
+// (l-major: F(l, c) at l * Wp + c) and its own copy of V_b (m x NB, row-major,
+// rows padded to NB + 1) in shared memory: the reflector of each step reaches
+// every CTA through DSMEM anyway, so V_b never touches global memory.
+//
+// Per pivot step k (block column jb):
+//   1. arg-max of the partial norms: per CTA, cluster barrier, DSMEM reduction;
+//   2. the owner of the pivot column applies the block's earlier reflectors to
+//      it (C(k:m, pc) -= V_b F(pc, :)^T), builds the reflector (dlarfg) and the
+//      product s_aux = V_b(k:m, 0:jb)^T v; cluster barrier, the other CTAs copy
+//      v and s_aux through DSMEM and append v to their V_b;
+//   3. every CTA forms F(jb, c) over its slab (one pass over C_bs(k+1:m, slab),
+//      row chunks whose count depends only on m and k, so the result does not
+//      depend on the cluster size), updates pivot row k of its columns and
+//      downdates their norms; a norm whose downdate lost accuracy (dlaqps's
+//      tol3z test) is recomputed at once from C_bs - V_b F^T of its column.
+// After the block, the rows below it get C -= V_b F^T (active columns only).
+// The loop stops at the rank (|R_kk| < tol |R_00|); the rows of R above it are
+// already final, so no trailing update follows the last block.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "kernels.hpp"
+#include "rrqr_common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace spq {
+namespace {
+
+using namespace rrqr;
+
+constexpr int kBT = 512;                    // threads per CTA
+constexpr int kGMax = 8;                    // row chunks of the per-step product (fixed: cluster-independent)
+constexpr int kBU = 4;                      // 16-byte column vectors per lane in the per-step product
+constexpr int kTRows = 64;                  // rows of a trailing-update tile (16 row groups of 4)
+constexpr size_t kBlkSmemCap = 216 * 1024;  // dynamic shared memory of one CTA (static use is ~3 KB)
+
+// Pivot steps per block: 32 in FP32, 16 in FP64 (the F and V_b copies of a CTA
+// stay within shared memory for slabs of a few hundred columns).
+template <class T>
+struct BlkNB {
+    static constexpr int v = sizeof(T) == 4 ? 32 : 16;
+};
+
+// Shared-memory elements of one CTA for slab width Wp (a multiple of the
+// vector tile 32 * VEC) and m rows: F, partials, reflector, V_b (rows padded).
+template <class T>
+__host__ __device__ constexpr size_t blk_smem_elems(int Wp, int m) {
+    return (size_t)(BlkNB<T>::v + kGMax) * Wp + (size_t)((m + 7) & ~7) * (BlkNB<T>::v + 2);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int Wp, int mpad) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int VEC = Vec<T>::n;
+    constexpr int kBNB = BlkNB<T>::v;
+    constexpr int VP = kBNB + 1;  // padded V_b row: conflict-free row-parallel reads
+    using VT = typename Vec<T>::type;
+    T* F = reinterpret_cast<T*>(smem_raw);  // kBNB x Wp, l-major
+    T* part = F + (size_t)kBNB * Wp;        // kGMax x Wp: row-chunk partials of C_bs^T v
+    T* vsh = part + (size_t)kGMax * Wp;     // mpad: the current reflector
+    T* Vs = vsh + mpad;                     // mpad x VP: V_b(i, l) at i * VP + l
+    __shared__ T red[32];
+    __shared__ T wv[32];
+    __shared__ int wp[32], wc[32];
+    __shared__ T s_val, s_beta, s_tau, s_alpha;
+    __shared__ int s_pos, s_col, s_gp, s_gc, s_nflag;
+    __shared__ T s_aux[kBNB];  // V_b(k:m, l)^T v for l < jb, zero after
+    __shared__ T s_fp[kBNB];   // F(l, pivot column), zero for l >= jb
+    __shared__ T s_wpart[(kBT / 32) * kBNB];
+
+    cg::cluster_group cl = cg::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int cr = (int)cl.block_rank();
+    const RRQRTaskRM<T> t = tasks[ids[blockIdx.x / CL]];
+    const int m = t.m, n = t.n;
+    const size_t ld = (size_t)t.ldc;
+    T* C = t.C;
+    const int W = (((n + CL - 1) / CL) + 31) & ~31;
+    const int j0 = min(n, cr * W), j1 = min(n, j0 + W);
+    const int Wc = j1 - j0;
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+
+    for (int j = j0 + tid; j < j1; j += nth) {
+        T s = T(0);
+#pragma unroll 8
+        for (int i = 0; i < m; ++i) {
+            const T v = C[i * ld + j];
+            s += v * v;
+        }
+        const T nv = sqrt(s);
+        t.vn1[j] = nv;
+        t.vn2[j] = nv;
+        t.pos[j] = j;
+        t.colat[j] = j;
+    }
+    cl.sync();
+
+    const int kmax = min(m, n);
+    const double tol = t.tol;
+    int rank = kmax;
+    const int ksteps = (tol != 0.0 && tol >= 1.0) ? 0 : kmax;
+    if (ksteps == 0) rank = 0;
+    T r00 = T(0);
+    bool done = false;
+    int k = 0;
+    while (k < ksteps && !done) {
+        const int k0 = k;
+        const int nbk = min(kBNB, ksteps - k0);
+        // a block starts from zero F and V_b: entries past the current step are
+        // exact zeros, so the products below run over all kBNB columns unmasked
+        for (int e = tid; e < kBNB * Wp; e += nth) F[e] = T(0);
+        for (int e = tid; e < m * VP; e += nth) Vs[e] = T(0);
+        __syncthreads();
+        int steps = 0;
+        for (int jb = 0; jb < nbk; ++jb) {
+            k = k0 + jb;
+            // 1. pivot: largest partial norm, ties to the smallest position
+            T bv = T(-1);
+            int bp = INT_MAX, bc = -1;
+            for (int j = j0 + tid; j < j1; j += nth) {
+                const int p = t.pos[j];
+                if (p < k) continue;
+                const T v = t.vn1[j];
+                if (better(v, p, bv, bp)) {
+                    bv = v;
+                    bp = p;
+                    bc = j;
+                }
+            }
+            warp_best(bv, bp, bc);
+            if (lane == 0) {
+                wv[warp] = bv;
+                wp[warp] = bp;
+                wc[warp] = bc;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                bv = lane < nw ? wv[lane] : T(-1);
+                bp = lane < nw ? wp[lane] : INT_MAX;
+                bc = lane < nw ? wc[lane] : -1;
+                warp_best(bv, bp, bc);
+                if (lane == 0) {
+                    s_val = bv;
+                    s_pos = bp;
+                    s_col = bc;
+                }
+            }
+            cl.sync();
+            if (warp == 0) {  // every CTA reduces the cluster's candidates (lane r reads CTA r)
+                T v = T(-1);
+                int p = INT_MAX, c = -1;
+                if (lane < CL) {
+                    c = *cl.map_shared_rank(&s_col, lane);
+                    if (c >= 0) {
+                        v = *cl.map_shared_rank(&s_val, lane);
+                        p = *cl.map_shared_rank(&s_pos, lane);
+                    }
+                }
+                warp_best(v, p, c);
+                if (lane == 0) {
+                    s_gp = p;
+                    s_gc = c;
+                }
+            }
+            __syncthreads();
+            const int gp = s_gp, pc = s_gc;
+            if (pc < 0) {  // no finite partial norm left (NaN input): stop, uniformly over the cluster
+                rank = k;
+                done = true;
+                break;
+            }
+            const int owner = pc / W;
+            // 2. the owner brings the pivot column up to date and builds its reflector
+            if (cr == owner) {
+                if (tid < kBNB) s_fp[tid] = F[tid * Wp + (pc - j0)];  // zero for l >= jb
+                __syncthreads();
+                T acc = T(0);
+                for (int i = k + tid; i < m; i += nth) {
+                    T x = C[i * ld + pc];
+                    if (jb > 0) {
+#pragma unroll
+                        for (int l = 0; l < kBNB; ++l) x -= Vs[i * VP + l] * s_fp[l];
+                        C[i * ld + pc] = x;
+                    }
+                    if (i == k)
+                        s_alpha = x;
+                    else
+                        acc += x * x;
+                }
+                const T xn2 = bsum(acc, red);
+                const T alpha = s_alpha;
+                T tau, beta, scal;
+                if (xn2 == T(0)) {
+                    tau = T(0);
+                    beta = alpha;
+                    scal = T(1);
+                } else {
+                    const T nrm = dhypot(alpha, (T)sqrt(xn2));
+                    beta = alpha >= T(0) ? -nrm : nrm;
+                    tau = (beta - alpha) / beta;
+                    scal = T(1) / (alpha - beta);
+                }
+                // the reflector and the rows of s_aux in one pass (same row mapping as above)
+                T sa[kBNB];
+#pragma unroll
+                for (int l = 0; l < kBNB; ++l) sa[l] = T(0);
+                for (int i = k + tid; i < m; i += nth) {
+                    T v;
+                    if (i == k) {
+                        v = T(1);
+                        C[i * ld + pc] = beta;
+                    } else {
+                        v = C[i * ld + pc];
+                        if (tau != T(0)) {
+                            v *= scal;
+                            C[i * ld + pc] = v;
+                        }
+                    }
+                    vsh[i] = v;
+#pragma unroll
+                    for (int l = 0; l < kBNB; ++l) sa[l] += Vs[i * VP + l] * v;  // columns >= jb are zero
+                }
+                // warp transpose-sum: lane l (mod kBNB) ends with the warp's sum of sa[l]
+#pragma unroll
+                for (int sft = kBNB / 2; sft >= 1; sft >>= 1) {
+                    const bool upper = (lane & sft) != 0;
+#pragma unroll
+                    for (int q = 0; q < sft; ++q) {
+                        const T send = upper ? sa[q] : sa[q + sft];
+                        const T keep = upper ? sa[q + sft] : sa[q];
+                        sa[q] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+                    }
+                }
+                // with kBNB < 32, lanes l and l + kBNB hold halves of the same sum
+                T part0 = sa[0];
+                if (kBNB < 32) part0 += __shfl_xor_sync(0xffffffffu, part0, kBNB);
+                if (lane < kBNB) s_wpart[warp * kBNB + lane] = part0;
+                __syncthreads();
+                if (tid < kBNB) {
+                    T s = T(0);
+                    for (int q = 0; q < nw; ++q) s += s_wpart[q * kBNB + tid];
+                    s_aux[tid] = s;
+                }
+                if (tid == 0) {
+                    s_beta = beta;
+                    s_tau = tau;
+                    t.tau[k] = tau;
+                }
+            }
+            cl.sync();
+            const T beta = *cl.map_shared_rank(&s_beta, owner);
+            const T tau = *cl.map_shared_rank(&s_tau, owner);
+            if (cr != owner) {
+                const T* ov = cl.map_shared_rank(vsh, owner);
+                for (int i = k + tid; i < m; i += nth) vsh[i] = ov[i];
+                if (tid < kBNB) s_aux[tid] = *cl.map_shared_rank(&s_aux[tid], owner);
+            }
+            if (tol != 0.0 && kmax > 1) {
+                if (k == 0) {
+                    r00 = fabs(beta);
+                } else if (!((double)fabs(beta) / (double)r00 >= tol)) {
+                    rank = k;
+                    done = true;
+                    break;  // uniform over the cluster: every CTA read the same beta
+                }
+            }
+            if (cr == 0 && tid == 0) {  // LAPACK's column swap, as positions
+                const int c0 = t.colat[k];
+                t.colat[gp] = c0;
+                t.pos[c0] = gp;
+                t.colat[k] = pc;
+                t.pos[pc] = k;
+            }
+            if (tid == 0) s_nflag = 0;
+            __syncthreads();
+            for (int i = k + tid; i < m; i += nth) Vs[i * VP + jb] = vsh[i];  // V_b(:, jb); rows < k stay 0
+            // 3a. partials of C_bs(k+1:m, slab)^T v: lanes own 16-byte column vectors
+            //     (kBU per lane), the rows are cut in Gs chunks taken by different warps
+            const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);
+            const int ntg = (nvt + kBU - 1) / kBU;
+            const int Gs = max(1, min(kGMax, (m - k - 1 + 31) / 32));
+            const int Lr = (m - k - 1 + Gs - 1) / Gs;
+            constexpr int kRowUnroll = sizeof(T) == 4 ? 4 : 2;
+            if (tau != T(0)) {
+                for (int item = warp; item < Gs * ntg; item += nw) {
+                    const int g = item % Gs, tg = item / Gs;
+                    const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
+                    T sv[kBU][VEC];
+                    const T* cp[kBU];
+#pragma unroll
+                    for (int u = 0; u < kBU; ++u) {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) sv[u][q] = T(0);
+                        const int jl = ((tg * kBU + u) * 32 + lane) * VEC;
+                        cp[u] = C + j0 + (jl < Wc ? jl : 0);  // past the slab: reads its first vector
+                    }
+#pragma unroll kRowUnroll
+                    for (int i = i0; i < i1; ++i) {
+                        const T vi = vsh[i];
+                        VT x[kBU];
+#pragma unroll
+                        for (int u = 0; u < kBU; ++u) x[u] = *reinterpret_cast<const VT*>(cp[u] + i * ld);
+#pragma unroll
+                        for (int u = 0; u < kBU; ++u) {
+                            const T* xs = reinterpret_cast<const T*>(&x[u]);
+#pragma unroll
+                            for (int q = 0; q < VEC; ++q) sv[u][q] += vi * xs[q];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kBU; ++u) {
+                        const int jl = ((tg * kBU + u) * 32 + lane) * VEC;
+                        if (jl < Wp) {
+#pragma unroll
+                            for (int q = 0; q < VEC; ++q) part[g * Wp + jl + q] = sv[u][q];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // 3b. F(jb, c), pivot row k, partial norms
+            T vk[kBNB];  // V_b(k, 0:jb], zero after
+#pragma unroll
+            for (int l = 0; l < kBNB; ++l) vk[l] = Vs[k * VP + l];
+            for (int jl = tid; jl < Wc; jl += nth) {
+                const int c = j0 + jl;
+                if (c == pc || t.pos[c] < k) continue;
+                const T ck0 = C[k * ld + c];
+                if (tau != T(0)) {
+                    T g = ck0;
+                    for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
+                    T corr = T(0);
+#pragma unroll
+                    for (int l = 0; l < kBNB; ++l) corr += F[l * Wp + jl] * s_aux[l];
+                    F[jb * Wp + jl] = tau * (g - corr);
+                }
+                T upd = T(0);
+#pragma unroll
+                for (int l = 0; l < kBNB; ++l) upd += vk[l] * F[l * Wp + jl];
+                const T ck = ck0 - upd;
+                C[k * ld + c] = ck;
+                const T n1 = t.vn1[c];
+                if (n1 != T(0)) {
+                    const T rk = fabs(ck) / n1;
+                    T temp = T(1) - rk * rk;
+                    temp = temp < T(0) ? T(0) : temp;
+                    const T qq = n1 / t.vn2[c];
+                    const T temp2 = temp * qq * qq;
+                    if (temp2 <= Tol3z<T>::v()) {
+                        t.vn2[c] = T(-1);  // recomputed below from the up-to-date column
+                        atomicAdd(&s_nflag, 1);
+                    } else {
+                        t.vn1[c] = n1 * (T)sqrt(temp);
+                    }
+                }
+            }
+            __syncthreads();
+            // 3c. norms whose downdate lost accuracy, from C_bs(k+1:m, c) - V_b F(:, c)^T
+            //     (one warp per column)
+            if (s_nflag > 0) {
+                for (int jl = warp; jl < Wc; jl += nw) {
+                    const int c = j0 + jl;
+                    if (!(t.vn2[c] < T(0)) || c == pc || t.pos[c] < k) continue;
+                    T fr[kBNB];
+#pragma unroll
+                    for (int l = 0; l < kBNB; ++l) fr[l] = F[l * Wp + jl];
+                    T ss = T(0);
+                    for (int i = k + 1 + lane; i < m; i += 32) {
+                        T x = C[i * ld + c];
+#pragma unroll
+                        for (int l = 0; l < kBNB; ++l) x -= Vs[i * VP + l] * fr[l];
+                        ss += x * x;
+                    }
+                    ss = wsum(ss);
+                    if (lane == 0) {
+                        const T nv = (k + 1 < m) ? (T)sqrt(ss) : T(0);
+                        t.vn1[c] = nv;
+                        t.vn2[c] = nv;
+                    }
+                }
+            }
+            cl.sync();  // positions and norms of step k visible to every CTA
+            steps = jb + 1;
+        }
+        if (done) break;
+        k = k0 + steps;
+        if (k >= ksteps) break;  // full rank reached: rows of R final, nothing below to update
+        // 4. C(k:m, c) -= V_b(k:m, :) F(:, c) for the active columns of the slab: a thread
+        //    owns 4 rows x one 16-byte column vector of each 64 x (32 VEC) tile
+        const int rg = tid >> 5;  // 16 row groups of 4 rows
+        for (int r0 = k; r0 < m; r0 += kTRows) {
+            for (int c0 = 0; c0 < Wc; c0 += 32 * VEC) {
+                const int cl0 = c0 + lane * VEC;
+                if (cl0 >= Wc) continue;
+                VT x[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int i = min(r0 + rg * 4 + r, m - 1);
+                    x[r] = *reinterpret_cast<const VT*>(C + i * ld + j0 + cl0);
+                }
+                T acc[4][VEC];
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) acc[r][q] = T(0);
+#pragma unroll 4
+                for (int l = 0; l < kBNB; ++l) {
+                    const VT b = *reinterpret_cast<const VT*>(F + l * Wp + cl0);
+                    const T* bs = reinterpret_cast<const T*>(&b);
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const T a = Vs[min(r0 + rg * 4 + r, m - 1) * VP + l];
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) acc[r][q] += a * bs[q];
+                    }
+                }
+                bool act[VEC];
+                bool all = true;
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    act[q] = cl0 + q < Wc && t.pos[j0 + cl0 + q] >= k;
+                    all = all && act[q];
+                }
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int i = r0 + rg * 4 + r;
+                    if (i >= m) break;
+                    T* xs = reinterpret_cast<T*>(&x[r]);
+                    T* px = C + i * ld + j0 + cl0;
+                    if (all) {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) xs[q] -= acc[r][q];
+                        *reinterpret_cast<VT*>(px) = x[r];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q)
+                            if (act[q]) px[q] = xs[q] - acc[r][q];
+                    }
+                }
+            }
+        }
+        __syncthreads();  // F and V_b are cleared for the next block
+    }
+    // No CTA may exit while another still reads its shared memory (the early
+    // exit at the rank leaves right after the DSMEM reads of that step).
+    cl.sync();
+    if (cr == 0 && tid == 0) *t.rank = rank;
+}
+
+}  // namespace
+
+template <class T>
+bool rrqr_blk_fits(int max_m, int max_n, int cluster) {
+    constexpr int tile = 32 * Vec<T>::n;
+    if (cluster < 1 || max_m < 1) return false;
+    const int W = (((max_n + cluster - 1) / cluster) + 31) & ~31;
+    const int Wp = (W + tile - 1) / tile * tile;
+    return blk_smem_elems<T>(Wp, max_m) * sizeof(T) <= kBlkSmemCap;
+}
+
+template <class T>
+cudaError_t launch_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,
+                            int max_n, cudaStream_t s) {
+    if (ntasks <= 0) return cudaSuccess;
+    if (!rrqr_blk_fits<T>(max_m, max_n, cluster)) return cudaErrorInvalidValue;
+    constexpr int tile = 32 * Vec<T>::n;
+    const int W = (((max_n + cluster - 1) / cluster) + 31) & ~31;
+    const int Wp = (W + tile - 1) / tile * tile;
+    const int mpad = (max_m + 7) & ~7;
+    const size_t smem_bytes = blk_smem_elems<T>(Wp, max_m) * sizeof(T);
+    once_per_device(reinterpret_cast<const void*>(&k_rrqr_blk<T>), [] {
+        cudaFuncSetAttribute(k_rrqr_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlkSmemCap);
+        cudaFuncSetAttribute(k_rrqr_blk<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(ntasks * cluster), 1, 1);
+    cfg.blockDim = dim3(kBT, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_rrqr_blk<T>, tasks, ids, Wp, mpad);
+}
+
+template bool rrqr_blk_fits<double>(int, int, int);
+template bool rrqr_blk_fits<float>(int, int, int);
+template cudaError_t launch_rrqr_blk<double>(const RRQRTaskRM<double>*, const int*, int, int, int, int,
+                                             cudaStream_t);
+template cudaError_t launch_rrqr_blk<float>(const RRQRTaskRM<float>*, const int*, int, int, int, int, cudaStream_t);
+
+}  // namespace spq

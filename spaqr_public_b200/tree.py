@@ -250,3 +250,21 @@ def column_normalize(A):
     out = va.copy()
     check(lib().spq_column_normalize(m, n, iptr(cp), iptr(ri), dptr(out)))
     return (m, n, cp, ri, out)
+
+
+def autotune(mode=None, reset=False, save=None, load=None):
+    """The library's launch-shape autotuner (process-wide; shapes it picks never
+    change results). ``mode``: 0 off, 1 online (default), 2 frozen table;
+    ``reset`` clears the table; ``save`` / ``load`` a text table file.
+    Returns (mode, number of table entries)."""
+    if reset:
+        check(lib().spq_autotune_reset())
+    if load is not None:
+        check(lib().spq_autotune_load(str(load).encode()))
+    if mode is not None:
+        check(lib().spq_autotune_set_mode(int(mode)))
+    if save is not None:
+        check(lib().spq_autotune_save(str(save).encode()))
+    md, ne = C.c_int(0), C.c_int(0)
+    check(lib().spq_autotune_get(C.byref(md), C.byref(ne)))
+    return md.value, ne.value
