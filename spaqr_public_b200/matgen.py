@@ -277,7 +277,7 @@ def write_mm(path, A):
         f.write("%%MatrixMarket matrix coordinate real general\n")
         f.write(f"{m} {n} {nnz}\n")
         for r, c, v in zip(ri, cols, va):
-            f.write(f"{r + 1} {c + 1} {v!r}\n")
+            f.write(f"{int(r) + 1} {int(c) + 1} {float(v)!r}\n")
 
 
 def read_mm(path):
