@@ -17,25 +17,30 @@
 // Layout as in the unblocked kernel: C (m x n) row-major with stride ldc, the
 // columns split in contiguous 32-aligned slabs over the CTAs of the cluster;
 // pivoting is kept as positions (pos / colat), so ties break on the current
-// position exactly as LAPACK's swaps would. Each CTA keeps F of its slab
-// (l-major: F(l, c) at l * Wp + c) and its own copy of V_b (m x NB, row-major,
-// rows padded to NB + 1) in shared memory: the reflector of each step reaches
-// every CTA through DSMEM anyway, so V_b never touches global memory.
+// position exactly as LAPACK's swaps would. Each CTA keeps in shared memory
+// the F rows of its slab (l-major: F(l, c) at l * Wp + c), its own copy of V_b
+// (m x NB, row-major, rows padded to NB + 1), and the partial norms and
+// positions of its slab's columns.
 //
-// Per pivot step k (block column jb):
-//   1. arg-max of the partial norms: per CTA, cluster barrier, DSMEM reduction;
-//   2. the owner of the pivot column applies the block's earlier reflectors to
-//      it (C(k:m, pc) -= V_b F(pc, :)^T), builds the reflector (dlarfg) and the
-//      product s_aux = V_b(k:m, 0:jb)^T v; cluster barrier, the other CTAs copy
-//      v and s_aux through DSMEM and append v to their V_b;
+// Per pivot step k (block column jb), with ONE cluster barrier:
+//   1. arg-max of the partial norms over the slab; the CTAs publish their
+//      candidates in alternating slots, cluster barrier, each CTA reduces the
+//      candidates through DSMEM;
+//   2. every CTA brings the pivot column up to date (C_bs(k:m, pc) -
+//      V_b F(pc, :)^T, reading F(pc, :) from the owner's shared memory), builds
+//      the reflector (dlarfg) and s_aux = V_b(k:m, 0:jb)^T v: same inputs and
+//      arithmetic give bitwise the same v in every CTA, so nothing is
+//      broadcast; the swap is applied to the positions each CTA keeps;
 //   3. every CTA forms F(jb, c) over its slab (one pass over C_bs(k+1:m, slab),
 //      row chunks whose count depends only on m and k, so the result does not
 //      depend on the cluster size), updates pivot row k of its columns and
 //      downdates their norms; a norm whose downdate lost accuracy (dlaqps's
 //      tol3z test) is recomputed at once from C_bs - V_b F^T of its column.
-// After the block, the rows below it get C -= V_b F^T (active columns only).
-// The loop stops at the rank (|R_kk| < tol |R_00|); the rows of R above it are
-// already final, so no trailing update follows the last block.
+// At the end of a block (cluster barrier) the owners store R_kk and the
+// reflector of each pivot in its column, and the rows below the block get
+// C -= V_b F^T (active columns only; cluster barrier). The loop stops at the
+// rank (|R_kk| < tol |R_00|); the rows of R above it are already final, so no
+// trailing update follows the last block.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -65,10 +70,11 @@ struct BlkNB {
 };
 
 // Shared-memory elements of one CTA for slab width Wp (a multiple of the
-// vector tile 32 * VEC) and m rows: F, partials, reflector, V_b (rows padded).
+// vector tile 32 * VEC) and m rows: F, partials, the slab's norms and
+// positions, reflector, V_b (rows padded).
 template <class T>
 __host__ __device__ constexpr size_t blk_smem_elems(int Wp, int m) {
-    return (size_t)(BlkNB<T>::v + kGMax) * Wp + (size_t)((m + 7) & ~7) * (BlkNB<T>::v + 2);
+    return (size_t)(BlkNB<T>::v + kGMax + 3) * Wp + (size_t)((m + 7) & ~7) * (BlkNB<T>::v + 2);
 }
 
 template <class T>
@@ -78,17 +84,24 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
     constexpr int kBNB = BlkNB<T>::v;
     constexpr int VP = kBNB + 1;  // padded V_b row: conflict-free row-parallel reads
     using VT = typename Vec<T>::type;
-    T* F = reinterpret_cast<T*>(smem_raw);  // kBNB x Wp, l-major
-    T* part = F + (size_t)kBNB * Wp;        // kGMax x Wp: row-chunk partials of C_bs^T v
-    T* vsh = part + (size_t)kGMax * Wp;     // mpad: the current reflector
-    T* Vs = vsh + mpad;                     // mpad x VP: V_b(i, l) at i * VP + l
+    T* F = reinterpret_cast<T*>(smem_raw);            // kBNB x Wp, l-major
+    T* part = F + (size_t)kBNB * Wp;                  // kGMax x Wp: row-chunk partials of C_bs^T v
+    T* vn1 = part + (size_t)kGMax * Wp;               // Wp: partial column norms of the slab
+    T* vn2 = vn1 + Wp;                                // Wp: norms at their last recomputation
+    int* pos = reinterpret_cast<int*>(vn2 + Wp);      // Wp: current position of each slab column
+    T* vsh = vn2 + 2 * (size_t)Wp;                    // mpad: the current reflector (pos takes <= Wp elements)
+    T* Vs = vsh + mpad;                               // mpad x VP: V_b(i, l) at i * VP + l
     __shared__ T red[32];
     __shared__ T wv[32];
     __shared__ int wp[32], wc[32];
-    __shared__ T s_val, s_beta, s_tau, s_alpha;
-    __shared__ int s_pos, s_col, s_gp, s_gc, s_nflag;
-    __shared__ T s_aux[kBNB];  // V_b(k:m, l)^T v for l < jb, zero after
-    __shared__ T s_fp[kBNB];   // F(l, pivot column), zero for l >= jb
+    __shared__ T s_val[2];
+    __shared__ int s_pos[2], s_col[2];
+    __shared__ T s_alpha;
+    __shared__ int s_gp, s_gc, s_c0, s_nflag;
+    __shared__ T s_aux[kBNB];    // V_b(k:m, l)^T v for l < jb, zero after
+    __shared__ T s_fp[kBNB];     // F(l, pivot column), zero for l >= jb
+    __shared__ int s_pcs[kBNB];  // pivot column of each step of the block
+    __shared__ T s_betas[kBNB];  // R_kk of each step of the block
     __shared__ T s_wpart[(kBT / 32) * kBNB];
 
     cg::cluster_group cl = cg::this_cluster();
@@ -103,20 +116,19 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
     const int Wc = j1 - j0;
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
 
-    for (int j = j0 + tid; j < j1; j += nth) {
+    for (int jl = tid; jl < Wc; jl += nth) {
         T s = T(0);
 #pragma unroll 8
         for (int i = 0; i < m; ++i) {
-            const T v = C[i * ld + j];
+            const T v = C[i * ld + j0 + jl];
             s += v * v;
         }
         const T nv = sqrt(s);
-        t.vn1[j] = nv;
-        t.vn2[j] = nv;
-        t.pos[j] = j;
-        t.colat[j] = j;
+        vn1[jl] = nv;
+        vn2[jl] = nv;
+        pos[jl] = j0 + jl;
     }
-    cl.sync();
+    __syncthreads();
 
     const int kmax = min(m, n);
     const double tol = t.tol;
@@ -137,17 +149,22 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
         int steps = 0;
         for (int jb = 0; jb < nbk; ++jb) {
             k = k0 + jb;
-            // 1. pivot: largest partial norm, ties to the smallest position
+            const int buf = k & 1;  // candidate slots alternate, so one cluster barrier per step suffices
+            // 1. pivot: largest partial norm, ties to the smallest position; the
+            //    column now at position k is noted for the swap
+            if (tid == 0) s_c0 = -1;
+            __syncthreads();
             T bv = T(-1);
             int bp = INT_MAX, bc = -1;
-            for (int j = j0 + tid; j < j1; j += nth) {
-                const int p = t.pos[j];
+            for (int jl = tid; jl < Wc; jl += nth) {
+                const int p = pos[jl];
                 if (p < k) continue;
-                const T v = t.vn1[j];
+                if (p == k) s_c0 = j0 + jl;
+                const T v = vn1[jl];
                 if (better(v, p, bv, bp)) {
                     bv = v;
                     bp = p;
-                    bc = j;
+                    bc = j0 + jl;
                 }
             }
             warp_best(bv, bp, bc);
@@ -163,9 +180,9 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 bc = lane < nw ? wc[lane] : -1;
                 warp_best(bv, bp, bc);
                 if (lane == 0) {
-                    s_val = bv;
-                    s_pos = bp;
-                    s_col = bc;
+                    s_val[buf] = bv;
+                    s_pos[buf] = bp;
+                    s_col[buf] = bc;
                 }
             }
             cl.sync();
@@ -173,10 +190,10 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 T v = T(-1);
                 int p = INT_MAX, c = -1;
                 if (lane < CL) {
-                    c = *cl.map_shared_rank(&s_col, lane);
+                    c = *cl.map_shared_rank(&s_col[buf], lane);
                     if (c >= 0) {
-                        v = *cl.map_shared_rank(&s_val, lane);
-                        p = *cl.map_shared_rank(&s_pos, lane);
+                        v = *cl.map_shared_rank(&s_val[buf], lane);
+                        p = *cl.map_shared_rank(&s_pos[buf], lane);
                     }
                 }
                 warp_best(v, p, c);
@@ -193,90 +210,72 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 break;
             }
             const int owner = pc / W;
-            // 2. the owner brings the pivot column up to date and builds its reflector
-            if (cr == owner) {
-                if (tid < kBNB) s_fp[tid] = F[tid * Wp + (pc - j0)];  // zero for l >= jb
-                __syncthreads();
-                T acc = T(0);
-                for (int i = k + tid; i < m; i += nth) {
-                    T x = C[i * ld + pc];
-                    if (jb > 0) {
+            // 2. every CTA brings the pivot column up to date (C_bs - V_b F(pc, :)^T, F
+            //    from the owner's shared memory) and builds the same reflector: the
+            //    same inputs and the same arithmetic give bitwise the same v in every
+            //    CTA, so v needs no broadcast. The owner stores the column at the end
+            //    of the block, once no CTA reads its block-start values any more.
+            if (tid < kBNB) s_fp[tid] = *cl.map_shared_rank(&F[tid * Wp + (pc - owner * W)], owner);
+            __syncthreads();
+            T acc = T(0);
+            for (int i = k + tid; i < m; i += nth) {
+                T x = C[i * ld + pc];
 #pragma unroll
-                        for (int l = 0; l < kBNB; ++l) x -= Vs[i * VP + l] * s_fp[l];
-                        C[i * ld + pc] = x;
-                    }
-                    if (i == k)
-                        s_alpha = x;
-                    else
-                        acc += x * x;
-                }
-                const T xn2 = bsum(acc, red);
-                const T alpha = s_alpha;
-                T tau, beta, scal;
-                if (xn2 == T(0)) {
-                    tau = T(0);
-                    beta = alpha;
-                    scal = T(1);
-                } else {
-                    const T nrm = dhypot(alpha, (T)sqrt(xn2));
-                    beta = alpha >= T(0) ? -nrm : nrm;
-                    tau = (beta - alpha) / beta;
-                    scal = T(1) / (alpha - beta);
-                }
-                // the reflector and the rows of s_aux in one pass (same row mapping as above)
-                T sa[kBNB];
+                for (int l = 0; l < kBNB; ++l) x -= Vs[i * VP + l] * s_fp[l];  // zero past jb
+                vsh[i] = x;
+                if (i == k)
+                    s_alpha = x;
+                else
+                    acc += x * x;
+            }
+            const T xn2 = bsum(acc, red);
+            const T alpha = s_alpha;
+            T tau, beta, scal;
+            if (xn2 == T(0)) {
+                tau = T(0);
+                beta = alpha;
+                scal = T(1);
+            } else {
+                const T nrm = dhypot(alpha, (T)sqrt(xn2));
+                beta = alpha >= T(0) ? -nrm : nrm;
+                tau = (beta - alpha) / beta;
+                scal = T(1) / (alpha - beta);
+            }
+            // the reflector, V_b(:, jb) and the rows of s_aux in one pass (same row mapping)
+            T sa[kBNB];
 #pragma unroll
-                for (int l = 0; l < kBNB; ++l) sa[l] = T(0);
-                for (int i = k + tid; i < m; i += nth) {
-                    T v;
-                    if (i == k) {
-                        v = T(1);
-                        C[i * ld + pc] = beta;
-                    } else {
-                        v = C[i * ld + pc];
-                        if (tau != T(0)) {
-                            v *= scal;
-                            C[i * ld + pc] = v;
-                        }
-                    }
-                    vsh[i] = v;
-#pragma unroll
-                    for (int l = 0; l < kBNB; ++l) sa[l] += Vs[i * VP + l] * v;  // columns >= jb are zero
+            for (int l = 0; l < kBNB; ++l) sa[l] = T(0);
+            for (int i = k + tid; i < m; i += nth) {
+                T v = T(1);
+                if (i != k) {
+                    v = vsh[i];
+                    if (tau != T(0)) v *= scal;
                 }
-                // warp transpose-sum: lane l (mod kBNB) ends with the warp's sum of sa[l]
 #pragma unroll
-                for (int sft = kBNB / 2; sft >= 1; sft >>= 1) {
-                    const bool upper = (lane & sft) != 0;
+                for (int l = 0; l < kBNB; ++l) sa[l] += Vs[i * VP + l] * v;  // columns >= jb are zero
+                vsh[i] = v;
+                Vs[i * VP + jb] = v;
+            }
+            // warp transpose-sum: lane l (mod kBNB) ends with the warp's sum of sa[l]
 #pragma unroll
-                    for (int q = 0; q < sft; ++q) {
-                        const T send = upper ? sa[q] : sa[q + sft];
-                        const T keep = upper ? sa[q + sft] : sa[q];
-                        sa[q] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
-                    }
-                }
-                // with kBNB < 32, lanes l and l + kBNB hold halves of the same sum
-                T part0 = sa[0];
-                if (kBNB < 32) part0 += __shfl_xor_sync(0xffffffffu, part0, kBNB);
-                if (lane < kBNB) s_wpart[warp * kBNB + lane] = part0;
-                __syncthreads();
-                if (tid < kBNB) {
-                    T s = T(0);
-                    for (int q = 0; q < nw; ++q) s += s_wpart[q * kBNB + tid];
-                    s_aux[tid] = s;
-                }
-                if (tid == 0) {
-                    s_beta = beta;
-                    s_tau = tau;
-                    t.tau[k] = tau;
+            for (int sft = kBNB / 2; sft >= 1; sft >>= 1) {
+                const bool upper = (lane & sft) != 0;
+#pragma unroll
+                for (int q = 0; q < sft; ++q) {
+                    const T send = upper ? sa[q] : sa[q + sft];
+                    const T keep = upper ? sa[q + sft] : sa[q];
+                    sa[q] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
                 }
             }
-            cl.sync();
-            const T beta = *cl.map_shared_rank(&s_beta, owner);
-            const T tau = *cl.map_shared_rank(&s_tau, owner);
-            if (cr != owner) {
-                const T* ov = cl.map_shared_rank(vsh, owner);
-                for (int i = k + tid; i < m; i += nth) vsh[i] = ov[i];
-                if (tid < kBNB) s_aux[tid] = *cl.map_shared_rank(&s_aux[tid], owner);
+            // with kBNB < 32, lanes l and l + kBNB hold halves of the same sum
+            T part0 = sa[0];
+            if (kBNB < 32) part0 += __shfl_xor_sync(0xffffffffu, part0, kBNB);
+            if (lane < kBNB) s_wpart[warp * kBNB + lane] = part0;
+            __syncthreads();
+            if (tid < kBNB) {
+                T sacc = T(0);
+                for (int q = 0; q < nw; ++q) sacc += s_wpart[q * kBNB + tid];
+                s_aux[tid] = tid < jb ? sacc : T(0);
             }
             if (tol != 0.0 && kmax > 1) {
                 if (k == 0) {
@@ -284,19 +283,19 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 } else if (!((double)fabs(beta) / (double)r00 >= tol)) {
                     rank = k;
                     done = true;
-                    break;  // uniform over the cluster: every CTA read the same beta
+                    break;  // uniform over the cluster: every CTA computed the same beta
                 }
             }
-            if (cr == 0 && tid == 0) {  // LAPACK's column swap, as positions
-                const int c0 = t.colat[k];
-                t.colat[gp] = c0;
-                t.pos[c0] = gp;
-                t.colat[k] = pc;
-                t.pos[pc] = k;
+            if (tid == 0) {
+                s_pcs[jb] = pc;
+                s_betas[jb] = beta;
+                if (cr == 0) t.tau[k] = tau;
+                // LAPACK's column swap, as positions of the slab's own columns
+                if (s_c0 >= 0) pos[s_c0 - j0] = gp;
+                if (pc >= j0 && pc < j1) pos[pc - j0] = k;
             }
-            if (tid == 0) s_nflag = 0;
+            steps = jb + 1;
             __syncthreads();
-            for (int i = k + tid; i < m; i += nth) Vs[i * VP + jb] = vsh[i];  // V_b(:, jb); rows < k stay 0
             // 3a. partials of C_bs(k+1:m, slab)^T v: lanes own 16-byte column vectors
             //     (kBU per lane), the rows are cut in Gs chunks taken by different warps
             const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);
@@ -340,6 +339,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                     }
                 }
             }
+            if (tid == 0) s_nflag = 0;
             __syncthreads();
             // 3b. F(jb, c), pivot row k, partial norms
             T vk[kBNB];  // V_b(k, 0:jb], zero after
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             for (int l = 0; l < kBNB; ++l) vk[l] = Vs[k * VP + l];
             for (int jl = tid; jl < Wc; jl += nth) {
                 const int c = j0 + jl;
-                if (c == pc || t.pos[c] < k) continue;
+                if (c == pc || pos[jl] < k) continue;
                 const T ck0 = C[k * ld + c];
                 if (tau != T(0)) {
                     T g = ck0;
@@ -362,18 +362,18 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 for (int l = 0; l < kBNB; ++l) upd += vk[l] * F[l * Wp + jl];
                 const T ck = ck0 - upd;
                 C[k * ld + c] = ck;
-                const T n1 = t.vn1[c];
+                const T n1 = vn1[jl];
                 if (n1 != T(0)) {
                     const T rk = fabs(ck) / n1;
                     T temp = T(1) - rk * rk;
                     temp = temp < T(0) ? T(0) : temp;
-                    const T qq = n1 / t.vn2[c];
+                    const T qq = n1 / vn2[jl];
                     const T temp2 = temp * qq * qq;
                     if (temp2 <= Tol3z<T>::v()) {
-                        t.vn2[c] = T(-1);  // recomputed below from the up-to-date column
+                        vn2[jl] = T(-1);  // recomputed below from the up-to-date column
                         atomicAdd(&s_nflag, 1);
                     } else {
-                        t.vn1[c] = n1 * (T)sqrt(temp);
+                        vn1[jl] = n1 * (T)sqrt(temp);
                     }
                 }
             }
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             if (s_nflag > 0) {
                 for (int jl = warp; jl < Wc; jl += nw) {
                     const int c = j0 + jl;
-                    if (!(t.vn2[c] < T(0)) || c == pc || t.pos[c] < k) continue;
+                    if (!(vn2[jl] < T(0)) || c == pc || pos[jl] < k) continue;
                     T fr[kBNB];
 #pragma unroll
                     for (int l = 0; l < kBNB; ++l) fr[l] = F[l * Wp + jl];
@@ -397,13 +397,21 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                     ss = wsum(ss);
                     if (lane == 0) {
                         const T nv = (k + 1 < m) ? (T)sqrt(ss) : T(0);
-                        t.vn1[c] = nv;
-                        t.vn2[c] = nv;
+                        vn1[jl] = nv;
+                        vn2[jl] = nv;
                     }
                 }
+                __syncthreads();
             }
-            cl.sync();  // positions and norms of step k visible to every CTA
-            steps = jb + 1;
+        }
+        // every CTA is past its last read of this block's block-start pivot columns
+        // and of the owners' F: the owners store R_kk and the reflector of each
+        // accepted pivot in its column
+        cl.sync();
+        for (int j = 0; j < steps; ++j) {
+            const int pcj = s_pcs[j], kj = k0 + j;
+            if (pcj < j0 || pcj >= j1) continue;
+            for (int i = kj + tid; i < m; i += nth) C[i * ld + pcj] = i == kj ? s_betas[j] : Vs[i * VP + j];
         }
         if (done) break;
         k = k0 + steps;
@@ -441,7 +449,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 bool all = true;
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
-                    act[q] = cl0 + q < Wc && t.pos[j0 + cl0 + q] >= k;
+                    act[q] = cl0 + q < Wc && pos[cl0 + q] >= k;
                     all = all && act[q];
                 }
 #pragma unroll
@@ -462,11 +470,18 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 }
             }
         }
-        __syncthreads();  // F and V_b are cleared for the next block
+        // the next block's first pivot columns are read (global) by every CTA
+        cl.sync();
     }
-    // No CTA may exit while another still reads its shared memory (the early
-    // exit at the rank leaves right after the DSMEM reads of that step).
-    cl.sync();
+    __syncthreads();
+    // positions out: pos, and colat as their inverse (positions are a permutation)
+    for (int jl = tid; jl < Wc; jl += nth) {
+        const int p = pos[jl];
+        t.pos[j0 + jl] = p;
+        t.colat[p] = j0 + jl;
+        t.vn1[j0 + jl] = vn1[jl];
+        t.vn2[j0 + jl] = vn2[jl];
+    }
     if (cr == 0 && tid == 0) *t.rank = rank;
 }
 
