@@ -57,7 +57,35 @@ inline cudaMemPool_t device_pool(int dev) {
     pools[dev] = p;
     return p;
 }
+// Buffers a destroyed handle leaves for the next one (its stream drained
+// first, so they are idle): the device scratch buffer of each device, and
+// the pinned staging chunks. A new handle takes them instead of growing a
+// scratch buffer and pinning host pages again, which costs tens of ms per
+// 8 MiB chunk on a busy host.
+struct HandoffCache {
+    std::mutex mu;
+    std::map<int, std::pair<void*, size_t>> scratch;  // device -> (buffer, bytes)
+    std::vector<std::pair<char*, size_t>> pinned;     // free pinned chunks
+};
+inline HandoffCache& handoff_cache() {
+    static HandoffCache c;
+    return c;
+}
 inline void trim_device_pools() {
+    {
+        HandoffCache& c = handoff_cache();
+        std::lock_guard<std::mutex> g(c.mu);
+        int cur = 0;
+        cudaGetDevice(&cur);
+        for (auto& kv : c.scratch) {
+            cudaSetDevice(kv.first);
+            cudaFree(kv.second.first);
+        }
+        cudaSetDevice(cur);
+        c.scratch.clear();
+        for (auto& ch : c.pinned) cudaFreeHost(ch.first);
+        c.pinned.clear();
+    }
     std::lock_guard<std::mutex> g(pool_mutex());
     for (auto& kv : pool_table()) cudaMemPoolTrimTo(kv.second, 0);
 }
@@ -127,8 +155,21 @@ private:
 // buffer finishes first without a host wait.
 class Scratch {
 public:
-    void set_pool(cudaMemPool_t pool) { pool_ = pool; }
+    void set_pool(cudaMemPool_t pool, int device) {
+        pool_ = pool;
+        dev_ = device;
+    }
     void* get(size_t bytes, cudaStream_t s) {
+        if (!p_) {  // the buffer a destroyed handle left on this device
+            HandoffCache& c = handoff_cache();
+            std::lock_guard<std::mutex> g(c.mu);
+            auto it = c.scratch.find(dev_);
+            if (it != c.scratch.end()) {
+                p_ = it->second.first;
+                cap_ = it->second.second;
+                c.scratch.erase(it);
+            }
+        }
         if (bytes > cap_) {
             const double t0 = wall_seconds();
             if (p_) cudaFreeAsync(p_, s);
@@ -146,10 +187,27 @@ public:
         p_ = nullptr;
         cap_ = 0;
     }
+    // Leaves the buffer for the next handle on the device (the stream must be
+    // drained); the smaller of two buffers goes back to the pool.
+    void hand_off(cudaStream_t s) {
+        if (!p_) return;
+        HandoffCache& c = handoff_cache();
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.scratch.find(dev_);
+        if (it != c.scratch.end() && it->second.second >= cap_) {
+            cudaFreeAsync(p_, s);
+        } else {
+            if (it != c.scratch.end()) cudaFreeAsync(it->second.first, s);
+            c.scratch[dev_] = {p_, cap_};
+        }
+        p_ = nullptr;
+        cap_ = 0;
+    }
     size_t capacity() const { return cap_; }
     double grow_seconds() const { return grow_seconds_; }
 
 private:
+    int dev_ = 0;
     cudaMemPool_t pool_ = nullptr;
     void* p_ = nullptr;
     size_t cap_ = 0;
@@ -163,8 +221,11 @@ private:
 // when the stream has drained every copy issued from the stage.
 class PinnedStage {
 public:
+    // The chunks go to the handoff cache (the owner drained its stream first).
     ~PinnedStage() {
-        for (auto& c : chunks_) cudaFreeHost(c.first);
+        HandoffCache& c = handoff_cache();
+        std::lock_guard<std::mutex> g(c.mu);
+        for (auto& ch : chunks_) c.pinned.push_back(ch);
     }
     char* get(size_t bytes) {
         bytes = (bytes + 15) & ~size_t(15);
@@ -174,9 +235,28 @@ public:
         }
         if (ci_ == chunks_.size()) {
             const size_t sz = bytes > kChunk ? bytes : kChunk;
-            void* p = nullptr;
-            cuda_check(cudaHostAlloc(&p, sz, cudaHostAllocDefault), "pinned staging");
-            chunks_.emplace_back(static_cast<char*>(p), sz);
+            char* p = nullptr;
+            size_t got = 0;
+            {  // a chunk a destroyed handle left, else newly pinned pages
+                HandoffCache& c = handoff_cache();
+                std::lock_guard<std::mutex> g(c.mu);
+                for (size_t i = 0; i < c.pinned.size(); ++i)
+                    if (c.pinned[i].second >= sz) {
+                        p = c.pinned[i].first;
+                        got = c.pinned[i].second;
+                        c.pinned.erase(c.pinned.begin() + (long)i);
+                        break;
+                    }
+            }
+            if (!p) {
+                const double t0 = wall_seconds();
+                void* q = nullptr;
+                cuda_check(cudaHostAlloc(&q, sz, cudaHostAllocPortable), "pinned staging");
+                alloc_seconds_ += wall_seconds() - t0;
+                p = static_cast<char*>(q);
+                got = sz;
+            }
+            chunks_.emplace_back(p, got);
             used_ = 0;
         }
         char* p = chunks_[ci_].first + used_;
@@ -187,9 +267,12 @@ public:
         ci_ = 0;
         used_ = 0;
     }
+    double alloc_seconds() const { return alloc_seconds_; }
+    size_t chunks() const { return chunks_.size(); }
 
 private:
     static constexpr size_t kChunk = size_t(8) << 20;
+    double alloc_seconds_ = 0;
     std::vector<std::pair<char*, size_t>> chunks_;
     size_t ci_ = 0, used_ = 0;
 };

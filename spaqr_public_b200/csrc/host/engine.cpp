@@ -108,7 +108,7 @@ public:
         cudaStreamSynchronize(stream_);
         arena_.release();
         desc_arena_.release();
-        scratch_.release(stream_);
+        scratch_.hand_off(stream_);
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
     }
@@ -119,7 +119,7 @@ public:
         cudaMemPool_t pool = device_pool(cfg_.device);
         arena_.set_stream(stream_, pool);
         desc_arena_.set_stream(stream_, pool);
-        scratch_.set_pool(pool);
+        scratch_.set_pool(pool, cfg_.device);
         prepare_kernels<T>();
     }
 
@@ -595,6 +595,9 @@ private:
     // Issues the jobs of one wave (already built), then extra copies (after the QR).
     void run_qr_wave(std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm,
                      const std::vector<CopyDesc<T>>& post) {
+        const double tw_wave = wall();
+        const double pin0 = pinned_.alloc_seconds(), grow0 = scratch_.grow_seconds(),
+                     ar0 = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
         size_t tr_elems = 0;
         for (auto& j : jobs) {
             j.tr_off = tr_elems;
@@ -720,6 +723,26 @@ private:
             ++launches_fact_;
         }
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_post), post);
+        if (cfg_.verbose >= 3) {  // diagnostics: the wave's shape and its time (synchronizes)
+            const double tsub = wall();
+            cuda_check(cudaStreamSynchronize(stream_), "wave sync");
+            int mk = 0, mn = 0;
+            size_t nt = 0;
+            double work = 0;
+            for (auto& q : qt) {
+                mk = std::max(mk, q.k);
+                mn = std::max(mn, q.ntr);
+                work += (double)q.m * q.k * (q.k + q.ntr);
+            }
+            for (auto& tl : tiles) nt += tl.size();
+            std::fprintf(stderr, "    qr wave: %zu tasks, max m %d, max k %d, max ntr %d, %zu panel steps, %zu tiles, "
+                         "m k (k + ntr) %.3e, %zu trsm tasks, %.2f ms (host %.2f: pinned %.2f scratch %.2f "
+                         "arena %.2f, %zu pinned chunks)\n",
+                         qt.size(), maxR, mk, mn, ids.size(), nt, work, trsm.size(), (wall() - tw_wave) * 1e3,
+                         (tsub - tw_wave) * 1e3, (pinned_.alloc_seconds() - pin0) * 1e3,
+                         (scratch_.grow_seconds() - grow0) * 1e3,
+                         (arena_.alloc_seconds() + desc_arena_.alloc_seconds() - ar0) * 1e3, pinned_.chunks());
+        }
     }
 
     void issue_copies(const CopyDesc<T>* d, const std::vector<CopyDesc<T>>& h) {
@@ -1116,12 +1139,22 @@ private:
         for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
             const size_t rq = rqs[gi++];
             if (rq == SIZE_MAX) continue;
+            // algorithmic bytes: the norm pass, then per pivot step one read of the
+            // active rows x columns (dlaqps: C_bs^T v) plus a read and a write of the
+            // rows below each finished block (the rank-NB update); the unblocked
+            // kernel reads the active part twice and writes it once per step
+            const bool blocked = kv.first.first == 1;
+            const int nb = sizeof(T) == 4 ? 32 : 16;
             double f = 0, by = 0;
             for (int q : kv.second) {
                 const double m = jobs[q].m, n = jobs[q].n;
-                const double r = ranks[q] >= jobs[q].m ? std::min(jobs[q].m, jobs[q].n) : ranks[q];
-                f += 4 * m * n * r - 2 * r * r * (m + n) + 4.0 / 3.0 * r * r * r;
-                by += 2 * m * n * sizeof(T);
+                const int r = ranks[q] >= jobs[q].m ? std::min(jobs[q].m, jobs[q].n) : ranks[q];
+                f += 4 * m * n * r - 2.0 * r * r * (m + n) + 4.0 / 3.0 * r * r * r;
+                double words = m * n;
+                for (int k = 0; k < r; ++k) words += (m - k) * (n - k) * (blocked ? 1.0 : 3.0);
+                if (blocked)
+                    for (int ke = nb; ke < r; ke += nb) words += 2.0 * (m - ke) * (n - ke);
+                by += words * sizeof(T);
             }
             pend_[rq].flops = f;
             pend_[rq].bytes = by;
