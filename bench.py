@@ -235,12 +235,12 @@ def roofline(info, peaks):
     achieved = bytes_per_launch / per_launch_s / 1e9
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    prof = os.path.join(ROOT, "profiles", "traffic.txt")  # "family bytes_per_launch" lines from ncu
     if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get(dom)
-        except Exception:
-            traffic = None
+        for ln in open(prof):
+            f2 = ln.split()
+            if len(f2) == 2 and not ln.startswith("#") and f2[0] == dom:
+                traffic = float(f2[1])
     total_ms = sum(v["ms"] for v in fams.values())
     return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 5), "traffic": traffic,
@@ -337,9 +337,20 @@ def run_ours(args):
     csr = device_csr(A)
     d_b = torch.tensor(b, dtype=torch.float64, device="cuda")
     result = {}
+    from spaqr_public_b200 import autotune
+    tuning = {}
     for prec, name in ((1, "fp32"), (0, "fp64")):
         for _ in range(args.warmup):
             timed_step(w, A, csr, d_b, prec, local)
+        # the online autotuner explores launch shapes (results do not depend on
+        # them) during warm-up: a few more untimed steps until it has no pending
+        # timings, so the timed steps use the tuned shapes
+        extra = 0
+        while extra < 8 and autotune()[2] > 0:
+            timed_step(w, A, csr, d_b, prec, local)
+            extra += 1
+        barrier(d)
+        tuning[name] = {"extra_warmup_steps": extra, "pending_after": autotune()[2], "table_entries": autotune()[1]}
         times, infos = [], []
         barrier(d)
         with Clocks(local) as clk:
@@ -372,6 +383,7 @@ def run_ours(args):
         "config": {"workload": f"{WORKLOAD} (n=262144, 12 levels, tol 1e-2, skip 2, target 1e-10)",
                    "step": "factorize + FP64 GMRES refinement to true residual 1e-10 (partition/assemble untimed)",
                    "l2": "inputs larger than L2 (no flush needed)",
+                   "autotune": tuning,
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
         "fp64_form": {"value": f64["value"], "unit": "s", "gmres_its": f64["info"]["its"],
                       "residual": f64["info"]["res"], "speedup_fp32_over_fp64": f64["value"] / f32["value"]},

@@ -232,7 +232,7 @@ int spq_trim_memory(void);
  * save/load write/read a text table (one line per bucket and shape); load
  * merges into the current table. */
 int spq_autotune_set_mode(int mode);
-int spq_autotune_get(int* mode, int* entries);
+int spq_autotune_get(int* mode, int* entries, int* pending); /* pending: timings still to explore */
 int spq_autotune_reset(void);
 int spq_autotune_save(const char* path);
 int spq_autotune_load(const char* path);

@@ -66,7 +66,7 @@ SIGNATURES = {
     "spq_get_host_times": (_i, [_p, _dp]),
     "spq_trim_memory": (_i, []),
     "spq_autotune_set_mode": (_i, [_i]),
-    "spq_autotune_get": (_i, [_ip, _ip]),
+    "spq_autotune_get": (_i, [_ip, _ip, _ip]),
     "spq_autotune_reset": (_i, []),
     "spq_autotune_save": (_i, [C.c_char_p]),
     "spq_autotune_load": (_i, [C.c_char_p]),

@@ -34,6 +34,7 @@ void Autotuner::set_mode(int mode) {
 int Autotuner::choose(const TuneKey& key, const std::vector<int>& cands, int dflt) {
     std::lock_guard<std::mutex> g(mu_);
     if (mode_ == 0 || cands.empty()) return dflt;
+    cands_[key] = cands;
     auto it = tab_.find(key);
     int best = -1;
     double bc = 0;
@@ -79,6 +80,24 @@ void Autotuner::record(const TuneKey& key, int cand, double cost) {
 void Autotuner::reset() {
     std::lock_guard<std::mutex> g(mu_);
     tab_.clear();
+    cands_.clear();
+}
+
+int Autotuner::pending() const {
+    std::lock_guard<std::mutex> g(mu_);
+    int n = 0;
+    for (auto& kv : cands_) {
+        auto it = tab_.find(kv.first);
+        for (int c : kv.second) {
+            int have = 0;
+            if (it != tab_.end()) {
+                auto jt = it->second.find(c);
+                if (jt != it->second.end()) have = jt->second.count;
+            }
+            n += std::max(0, kTries - have);
+        }
+    }
+    return n;
 }
 
 int Autotuner::entries() const {

@@ -44,6 +44,9 @@ public:
     void record(const TuneKey& key, int cand, double cost);
     void reset();
     int entries() const;  // number of (key, candidate) records
+    // timed launches still needed before every key seen so far has all its
+    // candidates explored (mode 1)
+    int pending() const;
     bool save(const std::string& path) const;
     bool load(const std::string& path);
 
@@ -55,6 +58,7 @@ private:
     mutable std::mutex mu_;
     int mode_ = 1;
     std::map<TuneKey, std::map<int, Rec>> tab_;
+    std::map<TuneKey, std::vector<int>> cands_;  // candidates offered for each key
 };
 
 }  // namespace spq

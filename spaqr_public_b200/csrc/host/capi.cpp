@@ -769,10 +769,11 @@ int spq_autotune_set_mode(int mode) {
     spq::Autotuner::get().set_mode(mode);
     return SPQ_OK;
 }
-int spq_autotune_get(int* mode, int* entries) {
-    if (!mode && !entries) return fail(SPQ_ERR_ARG, "null arguments");
+int spq_autotune_get(int* mode, int* entries, int* pending) {
+    if (!mode && !entries && !pending) return fail(SPQ_ERR_ARG, "null arguments");
     if (mode) *mode = spq::Autotuner::get().mode();
     if (entries) *entries = spq::Autotuner::get().entries();
+    if (pending) *pending = spq::Autotuner::get().pending();
     return SPQ_OK;
 }
 int spq_autotune_reset(void) {

@@ -256,7 +256,7 @@ def autotune(mode=None, reset=False, save=None, load=None):
     """The library's launch-shape autotuner (process-wide; shapes it picks never
     change results). ``mode``: 0 off, 1 online (default), 2 frozen table;
     ``reset`` clears the table; ``save`` / ``load`` a text table file.
-    Returns (mode, number of table entries)."""
+    Returns (mode, number of table entries, timed launches still to explore)."""
     if reset:
         check(lib().spq_autotune_reset())
     if load is not None:
@@ -265,6 +265,6 @@ def autotune(mode=None, reset=False, save=None, load=None):
         check(lib().spq_autotune_set_mode(int(mode)))
     if save is not None:
         check(lib().spq_autotune_save(str(save).encode()))
-    md, ne = C.c_int(0), C.c_int(0)
-    check(lib().spq_autotune_get(C.byref(md), C.byref(ne)))
-    return md.value, ne.value
+    md, ne, pe = C.c_int(0), C.c_int(0), C.c_int(0)
+    check(lib().spq_autotune_get(C.byref(md), C.byref(ne), C.byref(pe)))
+    return md.value, ne.value, pe.value

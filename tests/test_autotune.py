@@ -20,7 +20,7 @@ TABLE = """# kind dev elem rows_log2 cols_log2 tasks_log2 candidate count best_c
 
 @pytest.fixture
 def restore_tuner():
-    mode, _ = autotune()
+    mode = autotune()[0]
     yield
     autotune(mode=mode, reset=True)
 
@@ -32,7 +32,7 @@ def test_modes_and_argument_checks(restore_tuner):
     L = _abi.lib()
     assert L.spq_autotune_set_mode(3) == 1
     assert b"autotune mode" in L.spq_last_error()
-    assert L.spq_autotune_get(None, None) == 1
+    assert L.spq_autotune_get(None, None, None) == 1
     assert L.spq_autotune_save(None) == 1
 
 
@@ -84,7 +84,7 @@ def test_tuned_shapes_do_not_change_results(gpu, name, prec, restore_tuner):
     ys = []
     for _ in range(4):  # the default shape first, then the other fitting cluster sizes
         ys.append(_apply(name, prec, b))
-    _, entries = autotune()
+    _, entries, _ = autotune()
     assert entries > 0
     assert all(np.array_equal(ys[0], y) for y in ys[1:])
     autotune(mode=2)  # frozen: the explored table only
