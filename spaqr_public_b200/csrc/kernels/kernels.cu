@@ -730,16 +730,39 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
             } else {
                 tri_solve(xs, k, R, ldr, 1, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
+                // x_n -= B_n^T xs: a warp takes 8 neighbour columns at a time (their
+                // loads in flight together; columns past the block re-read its last
+                // column and are dropped), lanes stride the rows; each column's sum
+                // is the lane-strided partial sums folded by warp_sum
+                constexpr int kCG = 8;
+                const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
                 for (int b = 0; b < op.nseg; ++b) {
                     const GemvRef<T> g = gemv[op.seg0 + b];
                     const T* B = aptr<T>(g.boff);
-                    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-                    for (int j = warp; j < g.s; j += nw) {
-                        T s = T(0);
-#pragma unroll 4
-                        for (int i = lane; i < k; i += 32) s += B[i + (size_t)j * g.ld] * xs[i];
-                        s = warp_sum(s);
-                        if (lane == 0) x[g.xoff + j] -= s;
+                    const int ngrp = (g.s + kCG - 1) / kCG;
+                    for (int grp = warp; grp < ngrp; grp += nw) {
+                        const int j0 = grp * kCG;
+                        const T* bc[kCG];
+#pragma unroll
+                        for (int u = 0; u < kCG; ++u) bc[u] = B + (size_t)min(j0 + u, g.s - 1) * g.ld;
+                        T sacc[kCG];
+#pragma unroll
+                        for (int u = 0; u < kCG; ++u) sacc[u] = T(0);
+                        for (int i = lane; i < k; i += 32) {
+                            const T xi = xs[i];
+                            T bv[kCG];
+#pragma unroll
+                            for (int u = 0; u < kCG; ++u) bv[u] = bc[u][i];
+#pragma unroll
+                            for (int u = 0; u < kCG; ++u) sacc[u] += bv[u] * xi;
+                        }
+                        T mine = T(0);
+#pragma unroll
+                        for (int u = 0; u < kCG; ++u) {
+                            const T su = warp_sum(sacc[u]);
+                            if (lane == u) mine = su;
+                        }
+                        if (lane < kCG && j0 + lane < g.s) x[g.xoff + j0 + lane] -= mine;
                     }
                 }
             }
