@@ -60,7 +60,7 @@ int spq_destroy(spq_tree* t);
 
 int spq_set_tol(spq_tree* t, double tol);      /* -t   (default 1e-1 in the CLI; 0 in Tree) */
 int spq_set_scale(spq_tree* t, int scale);     /* --scale */
-int spq_set_order(spq_tree* t, float order);   /* --order (1 only; 1.5 -> SPQ_ERR_UNSUPPORTED) */
+int spq_set_order(spq_tree* t, float order);   /* --order 1 (sparsifyD) or 1.5 (sparsifyD_imp: keeps the E2 term) */
 int spq_set_hsl(spq_tree* t, int hsl);         /* --hsl (0 only) */
 int spq_set_square(spq_tree* t, int square);
 int spq_set_coords(spq_tree* t, int d, int n, const double* X); /* d x n, column-major */

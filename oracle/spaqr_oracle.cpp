@@ -1219,7 +1219,11 @@ public:
         rec(8, rows_before, c->rows(), 0, 0, 0, c->order);
     }
 
-    void sparsifyD(Cluster* c) {
+    // sparsifyD (src/tree.cpp:992-1114) and, with imp, sparsifyD_imp (order 1.5,
+    // src/tree.cpp:1117-1257): the same RRQR and block rewrite; imp also keeps
+    // the E2 term, (Q^T A_pm_top)(rank:, :), as edges from the neighbours into
+    // the fine cluster, whose QR op subtracts it in the backward sweep.
+    void sparsifyD(Cluster* c, bool imp = false) {
         int cols_before = c->cols();
         if (c->cols() == 0) { rec(3, 0, 0, 0, c->rows(), 0, c->order); return; }
         std::vector<Mat*> Apm, Amp;
@@ -1237,6 +1241,8 @@ public:
         for (Mat* m : Apm) { Apmc.set_block(0, cur, *m); cur += m->cols; }
         Mat rest;
         if (!square_) rest = Apmc.block(c->cols(), 0, c->rows() - c->cols(), spm);
+        Mat Apmc_top;
+        if (imp) Apmc_top = Apmc.block(0, 0, c->cols(), spm);
         cur = 0;
         for (Mat* m : Amp) {
             for (int j = 0; j < m->cols; ++j)
@@ -1271,6 +1277,7 @@ public:
         Mat selfb(c->rows() - cf_csize, rank);
         for (int j = 0; j < rank; ++j)
             for (int i = 0; i < rank; ++i) selfb(i, j) = (*e_self->A)(i, j);
+        const Mat self_old = imp ? *e_self->A : Mat();
         int rank_rows = rank + rest.rows;
         c->reset_size(rank_rows, rank);
         cur = 0;
@@ -1292,8 +1299,39 @@ public:
             cc += m->cols;
             *m = nm;
         }
-        *e_self->A = selfb.top_rows(c->rows());
+        if (!imp) {
+            *e_self->A = selfb.top_rows(c->rows());
+        } else {
+            // Aff = self(0:cf, 0:cf); self = its bottom-right rows x cols corner
+            Mat* Aff = new Mat(self_old.block(0, 0, cf->cols(), cf->cols()));
+            *e_self->A = self_old.block(self_old.rows - c->rows(), self_old.cols - c->cols(), c->rows(), c->cols());
+            Edge* eff = new Edge{cf, cf, std::unique_ptr<Mat>(Aff)};
+            owned_edges_.insert(eff);
+            cf->edgesOut.push_back(eff);
+            // E2: rows rank.. of Q^T A_pm_top (ormqr_trans_left, src/util.cpp:331-347)
+            if (spm > 0 && rank > 0)
+                L().dormqr(kColMajor, 'L', 'T', Apmc_top.rows, spm, rank, v.data(), v.rows, h.data(),
+                           Apmc_top.data(), Apmc_top.rows);
+            int cc2 = 0;
+            for (Edge* e : c->edgesIn) {
+                if (e->n1->eliminated) continue;
+                Cluster* mm = e->n1;
+                Mat* Afm = new Mat(Apmc_top.block(rank, cc2, cf->rows(), mm->cols()));
+                Edge* e2 = new Edge{mm, cf, std::unique_ptr<Mat>(Afm)};
+                owned_edges_.insert(e2);
+                cf->edgesIn.push_back(e2);
+                mm->edgesOut.push_back(e2);
+                cc2 += mm->cols();
+            }
+        }
         fine_[ilvl_].push_back(cf);
+        if (imp) {
+            const int kk = std::min(cf->rows(), cf->cols());
+            cf->tau.assign(kk, 0.0);
+            cf->T = Mat(kk, kk);
+            ops_.emplace_back(new OpQR(cf));
+            if (!square_) tops_.emplace_back(new TOpQR(cf));
+        }
         cf->eliminated = true;
         rec(3, cols_before, c->cols(), C.cols, c->rows(), 0, c->order);
     }
@@ -1319,8 +1357,7 @@ public:
                 for (Cluster* s : bottom_current()) {
                     if (!want_sparsify(s)) continue;
                     if (!scale_) throw std::runtime_error("--scale 0 sparsification is not restated");
-                    if (order_ == 1.5f) throw std::runtime_error("--order 1.5 sparsification is not restated");
-                    sparsifyD(s);
+                    sparsifyD(s, order_ == 1.5f);
                 }
             }
             if (ilvl_ < nlevels_ - 1) merge_all();

@@ -2,7 +2,7 @@
 // (spaQR.cpp:26-323), on the B200 library through its C ABI.
 //
 //   spaqr -m A.mtx [-l L] [-n N -d D | --coordinates X.mtx] [-t tol] [--skip s]
-//         [--scale 0|1] [--order 1] [--hsl 0] [-i iters] [--res r] [--rhs b.mtx]
+//         [--scale 1] [--order 1|1.5] [--hsl 0] [-i iters] [--res r] [--rhs b.mtx]
 //         [--precision fp64|fp32] [--target r] [--device k]
 //
 // Flow as in the reference: read the MatrixMarket matrix (transposed when it
@@ -14,7 +14,7 @@
 // b = that random vector or --rhs.
 //
 // Flags the reference has and this build does not run: --hsl != 0 and
-// --order 1.5 (the library returns SPQ_ERR_UNSUPPORTED), and the Eigen
+// --scale 0 (the library returns SPQ_ERR_UNSUPPORTED), and the Eigen
 // comparison solvers --useEigenLSCG / --useEigenQR / --useCholesky.
 // Added: --precision fp32 (FP32 factorization, FP64 Krylov), --target r (the
 // time-to-residual driver: refinement with GMRES corrections until the true
@@ -55,7 +55,7 @@ const Opt kOpts[] = {
     {"hsl", nullptr, true, "HSL bipartite row matching (0 only in this build)"},
     {"tol", "t", true, "Sparsification tolerance (default 1e-1)"},
     {"skip", nullptr, true, "Levels without sparsification (default 0)"},
-    {"order", nullptr, true, "Scheme order (1 only in this build)"},
+    {"order", nullptr, true, "Scheme order: 1 (default) or 1.5 (keeps the E2 term: more accurate, more memory)"},
     {"scale", nullptr, true, "Block scaling (default 1)"},
     {"iterations", "i", true, "Iterative solver iterations (default 300)"},
     {"rhs", nullptr, true, "Right-hand side in MatrixMarket array format"},

@@ -160,6 +160,7 @@ int spq_set_scale(spq_tree* t, int scale) {
 }
 int spq_set_order(spq_tree* t, float order) {
     SPQ_SETTER_GUARD
+    if (order != 1.0f && order != 1.5f) return fail(SPQ_ERR_ARG, "order must be 1 or 1.5");
     t->cfg.order = order;
     return SPQ_OK;
 }

@@ -237,7 +237,8 @@ public:
     void factorize() override {
         if (!assembled_) throw std::logic_error("factorize before assemble");
         if (factorized_) throw std::logic_error("factorize called twice");
-        if (cfg_.order != 1.0f) throw std::invalid_argument("--order 1.5 is not supported by this build");
+        if (cfg_.order != 1.0f && cfg_.order != 1.5f)
+            throw std::invalid_argument("--order must be 1 or 1.5");
         if (!cfg_.scale && cfg_.tol != 0) throw std::invalid_argument("--scale 0 is not supported by this build");
         double t0 = wall();
         launches_fact_ = 0;
@@ -1183,6 +1184,11 @@ private:
         std::vector<SpBlock<T>> blocks;
         std::vector<CopyDesc<T>> pre, post;  // least squares: extra rows of A_pm move up under the new top
         double wb_bytes = 0;
+        // order 1.5 (sparsifyD_imp, src/tree.cpp:1117-1257): the E2 term (Q^T A_pm_top)(rank:, :)
+        // of every sparsified interface, computed after the write-back from a copy of its
+        // block-start A_pm_top (taken with the pre copies) by the panel trailing kernel
+        const bool imp = cfg_.order == 1.5f;
+        std::vector<QRTask<T>> e2q;
         for (size_t q = 0; q < jobs.size(); ++q) {
             auto& j = jobs[q];
             Cluster* c = j.c;
@@ -1242,6 +1248,27 @@ private:
                 }
                 pre.push_back(cp(nullptr, j.self->A.p + r, 0, j.self->A.ld, nr, r));
             }
+            if (imp) {
+                int spm = 0;
+                for (Edge* e : j.apm) spm += e->A.cols;
+                T* G = spm > 0 ? arena_.alloc_n<T>((size_t)m * spm) : nullptr;
+                int coff = 0;
+                TapeOp fq;
+                fq.kind = TK_QR;
+                fq.c = cf;
+                fq.k = nf;
+                for (Edge* e : j.apm) {
+                    pre.push_back(cp(e->A.p, G + (size_t)coff * m, e->A.ld, m, m, e->A.cols));
+                    Blk b{G + r + (size_t)coff * m, m, nf, e->A.cols, next_uid_++};
+                    Edge* e2 = new_edge(e->n1, cf, b);
+                    cf->in.push_back(e2);
+                    e->n1->out.push_back(e2);
+                    fq.a12.push_back(A12{b.p, m, e->A.cols, e->n1});
+                    coff += e->A.cols;
+                }
+                if (spm > 0) e2q.push_back(QRTask<T>{V, G, tau, tp, m, r, spm, 1});
+                tape_.push_back(std::move(fq));  // QR(cf) right after the SplitD, as the reference
+            }
             // new shapes
             for (Edge* e : j.amp) e->A.cols = r;
             for (Edge* e : j.apm) e->A.rows = r + nr;
@@ -1271,6 +1298,33 @@ private:
                                       stream_);
             });
             ++launches_fact_;
+        }
+        if (!e2q.empty()) {  // E2 = Q^T A_pm_top, panel by panel (tiles of the copy only)
+            int maxr = 0;
+            for (auto& q : e2q) maxr = std::max(maxr, q.k);
+            std::vector<std::vector<TileRef>> tl;
+            for (int p = 0; p < maxr; p += kNB) {
+                std::vector<TileRef> v;
+                for (size_t t = 0; t < e2q.size(); ++t) {
+                    if (e2q[t].k <= p) continue;
+                    for (int c0 = 0, ti = 0; c0 < e2q[t].ntr; c0 += kTN, ++ti) v.push_back(TileRef{(int)t, ti});
+                }
+                tl.push_back(std::move(v));
+            }
+            Upload u4;
+            const size_t o_q = u4.add(e2q);
+            std::vector<size_t> o_t;
+            for (auto& v : tl) o_t.push_back(u4.add(v));
+            char* d4 = u4.commit(desc_arena_, stream_, pinned_);
+            for (size_t i = 0; i < tl.size(); ++i) {
+                if (tl[i].empty()) continue;
+                timed(KF_TRAILING, 0, 0, [&] {
+                    launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d4 + o_q),
+                                       reinterpret_cast<const TileRef*>(d4 + o_t[i]), (int)tl[i].size(),
+                                       (int)i * kNB, stream_);
+                });
+                ++launches_fact_;
+            }
         }
         if (!post.empty()) {
             Upload u3;
@@ -1700,7 +1754,8 @@ private:
                     break;
                 }
             }
-            fwd.push_back(std::move(f));
+            // the QR op of an order-1.5 fine cluster has no forward part (its T is zero)
+            if (!(t.kind == TK_QR && t.fac == nullptr)) fwd.push_back(std::move(f));
             bwd.push_back(std::move(b));
         }
         std::reverse(bwd.begin(), bwd.end());

@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, c
     const int m = t.m, k = t.k;
     const int w = min(kNB, k - p);
     const int R = m - p;
-    const int nf = k - p - w;
+    const int nf = t.tr_only ? 0 : k - p - w;
     const int ntot = nf + t.ntr;
     const int c0 = tr.tile * kTN;
     const int tn = min(kTN, ntot - c0);
@@ -718,17 +718,20 @@ __global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, con
             break;
         }
         case SK_TRI: {
+            // p0 == 0: R is the identity (the fine cluster of an order-1.5 sparsification,
+            // whose QR op only subtracts the E2 term)
             const int k = op.a, ldr = op.c;
             const T* R = aptr<T>(op.p0);
+            const bool has_r = op.p0 != 0;
             for (int i = tid; i < k; i += blockDim.x) xs[i] = x[op.x0 + i];
             __syncthreads();
             if (op.dir == 0) {
                 gemv_sub(xs, k, gemv + op.seg0, op.nseg, x, sh);
                 __syncthreads();
-                tri_solve(xs, k, R, ldr, 0, sh);
+                if (has_r) tri_solve(xs, k, R, ldr, 0, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
             } else {
-                tri_solve(xs, k, R, ldr, 1, sh);
+                if (has_r) tri_solve(xs, k, R, ldr, 1, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
                 // x_n -= B_n^T xs: a warp takes 8 neighbour columns at a time (their
                 // loads in flight together; columns past the block re-read its last

@@ -43,7 +43,8 @@ struct QRTask {
     T* tr;
     T* tau;
     T* tp;
-    int m, k, ntr, pad;
+    int m, k, ntr;
+    int tr_only;  // 1: the trailing updates touch tr only (fac holds finished reflectors: V of a sparsified interface)
 };
 struct TileRef {
     int task, tile;

@@ -124,3 +124,18 @@ def test_cli_least_squares_runs_cgls(gpu, tmp_path):
     assert m, out
     assert int(m.group(1)) <= 300 and float(m.group(2)) <= 1e-9
     assert np.isfinite(float(m.group(2)))
+
+
+@pytest.mark.gpu
+def test_cli_order15(gpu, tmp_path):
+    w = matgen.workload("advdiff2d_64")
+    mtx, rhs = tmp_path / "A.mtx", tmp_path / "b.mtx"
+    matgen.write_mm(mtx, w["A"])
+    write_vec(rhs, w["b"])
+    its = {}
+    for order in ("1", "1.5"):
+        rc, out, err = run("-m", mtx, "-n", 64, "-d", 2, "-l", w["levels"], "-t", 1e-1, "--order", order,
+                           "--rhs", rhs, "--res", 1e-12)
+        assert rc == 0, err
+        its[order] = _gmres_count(out)
+    assert its["1.5"] < its["1"]
