@@ -365,8 +365,12 @@ def run_ours(args):
     # instrumented step for the roofline (FP32 form, after the timed steps)
     _, pinfo = timed_step(w, A, csr, d_b, 1, local, profile=True)
     rl = roofline(pinfo, peaks)
-    e2e_sec, e2e_res, h2d, d2h = e2e_step(w, A, b, 1, local)
-    e2e_sec = max_over_ranks(d, e2e_sec)
+    # end to end through the public host API: three runs, the median reported
+    # (a single wall-clock sample carries the host's and the driver's noise)
+    e2e_runs = [e2e_step(w, A, b, 1, local) for _ in range(3)]
+    e2e_all = [r[0] for r in e2e_runs]
+    e2e_sec = max_over_ranks(d, float(statistics.median(e2e_all)))
+    _, e2e_res, h2d, d2h = e2e_runs[-1]
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         s = cpu_sample(40, cpu_threads())
@@ -389,7 +393,8 @@ def run_ours(args):
                       "residual": f64["info"]["res"], "speedup_fp32_over_fp64": f64["value"] / f32["value"]},
         "gmres_its": inf["its"], "residual": inf["res"],
         "e2e": {"value": e2e_sec, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "residual": e2e_res, "includes": "create+partition+assemble+factorize+refinement, host buffers"},
+                "residual": e2e_res, "runs": [round(v, 4) for v in e2e_all], "statistic": "median of 3",
+                "includes": "create+partition+assemble+factorize+refinement, host buffers"},
         "gpu_launches": inf["launches"]["total"],
         "roofline": rl,
         "cpu_baseline": cpu,

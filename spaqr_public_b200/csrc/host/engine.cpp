@@ -489,6 +489,10 @@ private:
 
 public:
     void set_profile(bool on) override { prof_ = on; }
+    double* krylov_workspace(size_t elems) override {
+        open_device();
+        return static_cast<double*>(scratch_.get(std::max<size_t>(elems, 1) * sizeof(double), stream_));
+    }
     KernelStat kernel_stat(int fam) override {
         flush_prof();
         return (fam >= 0 && fam < kNumFamilies) ? fam_[fam] : KernelStat{};

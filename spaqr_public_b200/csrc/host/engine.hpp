@@ -94,6 +94,10 @@ public:
     // True once the preconditioner's solve graph exists (built by the first
     // application); from then on an application allocates nothing.
     virtual bool solve_ready() const = 0;
+    // Device workspace of at least `elems` doubles on the handle's stream for a
+    // Krylov solve (the factorization's scratch buffer, idle between
+    // factorizations): valid until the next call or factorization.
+    virtual double* krylov_workspace(size_t elems) = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(const Config& cfg, int precision);

@@ -259,7 +259,9 @@ private:
 int gmres_device(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart, double tol,
                  double* res, long long* launches, bool adjoint) {
     if (restart < 1) restart = 1;
-    Gmres g(P, A, restart);
+    // the workspace (m x (restart + 1) Krylov basis) is the handle's scratch
+    // buffer, which persists across solves and handles: no allocation per call
+    Gmres g(P, A, restart, P.krylov_workspace(Gmres::workspace_elems(A.m, restart)));
     g.adjoint_ = adjoint;
     int it = g.run(d_b, d_x, iters, tol, res);
     if (launches) *launches = g.launches_;

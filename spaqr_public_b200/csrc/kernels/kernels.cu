@@ -299,15 +299,28 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
 }
 
 // ------------------------------------------------------------------ trailing update
-// C <- (I - V T V^T)^T C = C - V (T^T (V^T C)) on one tile of kTN columns.
+// C <- (I - V T V^T)^T C = C - V (T^T (V^T C)) on one tile of kTN columns, the
+// rows in kRC-row chunks staged in shared memory (the next chunk's loads are
+// issued before the current chunk's arithmetic). Y = V^T C: each thread owns a
+// 2 x 2 block of Y and sums it over the rows in order; C -= V Z: each thread
+// keeps its column of Z in registers and walks rows of V (V rows padded to an
+// even stride, so pairs and quads load together). Per element the sums run in
+// the same order as a plain row-by-row product.
+// Row stride of the staged V chunk: a multiple of 16 bytes (FP32) or 16 bytes
+// per pair (FP64), so a thread's pair and a row's quads are aligned loads.
+template <class T>
+struct TVP {
+    static constexpr int v = sizeof(T) == 4 ? 36 : 34;
+};
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, const TileRef* tiles, int p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int VP = kNB + 1, CP = kTN + 1;
+    constexpr int VP = TVP<T>::v, CP = kTN + 1, TP = kNB + 1;
+    constexpr int EPT = kRC * kNB / kThreads;  // 8 elements per thread per chunk (V and C each)
     T* Vs = reinterpret_cast<T*>(smem_raw);  // kRC x VP
     T* Cs = Vs + kRC * VP;                    // kRC x CP
     T* Ys = Cs + kRC * CP;                    // kNB x CP
-    T* Tsh = Ys + kNB * CP;                   // kNB x VP
+    T* Tsh = Ys + kNB * CP;                   // kNB x TP
     __shared__ T* colp[kTN];
     const TileRef tr = tiles[blockIdx.x];
     const QRTask<T> t = tasks[tr.task];
@@ -325,71 +338,91 @@ __global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, c
         if (tid < tn) ptr = vc < nf ? t.fac + (size_t)(p + w + vc) * m : t.tr + (size_t)(vc - nf) * m;
         colp[tid] = ptr;
     }
-    const T* V0 = t.fac + (size_t)p * m;  // column p
+    const T* V0 = t.fac + (size_t)p * m;
     for (int e = tid; e < kNB * kNB; e += blockDim.x) {
         int i = e % kNB, j = e / kNB;
-        Tsh[i * VP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
+        Tsh[i * TP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
     }
     __syncthreads();
-    auto load_v = [&](int r0, int rc) {
-        for (int e = tid; e < kRC * kNB; e += blockDim.x) {
-            int r = e % kRC, q = e / kRC;
-            T v = T(0);
-            int gr = r0 + r;
-            if (r < rc && q < w) v = gr < q ? T(0) : (gr == q ? T(1) : V0[p + gr + (size_t)q * m]);
-            Vs[r * VP + q] = v;
-        }
-    };
-    auto load_c = [&](int r0, int rc) {
-        for (int e = tid; e < kRC * kTN; e += blockDim.x) {
-            int r = e % kRC, c = e / kRC;
-            Cs[r * CP + c] = (r < rc && c < tn) ? colp[c][p + r0 + r] : T(0);
-        }
-    };
-    const int c = tid % kTN, jq = tid / kTN;  // jq in [0, 8)
-    constexpr int QPT = kNB / (kThreads / kTN);  // 4 rows of Y per thread
-    T acc[QPT];
+    T vr[EPT], cr[EPT];
+    auto fetch = [&](int r0, bool want_c) {
+        const int rc = min(kRC, R - r0);
 #pragma unroll
-    for (int u = 0; u < QPT; ++u) acc[u] = T(0);
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            const int gr = r0 + r;
+            const T x = V0[p + min(gr, R - 1) + (size_t)min(q, w - 1) * m];
+            vr[u] = (r < rc && q < w) ? (gr < q ? T(0) : (gr == q ? T(1) : x)) : T(0);
+            if (want_c) {
+                const T y = colp[min(q, tn - 1)][p + r0 + min(r, rc - 1)];
+                cr[u] = (r < rc && q < tn) ? y : T(0);
+            }
+        }
+    };
+    auto stash = [&](bool want_c) {
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            Vs[r * VP + q] = vr[u];
+            if (want_c) Cs[r * CP + q] = cr[u];
+        }
+    };
+    // Y = V^T C: thread (qp, cp) owns Y(2qp..2qp+1, 2cp..2cp+1), summed over the rows in order
+    const int qp = tid / 16, cp = tid % 16;
+    T a00 = T(0), a01 = T(0), a10 = T(0), a11 = T(0);
+    fetch(0, true);
     for (int r0 = 0; r0 < R; r0 += kRC) {
         const int rc = min(kRC, R - r0);
-        load_v(r0, rc);
-        load_c(r0, rc);
+        stash(true);
         __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC, true);
         for (int r = 0; r < rc; ++r) {
-            const T cv = Cs[r * CP + c];
-#pragma unroll
-            for (int u = 0; u < QPT; ++u) acc[u] += Vs[r * VP + jq * QPT + u] * cv;
+            const T v0 = Vs[r * VP + 2 * qp], v1 = Vs[r * VP + 2 * qp + 1];
+            const T x0 = Cs[r * CP + 2 * cp], x1 = Cs[r * CP + 2 * cp + 1];
+            a00 += v0 * x0;
+            a01 += v0 * x1;
+            a10 += v1 * x0;
+            a11 += v1 * x1;
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = acc[u];
+    Ys[(2 * qp) * CP + 2 * cp] = a00;
+    Ys[(2 * qp) * CP + 2 * cp + 1] = a01;
+    Ys[(2 * qp + 1) * CP + 2 * cp] = a10;
+    Ys[(2 * qp + 1) * CP + 2 * cp + 1] = a11;
     __syncthreads();
     // Z = T^T Y
+    const int c = tid % kTN, jq = tid / kTN;
+    constexpr int QPT = kNB / (kThreads / kTN);
     T z[QPT];
 #pragma unroll
     for (int u = 0; u < QPT; ++u) {
         const int i = jq * QPT + u;
         T s = T(0);
-        for (int l = 0; l <= i; ++l) s += Tsh[l * VP + i] * Ys[l * CP + c];
+        for (int l = 0; l <= i; ++l) s += Tsh[l * TP + i] * Ys[l * CP + c];
         z[u] = s;
     }
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = z[u];
     __syncthreads();
-    // C -= V Z
+    T zc[kNB];
+#pragma unroll
+    for (int q = 0; q < kNB; ++q) zc[q] = Ys[q * CP + c];
+    // C -= V Z: thread (c, jq) rows jq, jq + 8, ... of each chunk
     constexpr int RG = kThreads / kTN;
+    fetch(0, true);
     for (int r0 = 0; r0 < R; r0 += kRC) {
         const int rc = min(kRC, R - r0);
-        load_v(r0, rc);
-        load_c(r0, rc);
+        stash(true);
         __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC, true);
         for (int r = jq; r < rc; r += RG) {
             T s = T(0);
-#pragma unroll 8
-            for (int q = 0; q < kNB; ++q) s += Vs[r * VP + q] * Ys[q * CP + c];
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) s += Vs[r * VP + q] * zc[q];
             Cs[r * CP + c] -= s;
         }
         __syncthreads();
@@ -992,7 +1025,7 @@ inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
 
 template <class T>
 size_t trailing_smem() {
-    return sizeof(T) * ((size_t)kRC * (kNB + 1) + (size_t)kRC * (kTN + 1) + (size_t)kNB * (kTN + 1) +
+    return sizeof(T) * ((size_t)kRC * TVP<T>::v + (size_t)kRC * (kTN + 1) + (size_t)kNB * (kTN + 1) +
                         (size_t)kNB * (kNB + 1));
 }
 
