@@ -82,31 +82,44 @@ int check_csc(int m, int n, const int* cp, const int* ri, const double* va) {
     return SPQ_OK;
 }
 
-struct DevCsrOwned {
-    int* rp = nullptr;
-    int* ci = nullptr;
-    double* v = nullptr;
-    ~DevCsrOwned() {
-        cudaFree(rp);
-        cudaFree(ci);
-        cudaFree(v);
+// Device buffers of one host-API call, from the device's retained memory pool
+// in the order of the handle's stream (no cudaMalloc / cudaFree, which map
+// pages and synchronise the device, on every solve).
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    template <class U>
+    U* get(size_t n, cudaStream_t st) {
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        s = st;
+        p = pool_alloc(device_pool(dev), std::max<size_t>(n, 1) * sizeof(U), st, "host-API buffer");
+        return static_cast<U*>(p);
     }
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+struct DevCsrOwned {
+    DevBuf rp, ci, v;
 };
 
 // Host CSC -> device CSR (rows of A with sorted column indices).
 void upload_csr(const Csc& A, DevCsrOwned& o, DevCsr& d, cudaStream_t s) {
     Csc T = csc_transpose(A);  // column r of T = row r of A
-    cuda_check(cudaMalloc(&o.rp, sizeof(int) * (T.p.size())), "csr alloc");
-    cuda_check(cudaMalloc(&o.ci, sizeof(int) * std::max<size_t>(T.i.size(), 1)), "csr alloc");
-    cuda_check(cudaMalloc(&o.v, sizeof(double) * std::max<size_t>(T.v.size(), 1)), "csr alloc");
-    cuda_check(cudaMemcpyAsync(o.rp, T.p.data(), sizeof(int) * T.p.size(), cudaMemcpyHostToDevice, s), "csr up");
-    cuda_check(cudaMemcpyAsync(o.ci, T.i.data(), sizeof(int) * T.i.size(), cudaMemcpyHostToDevice, s), "csr up");
-    cuda_check(cudaMemcpyAsync(o.v, T.v.data(), sizeof(double) * T.v.size(), cudaMemcpyHostToDevice, s), "csr up");
+    int* rp = o.rp.get<int>(T.p.size(), s);
+    int* ci = o.ci.get<int>(T.i.size(), s);
+    double* va = o.v.get<double>(T.v.size(), s);
+    cuda_check(cudaMemcpyAsync(rp, T.p.data(), sizeof(int) * T.p.size(), cudaMemcpyHostToDevice, s), "csr up");
+    cuda_check(cudaMemcpyAsync(ci, T.i.data(), sizeof(int) * T.i.size(), cudaMemcpyHostToDevice, s), "csr up");
+    cuda_check(cudaMemcpyAsync(va, T.v.data(), sizeof(double) * T.v.size(), cudaMemcpyHostToDevice, s), "csr up");
+    // the host arrays are released when this returns: the copies must have read them
+    cuda_check(cudaStreamSynchronize(s), "csr up");
     d.m = A.m;
     d.n = A.n;
-    d.rp = o.rp;
-    d.ci = o.ci;
-    d.v = o.v;
+    d.rp = rp;
+    d.ci = ci;
+    d.v = va;
 }
 
 }  // namespace
@@ -273,15 +286,13 @@ int spq_solve(spq_tree* t, const double* b, double* x) {
     return guard_on(t, [&] {
         const int m = t->eng->nrows(), n = t->eng->ncols();
         cudaStream_t s = t->eng->stream();
-        double *db = nullptr, *dx = nullptr;
-        cuda_check(cudaMalloc(&db, sizeof(double) * m), "solve alloc");
-        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "solve alloc");
+        DevBuf buf_db, buf_dx;
+        double* db = buf_db.get<double>(m, s);
+        double* dx = buf_dx.get<double>(n, s);
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "solve h2d");
         t->eng->solve_dev(db, dx);
         cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "solve d2h");
         cuda_check(cudaStreamSynchronize(s), "solve");
-        cudaFree(db);
-        cudaFree(dx);
         return SPQ_OK;
     });
 }
@@ -304,15 +315,13 @@ int spq_solve_adjoint(spq_tree* t, const double* g, double* y) {
     return guard_on(t, [&] {
         const int m = t->eng->nrows(), n = t->eng->ncols();
         cudaStream_t s = t->eng->stream();
-        double *dg = nullptr, *dy = nullptr;
-        cuda_check(cudaMalloc(&dg, sizeof(double) * n), "adjoint alloc");
-        cuda_check(cudaMalloc(&dy, sizeof(double) * m), "adjoint alloc");
+        DevBuf buf_dg, buf_dy;
+        double* dg = buf_dg.get<double>(n, s);
+        double* dy = buf_dy.get<double>(m, s);
         cuda_check(cudaMemcpyAsync(dg, g, sizeof(double) * n, cudaMemcpyHostToDevice, s), "adjoint h2d");
         t->eng->solve_adjoint_dev(dg, dy);
         cuda_check(cudaMemcpyAsync(y, dy, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "adjoint d2h");
         cuda_check(cudaStreamSynchronize(s), "adjoint solve");
-        cudaFree(dg);
-        cudaFree(dy);
         return SPQ_OK;
     });
 }
@@ -373,21 +382,21 @@ int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* cp, const int* ri, c
         // the CSC arrays of A are the CSR arrays of A^T
         DevCsrOwned o;
         const size_t nnz = (size_t)cp[n];
-        cuda_check(cudaMalloc(&o.rp, sizeof(int) * (n + 1)), "csr alloc");
-        cuda_check(cudaMalloc(&o.ci, sizeof(int) * std::max<size_t>(nnz, 1)), "csr alloc");
-        cuda_check(cudaMalloc(&o.v, sizeof(double) * std::max<size_t>(nnz, 1)), "csr alloc");
-        cuda_check(cudaMemcpyAsync(o.rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
-        cuda_check(cudaMemcpyAsync(o.ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
-        cuda_check(cudaMemcpyAsync(o.v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        int* o_rp = o.rp.get<int>((size_t)n + 1, s);
+        int* o_ci = o.ci.get<int>(nnz, s);
+        double* o_v = o.v.get<double>(nnz, s);
+        cuda_check(cudaMemcpyAsync(o_rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(o_ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(o_v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
         DevCsr At;
         At.m = n;
         At.n = m;
-        At.rp = o.rp;
-        At.ci = o.ci;
-        At.v = o.v;
-        double *dg = nullptr, *dl = nullptr;
-        cuda_check(cudaMalloc(&dg, sizeof(double) * n), "adjoint alloc");
-        cuda_check(cudaMalloc(&dl, sizeof(double) * m), "adjoint alloc");
+        At.rp = o_rp;
+        At.ci = o_ci;
+        At.v = o_v;
+        DevBuf buf_dg, buf_dl;
+        double* dg = buf_dg.get<double>(n, s);
+        double* dl = buf_dl.get<double>(m, s);
         cuda_check(cudaMemcpyAsync(dg, g, sizeof(double) * n, cudaMemcpyHostToDevice, s), "adjoint h2d");
         cuda_check(cudaMemcpyAsync(dl, lam, sizeof(double) * m, cudaMemcpyHostToDevice, s), "adjoint h2d");
         long long l = 0;
@@ -395,8 +404,6 @@ int spq_gmres_adjoint(spq_tree* t, int m, int n, const int* cp, const int* ri, c
         t->launches_krylov += l;
         cuda_check(cudaMemcpyAsync(lam, dl, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "adjoint d2h");
         cuda_check(cudaStreamSynchronize(s), "adjoint gmres");
-        cudaFree(dg);
-        cudaFree(dl);
         return SPQ_OK;
     });
 }
@@ -418,15 +425,13 @@ int spq_solve_nrml(spq_tree* t, const double* b, double* x) {
     return guard_on(t, [&] {
         const int n = t->eng->ncols();
         cudaStream_t s = t->eng->stream();
-        double *db = nullptr, *dx = nullptr;
-        cuda_check(cudaMalloc(&db, sizeof(double) * n), "solve_nrml alloc");
-        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "solve_nrml alloc");
+        DevBuf buf_db, buf_dx;
+        double* db = buf_db.get<double>(n, s);
+        double* dx = buf_dx.get<double>(n, s);
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s), "solve_nrml h2d");
         t->eng->solve_nrml_dev(db, dx);
         cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "solve_nrml d2h");
         cuda_check(cudaStreamSynchronize(s), "solve_nrml");
-        cudaFree(db);
-        cudaFree(dx);
         return SPQ_OK;
     });
 }
@@ -444,9 +449,9 @@ int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const dou
         DevCsrOwned o;
         DevCsr A;
         upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
-        double *db = nullptr, *dx = nullptr;
-        cuda_check(cudaMalloc(&db, sizeof(double) * m), "gmres alloc");
-        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "gmres alloc");
+        DevBuf buf_db, buf_dx;
+        double* db = buf_db.get<double>(m, s);
+        double* dx = buf_dx.get<double>(n, s);
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "gmres h2d");
         cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "gmres h2d");
         long long l = 0;
@@ -454,8 +459,6 @@ int spq_gmres(spq_tree* t, int m, int n, const int* cp, const int* ri, const dou
         t->launches_krylov += l;
         cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gmres d2h");
         cuda_check(cudaStreamSynchronize(s), "gmres");
-        cudaFree(db);
-        cudaFree(dx);
         return SPQ_OK;
     });
 }
@@ -475,9 +478,9 @@ int spq_solve_to_residual(spq_tree* t, int m, int n, const int* cp, const int* r
         DevCsrOwned o;
         DevCsr A;
         upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
-        double *db = nullptr, *dx = nullptr;
-        cuda_check(cudaMalloc(&db, sizeof(double) * m), "alloc");
-        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "alloc");
+        DevBuf buf_db, buf_dx;
+        double* db = buf_db.get<double>(m, s);
+        double* dx = buf_dx.get<double>(n, s);
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "h2d");
         cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "h2d");
         int outer = 0;
@@ -486,8 +489,6 @@ int spq_solve_to_residual(spq_tree* t, int m, int n, const int* cp, const int* r
         t->launches_krylov += l;
         cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "d2h");
         cuda_check(cudaStreamSynchronize(s), "solve_to_residual");
-        cudaFree(db);
-        cudaFree(dx);
         return *true_res <= target ? SPQ_OK : fail(SPQ_ERR_NOCONV, "target residual not reached");
     });
 }
@@ -673,24 +674,22 @@ int spq_cgls(spq_tree* t, int m, int n, const int* cp, const int* ri, const doub
         upload_csr(csc_from(m, n, cp, ri, va), o, A, s);
         // the CSC arrays of A are the CSR arrays of A^T
         const size_t nnz = (size_t)cp[n];
-        cuda_check(cudaMalloc(&ot.rp, sizeof(int) * (n + 1)), "csr alloc");
-        cuda_check(cudaMalloc(&ot.ci, sizeof(int) * std::max<size_t>(nnz, 1)), "csr alloc");
-        cuda_check(cudaMalloc(&ot.v, sizeof(double) * std::max<size_t>(nnz, 1)), "csr alloc");
-        cuda_check(cudaMemcpyAsync(ot.rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
-        cuda_check(cudaMemcpyAsync(ot.ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
-        cuda_check(cudaMemcpyAsync(ot.v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
-        double *db = nullptr, *dx = nullptr;
-        cuda_check(cudaMalloc(&db, sizeof(double) * m), "cgls alloc");
-        cuda_check(cudaMalloc(&dx, sizeof(double) * n), "cgls alloc");
+        int* ot_rp = ot.rp.get<int>((size_t)n + 1, s);
+        int* ot_ci = ot.ci.get<int>(nnz, s);
+        double* ot_v = ot.v.get<double>(nnz, s);
+        cuda_check(cudaMemcpyAsync(ot_rp, cp, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(ot_ci, ri, sizeof(int) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        cuda_check(cudaMemcpyAsync(ot_v, va, sizeof(double) * nnz, cudaMemcpyHostToDevice, s), "csr up");
+        DevBuf buf_db, buf_dx;
+        double* db = buf_db.get<double>(m, s);
+        double* dx = buf_dx.get<double>(n, s);
         cuda_check(cudaMemcpyAsync(db, b, sizeof(double) * m, cudaMemcpyHostToDevice, s), "cgls h2d");
         cuda_check(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s), "cgls h2d");
-        const int r2 = spq_cgls_dev(t, m, n, A.rp, A.ci, A.v, ot.rp, ot.ci, ot.v, db, dx, iters, tol, its, res);
+        const int r2 = spq_cgls_dev(t, m, n, A.rp, A.ci, A.v, ot_rp, ot_ci, ot_v, db, dx, iters, tol, its, res);
         if (r2 == SPQ_OK) {
             cuda_check(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "cgls d2h");
             cuda_check(cudaStreamSynchronize(s), "cgls");
         }
-        cudaFree(db);
-        cudaFree(dx);
         return r2;
     });
 }
