@@ -40,6 +40,10 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "advdiff3d_64"
 TARGET = 1e-10
+# GMRES tolerance of each refinement correction with the FP32 factor: measured on
+# the 64^3 workload, 1e-3 .. 1e-5 need the fewest preconditioner applications
+# (11-12 iterations; 1e-6: 14, 1e-8: 18, 1e-10: 22)
+FP32_INNER = 1e-5
 METRIC = "time to ‖Ax−b‖/‖b‖≤1e-10 (factor+Krylov), FP32-batched vs plain FP64, 1 B200"
 
 
@@ -166,7 +170,7 @@ def timed_step(w, A, csr, d_b, precision, device, profile=False):
     stream = torch.cuda.ExternalStream(sp.value)
     x = torch.zeros(A[1], dtype=torch.float64, device="cuda")
     rp, ci, va = csr
-    inner = TARGET if precision == 0 else 1e-6
+    inner = TARGET if precision == 0 else FP32_INNER
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -211,7 +215,7 @@ def e2e_step(w, A, b, precision, device):
     t.partition(A)
     t.assemble(A)
     t.factorize()
-    x, its, res = solve_to_residual(A, b, t, target=TARGET, inner_tol=TARGET if precision == 0 else 1e-6)
+    x, its, res = solve_to_residual(A, b, t, target=TARGET, inner_tol=TARGET if precision == 0 else FP32_INNER)
     torch.cuda.synchronize()
     sec = time.perf_counter() - t0
     t.close()
@@ -434,8 +438,9 @@ def _tree_for(w, A, precision, square=1):
     return t
 
 
-def _gpu_square(w, A, precision, target, inner):
-    """factorize + refinement to the true residual target (CUDA events)."""
+def _gpu_square(w, A, precision, target, inner, max_outer=20):
+    """factorize + refinement to the true residual target (CUDA events), at most
+    max_outer GMRES corrections of 300 iterations."""
     import torch
     from spaqr_public_b200._abi import check, lib
     rp, ci, va = device_csr(A)
@@ -454,13 +459,14 @@ def _gpu_square(w, A, precision, target, inner):
     its, res = C.c_int(0), C.c_double(0)
     rc = lib().spq_solve_to_residual_dev(t._h, A[0], C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
                                          C.c_void_p(va.data_ptr()), C.c_void_p(d_b.data_ptr()),
-                                         C.c_void_p(x.data_ptr()), target, inner, 20, 300, C.byref(its), C.byref(res))
+                                         C.c_void_p(x.data_ptr()), target, inner, max_outer, 300, C.byref(its),
+                                         C.byref(res))
     e1.record(st)
     torch.cuda.synchronize()
-    if rc not in (0, 7):  # 7: target not reached within 20 corrections (reported, not raised)
+    if rc not in (0, 7):  # 7: target not reached within max_outer corrections (reported, not raised)
         check(rc)
     out = dict(total_s=e0.elapsed_time(e1) / 1e3, factor_s=e0.elapsed_time(e_f) / 1e3, its=its.value,
-               true_residual=res.value, converged=rc == 0)
+               true_residual=res.value, converged=rc == 0, max_outer=max_outer)
     t.close()
     return out, x.cpu().numpy()
 
@@ -538,9 +544,12 @@ def run_configs(args):
     rows = []
     for tol in (1e-1, 1e-2, 1e-3):
         w2 = dict(w, tol=tol)
-        for _ in range(2):
-            g32, x32 = _gpu_square(w2, A, FP32, 1e-10, 1e-6)
-        g64t, _ = _gpu_square(w2, A, FP64, 1e-10, 1e-10)
+        # tol 1e-1 leaves a preconditioner too weak for the 10^6 contrast: two
+        # corrections of 300 iterations show it (twenty took ~50 s per arm)
+        mo, reps = (2, 1) if tol >= 1e-1 else (20, 2)
+        for _ in range(reps):
+            g32, x32 = _gpu_square(w2, A, FP32, 1e-10, 1e-6, mo)
+        g64t, _ = _gpu_square(w2, A, FP64, 1e-10, 1e-10, mo)
         rows.append({"tol": tol, "fp32": g32, "fp64": g64t,
                      "rel_error_vs_fp64_tol1e-2": float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))})
     print(json.dumps({"config": "contrast2d_512 (512^2, 16x16 log-uniform patches in [1e-3, 1e3], 12 levels), FP32 "
