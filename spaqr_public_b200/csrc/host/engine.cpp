@@ -451,9 +451,12 @@ private:
         int fam;
         cudaEvent_t a, b;
         double flops, bytes;
+        std::string tag;
     };
     bool prof_ = false;
     std::vector<Pending> pend_;
+    std::string tag_;  // launch shape printed beside its time (profiling with verbose >= 4)
+    bool tracing() const { return prof_ && cfg_.verbose >= 4; }
     KernelStat fam_[kNumFamilies];
 
     template <class F>
@@ -468,7 +471,8 @@ private:
         cudaEventRecord(a, stream_);
         launch();
         cudaEventRecord(b, stream_);
-        pend_.push_back(Pending{fam, a, b, flops, bytes});
+        pend_.push_back(Pending{fam, a, b, flops, bytes, std::move(tag_)});
+        tag_.clear();
         return pend_.size() - 1;
     }
     void flush_prof() {
@@ -481,6 +485,7 @@ private:
             fam_[p.fam].ms += ms;
             fam_[p.fam].flops += p.flops;
             fam_[p.fam].bytes += p.bytes;
+            if (!p.tag.empty()) std::fprintf(stderr, "    trace %d %.4f ms %s\n", p.fam, ms, p.tag.c_str());
             cudaEventDestroy(p.a);
             cudaEventDestroy(p.b);
         }
@@ -655,18 +660,74 @@ private:
             while (c < 16 && (size_t)R > panel_cl_max_rows<T>(c)) ++c;
             return (size_t)R > panel_cl_max_rows<T>(c) ? 0 : c;
         };
-        std::vector<std::map<int, std::vector<int>>> pgroups(ids.size());
-        for (size_t i = 0; i < ids.size(); ++i)
-            for (int t : ids[i]) pgroups[i][panel_cluster(qt[t].m - (int)i * kNB)].push_back(t);
+        // panel launches of each step: tasks beyond the clusters (single-CTA kernel)
+        // apart; the cluster tasks in one launch whose cluster is the largest any of
+        // them needs, unless the idle CTAs of the smaller tasks would cost more than
+        // one more launch (the launch does not fit the SMs at once and a third or
+        // more of its CTAs would idle); then one launch per class of cluster sizes
+        // (1, 2, 3-4, 5-8, 9-16). ids: task indices then their cluster sizes.
+        // Panels of at most 16 * kPanelRegRows rows run register-resident
+        // (k_panel_reg, slabs of kPanelRegRows rows), taller ones from shared-memory
+        // slabs (k_panel_cl).
+        struct PanelLaunch {
+            int kind = 0;  // 0 single-CTA, 1 shared-memory slabs, 2 register-resident
+            int cluster = 0, max_slab = 0;
+            std::vector<int> ids;
+        };
+        std::vector<std::vector<PanelLaunch>> pgroups(ids.size());
+        for (size_t i = 0; i < ids.size(); ++i) {
+            const int p = (int)i * kNB;
+            PanelLaunch single;
+            std::vector<std::pair<int, int>> clt[2];  // (cluster size, task) of kinds 1 and 2
+            for (int t : ids[i]) {
+                const int R = qt[t].m - p;
+                if (R <= 16 * kPanelRegRows) {
+                    clt[1].push_back({std::max(1, (R + kPanelRegRows - 1) / kPanelRegRows), t});
+                    continue;
+                }
+                const int c = panel_cluster(R);
+                if (c == 0)
+                    single.ids.push_back(t);
+                else
+                    clt[0].push_back({c, t});
+            }
+            if (!single.ids.empty()) pgroups[i].push_back(std::move(single));
+            for (int kind = 1; kind <= 2; ++kind) {
+                auto& list = clt[kind - 1];
+                if (list.empty()) continue;
+                int cmax = 0;
+                long long used = 0;
+                for (auto& e : list) {
+                    cmax = std::max(cmax, e.first);
+                    used += e.first;
+                }
+                const long long total = (long long)cmax * (long long)list.size();
+                const bool one = total <= 2 * 148 || 3 * used >= 2 * total;
+                auto cls = [&](int c) { return one ? 0 : (c <= 2 ? c : c <= 4 ? 3 : c <= 8 ? 4 : 5); };
+                std::map<int, std::vector<std::pair<int, int>>> by;
+                for (auto& e : list) by[-cls(e.first)].push_back(e);
+                for (auto& kv : by) {
+                    PanelLaunch L;
+                    L.kind = kind;
+                    for (auto& e : kv.second) {
+                        L.cluster = std::max(L.cluster, e.first);
+                        L.max_slab = std::max(L.max_slab, (qt[e.second].m - p + e.first - 1) / e.first);
+                        L.ids.push_back(e.second);
+                    }
+                    for (auto& e : kv.second) L.ids.push_back(e.first);
+                    pgroups[i].push_back(std::move(L));
+                }
+            }
+        }
         Upload up;
         size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
                o_post = up.add(post);
         std::vector<size_t> o_ids, o_tiles;
-        std::vector<std::map<int, size_t>> o_pg(ids.size());
+        std::vector<std::vector<size_t>> o_pg(ids.size());
         for (size_t i = 0; i < ids.size(); ++i) {
             o_ids.push_back(up.add(ids[i]));
             o_tiles.push_back(up.add(tiles[i]));
-            for (auto& kv : pgroups[i]) o_pg[i][kv.first] = up.add(kv.second);
+            for (auto& L : pgroups[i]) o_pg[i].push_back(up.add(L.ids));
         }
         char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
@@ -690,22 +751,35 @@ private:
                 tb += (2 * R * tn + R * w) * sizeof(T);
             }
             const int smem_rows = std::min(rows, smem_limit);
+            if (tracing()) {
+                tag_ = "panel p " + std::to_string(p);
+                for (auto& L : pgroups[i])
+                    tag_ += " | kind " + std::to_string(L.kind) + " cl " + std::to_string(L.cluster) + " n " +
+                            std::to_string(L.kind ? L.ids.size() / 2 : L.ids.size()) + " slab " +
+                            std::to_string(L.max_slab);
+            }
             timed(KF_PANEL, pf, pb, [&] {
-                for (auto& kv : pgroups[i]) {
-                    const int* gids = reinterpret_cast<const int*>(d + o_pg[i][kv.first]);
+                for (size_t g = 0; g < pgroups[i].size(); ++g) {
+                    const PanelLaunch& L = pgroups[i][g];
+                    const int* gids = reinterpret_cast<const int*>(d + o_pg[i][g]);
                     const QRTask<T>* dq = reinterpret_cast<const QRTask<T>*>(d + o_q);
-                    if (kv.first == 0) {
-                        launch_panel<T>(dq, gids, (int)kv.second.size(), p, smem_rows, stream_);
-                    } else {
-                        int maxr = 0;
-                        for (int t : kv.second) maxr = std::max(maxr, qt[t].m - p);
-                        cuda_check(launch_panel_cl<T>(dq, gids, (int)kv.second.size(), kv.first, maxr, p, stream_),
+                    if (L.kind == 0)
+                        launch_panel<T>(dq, gids, (int)L.ids.size(), p, smem_rows, stream_);
+                    else if (L.kind == 1)
+                        cuda_check(launch_panel_cl<T>(dq, gids, (int)L.ids.size() / 2, L.cluster, L.max_slab, p,
+                                                      stream_),
                                    "panel launch");
-                    }
+                    else
+                        cuda_check(launch_panel_reg<T>(dq, gids, (int)L.ids.size() / 2, L.cluster, L.max_slab, p,
+                                                       stream_),
+                                   "panel launch");
                     ++launches_fact_;
                 }
             });
             if (!tiles[i].empty()) {
+                if (tracing())
+                    tag_ = "trailing p " + std::to_string(p) + " tiles " + std::to_string(tiles[i].size()) + " R " +
+                           std::to_string(rows);
                 timed(KF_TRAILING, tf, tb, [&] {
                     launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
                                        reinterpret_cast<const TileRef*>(d + o_tiles[i]), (int)tiles[i].size(), p,
@@ -1094,6 +1168,9 @@ private:
                     cuda_check(cudaEventCreate(&eb), "event");
                     cudaEventRecord(ea, stream_);
                 }
+                if (tracing())
+                    tag_ = "rrqr_blk n " + std::to_string(nt) + " cl " + std::to_string(cl) + " m " +
+                           std::to_string(maxm) + " k " + std::to_string(maxn);
                 rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
                     cudaError_t e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, stream_);
                     while (e != cudaSuccess && cl > 1 && rrqr_blk_fits<T>(maxm, maxn, cl / 2)) {

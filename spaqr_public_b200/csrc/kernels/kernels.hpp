@@ -53,15 +53,25 @@ struct TileRef {
 template <class T>
 void launch_panel(const QRTask<T>* tasks, const int* task_ids, int ntasks, int p, int smem_rows,
                   cudaStream_t s);
-// Panel p of every listed task on a thread-block cluster of `cluster` CTAs
-// (row slabs in shared memory, one DSMEM reduction per column). Every task's
-// panel height m - p must be at least 32 * cluster when cluster > 1 and at
-// most panel_cl_max_rows(cluster); max_rows = the largest height in the list.
+// Panel p of every listed task on thread-block clusters of `cluster` CTAs
+// (row slabs in shared memory, one cluster barrier per column). task_ids
+// holds ntasks task indices followed by each task's own cluster size CLt
+// (1 <= CLt <= cluster; the task uses its first CLt CTAs): the panel height
+// m - p must be at least 32 * CLt when CLt > 1 and at most
+// panel_cl_max_rows(CLt); max_slab = the largest ceil((m - p) / CLt).
 template <class T>
-cudaError_t launch_panel_cl(const QRTask<T>* tasks, const int* task_ids, int ntasks, int cluster, int max_rows, int p,
+cudaError_t launch_panel_cl(const QRTask<T>* tasks, const int* task_ids, int ntasks, int cluster, int max_slab, int p,
                             cudaStream_t s);
 template <class T>
 size_t panel_cl_max_rows(int cluster);
+// Panel p of every listed task held in registers: slabs of at most
+// kPanelRegRows rows, task_ids as for launch_panel_cl with
+// CLt = ceil((m - p) / kPanelRegRows) (so m - p <= 16 * kPanelRegRows);
+// max_slab = the largest ceil((m - p) / CLt) (it picks the rows per lane).
+constexpr int kPanelRegRows = 256;
+template <class T>
+cudaError_t launch_panel_reg(const QRTask<T>* tasks, const int* task_ids, int ntasks, int cluster, int max_slab,
+                             int p, cudaStream_t s);
 // Trailing update after panel p: tiles of kTN columns of [fac(:, p+NB:k) | tr].
 template <class T>
 void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s);
