@@ -277,32 +277,39 @@ private:
     size_t ci_ = 0, used_ = 0;
 };
 
-// Host staging of one batch of heterogeneous descriptor arrays, uploaded with
-// one copy into arena memory that stays valid for the handle's lifetime.
+// One batch of heterogeneous descriptor arrays, uploaded with one copy into
+// arena memory that stays valid for the handle's lifetime. add() records where
+// an array lies; commit() packs the arrays straight into the pinned stage, so
+// every array passed to add() must stay alive and unchanged until commit().
 class Upload {
 public:
     template <class U>
     size_t add(const std::vector<U>& v) {
-        size_t off = (buf_.size() + 15) & ~size_t(15);
-        buf_.resize(off + v.size() * sizeof(U));
-        if (!v.empty()) std::memcpy(buf_.data() + off, v.data(), v.size() * sizeof(U));
+        const size_t off = (size_ + 15) & ~size_t(15);
+        const size_t bytes = v.size() * sizeof(U);
+        if (bytes) spans_.push_back(Span{reinterpret_cast<const char*>(v.data()), bytes, off});
+        size_ = off + bytes;
         return off;
     }
     // Returns the device base; element arrays are at base + offset. The bytes
     // go through the pinned stage, so the copy does not wait for the stream.
     char* commit(Arena& arena, cudaStream_t s, PinnedStage& stage) {
-        if (buf_.empty()) return nullptr;
-        char* d = static_cast<char*>(arena.alloc(buf_.size()));
-        char* h = stage.get(buf_.size());
-        std::memcpy(h, buf_.data(), buf_.size());
-        cuda_check(cudaMemcpyAsync(d, h, buf_.size(), cudaMemcpyHostToDevice, s), "descriptor upload");
+        if (size_ == 0) return nullptr;
+        char* d = static_cast<char*>(arena.alloc(size_));
+        char* h = stage.get(size_);
+        for (const Span& sp : spans_) std::memcpy(h + sp.off, sp.p, sp.bytes);
+        cuda_check(cudaMemcpyAsync(d, h, size_, cudaMemcpyHostToDevice, s), "descriptor upload");
         return d;
     }
-    void clear() { buf_.clear(); }
-    bool empty() const { return buf_.empty(); }
+    bool empty() const { return size_ == 0; }
 
 private:
-    std::vector<char> buf_;
+    struct Span {
+        const char* p;
+        size_t bytes, off;
+    };
+    std::vector<Span> spans_;
+    size_t size_ = 0;
 };
 
 }  // namespace spq

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <deque>
 #include <map>
 #include <numeric>
 
@@ -67,7 +68,7 @@ public:
         Cid parentid;
         int rposparent = 0, cposparent = 0;
         std::vector<Cluster*> children;
-        std::set<Cluster*, ByOrder> rsparsity, cnbrs;
+        std::vector<Cluster*> rsparsity;  // by order
         std::vector<Edge*> out, in;
         int xcap = 0;
         int64_t xoff = -1;
@@ -219,7 +220,6 @@ public:
             }
             std::stable_sort(self->out.begin(), self->out.end(),
                              [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
-            self->cnbrs = cn;
         }
         uint64_t* d_addr = desc_arena_.alloc_n<uint64_t>(addr.size());
         double* d_vals = desc_arena_.alloc_n<double>(vals.size());
@@ -261,24 +261,35 @@ public:
                 t_phase_[k] += now - th;
                 th = now;
             };
+            size_t nfill = 0;
             for (Cluster* s : cur())
-                if (s->level() == ilvl_) get_sparsity(s);
+                if (s->level() == ilvl_) {
+                    get_sparsity(s);
+                    ++nfill;
+                }
+            if (cfg_.verbose >= 3)
+                std::fprintf(stderr, "[lvl %d] fill host: %zu of %zu clusters, %.2f ms\n", ilvl_, nfill, cur().size(),
+                             (wall() - th) * 1e3);
             lap(0);
             cudaEventRecord(ev[1], stream_);
+            phase_ = 1;
             elim_phase();
             lap(1);
             cudaEventRecord(ev[2], stream_);
             if (rect_ && ilvl_ < L - 1) reassign_phase();
             lap(2);
             cudaEventRecord(ev[3], stream_);  // shift (rectangular only)
+            phase_ = 3;
             const bool window = ilvl_ < L - 2 && ilvl_ >= cfg_.skip && cfg_.tol != 0;
             if (cfg_.scale && window) scale_phase();
             lap(3);
             cudaEventRecord(ev[4], stream_);
+            phase_ = 4;
             if (rect_ && cfg_.scale && window) extra_phase();
             if (window) sparsify_phase();
             lap(4);
             cudaEventRecord(ev[5], stream_);
+            phase_ = 5;
             if (ilvl_ < L - 1) merge_all();
             lap(5);
             cudaEventRecord(ev[6], stream_);
@@ -392,7 +403,7 @@ private:
     double t_phase_[6] = {0, 0, 0, 0, 0, 0};  // host time per phase: fill, elim, shift, scale, sparsify, merge
     std::vector<std::vector<Cluster*>> bottoms_, fine_;
     std::vector<std::unique_ptr<Cluster>> clusters_;
-    std::vector<std::unique_ptr<Edge>> edges_;
+    std::deque<Edge> edges_;  // stable addresses
     std::vector<TapeOp> tape_;
     std::vector<int> cperm_, rperm_;
     bool rect_ = false;  // least squares (no identity row matching): rows move, R^T R solves
@@ -452,7 +463,9 @@ private:
         cudaEvent_t a, b;
         double flops, bytes;
         std::string tag;
+        int level, phase;
     };
+    int phase_ = 0;  // factorization phase of the launches being issued (profiling trace)
     bool prof_ = false;
     std::vector<Pending> pend_;
     std::string tag_;  // launch shape printed beside its time (profiling with verbose >= 4)
@@ -471,7 +484,7 @@ private:
         cudaEventRecord(a, stream_);
         launch();
         cudaEventRecord(b, stream_);
-        pend_.push_back(Pending{fam, a, b, flops, bytes, std::move(tag_)});
+        pend_.push_back(Pending{fam, a, b, flops, bytes, std::move(tag_), ilvl_, phase_});
         tag_.clear();
         return pend_.size() - 1;
     }
@@ -485,7 +498,8 @@ private:
             fam_[p.fam].ms += ms;
             fam_[p.fam].flops += p.flops;
             fam_[p.fam].bytes += p.bytes;
-            if (!p.tag.empty()) std::fprintf(stderr, "    trace %d %.4f ms %s\n", p.fam, ms, p.tag.c_str());
+            if (prof_ && cfg_.verbose >= 4)
+                std::fprintf(stderr, "    trace %d %.4f ms L%d P%d %s\n", p.fam, ms, p.level, p.phase, p.tag.c_str());
             cudaEventDestroy(p.a);
             cudaEventDestroy(p.b);
         }
@@ -535,12 +549,11 @@ private:
         return b;
     }
     Edge* new_edge(Cluster* n1, Cluster* n2, const Blk& b) {
-        edges_.emplace_back(new Edge{n1, n2, b, true});
-        return edges_.back().get();
+        edges_.push_back(Edge{n1, n2, b, true});
+        return &edges_.back();
     }
     Edge* add_edge(Cluster* c1, Cluster* c2) {  // src/tree.cpp:251-261
         Edge* e = new_edge(c1, c2, new_block(c2->rsize, c1->csize));
-        c1->cnbrs.insert(c2);
         c1->out.push_back(e);
         if (c1 != c2) c2->in.push_back(e);
         return e;
@@ -550,6 +563,7 @@ private:
             if (e->n2 == n2) return e;
         return nullptr;
     }
+
     std::pair<int, int> topsize() const {
         int tr = 0, tc = 0;
         for (Cluster* s : cur())
@@ -561,33 +575,38 @@ private:
     }
 
     // src/tree.cpp:168-224
-    bool valid_fill(const Cid& cid, const Cid& nid, const std::set<Sep>& cols) const {
+    bool valid_fill(const Cid& cid, const Cid& nid, const std::vector<Sep>& cols) const {
         const Sep cs = cid.self, ns = nid.self;
         if (cs.lvl > ns.lvl) return false;
-        auto pw = [](int e) { return (int)std::pow(2.0, e); };
+        auto pw = [](int e) { return 1 << e; };
         if (cs.sep / pw(ns.lvl - cs.lvl) != ns.sep) return false;
         auto side_ok = [&](const Sep& s) {
             const int dl = s.lvl - cs.lvl;
             return s.lvl >= cs.lvl ? (cs.sep / pw(dl)) == s.sep : (s.sep / pw(-dl)) == cs.sep;
         };
         if (!side_ok(nid.l) && !side_ok(nid.r)) return false;
-        if (!cols.count(ns)) return false;
-        if (!cols.count(nid.l) && !cols.count(nid.r)) return false;
+        auto has = [&](const Sep& x) { return std::binary_search(cols.begin(), cols.end(), x); };
+        if (!has(ns)) return false;
+        if (!has(nid.l) && !has(nid.r)) return false;
         return true;
     }
     // src/tree.cpp:834-870 (geometric mode: purely symbolic)
     void get_sparsity(Cluster* c) {
-        std::set<Cluster*, ByOrder> rs;
-        std::set<Sep> cols;
-        for (Edge* e : c->out) cols.insert(e->n2->id.self);
+        std::vector<Cluster*> rs;
+        std::vector<Sep> cols;
+        for (Edge* e : c->out) cols.push_back(e->n2->id.self);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
         for (Edge* e : c->out) {
             if (!e->live) continue;
             Cluster* n = e->n2;
-            rs.insert(n);
+            rs.push_back(n);
             for (Edge* ein : n->in)
                 if (ein->live && ein->n1 != c && !ein->n1->elim && valid_fill(c->id, ein->n1->id, cols))
-                    rs.insert(ein->n1);
+                    rs.push_back(ein->n1);
         }
+        std::sort(rs.begin(), rs.end(), [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
+        rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
         c->rsparsity = std::move(rs);
     }
 
@@ -719,6 +738,7 @@ private:
                 }
             }
         }
+        const double tw_built = wall();
         Upload up;
         size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
                o_post = up.add(post);
@@ -730,6 +750,7 @@ private:
             for (auto& L : pgroups[i]) o_pg[i].push_back(up.add(L.ids));
         }
         char* d = up.commit(desc_arena_, stream_, pinned_);
+        const double tw_up = wall();
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
         const int smem_limit = (int)((160 * 1024) / (kNB * sizeof(T)));
         for (size_t i = 0; i < ids.size(); ++i) {
@@ -815,10 +836,11 @@ private:
             }
             for (auto& tl : tiles) nt += tl.size();
             std::fprintf(stderr, "    qr wave: %zu tasks, max m %d, max k %d, max ntr %d, %zu panel steps, %zu tiles, "
-                         "m k (k + ntr) %.3e, %zu trsm tasks, %.2f ms (host %.2f: pinned %.2f scratch %.2f "
-                         "arena %.2f, %zu pinned chunks)\n",
+                         "m k (k + ntr) %.3e, %zu trsm tasks, %.2f ms (host %.2f: build %.2f upload %.2f launch %.2f "
+                         "pinned %.2f scratch %.2f arena %.2f, %zu pinned chunks)\n",
                          qt.size(), maxR, mk, mn, ids.size(), nt, work, trsm.size(), (wall() - tw_wave) * 1e3,
-                         (tsub - tw_wave) * 1e3, (pinned_.alloc_seconds() - pin0) * 1e3,
+                         (tsub - tw_wave) * 1e3, (tw_built - tw_wave) * 1e3, (tw_up - tw_built) * 1e3,
+                         (tsub - tw_up) * 1e3, (pinned_.alloc_seconds() - pin0) * 1e3,
                          (scratch_.grow_seconds() - grow0) * 1e3,
                          (arena_.alloc_seconds() + desc_arena_.alloc_seconds() - ar0) * 1e3, pinned_.chunks());
         }
@@ -842,6 +864,7 @@ private:
 
     // ------------------------------------------------------------- elimination (src/tree.cpp:780-832)
     void elim_phase() {
+        const double te0 = wall();
         struct Task {
             QRJob job;
             std::vector<int> uids;
@@ -915,11 +938,15 @@ private:
             tasks.push_back(std::move(t));
         }
         if (tasks.empty()) return;
+        const double te1 = wall();
         std::vector<std::vector<int>> touched;
         for (auto& t : tasks) touched.push_back(t.uids);
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
         print_waves("elim", wave, nw);
+        if (cfg_.verbose >= 3)
+            std::fprintf(stderr, "[lvl %d] elim host: tasks %.2f ms, waves %.2f ms\n", ilvl_, (te1 - te0) * 1e3,
+                         (wall() - te1) * 1e3);
         for (int w = 0; w < nw; ++w) {
             std::vector<QRJob> jobs;
             for (size_t t = 0; t < tasks.size(); ++t)
@@ -1663,6 +1690,7 @@ private:
 
     // ------------------------------------------------------------- merge (src/tree.cpp:414-475, 872-881)
     void merge_all() {
+        const double tm0 = wall();
         ++cur_bottom_;
         for (Cluster* s : cur()) {
             int rs = 0, cs = 0;
@@ -1683,35 +1711,76 @@ private:
             tape_.push_back(std::move(op));
             rec(4, rs, cs, (long long)s->children.size(), 0, 0, s->order);
         }
+        const double tm1 = wall();
+        double t_nb = 0, t_add = 0, t_sort = 0, t_cp = 0;
         std::vector<CopyDesc<T>> copies;
+        {
+            size_t ne = 0;
+            for (Cluster* s : cur())
+                for (Cluster* so : s->children) ne += so->out.size();
+            copies.reserve(ne);
+        }
+        struct Move {  // one child block into its parent block
+            Edge* eo;
+            Cluster* so;
+            Cluster* np;  // the parent of the block's row cluster
+            int roff;     // row offset of that row cluster in its parent
+        };
+        std::vector<Move> moves;
+        std::vector<Cluster*> nb;
         for (Cluster* s : cur()) {
+            const double ta = wall();
+            nb.clear();
+            moves.clear();
             for (Cluster* so : s->children)
-                for (Edge* eo : so->out)
-                    if (!eo->n2->elim) s->cnbrs.insert(eo->n2->parent);
-            std::vector<Cluster*> nb(s->cnbrs.begin(), s->cnbrs.end());
-            for (Cluster* n : nb) add_edge(s, n);
-            std::stable_sort(s->out.begin(), s->out.end(),
-                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
-            for (Cluster* so : s->children) {
                 for (Edge* eo : so->out) {
-                    Cluster* nold = eo->n2;
-                    if (nold->elim || !eo->live) continue;
-                    Edge* f = find_out(s, nold->parent);
-                    if (!f) throw std::runtime_error("merge: missing parent edge");
+                    const Cluster* nold = eo->n2;
+                    if (nold->elim) continue;
+                    nb.push_back(nold->parent);
+                    if (!eo->live) continue;
                     if (eo->A.rows != nold->rsize || eo->A.cols != so->csize)
                         throw std::runtime_error("merge: block shape mismatch");
-                    copies.push_back(cp(eo->A.p, f->A.p + nold->rposparent + (size_t)so->cposparent * f->A.ld,
-                                        eo->A.ld, f->A.ld, eo->A.rows, eo->A.cols));
-                    eo->live = false;
+                    moves.push_back(Move{eo, so, nold->parent, nold->rposparent});
                 }
+            std::sort(nb.begin(), nb.end(), [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
+            nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+            const double tb = wall();
+            t_nb += tb - ta;
+            s->out.reserve(s->out.size() + nb.size());
+            std::vector<std::pair<Cluster*, Edge*>> pe;  // parent edges by neighbour address
+            pe.reserve(nb.size());
+            for (Cluster* n : nb) pe.emplace_back(n, add_edge(s, n));
+            std::sort(pe.begin(), pe.end());
+            const double tc = wall();
+            t_add += tc - tb;
+            std::stable_sort(s->out.begin(), s->out.end(),
+                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
+            const double td = wall();
+            t_sort += td - tc;
+            for (const Move& mv : moves) {
+                auto it = std::lower_bound(pe.begin(), pe.end(), std::make_pair(mv.np, (Edge*)nullptr));
+                if (it == pe.end() || it->first != mv.np) throw std::runtime_error("merge: missing parent edge");
+                Edge* f = it->second;
+                Edge* eo = mv.eo;
+                copies.push_back(cp(eo->A.p, f->A.p + mv.roff + (size_t)mv.so->cposparent * f->A.ld, eo->A.ld,
+                                    f->A.ld, eo->A.rows, eo->A.cols));
+                eo->live = false;
             }
+            t_cp += wall() - td;
         }
+        const double tm2 = wall();
         if (!copies.empty()) {
             Upload up;
             size_t o = up.add(copies);
             char* d = up.commit(desc_arena_, stream_, pinned_);
             issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
         }
+        if (cfg_.verbose >= 3)
+            std::fprintf(stderr,
+                         "[lvl %d] merge host: %zu clusters, %zu copies, sizes %.2f ms, neighbours %.2f, edges %.2f, "
+                         "sort %.2f, copy list %.2f, upload+launch %.2f\n",
+                         ilvl_, cur().size(), copies.size(), (tm1 - tm0) * 1e3, t_nb * 1e3, t_add * 1e3,
+                         t_sort * 1e3, t_cp * 1e3, (wall() - tm2) * 1e3);
     }
 
     // Diagnostic (verbose >= 2): tasks and waves of one phase.
@@ -1741,6 +1810,7 @@ private:
             build_nrml_plan();
             return;
         }
+        const double tq0 = wall();
         int64_t xtot = 0;
         for (auto& c : clusters_) {
             c->xoff = xtot;
@@ -1764,9 +1834,12 @@ private:
                 xo.push_back(c->xoff + i);
             }
         }
+        const double tq1 = wall();
         std::vector<XSeg> segs;
         std::vector<GemvRef<T>> gemv;
         std::vector<POp> fwd, bwd;
+        fwd.reserve(tape_.size());
+        bwd.reserve(tape_.size());
         auto ptr = [](const T* p) { return (int64_t)reinterpret_cast<uintptr_t>(p); };
         for (const TapeOp& t : tape_) {
             POp f{}, b{};
@@ -1840,6 +1913,7 @@ private:
             bwd.push_back(std::move(b));
         }
         std::reverse(bwd.begin(), bwd.end());
+        const double tq2 = wall();
         gemv_cols_.clear();
         for (auto& g : gemv) gemv_cols_.push_back(g.s);
         std::vector<std::vector<int>> fw, bw;
@@ -1849,6 +1923,7 @@ private:
         std::vector<WMeta> fm, bm;
         pack_waves(fwd, fw, all, fm);
         pack_waves(bwd, bw, all, bm);
+        const double tq3 = wall();
         Upload up;
         size_t o_ops = up.add(all), o_segs = up.add(segs), o_gemv = up.add(gemv), o_src = up.add(src),
                o_dst = up.add(dst), o_xin = up.add(xin), o_xo = up.add(xo);
@@ -1872,6 +1947,10 @@ private:
         // one application reads every stored factor word once (nnzH + nnzR + nnzQ) plus the
         // right-hand side and solution vectors
         solve_bytes_ = (double)(nnzH_ + nnzR_ + nnzQ_) * sizeof(T) + 8.0 * (nrows_ + ncols_);
+        if (cfg_.verbose >= 3)
+            std::fprintf(stderr,
+                         "solve plan host: %zu tape ops, buffers + maps %.2f ms, ops %.2f, waves %.2f, upload %.2f\n",
+                         tape_.size(), (tq1 - tq0) * 1e3, (tq2 - tq1) * 1e3, (tq3 - tq2) * 1e3, (wall() - tq3) * 1e3);
         const size_t smem_cap = (200 * 1024) / sizeof(T);
         for (auto* ws : {&fwd_waves_, &bwd_waves_})
             for (auto& w : *ws)
