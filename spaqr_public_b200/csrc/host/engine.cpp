@@ -111,12 +111,18 @@ public:
         desc_arena_.release();
         scratch_.hand_off(stream_);
         cudaStreamSynchronize(stream_);
+        if (side_) cudaStreamDestroy(side_);
+        if (ev_fork_) cudaEventDestroy(ev_fork_);
+        if (ev_join_) cudaEventDestroy(ev_join_);
         cudaStreamDestroy(stream_);
     }
     void open_device() {
         if (stream_) return;
         cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "event");
+        cuda_check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "event");
         cudaMemPool_t pool = device_pool(cfg_.device);
         arena_.set_stream(stream_, pool);
         desc_arena_.set_stream(stream_, pool);
@@ -395,6 +401,8 @@ public:
 private:
     Config cfg_;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t side_ = nullptr;  // second branch of a solve wave (forked from and joined to stream_)
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Arena arena_;
     Arena desc_arena_{size_t(16) << 20};
     Scratch scratch_;
@@ -433,6 +441,8 @@ private:
         int n, smem;
         double words;
         int hkind, ha, hb;
+        size_t boff;  // tall Q applications (cluster kernel): ops [boff, boff + nbig)
+        int nbig, bcl;
     };
     std::vector<POp> plan_fwd_, plan_bwd_;  // host copies, kept for the adjoint plan
     std::vector<int> gemv_cols_;            // columns of every neighbour block (work counts)
@@ -441,7 +451,31 @@ private:
         int nops, smem;
         double words;        // factor words the wave reads
         int hkind, ha, hb;   // kind and sizes of its largest op
+        const SolveOp* big;  // tall Q applications, one cluster of bcl CTAs each
+        int nbig, bcl;
     };
+    static constexpr int kApplyqBigRows = 384;
+    Wave make_wave(const SolveOp* d_ops, const WMeta& mt) const {
+        return Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb, d_ops + mt.boff, mt.nbig, mt.bcl};
+    }
+    // One sweep wave: the one-CTA ops and the tall Q applications (independent
+    // ops: the cluster launch runs on a branch forked from the stream).
+    int launch_wave(const Wave& w, T* xb) {
+        const bool fork = w.nops > 0 && w.nbig > 0;
+        if (fork) {
+            cuda_check(cudaEventRecord(ev_fork_, stream_), "fork");
+            cuda_check(cudaStreamWaitEvent(side_, ev_fork_, 0), "fork");
+        }
+        if (w.nbig > 0)
+            cuda_check(launch_applyq_cl<T>(w.big, w.nbig, w.bcl, d_segs_, xb, fork ? side_ : stream_),
+                       "solve cluster launch");
+        if (w.nops > 0) launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, stream_);
+        if (fork) {
+            cuda_check(cudaEventRecord(ev_join_, side_), "join");
+            cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+        }
+        return (w.nops > 0) + (w.nbig > 0);
+    }
     std::vector<Wave> fwd_waves_, bwd_waves_, adj_waves_;
     int64_t xtot_ = 0;
     double* d_adj_in_ = nullptr;
@@ -1937,8 +1971,8 @@ private:
         d_xout_pos_ = reinterpret_cast<int64_t*>(d + o_xo);
         fwd_waves_.clear();
         bwd_waves_.clear();
-        for (auto& mt : fm) fwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
-        for (auto& mt : bm) bwd_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+        for (auto& mt : fm) fwd_waves_.push_back(make_wave(d_ops, mt));
+        for (auto& mt : bm) bwd_waves_.push_back(make_wave(d_ops, mt));
         adj_waves_.clear();  // built on the first adjoint solve
         plan_fwd_ = std::move(fwd);
         plan_bwd_ = std::move(bwd);
@@ -2135,7 +2169,7 @@ private:
             for (auto& mt : meta[L]) {
                 if ((size_t)mt.smem > smem_cap)
                     throw std::runtime_error("solve_nrml: a cluster exceeds the shared-memory vector capacity");
-                nrml_waves_[L].push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+                nrml_waves_[L].push_back(make_wave(d_ops, mt));
             }
         }
         nin_ = (int)src.size();
@@ -2162,10 +2196,7 @@ private:
                 ++launches_solve_;
             }
             T* xb = L < 2 ? xtbuf_ : xbuf_;
-            for (auto& w : nrml_waves_[L]) {
-                launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, stream_);
-                ++launches_solve_;
-            }
+            for (auto& w : nrml_waves_[L]) launches_solve_ += launch_wave(w, xb);
         }
         launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
         ++launches_solve_;
@@ -2221,12 +2252,30 @@ private:
     }
     void pack_waves(const std::vector<POp>& ops, const std::vector<std::vector<int>>& waves,
                     std::vector<SolveOp>& all, std::vector<WMeta>& meta) const {
+        // Q applications of at least kApplyqBigRows rows go to the cluster kernel
+        // (after the wave's other ops in the array)
+        auto big = [](const SolveOp& o) {
+            return o.kind == SK_APPLYQ && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows;
+        };
         for (auto& w : waves) {
-            WMeta mt{all.size(), (int)w.size(), 0, 0.0, -1, 0, 0};
+            WMeta mt{all.size(), 0, 0, 0.0, -1, 0, 0, 0, 0, 0};
             double hw = -1;
+            int maxm = 0;
+            for (int i : w)
+                if (!big(ops[i].op)) {
+                    all.push_back(ops[i].op);
+                    mt.smem = std::max(mt.smem, ops[i].smem);
+                    ++mt.n;
+                }
+            mt.boff = all.size();
+            for (int i : w)
+                if (big(ops[i].op)) {
+                    all.push_back(ops[i].op);
+                    maxm = std::max(maxm, ops[i].op.a);
+                    ++mt.nbig;
+                }
+            mt.bcl = mt.nbig ? (maxm + kApplyqClRows - 1) / kApplyqClRows : 0;
             for (int i : w) {
-                all.push_back(ops[i].op);
-                mt.smem = std::max(mt.smem, ops[i].smem);
                 const double ow = op_words(ops[i].op);
                 mt.words += ow;
                 if (ow > hw) {
@@ -2290,7 +2339,7 @@ private:
         for (auto& mt : am) {
             if ((size_t)mt.smem > smem_cap)
                 throw std::runtime_error("adjoint solve: a cluster exceeds the shared-memory vector capacity");
-            adj_waves_.push_back(Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb});
+            adj_waves_.push_back(make_wave(d_ops, mt));
         }
         cuda_check(cudaStreamSynchronize(stream_), "adjoint plan upload");
         pinned_.reset();
@@ -2314,14 +2363,29 @@ public:
         std::vector<const Wave*> all;
         for (auto& w : fwd_waves_) all.push_back(&w);
         for (auto& w : bwd_waves_) all.push_back(&w);
+        std::vector<cudaEvent_t> mid;
         for (const Wave* w : all) {
-            launch_solve_step<T>(w->ops, w->nops, d_segs_, d_gemv_, nullptr, xbuf_, w->smem, stream_);
+            Wave a = *w, b = *w;
+            a.nbig = 0;
+            b.nops = 0;
+            launch_wave(a, xbuf_);
+            cudaEvent_t e;
+            cuda_check(cudaEventCreate(&e), "event");
+            cudaEventRecord(e, stream_);
+            mid.push_back(e);
+            launch_wave(b, xbuf_);
             rec_ev();
         }
         cuda_check(cudaStreamSynchronize(stream_), "profile solve");
         for (size_t i = 0; i < all.size(); ++i) {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            if (cfg_.verbose >= 3 && all[i]->nbig > 0) {
+                float m1 = 0;
+                cudaEventElapsedTime(&m1, ev[i], mid[i]);
+                std::fprintf(stderr, "solve wave %zu: %d ops %.4f ms, %d tall Q ops (cluster %d) %.4f ms\n", i,
+                             all[i]->nops, m1, all[i]->nbig, all[i]->bcl, ms - m1);
+            }
             out.push_back(ms);
             out.push_back(all[i]->nops);
             out.push_back(all[i]->smem);
@@ -2331,6 +2395,7 @@ public:
             out.push_back(all[i]->hb);
         }
         for (auto e : ev) cudaEventDestroy(e);
+        for (auto e : mid) cudaEventDestroy(e);
         return out;
     }
 
@@ -2339,14 +2404,8 @@ private:
         launches_solve_ = 0;
         launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, stream_);
         ++launches_solve_;
-        for (auto& w : fwd_waves_) {
-            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
-            ++launches_solve_;
-        }
-        for (auto& w : bwd_waves_) {
-            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
-            ++launches_solve_;
-        }
+        for (auto& w : fwd_waves_) launches_solve_ += launch_wave(w, xbuf_);
+        for (auto& w : bwd_waves_) launches_solve_ += launch_wave(w, xbuf_);
         launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
         ++launches_solve_;
     }
@@ -2355,8 +2414,7 @@ private:
     void run_adjoint_sweeps() {
         cuda_check(cudaMemsetAsync(xbuf_, 0, sizeof(T) * (size_t)xtot_, stream_), "adjoint zero");
         launch_gather_in<T>(d_adj_in_, d_dst_, d_xout_pos_, xbuf_, nout_, stream_);
-        for (auto& w : adj_waves_)
-            launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
+        for (auto& w : adj_waves_) launch_wave(w, xbuf_);
         launch_scatter_out<T>(xbuf_, d_xin_, d_src_, d_adj_out_, nin_, stream_);
     }
 };

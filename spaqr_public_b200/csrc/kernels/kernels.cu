@@ -512,11 +512,13 @@ __device__ __forceinline__ T warp_transpose_sum(T (&a)[32]) {
 }
 
 // Scratch of the solve-step CTA (static shared memory).
+constexpr int kGemvRefs = 48;  // neighbour-block descriptors a triangular op stages in shared memory
 template <class T>
 struct SolveShared {
     T wred[(kThreads / 32) * kNB];  // per-warp partials
     T y[kNB], z[kNB];
     T tsh[kNB * (kNB + 1)];         // panel T factor / diagonal block of R
+    GemvRef<T> gref[kGemvRefs];
 };
 
 // x(0:m) <- Q^T x (dir 0) or Q x (dir 1), Q from unit-lower V (ld ldv) with
@@ -669,34 +671,44 @@ __device__ void tri_solve(T* xs, int k, const T* R, int ldr, int trans, SolveSha
 
 // xs(0:k) -= sum_b B_b x_b over the neighbour blocks of a triangular op (B_b:
 // k x s_b, ld). Threads form G column groups of RT row threads; each thread
-// keeps eight loads in flight and the groups meet in shared memory.
+// keeps kGU loads of B in flight (a block's last batch clamped to its last
+// column and weighted by zero) and the groups meet in shared memory. The
+// block descriptors are staged in shared memory first, so walking the blocks
+// costs no dependent global load.
 template <class T>
 __device__ void gemv_sub(T* xs, int k, const GemvRef<T>* gv, int nb, const T* x, SolveShared<T>& sh) {
+    constexpr int kGU = 16;
     const int tid = threadIdx.x, nth = blockDim.x;
     const int RT = min(nth, (k + 31) & ~31);
     const int G = nth / RT;
     const int ri = tid % RT, g = tid / RT;
+    const bool staged = nb <= kGemvRefs;
+    if (staged)
+        for (int b = tid; b < nb; b += nth) sh.gref[b] = gv[b];
+    __syncthreads();
+    const GemvRef<T>* refs = staged ? sh.gref : gv;
     for (int i0 = 0; i0 < k; i0 += RT) {
         const int i = i0 + ri;
         T a[4] = {T(0), T(0), T(0), T(0)};
         if (g < G && i < k) {
             for (int bb = 0; bb < nb; ++bb) {
-                const GemvRef<T> r = gv[bb];
+                const GemvRef<T> r = refs[bb];
                 const T* B = aptr<T>(r.boff) + i;
                 const T* xn = x + r.xoff;
                 const size_t ld = (size_t)r.ld;
-                int j = g;
-                for (; j + 7 * G < r.s; j += 8 * G) {
-                    T bv[8], xv[8];
+                const int sl = r.s - 1;
+                for (int j = g; j < r.s; j += kGU * G) {
+                    T bv[kGU], xv[kGU];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        bv[u] = B[(size_t)(j + u * G) * ld];
-                        xv[u] = xn[j + u * G];
+                    for (int u = 0; u < kGU; ++u) {
+                        const int jj = min(j + u * G, sl);
+                        bv[u] = B[(size_t)jj * ld];
+                        xv[u] = xn[jj];
                     }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) a[u & 3] += bv[u] * xv[u];
+                    for (int u = 0; u < kGU; ++u)
+                        if (j + u * G <= sl) a[u & 3] += bv[u] * xv[u];
                 }
-                for (; j < r.s; j += G) a[0] += B[(size_t)j * ld] * xn[j];
             }
         }
         const T part = (a[0] + a[1]) + (a[2] + a[3]);
@@ -716,7 +728,7 @@ __device__ void gemv_sub(T* xs, int k, const GemvRef<T>* gv, int nb, const T* x,
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_solve_step(const SolveOp* ops, const XSeg* segs,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_solve_step(const SolveOp* ops, const XSeg* segs,
                                                         const GemvRef<T>* gemv, T* x) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* xs = reinterpret_cast<T*>(smem_raw);

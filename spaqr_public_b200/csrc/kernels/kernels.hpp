@@ -179,6 +179,11 @@ struct GemvRef {
 template <class T>
 void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const GemvRef<T>* gemv, const T* arena,
                        T* x, int smem_elems, cudaStream_t s);
+// SK_APPLYQ ops on thread-block clusters of `cluster` CTAs, each CTA holding
+// ceil(m / cluster) <= kApplyqClRows rows of the op's x.
+constexpr int kApplyqClRows = 256;
+template <class T>
+cudaError_t launch_applyq_cl(const SolveOp* ops, int nops, int cluster, const XSeg* segs, T* x, cudaStream_t s);
 // dst[pos[k]] = src[pos[k]] (one x buffer into the other at the given positions)
 template <class T>
 void launch_seg_copy(const T* src, T* dst, const int64_t* pos, int n, cudaStream_t s);

@@ -1,0 +1,167 @@
+// Tall Q applications of the preconditioner sweeps on thread-block clusters
+// (the Q^T / Q steps of Tree::solve, src/tree.cpp:1360-1460, for the
+// elimination, scaling and sparsification reflectors).
+//
+// One SK_APPLYQ op of m rows (x(0:m) <- Q^T x for dir 0, Q x for dir 1, Q
+// from unit-lower V with one kNB x kNB T factor per panel) runs on a cluster
+// of CL CTAs, CTA cr holding rows [cr S, (cr + 1) S) with S = ceil(m / CL) <=
+// 256: one row per thread, its x value in a register. A panel costs one pass
+// that loads the row's kNB entries of V into registers and forms the kNB
+// products v x, a warp transpose-sum and a CTA sum, the CTA's kNB sums stored
+// into slot cr of every CTA of the cluster (DSMEM, double-buffered by panel
+// parity), one cluster barrier, then in every warp y = the slots summed in
+// rank order, z = T^T y (dir 0) or T y (dir 1) by lane shuffles, and
+// x -= v^T z from the registers. V is read once per panel (the one-CTA form
+// reads it twice and walks m / 256 rows per thread in each pass).
+#include <cooperative_groups.h>
+
+#include "kernels.hpp"
+
+namespace spq {
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int kAThreads = 256;
+constexpr int kAWarps = kAThreads / 32;
+constexpr int kAMaxCl = 16;
+
+template <class T>
+__device__ __forceinline__ T tsum32(T (&a)[kNB]) {  // lane q returns sum over lanes of a[q]
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int q = 0; q < s; ++q) {
+            const T send = upper ? a[q] : a[q + s];
+            const T keep = upper ? a[q + s] : a[q];
+            a[q] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    return a[0];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, const XSeg* segs, T* x) {
+    __shared__ T part[2][kAMaxCl][kNB];
+    __shared__ T wred[kAWarps][kNB];
+    __shared__ T tsh[2][kNB][kNB + 1];
+    __shared__ T zw[kAWarps][kNB];
+    cg::cluster_group cl = cg::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int cr = (int)cl.block_rank();
+    const SolveOp op = ops[blockIdx.x / CL];
+    const int m = op.a, kq = op.b, ldv = op.c, dir = op.dir;
+    const T* V = reinterpret_cast<const T*>(op.p0);
+    const T* Tf = reinterpret_cast<const T*>(op.p1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int S = (m + CL - 1) / CL;
+    const int r0 = min(m, cr * S);
+    const int nr = min(m, r0 + S) - r0;
+    const int r = r0 + tid;
+    const bool has = tid < nr;
+    T* xp = nullptr;
+    if (has) {
+        if (op.nseg > 0) {
+            int cur = 0;
+            for (int s = 0; s < op.nseg; ++s) {
+                const XSeg sg = segs[op.seg0 + s];
+                if (r < cur + sg.len) {
+                    xp = x + sg.xoff + (r - cur);
+                    break;
+                }
+                cur += sg.len;
+            }
+        } else {
+            xp = x + op.x0 + r;
+        }
+    }
+    T xr = has ? *xp : T(0);
+    const int rl = has ? r : 0;  // a row that exists, for the unconditional loads
+    const int np = (kq + kNB - 1) / kNB;
+    for (int pi = 0; pi < np; ++pi) {
+        const int buf = pi & 1;
+        const int pidx = dir == 0 ? pi : np - 1 - pi;
+        const int p0 = pidx * kNB;
+        const int w = min(kNB, kq - p0);
+        const int wl = w - 1;
+        const T* Tp = Tf + (size_t)pidx * kNB * kNB;
+        for (int e = tid; e < kNB * kNB; e += kAThreads) tsh[buf][e % kNB][e / kNB] = Tp[e];
+        const int rr = r - p0;
+        const T* vr = V + (size_t)p0 * ldv + rl;
+        T v[kNB];
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) v[q] = vr[(size_t)min(q, wl) * ldv];
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) {  // unit diagonal, zeros above it and past the panel
+            const T vq = q < rr ? v[q] : (q == rr ? T(1) : T(0));
+            v[q] = (has && q < w) ? vq : T(0);
+        }
+        T a[kNB];
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) a[q] = v[q] * xr;
+        wred[warp][lane] = tsum32(a);
+        __syncthreads();
+        {
+            T s = T(0);
+#pragma unroll
+            for (int q = 0; q < kAWarps; ++q) s += wred[q][lane];
+            for (int dst = warp; dst < CL; dst += kAWarps) *cl.map_shared_rank(&part[buf][cr][lane], dst) = s;
+        }
+        cl.sync();
+        T y = T(0);
+        for (int q = 0; q < CL; ++q) y += part[buf][q][lane];
+        T z = T(0);  // lane j: z_j = sum_l T(l, j) y_l (dir 0) or T(j, l) y_l (dir 1); zero past w
+        if (dir == 0) {
+#pragma unroll
+            for (int l = 0; l < kNB; ++l) {
+                const T yl = __shfl_sync(0xffffffffu, y, l);
+                if (l <= lane) z += tsh[buf][l][lane] * yl;
+            }
+        } else {
+#pragma unroll
+            for (int l = 0; l < kNB; ++l) {
+                const T yl = __shfl_sync(0xffffffffu, y, l);
+                if (l >= lane && l < w) z += tsh[buf][lane][l] * yl;
+            }
+        }
+        zw[warp][lane] = lane < w ? z : T(0);
+        __syncwarp();
+        T s = T(0);
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) s += v[q] * zw[warp][q];
+        xr -= s;
+    }
+    if (has) *xp = xr;
+}
+
+}  // namespace
+
+template <class T>
+cudaError_t launch_applyq_cl(const SolveOp* ops, int nops, int cluster, const XSeg* segs, T* x, cudaStream_t s) {
+    if (nops <= 0) return cudaSuccess;
+    if (cluster < 1 || cluster > kAMaxCl) return cudaErrorInvalidValue;
+    once_per_device(reinterpret_cast<const void*>(&k_applyq_cl<T>), [] {
+        cudaFuncSetAttribute(k_applyq_cl<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nops * cluster), 1, 1);
+    cfg.blockDim = dim3(kAThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_applyq_cl<T>, ops, segs, x);
+}
+
+template cudaError_t launch_applyq_cl<double>(const SolveOp*, int, int, const XSeg*, double*, cudaStream_t);
+template cudaError_t launch_applyq_cl<float>(const SolveOp*, int, int, const XSeg*, float*, cudaStream_t);
+
+}  // namespace spq
