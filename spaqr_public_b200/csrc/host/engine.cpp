@@ -734,8 +734,11 @@ private:
             std::vector<std::pair<int, int>> clt[2];  // (cluster size, task) of kinds 1 and 2
             for (int t : ids[i]) {
                 const int R = qt[t].m - p;
-                if (R <= 16 * kPanelRegRows) {
-                    clt[1].push_back({std::max(1, (R + kPanelRegRows - 1) / kPanelRegRows), t});
+                if (R <= 16 * kPanelRegRows) {  // FP32 panels up to 512 rows: one CTA, no cluster barrier
+                    const int c = (sizeof(T) == 4 && R <= 2 * kPanelRegRows)
+                                      ? 1
+                                      : std::max(1, (R + kPanelRegRows - 1) / kPanelRegRows);
+                    clt[1].push_back({c, t});
                     continue;
                 }
                 const int c = panel_cluster(R);

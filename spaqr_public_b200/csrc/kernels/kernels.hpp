@@ -65,9 +65,10 @@ cudaError_t launch_panel_cl(const QRTask<T>* tasks, const int* task_ids, int nta
 template <class T>
 size_t panel_cl_max_rows(int cluster);
 // Panel p of every listed task held in registers: slabs of at most
-// kPanelRegRows rows, task_ids as for launch_panel_cl with
-// CLt = ceil((m - p) / kPanelRegRows) (so m - p <= 16 * kPanelRegRows);
-// max_slab = the largest ceil((m - p) / CLt) (it picks the rows per lane).
+// kPanelRegRows rows (2 kPanelRegRows in FP32 without clusters), task_ids as
+// for launch_panel_cl with CLt = ceil((m - p) / kPanelRegRows) (so
+// m - p <= 16 * kPanelRegRows); max_slab = the largest ceil((m - p) / CLt)
+// (it picks the rows per lane).
 constexpr int kPanelRegRows = 256;
 template <class T>
 cudaError_t launch_panel_reg(const QRTask<T>* tasks, const int* task_ids, int ntasks, int cluster, int max_slab,

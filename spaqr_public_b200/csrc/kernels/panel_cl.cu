@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(kPThreads) k_panel_cl(const QRTask<T>* tasks, 
 //      FMA per element, P[r, c] += (-tau d[c]) v[r] (coefficient zero for the
 //      finished columns), the owner then writing v and beta into column j.
 template <class T, bool kCl, int kRPL>
-__global__ void __launch_bounds__(kPThreads, (sizeof(T) == 4 || kRPL < 8) ? 2 : 1) k_panel_reg(const QRTask<T>* tasks, const int* ids, int n, int p) {
+__global__ void __launch_bounds__(kPThreads, ((sizeof(T) == 4 && kRPL < 16) || kRPL < 8) ? 2 : 1) k_panel_reg(const QRTask<T>* tasks, const int* ids, int n, int p) {
     constexpr int CPW = kNB / kPWarps;  // columns per warp
     constexpr int SR = 32 * kRPL;       // slab rows
     static_assert(CPW == 4, "the transposed reduction assumes four columns per warp");
@@ -482,10 +482,12 @@ template <class T>
 cudaError_t launch_panel_reg(const QRTask<T>* tasks, const int* ids, int ntasks, int cluster, int max_slab, int p,
                              cudaStream_t s) {
     if (ntasks <= 0) return cudaSuccess;
-    if (cluster < 1 || cluster > kMaxCl || max_slab > kPanelRegRows) return cudaErrorInvalidValue;
+    if (cluster < 1 || cluster > kMaxCl || max_slab > 2 * kPanelRegRows) return cudaErrorInvalidValue;
     if (max_slab <= 64) return launch_panel_reg_rpl<T, 2>(tasks, ids, ntasks, cluster, p, s);
     if (max_slab <= 128) return launch_panel_reg_rpl<T, 4>(tasks, ids, ntasks, cluster, p, s);
-    return launch_panel_reg_rpl<T, 8>(tasks, ids, ntasks, cluster, p, s);
+    if (max_slab <= kPanelRegRows) return launch_panel_reg_rpl<T, 8>(tasks, ids, ntasks, cluster, p, s);
+    if (sizeof(T) != 4) return cudaErrorInvalidValue;
+    return launch_panel_reg_rpl<T, 16>(tasks, ids, ntasks, cluster, p, s);
 }
 
 template cudaError_t launch_panel_reg<double>(const QRTask<double>*, const int*, int, int, int, int, cudaStream_t);

@@ -7,7 +7,9 @@
 // of CL CTAs, CTA cr holding rows [cr S, (cr + 1) S) with S = ceil(m / CL) <=
 // 256: one row per thread, its x value in a register. A panel costs one pass
 // that loads the row's kNB entries of V into registers and forms the kNB
-// products v x, a warp transpose-sum and a CTA sum, the CTA's kNB sums stored
+// products v x (the next panel's V and T loads are issued right after, so
+// they are in flight during this panel's exchange), a warp transpose-sum and
+// a CTA sum, the CTA's kNB sums stored
 // into slot cr of every CTA of the cluster (DSMEM, double-buffered by panel
 // parity), one cluster barrier, then in every warp y = the slots summed in
 // rank order, z = T^T y (dir 0) or T y (dir 1) by lane shuffles, and
@@ -81,24 +83,39 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
     T xr = has ? *xp : T(0);
     const int rl = has ? r : 0;  // a row that exists, for the unconditional loads
     const int np = (kq + kNB - 1) / kNB;
+    constexpr int TPT = kNB * kNB / kAThreads;  // T entries per thread
+    // raw V entries and T entries of panel pi (loaded one panel ahead)
+    T vraw[kNB], traw[TPT];
+    auto load_panel = [&](int pi, T (&vd)[kNB], T (&td)[TPT]) {
+        const int pidx = dir == 0 ? pi : np - 1 - pi;
+        const int p0 = pidx * kNB;
+        const int wl = min(kNB, kq - p0) - 1;
+        const T* vr = V + (size_t)p0 * ldv + rl;
+#pragma unroll
+        for (int q = 0; q < kNB; ++q) vd[q] = vr[(size_t)min(q, wl) * ldv];
+        const T* Tp = Tf + (size_t)pidx * kNB * kNB;
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) td[u] = Tp[tid + u * kAThreads];
+    };
+    load_panel(0, vraw, traw);
     for (int pi = 0; pi < np; ++pi) {
         const int buf = pi & 1;
         const int pidx = dir == 0 ? pi : np - 1 - pi;
         const int p0 = pidx * kNB;
         const int w = min(kNB, kq - p0);
-        const int wl = w - 1;
-        const T* Tp = Tf + (size_t)pidx * kNB * kNB;
-        for (int e = tid; e < kNB * kNB; e += kAThreads) tsh[buf][e % kNB][e / kNB] = Tp[e];
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+            const int e = tid + u * kAThreads;
+            tsh[buf][e % kNB][e / kNB] = traw[u];
+        }
         const int rr = r - p0;
-        const T* vr = V + (size_t)p0 * ldv + rl;
         T v[kNB];
 #pragma unroll
-        for (int q = 0; q < kNB; ++q) v[q] = vr[(size_t)min(q, wl) * ldv];
-#pragma unroll
         for (int q = 0; q < kNB; ++q) {  // unit diagonal, zeros above it and past the panel
-            const T vq = q < rr ? v[q] : (q == rr ? T(1) : T(0));
+            const T vq = q < rr ? vraw[q] : (q == rr ? T(1) : T(0));
             v[q] = (has && q < w) ? vq : T(0);
         }
+        if (pi + 1 < np) load_panel(pi + 1, vraw, traw);  // in flight during the exchange
         T a[kNB];
 #pragma unroll
         for (int q = 0; q < kNB; ++q) a[q] = v[q] * xr;
