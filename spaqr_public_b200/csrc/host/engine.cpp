@@ -933,11 +933,25 @@ private:
                 off += e->A.rows;
             }
             int nupd = 0, co = 0;
+            // H's row clusters by address: one pass over a neighbour's edges finds
+            // all of its blocks in those rows (the first edge per row cluster, as a
+            // scan per row cluster would); missing ones are added in H's order
+            std::vector<std::pair<const Cluster*, int>> hs;
+            hs.reserve(H.size());
+            for (size_t i = 0; i < H.size(); ++i) hs.emplace_back(H[i]->n2, (int)i);
+            std::sort(hs.begin(), hs.end());
+            std::vector<Edge*> found(H.size());
             for (Cluster* n : c->rsparsity) {
                 if (n->elim || n == c) continue;
+                std::fill(found.begin(), found.end(), nullptr);
+                for (Edge* e2 : n->out) {
+                    auto it = std::lower_bound(hs.begin(), hs.end(), std::make_pair((const Cluster*)e2->n2, -1));
+                    if (it != hs.end() && it->first == e2->n2 && !found[it->second]) found[it->second] = e2;
+                }
                 off = 0;
-                for (Edge* e : H) {
-                    Edge* ecn = find_out(n, e->n2);
+                for (size_t hi = 0; hi < H.size(); ++hi) {
+                    Edge* e = H[hi];
+                    Edge* ecn = found[hi];
                     if (!ecn) ecn = add_edge(n, e->n2);
                     const int pad = off + co * m;  // relative to the wave scratch of this job
                     j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
