@@ -669,6 +669,16 @@ private:
         T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(tr_elems, 1) * sizeof(T), stream_));
         std::vector<CopyDesc<T>> g, s;
         std::vector<QRTask<T>> qt;
+        {
+            size_t ng = 0, ns = 0;
+            for (auto& j : jobs) {
+                ng += j.gather.size();
+                ns += j.scatter.size();
+            }
+            g.reserve(ng);
+            s.reserve(ns);
+            qt.reserve(jobs.size());
+        }
         int maxk = 0, maxR = 0;
         for (auto& j : jobs) {
             T* tr = trbase + j.tr_off;
@@ -991,7 +1001,7 @@ private:
         if (tasks.empty()) return;
         const double te1 = wall();
         std::vector<std::vector<int>> touched;
-        for (auto& t : tasks) touched.push_back(t.uids);
+        for (auto& t : tasks) touched.push_back(std::move(t.uids));
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
         print_waves("elim", wave, nw);
@@ -1001,7 +1011,7 @@ private:
         for (int w = 0; w < nw; ++w) {
             std::vector<QRJob> jobs;
             for (size_t t = 0; t < tasks.size(); ++t)
-                if (wave[t] == w) jobs.push_back(tasks[t].job);
+                if (wave[t] == w) jobs.push_back(std::move(tasks[t].job));
             run_qr_wave(jobs, {}, {});
         }
     }
@@ -1066,7 +1076,7 @@ private:
         }
         if (tasks.empty()) return;
         std::vector<std::vector<int>> touched;
-        for (auto& t : tasks) touched.push_back(t.uids);
+        for (auto& t : tasks) touched.push_back(std::move(t.uids));
         int nw = 0;
         auto wave = assign_waves(touched, next_uid_, &nw);
         print_waves("scale", wave, nw);
@@ -1076,7 +1086,7 @@ private:
             std::vector<CopyDesc<T>> post;
             for (size_t t = 0; t < tasks.size(); ++t) {
                 if (wave[t] != w) continue;
-                jobs.push_back(tasks[t].job);
+                jobs.push_back(std::move(tasks[t].job));
                 tr.insert(tr.end(), tasks[t].trsm.begin(), tasks[t].trsm.end());
                 post.push_back(tasks[t].ident);
             }
