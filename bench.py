@@ -66,16 +66,20 @@ def init_dist(ws, local):
 
 def barrier(d):
     import torch
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if d is not None:
         d.barrier()
 
 
 def max_over_ranks(d, v):
+    """The largest of every rank's v (an all-reduce on the process group's
+    device: CUDA under NCCL, the host under gloo)."""
     if d is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if d.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     d.all_reduce(t, op=d.ReduceOp.MAX)
     return float(t.item())
 
