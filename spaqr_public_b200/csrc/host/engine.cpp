@@ -13,8 +13,10 @@
 #include <cmath>
 #include <cstdio>
 #include <deque>
+#include <exception>
 #include <map>
 #include <numeric>
+#include <thread>
 
 namespace spq {
 namespace {
@@ -267,12 +269,14 @@ public:
                 t_phase_[k] += now - th;
                 th = now;
             };
-            size_t nfill = 0;
+            std::vector<Cluster*> fill;
             for (Cluster* s : cur())
-                if (s->level() == ilvl_) {
-                    get_sparsity(s);
-                    ++nfill;
-                }
+                if (s->level() == ilvl_) fill.push_back(s);
+            // (threads) each cluster's fill set reads the graph and writes only its own set
+            host_parallel_for(fill.size(), [&](size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i) get_sparsity(fill[i]);
+            });
+            const size_t nfill = fill.size();
             if (cfg_.verbose >= 3)
                 std::fprintf(stderr, "[lvl %d] fill host: %zu of %zu clusters, %.2f ms\n", ilvl_, nfill, cur().size(),
                              (wall() - th) * 1e3);
@@ -591,6 +595,36 @@ private:
         c1->out.push_back(e);
         if (c1 != c2) c2->in.push_back(e);
         return e;
+    }
+    // fn(begin, end) over [0, n) on up to 8 host threads, in chunks of at least
+    // 256 items (one call on this thread below that); the first exception a
+    // chunk throws is rethrown after all have joined.
+    template <class F>
+    static void host_parallel_for(size_t n, F&& fn) {
+        const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+        const size_t nt = std::min<size_t>(std::min<size_t>(hw, 8), n / 256);
+        if (nt <= 1) {
+            fn(size_t(0), n);
+            return;
+        }
+        std::vector<std::thread> th;
+        std::vector<std::exception_ptr> err(nt);
+        for (size_t t = 1; t < nt; ++t)
+            th.emplace_back([&, t] {
+                try {
+                    fn(n * t / nt, n * (t + 1) / nt);
+                } catch (...) {
+                    err[t] = std::current_exception();
+                }
+            });
+        try {
+            fn(size_t(0), n / nt);
+        } catch (...) {
+            err[0] = std::current_exception();
+        }
+        for (auto& x : th) x.join();
+        for (auto& e : err)
+            if (e) std::rethrow_exception(e);
     }
     static Edge* find_out(Cluster* c, Cluster* n2) {
         for (Edge* e : c->out)
@@ -1774,61 +1808,80 @@ private:
         }
         const double tm1 = wall();
         double t_nb = 0, t_add = 0, t_sort = 0, t_cp = 0;
-        std::vector<CopyDesc<T>> copies;
-        {
-            size_t ne = 0;
-            for (Cluster* s : cur())
-                for (Cluster* so : s->children) ne += so->out.size();
-            copies.reserve(ne);
-        }
         struct Move {  // one child block into its parent block
             Edge* eo;
             Cluster* so;
             Cluster* np;  // the parent of the block's row cluster
             int roff;     // row offset of that row cluster in its parent
         };
-        std::vector<Move> moves;
-        std::vector<Cluster*> nb;
-        for (Cluster* s : cur()) {
-            const double ta = wall();
-            nb.clear();
-            moves.clear();
-            for (Cluster* so : s->children)
-                for (Edge* eo : so->out) {
-                    const Cluster* nold = eo->n2;
-                    if (nold->elim) continue;
-                    nb.push_back(nold->parent);
-                    if (!eo->live) continue;
-                    if (eo->A.rows != nold->rsize || eo->A.cols != so->csize)
-                        throw std::runtime_error("merge: block shape mismatch");
-                    moves.push_back(Move{eo, so, nold->parent, nold->rposparent});
-                }
-            std::sort(nb.begin(), nb.end(), [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
-            nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
-            const double tb = wall();
-            t_nb += tb - ta;
-            s->out.reserve(s->out.size() + nb.size());
-            std::vector<std::pair<Cluster*, Edge*>> pe;  // parent edges by neighbour address
-            pe.reserve(nb.size());
-            for (Cluster* n : nb) pe.emplace_back(n, add_edge(s, n));
-            std::sort(pe.begin(), pe.end());
-            const double tc = wall();
-            t_add += tc - tb;
-            std::stable_sort(s->out.begin(), s->out.end(),
-                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
-            const double td = wall();
-            t_sort += td - tc;
-            for (const Move& mv : moves) {
-                auto it = std::lower_bound(pe.begin(), pe.end(), std::make_pair(mv.np, (Edge*)nullptr));
-                if (it == pe.end() || it->first != mv.np) throw std::runtime_error("merge: missing parent edge");
-                Edge* f = it->second;
-                Edge* eo = mv.eo;
-                copies.push_back(cp(eo->A.p, f->A.p + mv.roff + (size_t)mv.so->cposparent * f->A.ld, eo->A.ld,
-                                    f->A.ld, eo->A.rows, eo->A.cols));
-                eo->live = false;
+        const std::vector<Cluster*>& par = cur();
+        const size_t np = par.size();
+        std::vector<std::vector<Cluster*>> nbs(np);
+        std::vector<std::vector<Move>> moves(np);
+        std::vector<std::vector<std::pair<Cluster*, Edge*>>> pes(np);  // parent edges by neighbour address
+        std::vector<std::vector<CopyDesc<T>>> cps(np);
+        // 1. (threads) each parent's neighbour parents and child-block moves: reads only
+        //    its own children's edges
+        host_parallel_for(np, [&](size_t b, size_t e) {
+            for (size_t pi = b; pi < e; ++pi) {
+                Cluster* s = par[pi];
+                std::vector<Cluster*>& nb = nbs[pi];
+                for (Cluster* so : s->children)
+                    for (Edge* eo : so->out) {
+                        const Cluster* nold = eo->n2;
+                        if (nold->elim) continue;
+                        nb.push_back(nold->parent);
+                        if (!eo->live) continue;
+                        if (eo->A.rows != nold->rsize || eo->A.cols != so->csize)
+                            throw std::runtime_error("merge: block shape mismatch");
+                        moves[pi].push_back(Move{eo, so, nold->parent, nold->rposparent});
+                    }
+                std::sort(nb.begin(), nb.end(),
+                          [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
+                nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
             }
-            t_cp += wall() - td;
+        });
+        const double tb = wall();
+        t_nb = tb - tm1;
+        // 2. (in order) the parent edges: blocks and uids in the reference's order
+        for (size_t pi = 0; pi < np; ++pi) {
+            Cluster* s = par[pi];
+            s->out.reserve(s->out.size() + nbs[pi].size());
+            pes[pi].reserve(nbs[pi].size());
+            for (Cluster* n : nbs[pi]) pes[pi].emplace_back(n, add_edge(s, n));
         }
+        const double tc = wall();
+        t_add = tc - tb;
+        // 3. (threads) each parent sorts its out list and lists its copies
+        host_parallel_for(np, [&](size_t b, size_t e) {
+            for (size_t pi = b; pi < e; ++pi) {
+                Cluster* s = par[pi];
+                std::stable_sort(s->out.begin(), s->out.end(),
+                                 [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
+                auto& pe = pes[pi];
+                std::sort(pe.begin(), pe.end());
+                cps[pi].reserve(moves[pi].size());
+                for (const Move& mv : moves[pi]) {
+                    auto it = std::lower_bound(pe.begin(), pe.end(), std::make_pair(mv.np, (Edge*)nullptr));
+                    if (it == pe.end() || it->first != mv.np) throw std::runtime_error("merge: missing parent edge");
+                    Edge* f = it->second;
+                    Edge* eo = mv.eo;
+                    cps[pi].push_back(cp(eo->A.p, f->A.p + mv.roff + (size_t)mv.so->cposparent * f->A.ld, eo->A.ld,
+                                         f->A.ld, eo->A.rows, eo->A.cols));
+                    eo->live = false;
+                }
+            }
+        });
+        const double td = wall();
+        t_sort = td - tc;
+        std::vector<CopyDesc<T>> copies;
+        {
+            size_t ne = 0;
+            for (auto& v : cps) ne += v.size();
+            copies.reserve(ne);
+            for (auto& v : cps) copies.insert(copies.end(), v.begin(), v.end());
+        }
+        t_cp = wall() - td;
         const double tm2 = wall();
         if (!copies.empty()) {
             Upload up;
@@ -1839,7 +1892,7 @@ private:
         if (cfg_.verbose >= 3)
             std::fprintf(stderr,
                          "[lvl %d] merge host: %zu clusters, %zu copies, sizes %.2f ms, neighbours %.2f, edges %.2f, "
-                         "sort %.2f, copy list %.2f, upload+launch %.2f\n",
+                         "sort + copy list %.2f, concatenate %.2f, upload+launch %.2f\n",
                          ilvl_, cur().size(), copies.size(), (tm1 - tm0) * 1e3, t_nb * 1e3, t_add * 1e3,
                          t_sort * 1e3, t_cp * 1e3, (wall() - tm2) * 1e3);
     }
