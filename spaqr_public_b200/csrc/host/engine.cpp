@@ -597,12 +597,12 @@ private:
         return e;
     }
     // fn(begin, end) over [0, n) on up to 8 host threads, in chunks of at least
-    // 256 items (one call on this thread below that); the first exception a
-    // chunk throws is rethrown after all have joined.
+    // min_chunk items (one call on this thread below that); the first exception
+    // a chunk throws is rethrown after all have joined.
     template <class F>
-    static void host_parallel_for(size_t n, F&& fn) {
+    static void host_parallel_for(size_t n, F&& fn, size_t min_chunk = 256) {
         const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-        const size_t nt = std::min<size_t>(std::min<size_t>(hw, 8), n / 256);
+        const size_t nt = std::min<size_t>(std::min<size_t>(hw, 8), n / min_chunk);
         if (nt <= 1) {
             fn(size_t(0), n);
             return;
@@ -690,19 +690,36 @@ private:
     };
 
     // Issues the jobs of one wave (already built), then extra copies (after the QR).
-    void run_qr_wave(std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm,
-                     const std::vector<CopyDesc<T>>& post) {
-        const double tw_wave = wall();
-        const double pin0 = pinned_.alloc_seconds(), grow0 = scratch_.grow_seconds(),
-                     ar0 = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
+    // One wave's descriptor arrays (host only), then its upload and launches.
+    struct PanelLaunch {
+        int kind = 0;  // 0 single-CTA, 1 shared-memory slabs, 2 register-resident
+        int cluster = 0, max_slab = 0;
+        std::vector<int> ids;
+    };
+    struct WaveBuild {
+        std::vector<CopyDesc<T>> g, s;
+        std::vector<QRTask<T>> qt;
+        int maxk = 0, maxR = 0;
+        std::vector<std::vector<int>> ids;
+        std::vector<std::vector<TileRef>> tiles;
+        std::vector<TileRef> trsm_tiles;
+        std::vector<std::vector<PanelLaunch>> pgroups;
+    };
+    // Places each job's trailing block in the wave scratch; returns its element count.
+    static size_t wave_scratch_elems(std::vector<QRJob>& jobs) {
         size_t tr_elems = 0;
         for (auto& j : jobs) {
             j.tr_off = tr_elems;
             tr_elems += (size_t)j.m * j.ntr;
         }
-        T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(tr_elems, 1) * sizeof(T), stream_));
-        std::vector<CopyDesc<T>> g, s;
-        std::vector<QRTask<T>> qt;
+        return tr_elems;
+    }
+    // Pure host work: reads the jobs, writes B (safe on any host thread).
+    static void build_wave(const std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm, T* trbase,
+                           WaveBuild& B) {
+        auto& g = B.g;
+        auto& s = B.s;
+        auto& qt = B.qt;
         {
             size_t ng = 0, ns = 0;
             for (auto& j : jobs) {
@@ -713,7 +730,8 @@ private:
             s.reserve(ns);
             qt.reserve(jobs.size());
         }
-        int maxk = 0, maxR = 0;
+        int& maxk = B.maxk;
+        int& maxR = B.maxR;
         for (auto& j : jobs) {
             T* tr = trbase + j.tr_off;
             for (auto c : j.gather) {
@@ -731,8 +749,8 @@ private:
             maxR = std::max(maxR, j.m);
         }
         // per-panel active lists and trailing tiles
-        std::vector<std::vector<int>> ids;
-        std::vector<std::vector<TileRef>> tiles;
+        auto& ids = B.ids;
+        auto& tiles = B.tiles;
         for (int p = 0; p < maxk; p += kNB) {
             std::vector<int> a;
             std::vector<TileRef> tl;
@@ -746,7 +764,7 @@ private:
             ids.push_back(std::move(a));
             tiles.push_back(std::move(tl));
         }
-        std::vector<TileRef> trsm_tiles;
+        auto& trsm_tiles = B.trsm_tiles;
         for (size_t t = 0; t < trsm.size(); ++t)
             for (int r0 = 0, ti = 0; r0 < trsm[t].rows; r0 += 128, ++ti) trsm_tiles.push_back(TileRef{(int)t, ti});
         // panel groups: cluster size by panel height (row slabs of about 256 rows, at
@@ -766,12 +784,8 @@ private:
         // Panels of at most 16 * kPanelRegRows rows run register-resident
         // (k_panel_reg, slabs of kPanelRegRows rows), taller ones from shared-memory
         // slabs (k_panel_cl).
-        struct PanelLaunch {
-            int kind = 0;  // 0 single-CTA, 1 shared-memory slabs, 2 register-resident
-            int cluster = 0, max_slab = 0;
-            std::vector<int> ids;
-        };
-        std::vector<std::vector<PanelLaunch>> pgroups(ids.size());
+        auto& pgroups = B.pgroups;
+        pgroups.assign(ids.size(), {});
         for (size_t i = 0; i < ids.size(); ++i) {
             const int p = (int)i * kNB;
             PanelLaunch single;
@@ -819,6 +833,30 @@ private:
                 }
             }
         }
+    }
+
+    void run_qr_wave(std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm,
+                     const std::vector<CopyDesc<T>>& post) {
+        const double tw_wave = wall();
+        const size_t tr_elems = wave_scratch_elems(jobs);
+        T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(tr_elems, 1) * sizeof(T), stream_));
+        WaveBuild B;
+        build_wave(jobs, trsm, trbase, B);
+        issue_wave(B, trsm, post, tw_wave);
+    }
+
+    void issue_wave(WaveBuild& B, const std::vector<TrsmTask<T>>& trsm, const std::vector<CopyDesc<T>>& post,
+                    double tw_wave) {
+        const double pin0 = pinned_.alloc_seconds(), grow0 = scratch_.grow_seconds(),
+                     ar0 = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
+        auto& g = B.g;
+        auto& s = B.s;
+        auto& qt = B.qt;
+        const int maxR = B.maxR;
+        auto& ids = B.ids;
+        auto& tiles = B.tiles;
+        auto& trsm_tiles = B.trsm_tiles;
+        auto& pgroups = B.pgroups;
         const double tw_built = wall();
         Upload up;
         size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
@@ -1042,12 +1080,26 @@ private:
         if (cfg_.verbose >= 3)
             std::fprintf(stderr, "[lvl %d] elim host: tasks %.2f ms, waves %.2f ms\n", ilvl_, (te1 - te0) * 1e3,
                          (wall() - te1) * 1e3);
-        for (int w = 0; w < nw; ++w) {
-            std::vector<QRJob> jobs;
-            for (size_t t = 0; t < tasks.size(); ++t)
-                if (wave[t] == w) jobs.push_back(std::move(tasks[t].job));
-            run_qr_wave(jobs, {}, {});
-        }
+        // every wave's descriptors first (host threads, one scratch sized for the
+        // largest wave), then the uploads and launches in wave order
+        std::vector<std::vector<QRJob>> wjobs(nw);
+        for (size_t t = 0; t < tasks.size(); ++t) wjobs[wave[t]].push_back(std::move(tasks[t].job));
+        const double tw0 = wall();
+        size_t maxe = 1;
+        for (auto& jobs : wjobs) maxe = std::max(maxe, wave_scratch_elems(jobs));
+        T* trbase = static_cast<T*>(scratch_.get(maxe * sizeof(T), stream_));
+        std::vector<WaveBuild> builds(nw);
+        const std::vector<TrsmTask<T>> no_trsm;
+        const std::vector<CopyDesc<T>> no_post;
+        host_parallel_for(
+            (size_t)nw,
+            [&](size_t b, size_t e) {
+                for (size_t w = b; w < e; ++w) build_wave(wjobs[w], no_trsm, trbase, builds[w]);
+            },
+            4);
+        if (cfg_.verbose >= 3)
+            std::fprintf(stderr, "[lvl %d] elim host: %d wave builds %.2f ms\n", ilvl_, nw, (wall() - tw0) * 1e3);
+        for (int w = 0; w < nw; ++w) issue_wave(builds[w], no_trsm, no_post, wall());
     }
 
     // ------------------------------------------------------------- scaling (src/tree.cpp:533-580)
