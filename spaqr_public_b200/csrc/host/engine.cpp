@@ -2387,7 +2387,7 @@ private:
         // Q applications of at least kApplyqBigRows rows go to the cluster kernel
         // (after the wave's other ops in the array)
         auto big = [](const SolveOp& o) {
-            return o.kind == SK_APPLYQ && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows;
+            return o.kind == SK_APPLYQ && o.b > 0 && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows;
         };
         for (auto& w : waves) {
             WMeta mt{all.size(), 0, 0, 0.0, -1, 0, 0, 0, 0, 0};

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
 #pragma unroll
         for (int u = 0; u < TPT; ++u) td[u] = Tp[tid + u * kAThreads];
     };
-    load_panel(0, vraw, traw);
+    if (np > 0) load_panel(0, vraw, traw);
     for (int pi = 0; pi < np; ++pi) {
         const int buf = pi & 1;
         const int pidx = dir == 0 ? pi : np - 1 - pi;
