@@ -65,6 +65,16 @@ int spq_set_hsl(spq_tree* t, int hsl);         /* --hsl (0 only) */
 int spq_set_square(spq_tree* t, int square);
 int spq_set_coords(spq_tree* t, int d, int n, const double* X); /* d x n, column-major */
 int spq_set_coords_grid(spq_tree* t, int n, int d);             /* -n/-d tensor grid */
+/* Without coordinates, spq_partition orders the columns from a leaf part per
+ * column (2^(nlevels-1) parts, the first cut in the highest bit), the place of
+ * the METIS part vector in MetisPartition (src/partition.cpp:374-426, used by
+ * Tree::partition at src/tree.cpp:610-616 when set_Xcoo was not called). The
+ * separators, interfaces and permutations then follow the reference's steps.
+ * spq_set_parts supplies that vector (for instance METIS's own); without it,
+ * spq_partition computes it with spq_graph_parts, this library's recursive
+ * bisection of the A^T A graph (host only; needs no GPU and no handle). */
+int spq_set_parts(spq_tree* t, int n, const int* parts);
+int spq_graph_parts(int m, int n, const int* colptr, const int* rowind, int nlevels, int* parts);
 int spq_set_precision(spq_tree* t, int precision);              /* spq_precision */
 int spq_set_device(spq_tree* t, int device);
 int spq_set_verbose(spq_tree* t, int verbose); /* 1: per-level print lines as src/tree.cpp:1417-1434 */

@@ -36,6 +36,7 @@ def lib():
         L.orc_last_error.restype = C.c_char_p
         L.orc_blas_threads.argtypes = [C.c_int]
         L.orc_set_coords.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p]
+        L.orc_set_parts.argtypes = [C.c_void_p, C.c_int, _i32p, C.c_int]
         for f in (L.orc_partition, L.orc_assemble):
             f.argtypes = [C.c_void_p, C.c_int, C.c_int, _i32p, _i32p, _f64p]
         L.orc_factorize.argtypes = [C.c_void_p]
@@ -96,6 +97,12 @@ class OracleTree:
     def set_coords_grid(self, n, d):
         X = linspace_nd(n, d)
         _check(lib().orc_set_coords(self.h, d, n ** d, X))
+
+    def set_parts(self, parts, numeric_fill=True):
+        """Leaf parts for the partition without coordinates (the METIS part
+        vector); numeric_fill keeps the reference's numeric fill test."""
+        p = np.ascontiguousarray(parts, dtype=np.int32)
+        _check(lib().orc_set_parts(self.h, int(p.size), p, int(bool(numeric_fill))))
 
     def partition(self, A):
         m, n, cp, ri, va = _csc(A)

@@ -335,6 +335,62 @@ static std::vector<ClusterID> geometric_partition_ata(const Csc& A, int nlevels,
     return cmap;
 }
 
+// MetisPartition after METIS_PartGraphRecursive (src/partition.cpp:374-426)
+// and getInterfacesUsingATA (src/partition.cpp:628-675). METIS is absent, so
+// the leaf part vector `parts` is an input (the reference gets it from
+// partition_metis_RB, src/partition.cpp:354-372).
+static std::vector<ClusterID> metis_partition(const Csc& A, int nlevels, const std::vector<int>& parts) {
+    Csc AtA = ata_pattern(A);
+    const int c = AtA.n;
+    if ((int)parts.size() != c) throw std::runtime_error("parts must have one entry per column");
+    std::vector<ClusterID> cmap(c);
+    for (int depth = 0; depth < nlevels - 1; ++depth) {
+        int l = nlevels - depth - 1;
+        for (int i = 0; i < c; ++i) {
+            if (cmap[i].self.lvl != -1) continue;
+            int pi = part_at_lvl(parts[i], l);
+            if (pi % 2 != 0) continue;
+            bool sep = false;
+            for (int q = AtA.p[i]; q < AtA.p[i + 1]; ++q) {
+                int j = AtA.i[q];
+                if (cmap[j].self.lvl == -1 && part_at_lvl(parts[j], l) == pi + 1) { sep = true; break; }
+            }
+            if (sep) cmap[i].self = SepID(l, pi / 2);
+        }
+    }
+    for (int i = 0; i < c; ++i)
+        if (cmap[i].self.lvl == -1) cmap[i].self = cmap[i].l = cmap[i].r = SepID(0, parts[i]);
+    // getInterfacesUsingATA
+    for (int i = 0; i < c; ++i) {
+        SepID self = cmap[i].self;
+        if (self.lvl > 0) {
+            SepID left(0, parts[i]), right(-1, 0);
+            int pi = part_at_lvl(parts[i], self.lvl);
+            for (int q = AtA.p[i]; q < AtA.p[i + 1]; ++q) {
+                int j = AtA.i[q];
+                SepID nbr = cmap[j].self;
+                if (nbr.lvl < self.lvl) {
+                    int pj = part_at_lvl(parts[j], self.lvl);
+                    if (pj <= pi) left = find_highest_common(nbr, left);
+                    else right = (right.lvl == -1) ? nbr : find_highest_common(nbr, right);
+                }
+            }
+            if (right.lvl == -1) throw std::runtime_error("separator without a right side");
+            cmap[i].l = left;
+            cmap[i].r = right;
+            cmap[i].section = parts[i];
+        }
+    }
+    for (int i = 0; i < c; ++i) {
+        if (cmap[i].self.lvl == 0) {
+            cmap[i].l = cmap[i].self;
+            cmap[i].r = cmap[i].self;
+            cmap[i].section = parts[i];
+        }
+    }
+    return cmap;
+}
+
 // initPermutation (src/tree.cpp:46-55)
 static void init_permutation(int nlevels, const std::vector<ClusterID>& cmap, std::vector<int>& cperm) {
     std::vector<ClusterID> pm = cmap;
@@ -769,6 +825,8 @@ public:
     float order_ = 1;
     int d_ = 0;
     std::vector<double> X_;
+    std::vector<int> parts_;    // leaf parts for the partition without coordinates
+    bool numeric_fill_ = true;  // without coordinates: the numeric fill test of src/tree.cpp:857-860
     int nrows_ = 0, ncols_ = 0, ilvl_ = -1, current_bottom_ = 0, max_order_ = 0;
     std::vector<int> cperm_, rperm_;
     std::vector<std::list<Cluster*>> bottoms_, fine_;
@@ -814,8 +872,10 @@ public:
         const int r = A.m, c = A.n;
         nrows_ = r;
         ncols_ = c;
-        if (X_.empty()) throw std::runtime_error("only the geometric partition is supported (set coordinates)");
-        std::vector<ClusterID> cmap = geometric_partition_ata(A, nlevels_, X_, d_);
+        if (X_.empty() && parts_.empty())
+            throw std::runtime_error("set coordinates, or the leaf parts of the partition without them");
+        std::vector<ClusterID> cmap =
+            X_.empty() ? metis_partition(A, nlevels_, parts_) : geometric_partition_ata(A, nlevels_, X_, d_);
         rperm_.resize(r);
         cperm_.resize(c);
         for (int i = 0; i < r; ++i) rperm_[i] = i;
@@ -947,9 +1007,22 @@ public:
         if (nr.lvl >= cself.lvl) ryes = (cself.sep / (int)std::pow(2.0, dr)) == nr.sep;
         else ryes = (nr.sep / (int)std::pow(2.0, -dr)) == cself.sep;
         if (!lyes && !ryes) return false;
+        if (X_.empty()) return true;  // the column-sparsity tests are geometric only
         if (!col_sparsity.count(nself)) return false;
         if (!col_sparsity.count(nl) && !col_sparsity.count(nr)) return false;
         return true;
+    }
+
+    // ||A1^T A2||_F (the numeric fill test's product, src/tree.cpp:858)
+    static double product_norm(const Mat& A1, const Mat& A2) {
+        double s = 0;
+        for (int a = 0; a < A1.cols; ++a)
+            for (int b = 0; b < A2.cols; ++b) {
+                double dot = 0;
+                for (int r = 0; r < A1.rows; ++r) dot += A1(r, a) * A2(r, b);
+                s += dot * dot;
+            }
+        return std::sqrt(s);
     }
 
     void get_sparsity(Cluster* c) {
@@ -962,7 +1035,11 @@ public:
             rs.insert(n);
             for (Edge* ein : n->edgesIn) {
                 if (ein->A && ein->n1 != c && !ein->n1->eliminated) {
-                    if (check_if_valid(c->id, ein->n1->id, cs)) rs.insert(ein->n1);
+                    Cluster* nin = ein->n1;
+                    bool valid = check_if_valid(c->id, nin->id, cs);
+                    if (X_.empty() && numeric_fill_ && valid && !(nin->id.l == c->id.self || nin->id.r == c->id.self))
+                        valid = product_norm(*e->A, *ein->A) > 1e-14;
+                    if (valid) rs.insert(nin);
                 }
             }
         }
@@ -1640,6 +1717,12 @@ int orc_set_coords(orc_tree* t, int d, int n, const double* X) {
     return guarded([&] {
         t->t->d_ = d;
         t->t->X_.assign(X, X + (size_t)d * n);
+    });
+}
+int orc_set_parts(orc_tree* t, int n, const int* parts, int numeric_fill) {
+    return guarded([&] {
+        t->t->parts_.assign(parts, parts + n);
+        t->t->numeric_fill_ = numeric_fill != 0;
     });
 }
 int orc_partition(orc_tree* t, int m, int n, const int* cp, const int* ri, const double* va) {

@@ -32,6 +32,13 @@ int orc_blas_threads(int nthreads); /* sets OpenBLAS threads; returns the count 
 /* Coordinates: d x n, column-major (set_Xcoo). */
 int orc_set_coords(orc_tree* t, int d, int n, const double* X);
 
+/* Without coordinates: the leaf part of every column (the METIS part vector of
+ * MetisPartition, src/partition.cpp:374-426; METIS itself is absent, so the
+ * vector is an input). numeric_fill = 1 keeps the reference's numeric fill test
+ * (src/tree.cpp:857-860); 0 keeps every candidate that passes the separator
+ * tests (the GPU library's rule). */
+int orc_set_parts(orc_tree* t, int n, const int* parts, int numeric_fill);
+
 /* A in CSC (sorted row indices), m >= n. */
 int orc_partition(orc_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val);
 int orc_assemble(orc_tree* t, int m, int n, const int* colptr, const int* rowind, const double* val);

@@ -6,7 +6,7 @@ reference's ``Tree`` / ``gmres`` / ``cgls`` surface plus the seeded workload
 generators.
 """
 from .tree import (FP32, FP64, Tree, autotune, cgls, column_normalize, factorize_batch, gmres,  # noqa: F401
-                   gmres_adjoint, launches, solve_to_residual)
+                   gmres_adjoint, graph_parts, launches, solve_to_residual)
 
 __all__ = ["Tree", "gmres", "gmres_adjoint", "cgls", "solve_to_residual", "launches", "column_normalize",
-           "factorize_batch", "autotune", "FP32", "FP64"]
+           "factorize_batch", "autotune", "graph_parts", "FP32", "FP64"]

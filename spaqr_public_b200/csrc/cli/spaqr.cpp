@@ -7,7 +7,9 @@
 //
 // Flow as in the reference: read the MatrixMarket matrix (transposed when it
 // has fewer rows than columns), scale its columns to norm 10, build the tree
-// (geometric partition from a tensor grid or a coordinate file), partition,
+// (geometric partition from a tensor grid or a coordinate file; without
+// coordinates, the library's recursive bisection of the A^T A graph in the
+// place of the reference's METIS / PaToH partition), partition,
 // assemble, factorize (per-level lines), one solve with the seeded random
 // right-hand side (mt19937 seed 2021, uniform on [-1, 1], src/util.cpp:943-952)
 // and its residual, then GMRES (square) or CGLS (more rows than columns) with
@@ -251,10 +253,9 @@ int main(int argc, char** argv) {
     if (!rc && nrows == ncols) rc = check(spq_set_square(t, 1), "square");
     if (!rc && geo_tensor) rc = check(spq_set_coords_grid(t, cn, cd), "coordinates");
     if (!rc && geo_file) rc = check(spq_set_coords(t, xd, ncols, X.data()), "coordinates");
-    if (!rc && !geo) {
-        std::cerr << "a geometric partition is needed (-n/-d or --coordinates): the non-geometric "
-                     "partitioners of the reference (PaToH / METIS) are not part of this build\n";
-        rc = SPQ_ERR_UNSUPPORTED;
+    if (!rc) {  // Tree::partition's banner (src/tree.cpp:605-616)
+        if (geo) std::cout << "Using GeometricPartition... " << std::endl;
+        else std::cout << "Using graph bisection partition (A^T A)... " << std::endl;
     }
     rc = rc ? rc : check(spq_set_verbose(t, 1), "verbose");
     const int* cp = A.colptr.data();

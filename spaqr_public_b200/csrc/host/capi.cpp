@@ -68,8 +68,8 @@ int guard_on(spq_tree* t, F&& f) {
     return guard(std::forward<F>(f));
 }
 
-int check_csc(int m, int n, const int* cp, const int* ri, const double* va) {
-    if (m <= 0 || n <= 0 || !cp || (!ri && cp[n] > 0) || (!va && cp[n] > 0))
+int check_csc(int m, int n, const int* cp, const int* ri, const double* va, bool need_values = true) {
+    if (m <= 0 || n <= 0 || !cp || (!ri && cp[n] > 0) || (need_values && !va && cp[n] > 0))
         return fail(SPQ_ERR_ARG, "invalid CSC matrix");
     if (cp[0] != 0) return fail(SPQ_ERR_ARG, "colptr[0] must be 0");
     for (int j = 0; j < n; ++j) {
@@ -211,6 +211,31 @@ int spq_set_coords_grid(spq_tree* t, int n, int d) {
     }
     return SPQ_OK;
 }
+int spq_set_parts(spq_tree* t, int n, const int* parts) {
+    SPQ_SETTER_GUARD
+    if (n < 1 || !parts) return fail(SPQ_ERR_ARG, "invalid part vector");
+    const int nleaves = t->cfg.nlevels >= 2 ? 1 << (t->cfg.nlevels - 1) : 1;
+    for (int i = 0; i < n; ++i)
+        if (parts[i] < 0 || parts[i] >= nleaves) return fail(SPQ_ERR_ARG, "part index out of range for nlevels");
+    t->cfg.parts.assign(parts, parts + n);
+    return SPQ_OK;
+}
+int spq_graph_parts(int m, int n, const int* cp, const int* ri, int nlevels, int* parts) {
+    int rc = check_csc(m, n, cp, ri, nullptr, false);
+    if (rc) return rc;
+    if (nlevels < 1 || nlevels > 30 || !parts) return fail(SPQ_ERR_ARG, "need 1 <= nlevels <= 30 and an output");
+    return guard([&] {
+        Csc A;
+        A.m = m;
+        A.n = n;
+        A.p.assign(cp, cp + n + 1);
+        A.i.assign(ri, ri + cp[n]);
+        A.v.assign((size_t)cp[n], 0.0);  // pattern only; the values are not read
+        const std::vector<int> p = graph_bisection(A, nlevels);
+        std::copy(p.begin(), p.end(), parts);
+        return SPQ_OK;
+    });
+}
 int spq_set_precision(spq_tree* t, int precision) {
     SPQ_SETTER_GUARD
     if (precision != SPQ_FP64 && precision != SPQ_FP32) return fail(SPQ_ERR_ARG, "unknown precision");
@@ -234,9 +259,10 @@ int spq_partition(spq_tree* t, int m, int n, const int* cp, const int* ri, const
     int rc = check_csc(m, n, cp, ri, va);
     if (rc) return rc;
     if (m < n) return fail(SPQ_ERR_ARG, "need rows >= cols (factor the transpose instead)");
-    if (t->cfg.X.empty())
-        return fail(SPQ_ERR_UNSUPPORTED, "only the geometric partition is built: set coordinates first");
-    if ((int64_t)t->cfg.X.size() != (int64_t)t->cfg.d * n) return fail(SPQ_ERR_ARG, "coordinates must be d x ncols");
+    if (!t->cfg.X.empty() && (int64_t)t->cfg.X.size() != (int64_t)t->cfg.d * n)
+        return fail(SPQ_ERR_ARG, "coordinates must be d x ncols");
+    if (t->cfg.X.empty() && !t->cfg.parts.empty() && (int64_t)t->cfg.parts.size() != n)
+        return fail(SPQ_ERR_ARG, "parts must have one entry per column");
     return guard([&] {
         if (!t->eng) t->eng = make_engine(t->cfg, t->precision);
         t->eng->partition(csc_from(m, n, cp, ri, va));

@@ -143,13 +143,16 @@ public:
     // ------------------------------------------------------------- partition
     void partition(const Csc& A) override {
         double t0 = wall();
-        if (cfg_.X.empty()) throw std::invalid_argument("only the geometric partition is built: set coordinates");
         if (A.m < A.n) throw std::invalid_argument("need rows >= cols");
         if (cfg_.square && A.m != A.n) throw std::invalid_argument("square (identity matching) needs m == n");
         nrows_ = A.m;
         ncols_ = A.n;
         rect_ = !cfg_.square;
-        Ordering o = geometric_ordering(A, cfg_.nlevels, cfg_.d, cfg_.X, cfg_.square != 0);
+        geo_ = !cfg_.X.empty();
+        Ordering o = geo_ ? geometric_ordering(A, cfg_.nlevels, cfg_.d, cfg_.X, cfg_.square != 0)
+                          : graph_ordering(A, cfg_.nlevels,
+                                           cfg_.parts.empty() ? graph_bisection(A, cfg_.nlevels) : cfg_.parts,
+                                           cfg_.square != 0);
         cperm_ = o.cperm;
         rperm_ = o.rperm;
         const int c = A.n;
@@ -419,6 +422,7 @@ private:
     std::vector<TapeOp> tape_;
     std::vector<int> cperm_, rperm_;
     bool rect_ = false;  // least squares (no identity row matching): rows move, R^T R solves
+    bool geo_ = true;    // ordering from coordinates (the fill test uses the column-sparsity checks)
     int nrows_ = 0, ncols_ = 0, ilvl_ = -1, cur_bottom_ = 0, max_order_ = 0, next_uid_ = 0;
     bool assembled_ = false, factorized_ = false;
     unsigned long long nnzA_ = 0, nnzR_ = 0, nnzH_ = 0, nnzQ_ = 0;
@@ -642,7 +646,12 @@ private:
         return c->level() > ilvl_ && c->id.l.lvl <= ilvl_ && c->id.r.lvl <= ilvl_;
     }
 
-    // src/tree.cpp:168-224
+    // src/tree.cpp:168-224. Without coordinates the reference skips the two
+    // column-sparsity tests and instead drops a candidate whose coupling block
+    // product has norm <= 1e-14 (src/tree.cpp:857-860); that numeric test is not
+    // made here: every candidate that passes the separator tests is kept. The
+    // blocks it would drop receive updates of rounding size, so the factors
+    // agree to rounding, with more (near-zero) fill blocks.
     bool valid_fill(const Cid& cid, const Cid& nid, const std::vector<Sep>& cols) const {
         const Sep cs = cid.self, ns = nid.self;
         if (cs.lvl > ns.lvl) return false;
@@ -653,12 +662,13 @@ private:
             return s.lvl >= cs.lvl ? (cs.sep / pw(dl)) == s.sep : (s.sep / pw(-dl)) == cs.sep;
         };
         if (!side_ok(nid.l) && !side_ok(nid.r)) return false;
+        if (!geo_) return true;
         auto has = [&](const Sep& x) { return std::binary_search(cols.begin(), cols.end(), x); };
         if (!has(ns)) return false;
         if (!has(nid.l) && !has(nid.r)) return false;
         return true;
     }
-    // src/tree.cpp:834-870 (geometric mode: purely symbolic)
+    // src/tree.cpp:834-870 (purely symbolic, with or without coordinates)
     void get_sparsity(Cluster* c) {
         std::vector<Cluster*> rs;
         std::vector<Sep> cols;

@@ -33,6 +33,9 @@ struct Config {
     int hsl = 0, verbose = 0, device = 0;
     int d = 0;
     std::vector<double> X;
+    // Leaf part of every column for the ordering without coordinates (empty:
+    // graph_bisection computes it); ignored when coordinates are set.
+    std::vector<int> parts;
 };
 
 // Event log record: [type, ilvl, order, a, b, c, d, e] (same layout as the

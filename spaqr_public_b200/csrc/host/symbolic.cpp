@@ -1,4 +1,6 @@
-// Geometric nested dissection ordering, bit-exact with the reference.
+// Nested-dissection orderings: geometric (bit-exact with the reference) and,
+// without coordinates, a graph bisection of A^T A whose part vector goes
+// through the reference's MetisPartition steps.
 //
 // Reference steps and where they live:
 //   A^T A pattern, recursive geometric bisection     src/partition.cpp:241-304
@@ -8,12 +10,15 @@
 //   interface (left/right) inference on A             src/partition.cpp:506-578
 //   hierarchical column sort                          src/tree.cpp:46-55
 //   row permutation (rectangular input)               src/tree.cpp:100-163
+//   separators from a part vector (no coordinates)    src/partition.cpp:374-426
+//   interfaces on A^T A (no coordinates)              src/partition.cpp:628-675
 #include "symbolic.hpp"
 
 #include <algorithm>
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <set>
 #include <stdexcept>
 
 namespace spq {
@@ -186,6 +191,57 @@ void rows_by_norm(const Csc& At_perm, const std::vector<Cid>& cid_of_pos, std::v
     }
 }
 
+// Hierarchical column sort (initPermutation, src/tree.cpp:46-55) of the column
+// ids, then the rows: identity for square input, else each row joins the first
+// column of its largest-norm run of equal ids (form_rmap, src/tree.cpp:57-98).
+Ordering finish_ordering(const Csc& A, int nlevels, const std::vector<Cid>& ids, bool square) {
+    const int n = A.n, m = A.m;
+    // Hierarchical column sort: by id, then by the id lifted to each level.
+    Ordering o;
+    o.cperm.resize(n);
+    std::iota(o.cperm.begin(), o.cperm.end(), 0);
+    std::vector<Cid> key(ids);
+    auto by_key = [&key](int a, int b) { return key[a] < key[b]; };
+    std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
+    for (int lvl = 1; lvl < nlevels; ++lvl) {
+        for (auto& k : key) k = lift(k, lvl);
+        std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
+    }
+    o.cid_of_pos.resize(n);
+    for (int k = 0; k < n; ++k) o.cid_of_pos[k] = ids[o.cperm[k]];
+
+    if (square) {
+        if (m != n) throw std::invalid_argument("identity row matching needs a square matrix");
+        o.rperm = o.cperm;
+        o.rows_of_col.assign(n, 1);
+    } else {
+        // Each row goes to the first column (permuted order) of its max-norm run.
+        const Csc Atp = csc_transpose(csc_gather_cols(A, o.cperm));
+        o.rows_of_col.assign(n, 0);
+        std::vector<std::vector<int>> owned(n);
+        for (int r = 0; r < m; ++r) {
+            double best = -1;
+            int pick = -1;
+            int q = Atp.p[r], e = Atp.p[r + 1];
+            while (q < e) {
+                const Cid cur = o.cid_of_pos[Atp.i[q]];
+                double acc = Atp.v[q] * Atp.v[q];
+                int t = q + 1;
+                while (t < e && o.cid_of_pos[Atp.i[t]] == cur) { acc += Atp.v[t] * Atp.v[t]; ++t; }
+                if (acc > best) { best = acc; pick = Atp.i[q]; }
+                q = t;
+            }
+            if (pick < 0) pick = n - 1;
+            o.rows_of_col[pick]++;
+            owned[pick].push_back(r);
+        }
+        o.rperm.clear();
+        o.rperm.reserve(m);
+        for (int k = 0; k < n; ++k) o.rperm.insert(o.rperm.end(), owned[k].begin(), owned[k].end());
+    }
+    return o;
+}
+
 }  // namespace
 
 Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X, bool square) {
@@ -273,50 +329,222 @@ Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<
     }
     // cmap = rmap (first n entries are the ones the column sort reads)
 
-    // Hierarchical column sort: by id, then by the id lifted to each level.
-    Ordering o;
-    o.cperm.resize(n);
-    std::iota(o.cperm.begin(), o.cperm.end(), 0);
-    std::vector<Cid> key(rmap.begin(), rmap.begin() + n);
-    auto by_key = [&key](int a, int b) { return key[a] < key[b]; };
-    std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
-    for (int lvl = 1; lvl < nlevels; ++lvl) {
-        for (auto& k : key) k = lift(k, lvl);
-        std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
-    }
-    o.cid_of_pos.resize(n);
-    for (int k = 0; k < n; ++k) o.cid_of_pos[k] = rmap[o.cperm[k]];
+    return finish_ordering(A, nlevels, std::vector<Cid>(rmap.begin(), rmap.begin() + n), square);
+}
 
-    if (square) {
-        if (m != n) throw std::invalid_argument("identity row matching needs a square matrix");
-        o.rperm = o.cperm;
-        o.rows_of_col.assign(n, 1);
-    } else {
-        // Each row goes to the first column (permuted order) of its max-norm run.
-        const Csc Atp = csc_transpose(csc_gather_cols(A, o.cperm));
-        o.rows_of_col.assign(n, 0);
-        std::vector<std::vector<int>> owned(n);
-        for (int r = 0; r < m; ++r) {
-            double best = -1;
-            int pick = -1;
-            int q = Atp.p[r], e = Atp.p[r + 1];
-            while (q < e) {
-                const Cid cur = o.cid_of_pos[Atp.i[q]];
-                double acc = Atp.v[q] * Atp.v[q];
-                int t = q + 1;
-                while (t < e && o.cid_of_pos[Atp.i[t]] == cur) { acc += Atp.v[t] * Atp.v[t]; ++t; }
-                if (acc > best) { best = acc; pick = Atp.i[q]; }
-                q = t;
-            }
-            if (pick < 0) pick = n - 1;
-            o.rows_of_col[pick]++;
-            owned[pick].push_back(r);
+// ---------------------------------------------------------------- graph ordering
+namespace {
+
+// One bisection of the vertex set `mem` (ascending) of the A^T A graph: a
+// breadth-first level structure from a pseudo-peripheral vertex gives the
+// first ceil(|mem|/2) vertices side 0, then Fiduccia-Mattheyses passes move
+// boundary vertices to lower the edge cut while |side 0| stays within
+// |mem|/200 + 1 of that size. Deterministic: every tie goes to the lowest index.
+void bisect_graph(const Adjacency& G, const std::vector<int>& mem, std::vector<int>& loc, std::vector<char>& side) {
+    const int N = (int)mem.size();
+    side.assign(N, 0);
+    if (N < 2) return;
+    for (int t = 0; t < N; ++t) loc[mem[t]] = t;
+    // local adjacency (members only, no self loops)
+    std::vector<int> lp(N + 1, 0), li;
+    li.reserve((size_t)N * 8);
+    for (int t = 0; t < N; ++t) {
+        const int v = mem[t];
+        for (int64_t q = G.p[v]; q < G.p[v + 1]; ++q) {
+            const int u = G.i[q];
+            const int lu = loc[u];
+            if (u != v && lu >= 0 && lu < N && mem[lu] == u) li.push_back(lu);
         }
-        o.rperm.clear();
-        o.rperm.reserve(m);
-        for (int k = 0; k < n; ++k) o.rperm.insert(o.rperm.end(), owned[k].begin(), owned[k].end());
+        lp[t + 1] = (int)li.size();
     }
-    return o;
+    // breadth-first search from r; returns the visit order, dist filled (-1 unvisited)
+    std::vector<int> dist(N, -1), order;
+    order.reserve(N);
+    auto bfs = [&](int r) {
+        order.clear();
+        std::fill(dist.begin(), dist.end(), -1);
+        dist[r] = 0;
+        order.push_back(r);
+        for (size_t h = 0; h < order.size(); ++h) {
+            const int v = order[h];
+            for (int q = lp[v]; q < lp[v + 1]; ++q)
+                if (dist[li[q]] < 0) { dist[li[q]] = dist[v] + 1; order.push_back(li[q]); }
+        }
+    };
+    // pseudo-peripheral start (George-Liu): move to a minimum-degree vertex of
+    // the last level while the eccentricity grows
+    int r = 0, ecc = -1;
+    for (int it = 0; it < 16; ++it) {
+        bfs(r);
+        const int e = dist[order.back()];
+        if (e <= ecc) break;
+        ecc = e;
+        int best = -1;
+        for (int v : order)
+            if (dist[v] == e && (best < 0 || lp[v + 1] - lp[v] < lp[best + 1] - lp[best] ||
+                                 (lp[v + 1] - lp[v] == lp[best + 1] - lp[best] && v < best)))
+                best = v;
+        r = best;
+    }
+    bfs(r);
+    for (int v = 0; (int)order.size() < N; ++v) {  // other components, in index order
+        if (dist[v] >= 0) continue;
+        size_t h = order.size();
+        dist[v] = 0;
+        order.push_back(v);
+        for (; h < order.size(); ++h) {
+            const int x = order[h];
+            for (int q = lp[x]; q < lp[x + 1]; ++q)
+                if (dist[li[q]] < 0) { dist[li[q]] = dist[x] + 1; order.push_back(li[q]); }
+        }
+    }
+    const int target = (N + 1) / 2, slack = N / 200 + 1;
+    for (int t = target; t < N; ++t) side[order[t]] = 1;
+    int w0 = target;
+
+    // Fiduccia-Mattheyses refinement of the edge cut
+    std::vector<int> gain(N);
+    auto compute_gain = [&](int v) {
+        int g = 0;
+        for (int q = lp[v]; q < lp[v + 1]; ++q) g += side[li[q]] != side[v] ? 1 : -1;
+        return g;
+    };
+    std::vector<char> locked(N), queued(N);
+    std::vector<int> moves;
+    for (int pass = 0; pass < 6; ++pass) {
+        for (int v = 0; v < N; ++v) gain[v] = compute_gain(v);
+        std::set<std::pair<int, int>> pq[2];  // (-gain, v) per side
+        std::fill(locked.begin(), locked.end(), 0);
+        std::fill(queued.begin(), queued.end(), 0);
+        for (int v = 0; v < N; ++v) {
+            bool boundary = false;
+            for (int q = lp[v]; q < lp[v + 1] && !boundary; ++q) boundary = side[li[q]] != side[v];
+            if (boundary) { pq[(int)side[v]].insert({-gain[v], v}); queued[v] = 1; }
+        }
+        moves.clear();
+        int cum = 0, best = 0, best_len = 0, best_imb = std::abs(w0 - target), idle = 0;
+        const int max_idle = std::max(64, N / 50);
+        while (idle < max_idle) {
+            int pick = -1;
+            for (int sd = 0; sd < 2; ++sd) {
+                if (pq[sd].empty()) continue;
+                const int w_after = w0 + (sd == 0 ? -1 : 1);
+                if (std::abs(w_after - target) > slack) continue;
+                const auto& top = *pq[sd].begin();
+                if (pick < 0 || top.first < -gain[pick] || (top.first == -gain[pick] && top.second < pick))
+                    pick = top.second;
+            }
+            if (pick < 0) break;
+            const int sd = side[pick];
+            pq[sd].erase({-gain[pick], pick});
+            queued[pick] = 0;
+            locked[pick] = 1;
+            cum += gain[pick];
+            side[pick] = (char)(1 - sd);
+            w0 += sd == 0 ? -1 : 1;
+            gain[pick] = -gain[pick];
+            moves.push_back(pick);
+            for (int q = lp[pick]; q < lp[pick + 1]; ++q) {
+                const int u = li[q];
+                if (locked[u]) continue;
+                if (queued[u]) pq[(int)side[u]].erase({-gain[u], u});
+                gain[u] += side[u] == side[pick] ? -2 : 2;
+                pq[(int)side[u]].insert({-gain[u], u});
+                queued[u] = 1;
+            }
+            const int imb = std::abs(w0 - target);
+            if (cum > best || (cum == best && imb < best_imb)) {
+                best = cum;
+                best_len = (int)moves.size();
+                best_imb = imb;
+                idle = 0;
+            } else {
+                ++idle;
+            }
+        }
+        for (int t = (int)moves.size() - 1; t >= best_len; --t) {  // undo past the best prefix
+            const int v = moves[t];
+            w0 += side[v] == 0 ? -1 : 1;
+            side[v] = (char)(1 - side[v]);
+        }
+        if (best <= 0) break;
+    }
+    for (int t = 0; t < N; ++t) loc[mem[t]] = -1;
+}
+
+}  // namespace
+
+std::vector<int> graph_bisection(const Csc& A, int nlevels) {
+    if (nlevels < 1) throw std::invalid_argument("nlevels must be >= 1");
+    const int n = A.n;
+    const Adjacency G = ata_adjacency(A, csc_transpose(A));
+    std::vector<int> part(n, 0), next(n, 0), loc(n, -1);
+    std::vector<char> side;
+    for (int depth = 0; depth + 1 < nlevels; ++depth) {
+        const int nparts = 1 << depth;
+        std::vector<std::vector<int>> members(nparts);
+        for (int i = 0; i < n; ++i) members[part[i]].push_back(i);
+        for (int k = 0; k < nparts; ++k) {
+            bisect_graph(G, members[k], loc, side);
+            for (size_t t = 0; t < members[k].size(); ++t) next[members[k][t]] = 2 * k + side[t];
+        }
+        part.swap(next);
+    }
+    return part;
+}
+
+Ordering graph_ordering(const Csc& A, int nlevels, const std::vector<int>& parts, bool square) {
+    if (nlevels < 1) throw std::invalid_argument("nlevels must be >= 1");
+    const int n = A.n;
+    if ((int)parts.size() != n) throw std::invalid_argument("parts must have one entry per column");
+    const int nleaves = nlevels >= 2 ? 1 << (nlevels - 1) : 1;
+    for (int p : parts)
+        if (p < 0 || p >= nleaves) throw std::invalid_argument("part index out of range for nlevels");
+    const Adjacency G = ata_adjacency(A, csc_transpose(A));
+
+    // Separators, top level first (src/partition.cpp:384-414): a column on the
+    // even side of a cut with an unassigned neighbour on the odd side joins it.
+    std::vector<Cid> cmap(n);
+    for (int depth = 0; depth + 1 < nlevels; ++depth) {
+        const int l = nlevels - depth - 1;
+        for (int i = 0; i < n; ++i) {
+            if (cmap[i].self.lvl != -1) continue;
+            const int pi = side_at(parts[i], l);
+            if (pi & 1) continue;
+            for (int64_t q = G.p[i]; q < G.p[i + 1]; ++q) {
+                const int j = G.i[q];
+                if (cmap[j].self.lvl == -1 && side_at(parts[j], l) == pi + 1) {
+                    cmap[i].self = Sep(l, pi / 2);
+                    break;
+                }
+            }
+        }
+    }
+    // Leaves (src/partition.cpp:416-423), then the two sides of every separator
+    // column from its lower-level neighbours: the left side starts at the
+    // column's own leaf, both sides climb to the highest common ancestor
+    // (getInterfacesUsingATA, src/partition.cpp:628-675). Every column's
+    // section is its leaf part.
+    for (int i = 0; i < n; ++i)
+        if (cmap[i].self.lvl == -1) cmap[i].self = cmap[i].l = cmap[i].r = Sep(0, parts[i]);
+    for (int i = 0; i < n; ++i) {
+        const Sep self = cmap[i].self;
+        cmap[i].section = parts[i];
+        if (self.lvl <= 0) continue;
+        Sep left(0, parts[i]), right;
+        const int pi = side_at(parts[i], self.lvl);
+        for (int64_t q = G.p[i]; q < G.p[i + 1]; ++q) {
+            const int j = G.i[q];
+            const Sep nb = cmap[j].self;
+            if (nb.lvl >= self.lvl) continue;
+            if (side_at(parts[j], self.lvl) <= pi) left = common_ancestor(nb, left);
+            else right = (right.lvl == -1) ? nb : common_ancestor(nb, right);
+        }
+        if (right.lvl == -1) throw std::logic_error("graph ordering: separator column without a right side");
+        cmap[i].l = left;
+        cmap[i].r = right;
+    }
+    return finish_ordering(A, nlevels, cmap, square);
 }
 
 }  // namespace spq

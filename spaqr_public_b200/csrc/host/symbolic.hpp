@@ -1,6 +1,7 @@
-// Host symbolic layer: sparse patterns, separator/cluster identifiers and the
-// geometric nested-dissection ordering. Bit-exact with the reference's ordering
-// (src/partition.cpp, src/tree.cpp:46-163, include/cluster.h:22-111).
+// Host symbolic layer: sparse patterns, separator/cluster identifiers, the
+// geometric nested-dissection ordering (bit-exact with the reference's) and the
+// ordering without coordinates (src/partition.cpp, src/tree.cpp:46-163,
+// include/cluster.h:22-111).
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -64,5 +65,16 @@ struct Ordering {
 // the rows follow the columns; otherwise every row joins the first column of
 // its largest-norm run of equal cluster ids (src/tree.cpp:100-163).
 Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<double>& X, bool square = true);
+
+// Ordering without coordinates. graph_bisection splits the A^T A graph
+// recursively into 2^(nlevels-1) leaf parts (this library's own partitioner,
+// standing in for METIS_PartGraphRecursive at src/partition.cpp:354-372); the
+// leaf index holds the cuts from the top, first cut in the highest bit.
+// graph_ordering turns any such part vector (this one, or one computed by
+// METIS) into separators, interfaces and the permutations exactly as the
+// reference's MetisPartition (src/partition.cpp:374-426) followed by
+// getInterfacesUsingATA (src/partition.cpp:628-675) and Tree::partition.
+std::vector<int> graph_bisection(const Csc& A, int nlevels);
+Ordering graph_ordering(const Csc& A, int nlevels, const std::vector<int>& parts, bool square = true);
 
 }  // namespace spq

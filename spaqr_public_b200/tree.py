@@ -93,6 +93,12 @@ class Tree:
     def set_coords_grid(self, n, d):
         check(lib().spq_set_coords_grid(self._h, int(n), int(d)))
 
+    def set_parts(self, parts):
+        """Leaf part of every column for the ordering without coordinates
+        (the METIS part vector of src/partition.cpp:374-426)."""
+        p = np.ascontiguousarray(parts, dtype=np.int32)
+        check(lib().spq_set_parts(self._h, int(p.size), iptr(p)))
+
     # main steps (include/tree.h:139-147)
     def partition(self, A):
         m, n, cp, ri, va = _csc(A)
@@ -250,6 +256,16 @@ def column_normalize(A):
     out = va.copy()
     check(lib().spq_column_normalize(m, n, iptr(cp), iptr(ri), dptr(out)))
     return (m, n, cp, ri, out)
+
+
+def graph_parts(A, nlevels):
+    """Leaf parts (2^(nlevels-1), first cut in the highest bit) of this library's
+    recursive bisection of the A^T A graph: the ordering used when no
+    coordinates are set. Host only."""
+    m, n, cp, ri, _ = _csc(A)
+    parts = np.zeros(n, dtype=np.int32)
+    check(lib().spq_graph_parts(m, n, iptr(cp), iptr(ri), int(nlevels), iptr(parts)))
+    return parts
 
 
 def autotune(mode=None, reset=False, save=None, load=None):

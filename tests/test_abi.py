@@ -48,12 +48,16 @@ def test_version_and_errors():
     assert L.spq_factorize(None) == 1
 
 
-def test_partition_requires_coordinates():
+def test_partition_without_coordinates_uses_graph_ordering():
     A = matgen.advdiff2d(8)
     t = Tree(3, 0)
+    t.partition(A)  # graph bisection of A^T A (host only)
+    assert t.bottom()[:, 1].sum() == 64
+    t = Tree(3, 0)
+    t.set_coords(np.zeros((2, 10)))  # coordinates for 10 columns, matrix has 64
     with pytest.raises(_abi.SpqError) as e:
         t.partition(A)
-    assert e.value.code == 6
+    assert e.value.code == 1
 
 
 def test_invalid_csc_rejected():
