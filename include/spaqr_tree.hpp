@@ -45,6 +45,9 @@ public:
     // set_Xcoo: X is d x ncols, column-major (column j = coordinates of unknown j)
     void set_Xcoo(const double* X, int d, int ncols) { check(spq_set_coords(h_, d, ncols, X)); }
     void set_grid(int n, int d) { check(spq_set_coords_grid(h_, n, d)); }  // -n / -d
+    // Without coordinates: the leaf part of every column (e.g. METIS's part
+    // vector); when neither is set, partition() bisects the A^T A graph itself.
+    void set_parts(const int* parts, int ncols) { check(spq_set_parts(h_, ncols, parts)); }
     void set_precision(int p) { check(spq_set_precision(h_, p)); }
 
     void partition(const CscView& A) {
