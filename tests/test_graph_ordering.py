@@ -11,7 +11,7 @@ bisection of the A^T A graph (or takes one from the caller). Checked here:
   bit-exact with the oracle's restatement of those reference steps, on the
   same part vector (the library's own, and caller-supplied ones);
 * the bisection is deterministic, balanced, and its top separator is close to
-  the geometric one on a grid;
+  the geometric one on a grid; coupled columns never sit in disjoint subtrees;
 * the oracle's factorization on this ordering: the reference's numeric fill
   test (src/tree.cpp:857-860) against the library's rule (every candidate that
   passes the separator tests is kept) gives the same ranks and Krylov
@@ -20,6 +20,7 @@ bisection of the A^T A graph (or takes one from the caller). Checked here:
 """
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 from oracle import oracle_py as O
 from spaqr_public_b200 import Tree, graph_parts, matgen
@@ -151,3 +152,31 @@ def test_parts_argument_errors():
         t.partition(A)  # one part per column
     with pytest.raises(SpqError):
         graph_parts(A, 0)
+
+
+def _ata_pairs(A):
+    m, n, cp, ri, _ = A
+    S = sp.csc_matrix((np.ones(len(ri)), ri, cp), shape=(m, n))
+    G = (S.T @ S).tocoo()
+    return G.row, G.col
+
+
+@pytest.mark.parametrize("kind,n,levels", [("2d", 48, 7), ("3d", 14, 7)])
+def test_separators_separate(kind, n, levels):
+    # nested-dissection invariant of the ordering: two coupled columns (an
+    # A^T A edge) lie on separators in an ancestor/descendant relation of the
+    # bisection tree (a leaf is level 0), never in two disjoint subtrees
+    A = matgen.column_normalize(matgen.advdiff2d(n, seed=3) if kind == "2d" else matgen.advdiff3d(n, seed=3))
+    t, _ = _compare(A, levels)
+    cp, _ = t.perms()
+    b = t.bottom()
+    lvl = np.empty(A[1], dtype=np.int64)
+    sep = np.empty(A[1], dtype=np.int64)
+    for row in b:
+        cols = cp[row[0]:row[0] + row[1]]
+        lvl[cols] = row[4]
+        sep[cols] = row[5]
+    i, j = _ata_pairs(A)
+    lo = np.where(lvl[i] <= lvl[j], i, j)
+    hi = np.where(lvl[i] <= lvl[j], j, i)
+    assert np.all((sep[lo] >> (lvl[hi] - lvl[lo])) == sep[hi])
