@@ -519,6 +519,15 @@ static void geqp3(Mat& A, std::vector<int>& jpvt, std::vector<double>& tau) {
     L().dgeqp3(kColMajor, A.rows, A.cols, A.data(), A.rows, jpvt.data(), tau.data());
     for (int& j : jpvt) j--;
 }
+// gesvd_values (src/util.cpp:767-782): singular values only, same job flags.
+static std::vector<double> gesvd_values(Mat A) {
+    const int m = A.rows, n = A.cols, k = std::min(m, n);
+    std::vector<double> S(k, 0.0);
+    if (k == 0) return S;
+    std::vector<double> U((size_t)m * m), VT((size_t)n * n), superb(std::max(1, k - 1));
+    L().dgesvd(kColMajor, 'O', 'N', m, n, A.data(), m, S.data(), U.data(), m, VT.data(), n, superb.data());
+    return S;
+}
 static void trsm_right_upper(const Mat& R, Mat& B) {
     if (B.rows == 0 || B.cols == 0) return;
     L().dtrsm(kColMajor, kRight, kUpper, kNoTrans, kNonUnit, B.rows, B.cols, 1.0, R.data(), R.rows, B.data(),
@@ -649,6 +658,34 @@ struct OpOrthD : Op {
     void fwd() override { ormqr_vec(V, tau, c->x.data(), hs, 'T'); }
     void bwd() override { ormqr_vec(V, tau, c->x.data(), V.rows, 'N'); }
     const char* name() const override { return "OrthogonalD"; }
+};
+
+// Orthogonal (src/operations.cpp:87, include/operations.h:113-129): no forward
+// part; backward x_head <- Q x_head over the cluster's columns before the split.
+struct OpOrth : Op {
+    Cluster* c;
+    Mat V;
+    std::vector<double> tau;
+    OpOrth(Cluster* c_, Mat V_, std::vector<double> tau_) : c(c_), V(std::move(V_)), tau(std::move(tau_)) {}
+    void fwd() override {}
+    void bwd() override { ormqr_vec(V, tau, c->x.data(), V.rows, 'N'); }
+    const char* name() const override { return "Orthogonal"; }
+};
+
+// Split (src/operations.cpp:118-119, include/operations.h:165-177): the fine
+// cluster takes the last rows of the coarse one's full segment (forward) and
+// gives its values back to the last entries of the coarse head (backward).
+struct OpSplit : Op {
+    Cluster *c, *f;
+    int chead, cfull, fs;
+    OpSplit(Cluster* c_, Cluster* f_) : c(c_), f(f_), chead(c_->cols()), cfull(c_->rows()), fs(f_->rows()) {}
+    void fwd() override {
+        for (int q = 0; q < fs; ++q) f->x[q] = c->x[cfull - fs + q];
+    }
+    void bwd() override {
+        for (int q = 0; q < fs; ++q) c->x[chead - fs + q] = f->x[q];
+    }
+    const char* name() const override { return "Split"; }
 };
 
 // Merge (src/operations.cpp:94-115)
@@ -1296,6 +1333,112 @@ public:
         rec(8, rows_before, c->rows(), 0, 0, 0, c->order);
     }
 
+    // -------- sparsify without block scaling (--scale 0, src/tree.cpp:887-989) --------
+    // C = [A_mp^T | (1/s) A_pp^T A_pm] with s the smallest singular value of
+    // [A_pp; A_mp]; the RRQR's reflectors Q rotate the cluster's columns
+    // (A_pp <- A_pp Q, A_mp <- its rank rows of R), the last columns and rows
+    // split off into a fine cluster, which is eliminated at once.
+    void sparsify(Cluster* c) {
+        int cols_before = c->cols();
+        if (c->cols() == 0) { rec(3, 0, 0, 0, c->rows(), 0, c->order); return; }
+        std::vector<Mat*> Apm, Amp;
+        Mat* App = nullptr;
+        int spm = 0, smp = 0;
+        for (Edge* e : c->edgesIn)
+            if (!e->n1->eliminated) { Apm.push_back(e->A.get()); spm += e->A->cols; }
+        for (Edge* e : c->edgesOut) {
+            if (e->n2->eliminated) continue;
+            if (e->n2 != c) { Amp.push_back(e->A.get()); smp += e->A->rows; }
+            else App = e->A.get();
+        }
+        if (!App) throw std::runtime_error("sparsify: cluster without its diagonal block");
+        Mat Apmc(c->rows(), spm);
+        int cur = 0;
+        for (Mat* m : Apm) { Apmc.set_block(0, cur, *m); cur += m->cols; }
+        Mat Ap(App->rows + smp, c->cols());
+        Ap.set_block(0, 0, *App);
+        Mat C(c->cols(), smp + spm);
+        cur = 0;
+        for (Mat* m : Amp) {
+            Ap.set_block(App->rows + cur, 0, *m);
+            for (int j = 0; j < m->cols; ++j)
+                for (int i = 0; i < m->rows; ++i) C(j, cur + i) = (*m)(i, j);
+            cur += m->rows;
+        }
+        const std::vector<double> S = gesvd_values(Ap);
+        const double sinv = 1.0 / S[std::min(Ap.rows, Ap.cols) - 1];
+        for (int j = 0; j < spm; ++j)
+            for (int i = 0; i < c->cols(); ++i) {
+                double acc = 0;
+                for (int r = 0; r < App->rows; ++r) acc += (*App)(r, i) * Apmc(r, j);
+                C(i, smp + j) = sinv * acc;
+            }
+        std::vector<int> jpvt(C.cols, 0);
+        std::vector<double> t(std::min(C.rows, C.cols), 0.0);
+        geqp3(C, jpvt, t);
+        std::vector<double> rii(std::min(C.rows, C.cols));
+        for (size_t q = 0; q < rii.size(); ++q) rii[q] = C(q, q);
+        int rank = choose_rank(rii, tol_);
+        if (rank >= C.rows) { rec(3, cols_before, c->cols(), C.cols, c->rows(), 0, c->order); return; }
+        Mat v = C.block(0, 0, C.rows, rank);
+        std::vector<double> h(t.begin(), t.begin() + rank);
+        if (App->rows > 0)  // ormqr_notrans_right (src/util.cpp:358-369): A_pp <- A_pp Q
+            L().dormqr(kColMajor, 'R', 'N', App->rows, App->cols, rank, v.data(), v.rows, h.data(), App->data(),
+                       App->rows);
+        ops_.emplace_back(new OpOrth(c, v, h));
+        const int cf_csize = c->cols() - rank;
+        Cluster* cf = new_cluster(c->cstart + rank, cf_csize, c->rstart + c->rows() - cf_csize, cf_csize, c->id);
+        ops_.emplace_back(new OpSplit(c, cf));
+        c->reset_size(c->rows() - cf_csize, rank);
+        Mat Cr(rank, C.cols);  // upper(C.topRows(rank)) * P^T
+        for (int q = 0; q < C.cols; ++q)
+            for (int i = 0; i < rank && i <= q; ++i) Cr(i, jpvt[q]) = C(i, q);
+        cur = 0;
+        for (Mat* m : Amp) {
+            Mat nb(m->rows, rank);
+            for (int j = 0; j < rank; ++j)
+                for (int i = 0; i < m->rows; ++i) nb(i, j) = Cr(j, cur + i);
+            cur += m->rows;
+            *m = std::move(nb);
+        }
+        split_edges(c, cf);
+        fine_[ilvl_].push_back(cf);
+        eliminate_cluster(cf);
+        rec(3, cols_before, c->cols(), C.cols, c->rows(), 0, c->order);
+    }
+
+    // split_edges (src/tree.cpp:480-530): the fine cluster takes the last rows
+    // of every block in the coarse cluster's row, and the diagonal block splits
+    // into [A_cc A_cf; A_fc A_ff].
+    void split_edges(Cluster* c, Cluster* f) {
+        for (Edge* e : c->edgesIn) {
+            if (e->n1->eliminated) continue;
+            const Mat& A = *e->A;
+            Edge* ef = new Edge{e->n1, f, std::unique_ptr<Mat>(new Mat(A.block(A.rows - f->rows(), 0, f->rows(), A.cols)))};
+            owned_edges_.insert(ef);
+            *e->A = A.top_rows(c->rows());
+            f->edgesIn.push_back(ef);
+            f->rsparsity.insert(e->n1);
+            e->n1->edgesOut.push_back(ef);
+        }
+        Edge* es = c->self_edge();
+        if (!es) throw std::runtime_error("split_edges: cluster without its diagonal block");
+        const Mat S = *es->A;
+        Edge* eff = new Edge{f, f, std::unique_ptr<Mat>(new Mat(S.block(S.rows - f->rows(), S.cols - f->cols(), f->rows(), f->cols())))};
+        Edge* efc = new Edge{f, c, std::unique_ptr<Mat>(new Mat(S.block(0, S.cols - f->cols(), c->rows(), f->cols())))};
+        Edge* ecf = new Edge{c, f, std::unique_ptr<Mat>(new Mat(S.block(S.rows - f->rows(), 0, f->rows(), c->cols())))};
+        *es->A = S.block(0, 0, c->rows(), c->cols());
+        for (Edge* e : {eff, efc, ecf}) owned_edges_.insert(e);
+        f->edgesOut.push_back(eff);
+        f->edgesOut.push_back(efc);
+        f->edgesIn.push_back(ecf);
+        c->edgesOut.push_back(ecf);
+        f->cnbrs.insert(c);
+        f->cnbrs.insert(f);
+        f->rsparsity.insert(c);
+        f->edgesOut.sort([](const Edge* a, const Edge* b) { return a->n2->order > b->n2->order; });
+    }
+
     // sparsifyD (src/tree.cpp:992-1114) and, with imp, sparsifyD_imp (order 1.5,
     // src/tree.cpp:1117-1257): the same RRQR and block rewrite; imp also keeps
     // the E2 term, (Q^T A_pm_top)(rank:, :), as edges from the neighbours into
@@ -1433,8 +1576,9 @@ public:
                         if (want_sparsify(s)) sparsify_extra(s);
                 for (Cluster* s : bottom_current()) {
                     if (!want_sparsify(s)) continue;
-                    if (!scale_) throw std::runtime_error("--scale 0 sparsification is not restated");
-                    sparsifyD(s, order_ == 1.5f);
+                    if (scale_) sparsifyD(s, order_ == 1.5f);
+                    else if (square_) sparsify(s);
+                    else throw std::runtime_error("--scale 0 is restated for square systems only");
                 }
             }
             if (ilvl_ < nlevels_ - 1) merge_all();

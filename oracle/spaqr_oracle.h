@@ -2,7 +2,9 @@
  *
  * The oracle is a CPU restatement of the spaQR reference algorithm
  * (Abeynaya/spaQR_public): geometric nested dissection on A^T A, the cluster
- * tree, Householder elimination, block scaling, RRQR sparsification, merging,
+ * tree (or, without coordinates, the MetisPartition steps on a given part
+ * vector), Householder elimination, block scaling, RRQR sparsification (with
+ * block scaling, and without it: --scale 0, square systems), merging,
  * the op-tape solves and the GMRES/CGLS drivers. Its dense kernels are the same
  * LAPACK routines the reference calls (dgeqrf, dlarft, dlarfb, dgeqp3, dormqr,
  * dtrsm, dtrsv), taken from OpenBLAS.
