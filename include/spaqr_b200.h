@@ -41,7 +41,7 @@ enum spq_status {
     SPQ_ERR_CUDA = 3,        /* CUDA runtime error (no device, launch failure, ...) */
     SPQ_ERR_NUMERIC = 4,     /* NaN/Inf or a zero pivot reported by a kernel */
     SPQ_ERR_ALLOC = 5,       /* device or host allocation failed */
-    SPQ_ERR_UNSUPPORTED = 6, /* option outside the built path (e.g. non-geometric partition) */
+    SPQ_ERR_UNSUPPORTED = 6, /* option outside the built path (e.g. --scale 0, --hsl 1) */
     SPQ_ERR_NOCONV = 7       /* Krylov solver did not reach the tolerance */
 };
 
