@@ -147,8 +147,10 @@ int spq_gmres_dev(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, 
  * exits; larger requests return SPQ_ERR_ARG with the sizes. Preconditions: the
  * handle is factorized and its preconditioner has been applied at least once
  * (spq_solve, spq_solve_dev or spq_gmres_dev build the solve graph), else
- * SPQ_ERR_STATE. The first call on a device looks up the array's device
- * address, so make that first call before any stream capture. All calls share
+ * SPQ_ERR_STATE. The array's device address is looked up, and the array and
+ * the Krylov kernels are loaded onto the device, when a handle binds its
+ * device (spq_partition), so the call itself takes no device memory, even
+ * under lazy module loading. All calls share
  * the one array: calls that overlap on the GPU (several handles, streams or
  * threads at once) race on it. The workspace is re-initialised by every call. */
 int spq_gmres_dev_noalloc(spq_tree* t, int m, const int* d_rowptr, const int* d_colind, const double* d_val,
@@ -230,6 +232,11 @@ int spq_get_host_times(spq_tree* t, double* out11);
  * next handle (no allocation cost on refactorization); this returns the
  * cached, unused part to the device. */
 int spq_trim_memory(void);
+/* Bytes of the device's memory pool in use by live buffers and held by the
+ * pool (in use plus cached), for memory accounting; 0 and 0 before the first
+ * handle binds the device. No counterpart in the reference (Eigen allocates on
+ * the host heap). */
+int spq_pool_memory(int device, unsigned long long* used, unsigned long long* reserved);
 
 /* Autotuner of launch shapes that do not change results (today the cluster
  * size of the blocked RRQR of sparsifyD, src/tree.cpp:1022-1049, whose output

@@ -67,6 +67,7 @@ SIGNATURES = {
     "spq_get_level_times": (_i, [_p, _dp]),
     "spq_get_host_times": (_i, [_p, _dp]),
     "spq_trim_memory": (_i, []),
+    "spq_pool_memory": (_i, [_i, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "spq_autotune_set_mode": (_i, [_i]),
     "spq_autotune_get": (_i, [_ip, _ip, _ip]),
     "spq_autotune_reset": (_i, []),

@@ -18,10 +18,6 @@
 
 using namespace spq;
 
-namespace spq {
-cudaError_t noalloc_scratch(double** ptr, size_t* elems);  // noalloc_scratch.cu
-}
-
 struct spq_tree {
     Config cfg;
     int precision = SPQ_FP64;
@@ -787,6 +783,25 @@ int spq_factorize_batch(spq_tree* const* ts, int n, int nthreads) {
 int spq_trim_memory(void) {
     return guard([&] {
         trim_device_pools();
+        return SPQ_OK;
+    });
+}
+int spq_pool_memory(int device, unsigned long long* used, unsigned long long* reserved) {
+    if (!used || !reserved || device < 0) return fail(SPQ_ERR_ARG, "invalid arguments");
+    return guard([&] {
+        *used = *reserved = 0;
+        cudaMemPool_t pool = nullptr;
+        {
+            std::lock_guard<std::mutex> g(pool_mutex());
+            auto it = pool_table().find(device);
+            if (it != pool_table().end()) pool = it->second;
+        }
+        if (!pool) return SPQ_OK;
+        uint64_t u = 0, r = 0;
+        cuda_check(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u), "pool used memory");
+        cuda_check(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r), "pool reserved memory");
+        *used = u;
+        *reserved = r;
         return SPQ_OK;
     });
 }

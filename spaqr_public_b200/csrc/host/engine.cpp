@@ -5,6 +5,7 @@
 // wave concurrently gives the same result as the reference's sequential loop),
 // and issued as batched kernels on the handle's stream.
 #include "engine.hpp"
+#include "krylov.hpp"
 
 #include "autotune.hpp"
 
@@ -130,6 +131,14 @@ public:
         desc_arena_.set_stream(stream_, pool);
         scratch_.set_pool(pool, cfg_.device);
         prepare_kernels<T>();
+        // The no-allocation GMRES must not make the driver place anything on
+        // the device when it runs: with lazy module loading the fixed
+        // workspace array and the Krylov kernels would otherwise be loaded
+        // (device memory taken) by its first call. Bind time loads both.
+        prepare_krylov_kernels();
+        double* ws = nullptr;
+        size_t ws_elems = 0;
+        cuda_check(noalloc_scratch(&ws, &ws_elems), "no-allocation workspace address");
     }
 
     cudaStream_t stream() const override { return stream_; }

@@ -79,8 +79,8 @@ public:
         v_.alloc(m_, s_);
         xnew_.alloc(m_, s_);
         part_.alloc(nblk_ + 1, s_);
-        scal_.alloc(2 * (restart + 1) + 4, s_);
-        H_.alloc((size_t)m_ * (restart + 1), s_);
+        scal_.alloc(2 * (size_t(restart) + 1) + 4, s_);
+        H_.alloc(size_t(m_) * (size_t(restart) + 1), s_);
         hpart_.resize(nblk_);
     }
     // Same driver on a caller-provided workspace of workspace_elems(m, restart)
@@ -99,13 +99,16 @@ public:
         take(v_, m_);
         take(xnew_, m_);
         take(part_, nblk_ + 1);
-        take(scal_, 2 * (restart + 1) + 4);
-        take(H_, (size_t)m_ * (restart + 1));
+        take(scal_, 2 * (size_t(restart) + 1) + 4);
+        take(H_, size_t(m_) * (size_t(restart) + 1));
         hpart_.resize(nblk_);
     }
     static size_t workspace_elems(int m, int restart) {
         auto r = [](size_t n) { return (std::max<size_t>(n, 1) + 31) & ~size_t(31); };
-        return 5 * r(m) + r(reduce_blocks() + 1) + r(2 * (restart + 1) + 4) + r((size_t)m * (restart + 1));
+        // sizes in size_t: restart near INT_MAX must not overflow before the
+        // caller compares the result with its workspace
+        const size_t rs = size_t(restart) + 1;
+        return 5 * r(size_t(m)) + r(size_t(reduce_blocks()) + 1) + r(2 * rs + 4) + r(size_t(m) * rs);
     }
 
     // Sum of a reduction's partials on the host, in fixed order.

@@ -25,6 +25,10 @@ size_t gmres_workspace_elems(int m, int restart);
 int gmres_device_ws(EngineBase& P, const DevCsr& A, const double* d_b, double* d_x, int iters, int restart,
                     double tol, double* res, long long* launches, double* workspace);
 
+// Device address and size (doubles) of the fixed no-allocation GMRES workspace
+// on the current device (noalloc_scratch.cu).
+cudaError_t noalloc_scratch(double** ptr, size_t* elems);
+
 // Preconditioned CGLS on the normal equations (src/is.cpp:274-345), with the
 // least-squares preconditioner P.solve_nrml_dev. A (m x n) and At (its
 // transpose, n x m) as device CSR; x holds the initial guess. Returns the

@@ -1129,6 +1129,19 @@ void launch_sub(int n, const double* a, const double* b, double* y, cudaStream_t
 }
 int reduce_blocks() { return kRedBlocks; }
 
+void prepare_krylov_kernels() {
+    once_per_device(reinterpret_cast<const void*>(&k_spmv), [] {
+        const void* fns[] = {reinterpret_cast<const void*>(&k_spmv), reinterpret_cast<const void*>(&k_dot_partials),
+                             reinterpret_cast<const void*>(&k_apply_reflector),
+                             reinterpret_cast<const void*>(&k_make_reflector), reinterpret_cast<const void*>(&k_axpby),
+                             reinterpret_cast<const void*>(&k_sub)};
+        for (const void* f : fns) {
+            cudaFuncAttributes a;
+            cudaFuncGetAttributes(&a, f);
+        }
+    });
+}
+
 void once_per_device(const void* key, void (*setup)()) {
     static std::mutex mu;
     static std::set<std::pair<const void*, int>> seen;

@@ -221,6 +221,9 @@ void launch_make_reflector(double* v, int k, int m, double* ess_col, double* tau
 void launch_axpby(int n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_sub(int n, const double* a, const double* b, double* y, cudaStream_t s);          // y = a - b
 int reduce_blocks();
+// Loads the Krylov kernels above on the current device (once per device), so
+// that a later launch does not load module code lazily.
+void prepare_krylov_kernels();
 
 // Sets the shared-memory opt-ins of the kernels (once per process and type);
 // called when a handle is created, outside any stream capture.

@@ -38,15 +38,29 @@ def _setup():
     return w, A, t, dev
 
 
-def _gmres(fn, t, A, dev, restart, tol):
+def _pool_bytes():
+    used, reserved = C.c_ulonglong(0), C.c_ulonglong(0)
+    check(lib().spq_pool_memory(0, C.byref(used), C.byref(reserved)))
+    return used.value, reserved.value
+
+
+def _gmres(fn, t, A, dev, restart, tol, memory=None):
+    """One GMRES call; with memory a list, appends the device pool's (used,
+    reserved) bytes and the device's free bytes just before and just after the
+    call (nothing else runs in between)."""
     import torch
     x = torch.zeros(A[1], dtype=torch.float64, device="cuda")
     its = C.c_int(0)
     res = C.c_double(0)
     torch.cuda.synchronize()
+    if memory is not None:
+        memory.append((_pool_bytes(), torch.cuda.mem_get_info()[0]))
     rc = fn(t._h, A[0], C.c_void_p(dev["rp"].data_ptr()), C.c_void_p(dev["ci"].data_ptr()),
             C.c_void_p(dev["va"].data_ptr()), C.c_void_p(dev["b"].data_ptr()), C.c_void_p(x.data_ptr()), 100,
             restart, tol, C.byref(its), C.byref(res))
+    if memory is not None:
+        torch.cuda.synchronize()
+        memory.append((_pool_bytes(), torch.cuda.mem_get_info()[0]))
     return rc, x.cpu().numpy(), its.value, res.value
 
 
@@ -60,8 +74,12 @@ def test_noalloc_gmres_matches_allocating_gmres(gpu):
     for _ in range(2):  # two calls in a row: the shared workspace keeps old contents
         rc, x_ref, its_ref, res_ref = _gmres(L.spq_gmres_dev, t, A, dev, 100, w["res"])
         check(rc)
-        rc, x, its, res = _gmres(L.spq_gmres_dev_noalloc, t, A, dev, 100, w["res"])
+        memory = []
+        rc, x, its, res = _gmres(L.spq_gmres_dev_noalloc, t, A, dev, 100, w["res"], memory)
         check(rc)
+        # nothing taken from the device pool, and no device memory at all
+        # (the workspace and the kernels were loaded when the handle bound the device)
+        assert memory[0] == memory[1]
         assert its == its_ref
         assert abs(res - res_ref) <= 1e-6 * res_ref
         assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
