@@ -1,0 +1,204 @@
+"""GPU parity on the full-size configurations, against committed oracle fixtures
+(tests/golden/config_*.npz, written by tests/golden/make_golden.py --configs).
+
+* advdiff3d_64 (the benchmark workload: 64^3 advection-diffusion, n = 262144,
+  12 levels, tol 1e-2, skip 2), plain FP64: the event log equals the oracle's
+  exactly (per-level separator sizes, every elimination shape, every RRQR rank,
+  merge sizes, nnzR / nnzH / nnzQ), the one-shot solve is within 1e-10 of the
+  oracle's, GMRES to 1e-10 takes the oracle's iteration count and reaches the
+  target; the FP32-factor form reaches the same target through the FP64
+  refinement, and its error against the FP64 oracle solution is stated.
+* contrast2d_512 (512^2 high-contrast diffusion) at tol 1e-1, 1e-2 and 1e-3,
+  plain FP64: log and GMRES iterations (converged or not within 300) equal the
+  oracle's.
+* lsq2d_256 (72090 x 65536 least squares): log, CGLS iterations and solution.
+* the differentiation batch (32 systems of sides 96..256): on its smallest,
+  median and largest system, the adjoint gradients (FP32 factor, FP64 GMRES)
+  match the FP64 CPU reference gradient and central finite differences.
+
+Vectors are compared through PROJ_ROWS seeded N(0, 1) projections: for
+||x - x_o|| <= eps ||x_o||, each projection differs by at most
+eps ||x_o|| sqrt(n) (a row's norm is about sqrt(n)), the bound asserted.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from spaqr_public_b200 import FP32, FP64, Tree, cgls, gmres, matgen, solve_to_residual
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+sys.path.insert(0, GOLDEN)
+from make_golden import CONFIGS, projections, spmv_t  # noqa: E402
+
+
+def _fixture(key):
+    return dict(np.load(os.path.join(GOLDEN, f"config_{key}.npz")))
+
+
+def _tree(w, A, prec, tol, square=1):
+    t = Tree(w["levels"], w["skip"], precision=prec)
+    t.set_tol(tol)
+    t.set_scale(1)
+    t.set_square(square)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    t.assemble(A)
+    t.factorize()
+    return t
+
+
+def _close(x, proj, norm, eps):
+    """x within eps (relative) of the oracle vector whose projections and norm are given."""
+    p = projections(x)
+    bound = eps * norm * np.sqrt(x.size)
+    assert abs(np.linalg.norm(x) - norm) <= eps * norm, (np.linalg.norm(x), norm)
+    assert np.max(np.abs(p - proj)) <= bound, (np.max(np.abs(p - proj)), bound)
+
+
+def _square_config(key, prec=FP64):
+    name, tol = CONFIGS[key]
+    w = matgen.workload(name)
+    A = matgen.column_normalize(w["A"])
+    f = _fixture(key)
+    t = _tree(w, A, prec, float(f["tol"]))
+    return w, A, t, f
+
+
+def test_advdiff3d_64_fp64_matches_oracle(gpu):
+    w, A, t, f = _square_config("advdiff3d_64")
+    log = t.log()
+    assert log.shape == f["log"].shape
+    assert np.array_equal(log, f["log"])
+    final = log[log[:, 0] == 6][0]
+    assert final[4:7].tolist() == [166546962, 130627940, 29449558]  # nnzR, nnzH, nnzQ
+    b = w["b"]
+    _close(t.solve(b), f["solve_proj"], float(f["solve_norm"]), 1e-10)
+    x, its, res = gmres(A, b, t, iters=300, tol=float(f["res_target"]))
+    assert its == int(f["its"]) == 11
+    assert abs(res - float(f["res"])) <= 1e-6 * float(f["res"])
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    assert true <= 1e-10
+    _close(x, f["x_proj"], float(f["x_norm"]), 1e-8)
+    t.close()
+
+
+def test_advdiff3d_64_fp32_form_reaches_target(gpu):
+    w, A, t, f = _square_config("advdiff3d_64", prec=FP32)
+    b = w["b"]
+    x, its, res = solve_to_residual(A, b, t, target=1e-10, inner_tol=1e-5)
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    assert res <= 1e-10 and true <= 1e-10
+    # error against the FP64 oracle solution (GMRES to 1e-10): both are
+    # 1e-10-residual solutions, so they agree to about cond(A) * 1e-10
+    p = projections(x)
+    rel = np.max(np.abs(p - f["x_proj"])) / (float(f["x_norm"]) * np.sqrt(x.size))
+    print(f"advdiff3d_64 FP32 form: {its} GMRES its, residual {true:.2e}, projected error vs FP64 oracle {rel:.2e}")
+    assert rel <= 1e-7
+    t.close()
+
+
+@pytest.mark.parametrize("key", ["contrast2d_512_t1e-1", "contrast2d_512_t1e-2", "contrast2d_512_t1e-3"])
+def test_contrast2d_512_sweep_matches_oracle(gpu, key):
+    w, A, t, f = _square_config(key)
+    assert np.array_equal(t.log(), f["log"])
+    b = w["b"]
+    _close(t.solve(b), f["solve_proj"], float(f["solve_norm"]), 1e-9)
+    x, its, res = gmres(A, b, t, iters=300, tol=1e-10)
+    assert its == int(f["its"])
+    assert abs(res - float(f["res"])) <= 1e-5 * float(f["res"])
+    true = np.linalg.norm(matgen.spmv(A, x) - b) / np.linalg.norm(b)
+    if int(f["its"]) < 300:  # the oracle converged: so must the device, to the same point
+        # GMRES is left preconditioned: it stops on the preconditioned residual,
+        # and with the 10^6 contrast the true residual stays well above it
+        # (oracle: 2.4e-8 at tol 1e-2, 1.3e-7 at tol 1e-3)
+        assert 0.5 * float(f["true_res"]) <= true <= 2 * float(f["true_res"])
+        _close(x, f["x_proj"], float(f["x_norm"]), 1e-6)
+    else:  # neither converges within 300 iterations: same stall
+        assert abs(true - float(f["true_res"])) <= 1e-3 * float(f["true_res"])
+    t.close()
+
+
+def test_lsq2d_256_matches_oracle(gpu):
+    w = matgen.workload("lsq2d_256")
+    A = matgen.column_normalize(w["A"])
+    f = _fixture("lsq2d_256")
+    t = _tree(w, A, FP64, float(f["tol"]), square=0)
+    assert np.array_equal(t.log(), f["log"])
+    b = np.asarray(w["b"], dtype=np.float64)
+    _close(t.solve_nrml(spmv_t(A, b)), f["solve_proj"], float(f["solve_norm"]), 1e-9)
+    x, its, res = cgls(A, b, t, iters=300, tol=1e-10)
+    # CGLS to 1e-10 here stops on a residual within a few percent of the
+    # tolerance, so rounding alone moves the count: the oracle itself takes
+    # 86, 87 or 88 iterations with 16, 1-2 or 8 OpenBLAS threads (same event
+    # log). The fixture is the 2-thread run.
+    assert abs(its - int(f["its"])) <= 2
+    assert res <= 1e-10
+    _close(x, f["x_proj"], float(f["x_norm"]), 1e-8)
+    t.close()
+
+
+def _batch_systems():
+    ws = matgen.diff_batch(32)
+    order = np.argsort([w["n"] for w in ws], kind="stable")
+    return [ws[order[0]], ws[order[len(ws) // 2]], ws[order[-1]]]
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_diff_batch_gradients(gpu, which):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import torch
+
+    from spaqr_public_b200.autograd import SparsePattern, spaqr_solve
+    w = _batch_systems()[which]
+    A = matgen.column_normalize(w["A"])
+    m, n, cp, ri, va = A
+    t = _tree(w, A, FP32, w["tol"])
+    pat = SparsePattern(A)
+    vals = torch.tensor(va, dtype=torch.float64, device="cuda", requires_grad=True)
+    b = torch.tensor(w["b"], dtype=torch.float64, device="cuda", requires_grad=True)
+    xstar = torch.tensor(w["xstar"], dtype=torch.float64, device="cuda")
+    x = spaqr_solve(vals, b, t, pat, target=1e-13, inner_tol=1e-6)
+    L = 0.5 * ((x - xstar) ** 2).sum()
+    L.backward()
+    gb = b.grad.cpu().numpy()
+    gA = vals.grad.cpu().numpy()
+    # FP64 CPU reference gradient: lambda = A^-T (x - x*), dL/dA_ij = -lambda_i x_j
+    As = sp.csc_matrix((va, ri, cp), shape=(m, n))
+    x_ref = spla.spsolve(As, w["b"])
+    lam_ref = spla.spsolve(As.T.tocsc(), x_ref - w["xstar"])
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    gA_ref = -lam_ref[ri] * x_ref[cols]
+    assert np.linalg.norm(gb - lam_ref) <= 1e-9 * np.linalg.norm(lam_ref)
+    assert np.linalg.norm(gA - gA_ref) <= 1e-9 * np.linalg.norm(gA_ref)
+
+    # central finite differences (step 1e-6, FP64 solves) on 64 seeded entries each of b and A
+    def loss(vv, bb):
+        with torch.no_grad():
+            xx = spaqr_solve(vv, bb, t, pat, target=1e-13, inner_tol=1e-6)
+            return 0.5 * float(((xx - xstar) ** 2).sum())
+
+    rng = np.random.default_rng(1004 + which)
+    h = 1e-6
+    vd, bd = vals.detach(), b.detach()
+    kb = rng.choice(m, 64, replace=False)
+    ka = rng.choice(len(va), 64, replace=False)
+    fd_b, fd_a = [], []
+    for k in kb:
+        e = torch.zeros_like(bd)
+        e[k] = h
+        fd_b.append((loss(vd, bd + e) - loss(vd, bd - e)) / (2 * h))
+    for k in ka:
+        e = torch.zeros_like(vd)
+        e[k] = h
+        fd_a.append((loss(vd + e, bd) - loss(vd - e, bd)) / (2 * h))
+    fd_b, fd_a = np.array(fd_b), np.array(fd_a)
+    rel_b = np.linalg.norm(fd_b - gb[kb]) / np.linalg.norm(gb[kb])
+    rel_a = np.linalg.norm(fd_a - gA[ka]) / np.linalg.norm(gA[ka])
+    print(f"diff batch system n={w['n']}: FD vs adjoint relative error b {rel_b:.2e}, A {rel_a:.2e}")
+    assert rel_b <= 1e-6 and rel_a <= 1e-6
+    t.close()
