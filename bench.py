@@ -17,10 +17,10 @@ needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the CPU restatement of the reference algorithm (oracle/,
-LAPACK from OpenBLAS) on the host cores, on a bounded sample (the same
-generator on a smaller cube) scaled to the full workload by the ratio of the
-reference's algorithmic flops (factorization) and factor-words x iterations
-(Krylov).
+LAPACK from OpenBLAS) on all host cores, on the same 64^3 workload with the
+same step boundary (partition and assembly untimed, then factorize + GMRES to
+1e-10), its level phases and solve sweeps run as conflict-free waves on host
+threads (bitwise the sequential results with one BLAS thread).
 """
 from __future__ import annotations
 
@@ -263,36 +263,36 @@ def roofline(info, peaks):
 
 
 # --------------------------------------------------------------------------- CPU arm
-def cpu_sample(n_side, threads):
-    """Oracle pipeline on the advdiff3d generator at n_side^3; returns timing parts."""
+def cpu_prepare(name, threads):
+    """The oracle tree of a workload, partitioned and assembled (untimed), set to
+    run its factorization and solves as conflict-free waves on `threads` host
+    threads (bitwise the sequential results with one BLAS thread; OpenBLAS keeps
+    `threads` threads for the waves that hold a single task)."""
     from oracle import oracle_py as O
-    from spaqr_public_b200 import matgen, work
-    w = matgen.workload(f"advdiff3d_{n_side}")
+    from spaqr_public_b200 import matgen
+    w = matgen.workload(name)
     A = matgen.column_normalize(w["A"])
-    if threads:
-        O.blas_threads(threads)
-    t0 = time.perf_counter()
+    O.blas_threads(threads)
     t = O.OracleTree(w["levels"], w["skip"], w["tol"], 1, 1.0, 1)
+    t.set_threads(threads)
     t.set_coords_grid(w["n"], w["d"])
     t.partition(A)
     t.assemble(A)
+    return w, A, t
+
+
+def cpu_step(w, A, t):
+    """One step of the CPU oracle with the GPU arm's step boundary: factorize +
+    GMRES (the reference's drivers, src/tree.cpp:1309-1437, src/is.cpp:94-272)
+    to a preconditioned tolerance of 1e-10; returns the step's seconds and the
+    true relative residual it reached."""
+    from spaqr_public_b200 import matgen
+    t0 = time.perf_counter()
     t.factorize()
-    t1 = time.perf_counter()
-    x, its, r = t.gmres(A, w["b"], iters=300, tol=TARGET)
-    t2 = time.perf_counter()
-    log = t.log()
-    return dict(n=n_side, factor_s=t1 - t0, krylov_s=t2 - t1, its=its, flops=work.total_flops(log, reference=True),
-                words=work.factor_bytes(log))
-
-
-def cpu_scaled(sample):
-    """Scales a sample's time to the 64^3 workload (reference flops for the
-    factorization, factor words x iterations for the Krylov part)."""
-    full = json.load(open(os.path.join(ROOT, "tests", "golden", "work_advdiff3d_64.json")))
-    fw = full["final"][4] + full["final"][5] + full["final"][6]
-    t_fact = sample["factor_s"] * full["reference_flops"] / sample["flops"]
-    t_kry = sample["krylov_s"] * (fw * full["gmres_its"]) / (sample["words"] * max(sample["its"], 1))
-    return t_fact + t_kry
+    x, its, res = t.gmres(A, w["b"], iters=300, tol=TARGET)
+    sec = time.perf_counter() - t0
+    true = float(np.linalg.norm(matgen.spmv(A, x) - w["b"]) / np.linalg.norm(w["b"]))
+    return sec, dict(its=its, res=res, true_res=true)
 
 
 def cpu_threads():
@@ -302,27 +302,39 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def cpu_sample_text(threads, info):
+    return (f"full {WORKLOAD} step (n=262144, 12 levels, tol 1e-2, skip 2): factorize + GMRES to 1e-10 "
+            f"({info['its']} its, true residual {info['true_res']:.2e}), partition/assembly untimed; CPU oracle "
+            f"(restatement of the reference, LAPACK from OpenBLAS) as conflict-free waves on {threads} threads")
+
+
 def run_reference(args):
+    """The reference arm: the CPU oracle on the benchmark workload itself, every
+    timed step a full 64^3 factorize + GMRES (warm-up steps on a 16^3 cube of the
+    same generator, untimed)."""
     ws, rank, local = dist_env()
     if rank != 0:
         return
     threads = cpu_threads()
-    n_side = 40 if (args.steps + args.warmup) <= 6 else 32
     for _ in range(args.warmup):
-        cpu_sample(n_side, threads)
-    vals = []
+        cpu_step(*cpu_prepare("advdiff3d_16", threads))
+    vals, info = [], None
     for _ in range(args.steps):
-        s = cpu_sample(n_side, threads)
-        vals.append(cpu_scaled(s))
+        w, A, t = cpu_prepare(WORKLOAD, threads)  # untimed setup
+        sec, info = cpu_step(w, A, t)
+        vals.append(sec)
+        del t
     v = float(np.mean(vals))
-    sample = (f"advdiff3d_{n_side} ({n_side}^3, same generator and settings) full pipeline, scaled to 64^3 by "
-              f"reference flops (factor) and factor words x iterations (GMRES)")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": {"workload": f"{WORKLOAD} (n=262144, 12 levels, tol 1e-2, skip 2, target 1e-10)",
-                       "parallelism": "cpu"},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+                       "step": "factorize + GMRES to 1e-10 (partition/assemble untimed)",
+                       "warmup": "advdiff3d_16 (16^3, same generator), untimed",
+                       "parallelism": f"cpu, {threads} threads"},
+            "gmres_its": info["its"], "true_residual": info["true_res"], "times": [round(x, 3) for x in vals],
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": cpu_sample_text(threads, info)},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -381,11 +393,9 @@ def run_ours(args):
     _, e2e_res, h2d, d2h = e2e_runs[-1]
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        s = cpu_sample(40, cpu_threads())
-        cpu = {"value": cpu_scaled(s), "unit": "s", "cores": cpu_threads(), "kind": "port",
-               "sample": ("oracle on advdiff3d_40 (40^3) full pipeline "
-                          f"({s['factor_s']:.1f}s factor + {s['krylov_s']:.1f}s GMRES), scaled to 64^3 by "
-                          "reference flops and factor words x iterations")}
+        th = cpu_threads()
+        sec, cinfo = cpu_step(*cpu_prepare(WORKLOAD, th))
+        cpu = {"value": sec, "unit": "s", "cores": th, "kind": "port", "sample": cpu_sample_text(th, cinfo)}
     f32, f64 = result["fp32"], result["fp64"]
     inf = f32["info"]
     line = {

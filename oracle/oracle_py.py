@@ -35,6 +35,7 @@ def lib():
         L.orc_destroy.argtypes = [C.c_void_p]
         L.orc_last_error.restype = C.c_char_p
         L.orc_blas_threads.argtypes = [C.c_int]
+        L.orc_set_threads.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_coords.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p]
         L.orc_set_parts.argtypes = [C.c_void_p, C.c_int, _i32p, C.c_int]
         for f in (L.orc_partition, L.orc_assemble):
@@ -93,6 +94,11 @@ class OracleTree:
         if getattr(self, "h", None):
             lib().orc_destroy(self.h)
             self.h = None
+
+    def set_threads(self, n):
+        """Host threads for the wave-parallel factorization and solve (CPU
+        baseline timing; bitwise the sequential results)."""
+        _check(lib().orc_set_threads(self.h, int(n)))
 
     def set_coords_grid(self, n, d):
         X = linspace_nd(n, d)

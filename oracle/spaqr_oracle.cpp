@@ -26,7 +26,12 @@
 #include "oracle_lapack.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -35,6 +40,7 @@
 #include <set>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace orc {
@@ -562,6 +568,13 @@ struct Op {
     virtual void fwd() = 0;
     virtual void bwd() = 0;
     virtual const char* name() const = 0;
+    // Solution segments (Cluster::x) the forward or backward part reads or
+    // writes, for the wave-parallel solve; nullptr stands for "all of them"
+    // (the op then runs alone, in tape order).
+    virtual void touch(bool fwd, std::vector<const void*>& keys) const {
+        (void)fwd;
+        keys.push_back(nullptr);
+    }
 };
 
 // QR (src/operations.cpp:12-57, include/operations.h:22-50)
@@ -612,6 +625,15 @@ struct OpQR : Op {
         trsv_upper(R, xs, ccols, false);
     }
     const char* name() const override { return "QR"; }
+    void touch(bool f, std::vector<const void*>& keys) const override {
+        if (f) {
+            for (Edge* e : c->edgesOut)
+                if (e->A) keys.push_back(e->n2);
+        } else {
+            keys.push_back(c);
+            for (Edge* e : c->edgesIn) keys.push_back(e->n1);
+        }
+    }
 };
 
 // Reassign (src/operations.cpp:60-69)
@@ -645,6 +667,7 @@ struct OpScaleD : Op {
         trsv_upper(R, c->x.data(), hs, false);
     }
     const char* name() const override { return "ScaleD"; }
+    void touch(bool, std::vector<const void*>& keys) const override { keys.push_back(c); }
 };
 
 // OrthogonalD (src/operations.cpp:89-90)
@@ -655,9 +678,14 @@ struct OpOrthD : Op {
     std::vector<double> tau;
     OpOrthD(Cluster* c_, Mat V_, std::vector<double> tau_) : c(c_), hs(c_->cols()), V(std::move(V_)),
                                                              tau(std::move(tau_)) {}
+    // c's column count before the split given explicitly (the wave-parallel
+    // sparsification resizes c before the op is recorded)
+    OpOrthD(Cluster* c_, Mat V_, std::vector<double> tau_, int hs_) : c(c_), hs(hs_), V(std::move(V_)),
+                                                                      tau(std::move(tau_)) {}
     void fwd() override { ormqr_vec(V, tau, c->x.data(), hs, 'T'); }
     void bwd() override { ormqr_vec(V, tau, c->x.data(), V.rows, 'N'); }
     const char* name() const override { return "OrthogonalD"; }
+    void touch(bool, std::vector<const void*>& keys) const override { keys.push_back(c); }
 };
 
 // Orthogonal (src/operations.cpp:87, include/operations.h:113-129): no forward
@@ -703,6 +731,10 @@ struct OpMerge : Op {
             for (int i = 0; i < c->cols(); ++i) c->x[i] = p->x[k++];
     }
     const char* name() const override { return "Merge"; }
+    void touch(bool, std::vector<const void*>& keys) const override {
+        keys.push_back(p);
+        for (Cluster* c : p->children) keys.push_back(c);
+    }
 };
 
 // SplitD (src/operations.cpp:121-131); shared by the transposed tape.
@@ -722,9 +754,16 @@ struct OpSplitD : Op {
     Cluster *c, *f;
     int crows, ccols, rank;
     OpSplitD(Cluster* c_, Cluster* f_, int r) : c(c_), f(f_), crows(c_->rows()), ccols(c_->cols()), rank(r) {}
+    // c's sizes before the split given explicitly (the wave-parallel
+    // sparsification resizes c before the op is recorded)
+    OpSplitD(Cluster* c_, Cluster* f_, int r, int cr, int cc) : c(c_), f(f_), crows(cr), ccols(cc), rank(r) {}
     void fwd() override { splitd_fwd(c->x.data(), f->x.data(), crows, ccols, rank); }
     void bwd() override { splitd_bwd(c->x.data(), f->x.data(), crows, ccols, rank); }
     const char* name() const override { return "SplitD"; }
+    void touch(bool, std::vector<const void*>& keys) const override {
+        keys.push_back(c);
+        keys.push_back(f);
+    }
 };
 
 // Transposed tape (src/toperations.cpp)
@@ -847,6 +886,89 @@ struct TOpSplitD : Op {
 // ---------------------------------------------------------------------------
 // Tree (src/tree.cpp, include/tree.h)
 // ---------------------------------------------------------------------------
+// Fixed pool of host threads for the wave-parallel mode: run(n, k, f) calls
+// f(0..n-1) on up to k threads (the caller included), each index once, and
+// rethrows the first exception after all have finished.
+class Pool {
+public:
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& th : workers_) th.join();
+    }
+    void run(int n, int k, const std::function<void(int)>& f) {
+        if (n <= 0) return;
+        k = std::max(1, std::min(k, n));
+        while ((int)workers_.size() < k - 1) workers_.emplace_back([this] { loop(); });
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_ = &f;
+            n_ = n;
+            next_ = 0;
+            tickets_ = k - 1;  // workers that may join this run
+            running_ = 0;
+            gen_++;
+            err_.clear();
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> g(mu_);
+        done_.wait(g, [&] { return tickets_ == 0 && running_ == 0; });
+        job_ = nullptr;
+        if (!err_.empty()) throw std::runtime_error(err_);
+    }
+
+private:
+    void work() {
+        for (;;) {
+            const int i = next_.fetch_add(1);
+            if (i >= n_) break;
+            try {
+                (*job_)(i);
+            } catch (const std::exception& e) {
+                std::lock_guard<std::mutex> g(mu_);
+                if (err_.empty()) err_ = e.what();
+            }
+        }
+    }
+    void loop() {
+        long long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return stop_ || (gen_ != seen && tickets_ > 0); });
+                if (stop_) return;
+                seen = gen_;
+                --tickets_;
+                ++running_;
+            }
+            work();
+            {
+                std::lock_guard<std::mutex> g(mu_);
+                --running_;
+            }
+            done_.notify_all();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    std::atomic<int> next_{0};
+    int n_ = 0, tickets_ = 0, running_ = 0;
+    long long gen_ = 0;
+    bool stop_ = false;
+    std::string err_;
+};
+
+static Pool& pool() {
+    static Pool p;
+    return p;
+}
+
 class Tree {
 public:
     Tree(int nlevels, int skip) : nlevels_(nlevels), skip_(skip), bottoms_(nlevels), fine_(nlevels) {}
@@ -1556,26 +1678,369 @@ public:
         rec(3, cols_before, c->cols(), C.cols, c->rows(), 0, c->order);
     }
 
+    // -------- wave-parallel execution (CPU baseline timing only) --------
+    // With threads_ > 1 the square, scaled, order-1 factorization runs each
+    // level's elimination, scaling and sparsification as conflict-free waves
+    // on host threads, and the solve runs its op tape the same way. A task
+    // joins the wave after the last earlier task that touched any of its
+    // blocks (or solution segments), so every block sees its updates in the
+    // sequential order: the event log and every number are bitwise those of
+    // the sequential path (tests/test_oracle_parallel.py). Graph changes (fill
+    // edges, new clusters, op records, counters, log records) are made on one
+    // thread in the sequential order; only the dense arithmetic is spread.
+    int threads_ = 1;
+    bool par_ok() const { return threads_ > 1 && square_ && scale_ && order_ != 1.5f && tol_ != 0; }
+
+    // wave of each of n tasks; touch(i, keys) lists task i's keys (nullptr: all)
+    template <class Touch>
+    static std::vector<int> waves_of(int n, Touch touch) {
+        std::unordered_map<const void*, int> last;
+        std::vector<int> w(n);
+        std::vector<const void*> keys;
+        int barrier = -1, top = -1;
+        for (int i = 0; i < n; ++i) {
+            keys.clear();
+            touch(i, keys);
+            int wv = barrier + 1;
+            bool all = false;
+            for (const void* k : keys) {
+                if (!k) { all = true; break; }
+                auto it = last.find(k);
+                if (it != last.end()) wv = std::max(wv, it->second + 1);
+            }
+            if (all) {
+                wv = top + 1;
+                barrier = wv;
+            } else {
+                for (const void* k : keys) last[k] = wv;
+            }
+            w[i] = wv;
+            top = std::max(top, wv);
+        }
+        return w;
+    }
+
+    // Runs f(i) for every task, wave by wave. A wave of one task keeps the
+    // BLAS thread count the caller set (orc_blas_threads), a wider wave runs
+    // one BLAS thread per task. OpenBLAS's threaded kernels round differently
+    // from its one-thread kernels, so the results are bitwise the sequential
+    // path's when BLAS runs one thread, and agree to rounding otherwise.
+    template <class F>
+    void run_waves(const std::vector<int>& wave, F f) {
+        int nw = 0;
+        for (int v : wave) nw = std::max(nw, v + 1);
+        std::vector<std::vector<int>> by(nw);
+        for (int i = 0; i < (int)wave.size(); ++i) by[wave[i]].push_back(i);
+        const Lapack& l = L();
+        const int blas = l.get_threads ? l.get_threads() : 1;
+        for (auto& g : by) {
+            if (g.empty()) continue;
+            if (l.set_threads && blas > 1) l.set_threads(g.size() == 1 ? blas : 1);
+            pool().run((int)g.size(), threads_, [&](int q) { f(g[q]); });
+        }
+        if (l.set_threads && blas > 1) l.set_threads(blas);
+    }
+
+    struct ElimTask {
+        Cluster* c;
+        std::vector<Edge*> col;                  // stacked column blocks
+        std::vector<Cluster*> upd;               // updated clusters (rsparsity order)
+        std::vector<std::vector<Edge*>> blocks;  // per updated cluster: its blocks in stacking order
+        int num_rows = 0, num_cols = 0;
+    };
+
+    // eliminate_cluster over the level's interiors (src/tree.cpp:780-832)
+    void eliminate_level_par() {
+        std::vector<ElimTask> tasks;
+        for (Cluster* c : bottom_current()) {
+            if (c->level() != ilvl_) continue;
+            ElimTask t;
+            t.c = c;
+            if (c->cols() > 0) {
+                for (Edge* e : c->edgesOut)
+                    if (e->A) { t.col.push_back(e); t.num_rows += e->A->rows; t.num_cols = e->A->cols; }
+                for (Cluster* n : c->rsparsity) {
+                    if (n->eliminated || c == n) continue;
+                    std::vector<Edge*> bl;
+                    for (Edge* e : t.col) {
+                        Edge* ecn = find_out(n, e->n2);
+                        if (!ecn) ecn = add_edge(n, e->n2);
+                        bl.push_back(ecn);
+                    }
+                    t.upd.push_back(n);
+                    t.blocks.push_back(std::move(bl));
+                }
+            }
+            c->eliminated = true;
+            tasks.push_back(std::move(t));
+        }
+        auto wave = waves_of((int)tasks.size(), [&](int i, std::vector<const void*>& k) {
+            for (Edge* e : tasks[i].col) k.push_back(e);
+            for (auto& bl : tasks[i].blocks)
+                for (Edge* e : bl) k.push_back(e);
+        });
+        run_waves(wave, [&](int i) {
+            ElimTask& t = tasks[i];
+            Cluster* c = t.c;
+            if (c->cols() == 0) return;
+            Mat Q(t.num_rows, t.num_cols);
+            int cur = 0;
+            for (Edge* e : t.col) { Q.set_block(cur, 0, *e->A); cur += e->A->rows; }
+            int k = std::min(t.num_rows, t.num_cols);
+            c->tau.assign(k, 0.0);
+            c->T = Mat(k, k);
+            geqrf(Q, c->tau);
+            cur = 0;
+            for (Edge* e : t.col) { *e->A = Q.block(cur, 0, e->A->rows, e->A->cols); cur += e->A->rows; }
+            larft(Q, c->tau, c->T);
+            for (size_t u = 0; u < t.upd.size(); ++u) {
+                Mat V(Q.rows, t.upd[u]->cols());
+                cur = 0;
+                for (Edge* e : t.blocks[u]) { V.set_block(cur, 0, *e->A); cur += e->A->rows; }
+                larfb_lt(Q, c->T, V.data(), V.rows, V.cols);
+                cur = 0;
+                for (Edge* e : t.blocks[u]) { *e->A = V.block(cur, 0, e->A->rows, e->A->cols); cur += e->A->rows; }
+            }
+        });
+        for (ElimTask& t : tasks) {
+            Cluster* c = t.c;
+            if (c->cols() == 0) { rec(1, 0, 0, 0, 0, 0, c->order); continue; }
+            nnzH_ += (unsigned long long)(t.num_rows * t.num_cols);
+            int wtr = 0;
+            for (Cluster* n : t.upd) {
+                nnzR_ += (unsigned long long)(c->cols() * n->cols());
+                wtr += n->cols();
+            }
+            ops_.emplace_back(new OpQR(c));
+            rec(1, t.num_rows, t.num_cols, (long long)t.upd.size(), (long long)t.col.size(), wtr, c->order);
+        }
+    }
+
+    struct ScaleTask {
+        Cluster* c;
+        Edge* self;
+        std::vector<Edge*> rowb, colb;
+        Mat Q;
+        std::vector<double> tau;
+        int wrow = 0, hcol = 0;
+    };
+
+    // diag_scale over the level's interfaces (src/tree.cpp:533-580), square
+    void scale_level_par() {
+        std::vector<ScaleTask> tasks;
+        for (Cluster* c : bottom_current()) {
+            if (!want_sparsify(c)) continue;
+            ScaleTask t;
+            t.c = c;
+            t.self = c->self_edge();
+            for (Edge* ei : c->edgesIn)
+                if (!ei->n1->eliminated) t.rowb.push_back(ei);
+            for (Edge* eo : c->edgesOut)
+                if (!eo->n2->eliminated && eo->n2 != c) t.colb.push_back(eo);
+            tasks.push_back(std::move(t));
+        }
+        auto wave = waves_of((int)tasks.size(), [&](int i, std::vector<const void*>& k) {
+            k.push_back(tasks[i].self);
+            for (Edge* e : tasks[i].rowb) k.push_back(e);
+            for (Edge* e : tasks[i].colb) k.push_back(e);
+        });
+        run_waves(wave, [&](int i) {
+            ScaleTask& t = tasks[i];
+            Cluster* c = t.c;
+            t.Q = *t.self->A;
+            t.tau.assign(c->cols(), 0.0);
+            geqrf(t.Q, t.tau);
+            Mat T(c->cols(), c->cols());
+            larft(t.Q, t.tau, T);
+            Mat R(c->cols(), c->cols());
+            for (int j = 0; j < c->cols(); ++j)
+                for (int r = 0; r <= j; ++r) R(r, j) = t.Q(r, j);
+            Mat& D = *t.self->A;
+            for (int j = 0; j < D.cols; ++j)
+                for (int r = 0; r < D.rows; ++r) D(r, j) = (r == j) ? 1.0 : 0.0;
+            for (Edge* ei : t.rowb) {
+                larfb_lt(t.Q, T, ei->A->data(), ei->A->rows, ei->A->cols);
+                t.wrow += ei->A->cols;
+            }
+            for (Edge* eo : t.colb) {
+                trsm_right_upper(R, *eo->A);
+                t.hcol += eo->A->rows;
+            }
+        });
+        for (ScaleTask& t : tasks) {
+            Cluster* c = t.c;
+            nnzR_ = (unsigned long long)((double)nnzR_ + 0.5 * c->cols() * c->cols());
+            nnzH_ += (unsigned long long)(c->rows() * c->cols());
+            rec(2, c->rows(), c->cols(), (long long)t.rowb.size(), (long long)t.colb.size(),
+                (long long)t.wrow * 100000 + t.hcol, c->order);
+            ops_.emplace_back(new OpScaleD(c, std::move(t.Q), std::move(t.tau), true));
+        }
+    }
+
+    struct SparsTask {
+        Cluster* c;
+        Edge* self = nullptr;
+        std::vector<Edge*> in, out;  // Apm (row blocks) and Amp (column blocks)
+        int cols_before = 0, rows_before = 0, ccols = 0, rank = 0;
+        bool split = false;
+        Mat v;
+        std::vector<double> h;
+    };
+
+    // sparsifyD over the level's interfaces (src/tree.cpp:992-1114), square, order 1
+    void sparsify_level_par() {
+        std::vector<SparsTask> tasks;
+        for (Cluster* c : bottom_current()) {
+            if (!want_sparsify(c)) continue;
+            SparsTask t;
+            t.c = c;
+            for (Edge* e : c->edgesIn)
+                if (!e->n1->eliminated) t.in.push_back(e);
+            for (Edge* e : c->edgesOut) {
+                if (!e->n2->eliminated && e->n2 != c) t.out.push_back(e);
+                else if (e->n2 == c) t.self = e;
+            }
+            tasks.push_back(std::move(t));
+        }
+        auto wave = waves_of((int)tasks.size(), [&](int i, std::vector<const void*>& k) {
+            if (tasks[i].self) k.push_back(tasks[i].self);
+            for (Edge* e : tasks[i].in) k.push_back(e);
+            for (Edge* e : tasks[i].out) k.push_back(e);
+        });
+        // numbers and this task's own blocks and sizes; ops, the fine cluster
+        // and the log record follow below in task order
+        run_waves(wave, [&](int i) {
+            SparsTask& t = tasks[i];
+            Cluster* c = t.c;
+            t.cols_before = c->cols();
+            t.rows_before = c->rows();
+            if (c->cols() == 0) return;
+            int spm = 0, smp = 0;
+            for (Edge* e : t.in) spm += e->A->cols;
+            for (Edge* e : t.out) smp += e->A->rows;
+            Mat C(c->cols(), spm + smp);
+            Mat Apmc(c->rows(), spm);
+            int cur = 0;
+            for (Edge* e : t.in) { Apmc.set_block(0, cur, *e->A); cur += e->A->cols; }
+            cur = 0;
+            for (Edge* e : t.out) {
+                const Mat& m = *e->A;
+                for (int j = 0; j < m.cols; ++j)
+                    for (int r = 0; r < m.rows; ++r) C(j, cur + r) = m(r, j);
+                cur += m.rows;
+            }
+            for (int j = 0; j < spm; ++j)
+                for (int r = 0; r < c->cols(); ++r) C(r, smp + j) = Apmc(r, j);
+            std::vector<int> jpvt(C.cols, 0);
+            std::vector<double> tt(std::min(C.rows, C.cols), 0.0);
+            geqp3(C, jpvt, tt);
+            std::vector<double> rii(std::min(C.rows, C.cols));
+            for (size_t q = 0; q < rii.size(); ++q) rii[q] = C(q, q);
+            const int rank = choose_rank(rii, tol_);
+            t.rank = rank;
+            t.ccols = C.cols;
+            if (rank >= C.rows) return;
+            t.split = true;
+            t.v = C.block(0, 0, C.rows, rank);
+            t.h.assign(tt.begin(), tt.begin() + rank);
+            Mat Cr(rank, C.cols);
+            for (int q = 0; q < C.cols; ++q)
+                for (int r = 0; r < rank && r <= q; ++r) Cr(r, jpvt[q]) = C(r, q);
+            const int cf_csize = c->cols() - rank;
+            Mat selfb(c->rows() - cf_csize, rank);
+            for (int j = 0; j < rank; ++j)
+                for (int r = 0; r < rank; ++r) selfb(r, j) = (*t.self->A)(r, j);
+            c->reset_size(rank, rank);  // square: rank rows
+            cur = 0;
+            for (Edge* e : t.out) {
+                Mat& m = *e->A;
+                Mat nm(m.rows, rank);
+                for (int j = 0; j < rank; ++j)
+                    for (int r = 0; r < m.rows; ++r) nm(r, j) = Cr(j, cur + r);
+                cur += m.rows;
+                m = std::move(nm);
+            }
+            int cc = cur;
+            for (Edge* e : t.in) {
+                Mat& m = *e->A;
+                Mat nm(c->rows(), m.cols);
+                for (int j = 0; j < m.cols; ++j)
+                    for (int r = 0; r < c->cols(); ++r) nm(r, j) = Cr(r, cc + j);
+                cc += m.cols;
+                m = std::move(nm);
+            }
+            *t.self->A = selfb.top_rows(c->rows());
+        });
+        for (SparsTask& t : tasks) {
+            Cluster* c = t.c;
+            if (t.cols_before == 0) { rec(3, 0, 0, 0, c->rows(), 0, c->order); continue; }
+            if (!t.split) { rec(3, t.cols_before, c->cols(), t.ccols, c->rows(), 0, c->order); continue; }
+            ops_.emplace_back(new OpOrthD(c, std::move(t.v), std::move(t.h), t.cols_before));
+            nnzQ_ += (unsigned long long)(t.cols_before * t.rank);
+            const int cf_csize = t.cols_before - t.rank;
+            Cluster* cf = new_cluster(c->cstart + t.rank, cf_csize, c->rstart + t.cols_before - cf_csize, cf_csize,
+                                      c->id);
+            ops_.emplace_back(new OpSplitD(c, cf, t.rank, t.rows_before, t.cols_before));
+            fine_[ilvl_].push_back(cf);
+            cf->eliminated = true;
+            rec(3, t.cols_before, c->cols(), t.ccols, c->rows(), 0, c->order);
+        }
+    }
+
+    // solve tape as waves: forward ops in order, backward ops in reverse order
+    std::vector<int> fwd_wave_, bwd_wave_;
+    void plan_solve_waves() {
+        const int n = (int)ops_.size();
+        fwd_wave_ = waves_of(n, [&](int i, std::vector<const void*>& k) { ops_[i]->touch(true, k); });
+        std::vector<int> b = waves_of(n, [&](int i, std::vector<const void*>& k) { ops_[n - 1 - i]->touch(false, k); });
+        bwd_wave_ = b;
+    }
+    void solve_par(const double* bin, double* xout) {
+        if (fwd_wave_.size() != ops_.size()) plan_solve_waves();
+        std::vector<double> b(nrows_);
+        for (int k = 0; k < nrows_; ++k) b[k] = bin[rperm_[k]];
+        for (Cluster* c : bottom_original())
+            for (int i = 0; i < c->rsize_org; ++i) c->x[i] = b[c->rstart + i];
+        const int n = (int)ops_.size();
+        run_waves(fwd_wave_, [&](int i) { ops_[i]->fwd(); });
+        run_waves(bwd_wave_, [&](int i) { ops_[n - 1 - i]->bwd(); });
+        std::vector<double> x(ncols_);
+        for (Cluster* c : bottom_original())
+            for (int i = 0; i < c->csize_org; ++i) x[c->cstart + i] = c->x[i];
+        for (int k = 0; k < ncols_; ++k) xout[cperm_[k]] = x[k];
+    }
+
     // -------- factorize (src/tree.cpp:1309-1437) --------
     void factorize() {
         double t0 = now();
         for (ilvl_ = 0; ilvl_ < nlevels_; ++ilvl_) {
             for (Cluster* s : bottom_current())
                 if (s->level() == ilvl_) get_sparsity(s);
-            for (Cluster* s : bottom_current())
-                if (s->level() == ilvl_) eliminate_cluster(s);
+            if (par_ok()) {
+                eliminate_level_par();
+            } else {
+                for (Cluster* s : bottom_current())
+                    if (s->level() == ilvl_) eliminate_cluster(s);
+            }
             if (ilvl_ < nlevels_ - 1 && !square_)
                 for (Cluster* s : bottom_current())
                     if (s->eliminated) reassign_rows(s);
-            if (scale_ && ilvl_ < nlevels_ - 2 && ilvl_ >= skip_ && tol_ != 0)
-                for (Cluster* s : bottom_current())
-                    if (want_sparsify(s)) diag_scale(s);
+            if (scale_ && ilvl_ < nlevels_ - 2 && ilvl_ >= skip_ && tol_ != 0) {
+                if (par_ok()) {
+                    scale_level_par();
+                } else {
+                    for (Cluster* s : bottom_current())
+                        if (want_sparsify(s)) diag_scale(s);
+                }
+            }
             if (ilvl_ >= skip_ && ilvl_ < nlevels_ - 2 && tol_ != 0) {
                 if (scale_ && !square_)
                     for (Cluster* s : bottom_current())
                         if (want_sparsify(s)) sparsify_extra(s);
+                const bool par = par_ok();
+                if (par) sparsify_level_par();
                 for (Cluster* s : bottom_current()) {
-                    if (!want_sparsify(s)) continue;
+                    if (par || !want_sparsify(s)) continue;
                     if (scale_) sparsifyD(s, order_ == 1.5f);
                     else if (square_) sparsify(s);
                     else throw std::runtime_error("--scale 0 is restated for square systems only");
@@ -1591,6 +2056,7 @@ public:
 
     // -------- solves (src/tree.cpp:1440-1517) --------
     void solve(const double* bin, double* xout) {
+        if (threads_ > 1 && square_) { solve_par(bin, xout); return; }
         std::vector<double> b(nrows_);
         for (int k = 0; k < nrows_; ++k) b[k] = bin[rperm_[k]];
         for (Cluster* c : bottom_original())
@@ -1856,6 +2322,11 @@ int orc_blas_threads(int n) {
     if (!l) { g_last_error = err; return -1; }
     if (n > 0 && l->set_threads) l->set_threads(n);
     return l->get_threads ? l->get_threads() : 1;
+}
+int orc_set_threads(orc_tree* t, int n) {
+    if (!t || n < 1) { g_last_error = "threads must be >= 1"; return -1; }
+    t->t->threads_ = n;
+    return 0;
 }
 int orc_set_coords(orc_tree* t, int d, int n, const double* X) {
     return guarded([&] {

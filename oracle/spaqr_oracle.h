@@ -30,6 +30,11 @@ orc_tree* orc_create(int nlevels, int skip, double tol, int scale, float order, 
 void orc_destroy(orc_tree* t);
 const char* orc_last_error(void);
 int orc_blas_threads(int nthreads); /* sets OpenBLAS threads; returns the count in use */
+/* Host threads for the factorization and the solve (default 1). With n > 1
+ * a square, scaled, order-1 factorization runs each level phase as
+ * conflict-free waves of tasks on n threads, and the solve runs its op tape in
+ * waves: bitwise the sequential results, used to time the CPU baseline. */
+int orc_set_threads(orc_tree* t, int n);
 
 /* Coordinates: d x n, column-major (set_Xcoo). */
 int orc_set_coords(orc_tree* t, int d, int n, const double* X);
