@@ -230,18 +230,64 @@ def e2e_step(w, A, b, precision, device):
     return sec, res, h2d, d2h
 
 
-def roofline(info, peaks):
-    """Dominant kernel family of the instrumented step, its algorithmic bytes per
-    launch over its average CUDA-event duration, against the measured HBM copy
-    bandwidth (all families are bandwidth/latency bound here: FP64 and FP32
-    SIMT work with no measured FP64 peak to compare against)."""
+def pipe_peaks():
+    """Measured arithmetic peaks of this GPU's pipes (FP32 / FP64 FMA, TF32 and
+    FP64 mma.sync): the library's microbenchmark run live (best of 5 CUDA-event
+    launches), else the committed PIPE_PEAKS.json of an earlier run."""
+    exe = os.path.join(ROOT, "spaqr_public_b200", "_build", "spq_pipe_peaks")
+    try:
+        out = subprocess.run([exe, str(int(os.environ.get("LOCAL_RANK", "0")))], capture_output=True, text=True,
+                             timeout=120, check=True).stdout
+        d = json.loads(out.strip().splitlines()[-1])
+        d["source"] = "measured live (spq_pipe_peaks)"
+        return d
+    except Exception:
+        try:
+            d = json.load(open(os.path.join(ROOT, "PIPE_PEAKS.json")))
+            d["source"] = "PIPE_PEAKS.json (spq_pipe_peaks, earlier run)"
+            return d
+        except Exception:
+            return {}
+
+
+# family -> (bound, pipe of the FP32 form, pipe of the FP64 form): the QR,
+# RRQR and TRSM kernels are arithmetic on SIMT FMA pipes, the trailing update
+# on the tensor pipe (3xTF32 / DMMA mma.sync); copies and write-backs are HBM
+PIPES = {"rrqr": ("compute", "fp32_fma_tflops", "fp64_fma_tflops"),
+         "panel_qr": ("compute", "fp32_fma_tflops", "fp64_fma_tflops"),
+         "trsm": ("compute", "fp32_fma_tflops", "fp64_fma_tflops"),
+         "trailing_update": ("tensor", "tf32_mma_tflops", "fp64_mma_tflops")}
+
+
+def families(info, pipes, fp32):
+    out = {}
+    for k, v in info["kernels"].items():
+        e = {"launches": v["launches"], "ms": round(v["ms"], 3),
+             "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None,
+             "GFLOPs": round(v["flops"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None}
+        if k in PIPES and v["ms"] and pipes:
+            pipe = PIPES[k][1 if fp32 else 2]
+            if pipe in pipes:
+                e["pipe"] = pipe
+                e["frac_of_pipe"] = round(v["flops"] / (v["ms"] / 1e3) / 1e12 / pipes[pipe], 5)
+        out[k] = e
+    return out
+
+
+def roofline(info, peaks, pipes, info64=None):
+    """Dominant kernel family of the instrumented FP32-form step. A factor kernel
+    is reported against the measured peak of the pipe it runs on (algorithmic
+    flops per launch over the average CUDA-event launch time; for the 3xTF32
+    trailing update the flops are counted once against the TF32 peak, so its
+    ceiling is a third of the pipe); a copy kernel against the measured HBM
+    copy bandwidth (algorithmic bytes: inputs read once, outputs written once)."""
     fams = info["kernels"]
     dom = max((k for k in fams if k != "precond_apply"), key=lambda k: fams[k]["ms"])
     f = fams[dom]
-    per_launch_s = f["ms"] / 1e3 / max(f["launches"], 1)
-    bytes_per_launch = f["bytes"] / max(f["launches"], 1)
-    achieved = bytes_per_launch / per_launch_s / 1e9
-    peak = peaks.get("hbm_gbs", 6650.0)
+    n = max(f["launches"], 1)
+    per_launch_s = f["ms"] / 1e3 / n
+    bytes_per_launch = f["bytes"] / n
+    flops_per_launch = f["flops"] / n
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.txt")  # "family bytes_per_launch" lines from ncu
     if os.path.exists(prof):
@@ -250,16 +296,25 @@ def roofline(info, peaks):
             if len(f2) == 2 and not ln.startswith("#") and f2[0] == dom:
                 traffic = float(f2[1])
     total_ms = sum(v["ms"] for v in fams.values())
-    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 5), "traffic": traffic,
-            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
-            "share_of_kernel_time": round(f["ms"] / total_ms, 3) if total_ms else None,
-            "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": f["ms"] / max(f["launches"], 1),
-            "algorithmic_flops_per_launch": f["flops"] / max(f["launches"], 1),
-            "families": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
-                             "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None,
-                             "GFLOPs": round(v["flops"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] else None}
-                         for k, v in fams.items()}}
+    if dom in PIPES and PIPES[dom][1] in pipes:
+        bound, pipe = PIPES[dom][0], PIPES[dom][1]
+        achieved = flops_per_launch / per_launch_s / 1e12
+        peak, unit = pipes[pipe], "TFLOP/s"
+        source = f"{pipe}, {pipes.get('source', 'spq_pipe_peaks')}"
+    else:
+        bound, unit = "hbm", "GB/s"
+        achieved = bytes_per_launch / per_launch_s / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        source = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"
+    out = {"bound": bound, "kernel": dom, "achieved": round(achieved, 3), "peak": peak, "unit": unit,
+           "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": source,
+           "share_of_kernel_time": round(f["ms"] / total_ms, 3) if total_ms else None,
+           "algorithmic_bytes_per_launch": bytes_per_launch, "algorithmic_flops_per_launch": flops_per_launch,
+           "avg_launch_ms": f["ms"] / n, "hbm_GBps": round(bytes_per_launch / per_launch_s / 1e9, 1),
+           "families": families(info, pipes, True)}
+    if info64 is not None:
+        out["families_fp64"] = families(info64, pipes, False)
+    return out
 
 
 # --------------------------------------------------------------------------- CPU arm
@@ -382,9 +437,12 @@ def run_ours(args):
                 infos.append(info)
         mean = max_over_ranks(d, float(np.mean(times)))
         result[name] = dict(value=mean, times=times, info=infos[-1], clocks=clk.summary())
-    # instrumented step for the roofline (FP32 form, after the timed steps)
+    # instrumented steps for the roofline (after the timed steps): per-launch
+    # CUDA events of every kernel family, FP32 form and FP64 form
     _, pinfo = timed_step(w, A, csr, d_b, 1, local, profile=True)
-    rl = roofline(pinfo, peaks)
+    _, pinfo64 = timed_step(w, A, csr, d_b, 0, local, profile=True)
+    pipes = pipe_peaks()
+    rl = roofline(pinfo, peaks, pipes, pinfo64)
     # end to end through the public host API: three runs, the median reported
     # (a single wall-clock sample carries the host's and the driver's noise)
     e2e_runs = [e2e_step(w, A, b, 1, local) for _ in range(3)]
@@ -415,6 +473,7 @@ def run_ours(args):
                 "includes": "create+partition+assemble+factorize+refinement, host buffers"},
         "gpu_launches": inf["launches"]["total"],
         "roofline": rl,
+        "pipe_peaks": {k: v for k, v in pipes.items() if k.endswith("tflops") or k == "source"},
         "cpu_baseline": cpu,
         "clocks": f32["clocks"],
         "clocks_fp64": f64["clocks"],

@@ -267,6 +267,9 @@ public:
         alloc0_ = arena_.alloc_seconds() + desc_arena_.alloc_seconds();
         grow0_ = scratch_.grow_seconds();
         const int L = cfg_.nlevels;
+        // numeric status word of this factorization (zeroed arena memory):
+        // the QR and RRQR kernels OR kStat* bits into it
+        d_status_ = arena_.template alloc_n<int>(1);
         level_ev_.assign((size_t)L * 7, nullptr);
         for (auto& e : level_ev_) {
             cuda_check(cudaEventCreate(&e), "event");
@@ -323,10 +326,21 @@ public:
         const double tp0 = wall();
         build_solve_plan();
         t_plan_ = wall() - tp0;
+        int status = 0;
+        cuda_check(cudaMemcpyAsync(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status");
         cuda_check(cudaStreamSynchronize(stream_), "factorize");
+        status_ = status;
         pinned_.reset();
         factorized_ = true;
         t_fact_ = wall() - t0;
+        if (status) {
+            std::string what = "numeric failure in the factorization:";
+            if (status & kStatNonFinite) what += " a QR or RRQR pivot is NaN or Inf (non-finite values in A or in a factor)";
+            if (status & kStatRRQRNaN) what += "; a sparsification met columns without a finite norm";
+            if (status & kStatZeroPivot) what += (status & kStatNonFinite) ? ";" : "";
+            if (status & kStatZeroPivot) what += " an elimination or scaling QR has an exactly zero pivot (singular block)";
+            throw std::runtime_error(what);
+        }
         if (cfg_.verbose) {
             std::printf("Tolerance set: %.3e\nTime to factorize:  %.3e\n", cfg_.tol, t_fact_);
             std::printf("Size of top separator: %d\n", bottoms_[L - 1].empty() ? 0 : bottoms_[L - 1].front()->csize);
@@ -420,6 +434,8 @@ private:
     cudaStream_t side_ = nullptr;  // second branch of a solve wave (forked from and joined to stream_)
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Arena arena_;
+    int* d_status_ = nullptr;  // device status word of the current factorization
+    int status_ = 0;           // its value at the end of the factorization
     Arena desc_arena_{size_t(16) << 20};
     Scratch scratch_;
     PinnedStage pinned_;
@@ -735,7 +751,7 @@ private:
     }
     // Pure host work: reads the jobs, writes B (safe on any host thread).
     static void build_wave(const std::vector<QRJob>& jobs, const std::vector<TrsmTask<T>>& trsm, T* trbase,
-                           WaveBuild& B) {
+                           int* status, WaveBuild& B) {
         auto& g = B.g;
         auto& s = B.s;
         auto& qt = B.qt;
@@ -763,7 +779,7 @@ private:
                 c.pad = 0;
                 s.push_back(c);
             }
-            qt.push_back(QRTask<T>{j.fac, tr, j.tau, j.tp, j.m, j.k, j.ntr, 0});
+            qt.push_back(QRTask<T>{j.fac, tr, j.tau, j.tp, j.m, j.k, j.ntr, 0, status});
             maxk = std::max(maxk, j.k);
             maxR = std::max(maxR, j.m);
         }
@@ -860,7 +876,7 @@ private:
         const size_t tr_elems = wave_scratch_elems(jobs);
         T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(tr_elems, 1) * sizeof(T), stream_));
         WaveBuild B;
-        build_wave(jobs, trsm, trbase, B);
+        build_wave(jobs, trsm, trbase, d_status_, B);
         issue_wave(B, trsm, post, tw_wave);
     }
 
@@ -1113,7 +1129,7 @@ private:
         host_parallel_for(
             (size_t)nw,
             [&](size_t b, size_t e) {
-                for (size_t w = b; w < e; ++w) build_wave(wjobs[w], no_trsm, trbase, builds[w]);
+                for (size_t w = b; w < e; ++w) build_wave(wjobs[w], no_trsm, trbase, d_status_, builds[w]);
             },
             4);
         if (cfg_.verbose >= 3)
@@ -1296,7 +1312,8 @@ private:
             T* tail = C + (size_t)j.m * j.ld;  // tau, vn1, vn2
             int* ii = ib + jobs.size() + j.i_off;
             int* rk = ib + rt.size();
-            rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, j.ld, 0, cfg_.tol});
+            rt.push_back(RRQRTaskRM<T>{C, ii, ii + nn, tail, tail + nn, tail + 2 * nn, rk, j.m, j.n, j.ld, 0, cfg_.tol,
+                                         d_status_});
         }
         auto cluster_of = [](const Job& j) {
             const double w = (double)j.m * j.n;
@@ -1414,22 +1431,16 @@ private:
         for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
             const size_t rq = rqs[gi++];
             if (rq == SIZE_MAX) continue;
-            // algorithmic bytes: the norm pass, then per pivot step one read of the
-            // active rows x columns (dlaqps: C_bs^T v) plus a read and a write of the
-            // rows below each finished block (the rank-NB update); the unblocked
-            // kernel reads the active part twice and writes it once per step
-            const bool blocked = kv.first.first == 1;
-            const int nb = sizeof(T) == 4 ? 32 : 16;
+            // algorithmic work: the flops of dgeqp3 stopped at rank r, and the
+            // bytes of reading C once and writing its factor once (R's first r
+            // rows, the r reflectors); the kernels' per-step passes over C run
+            // from L2 and shared memory, so they are not counted as HBM bytes
             double f = 0, by = 0;
             for (int q : kv.second) {
                 const double m = jobs[q].m, n = jobs[q].n;
                 const int r = ranks[q] >= jobs[q].m ? std::min(jobs[q].m, jobs[q].n) : ranks[q];
                 f += 4 * m * n * r - 2.0 * r * r * (m + n) + 4.0 / 3.0 * r * r * r;
-                double words = m * n;
-                for (int k = 0; k < r; ++k) words += (m - k) * (n - k) * (blocked ? 1.0 : 3.0);
-                if (blocked)
-                    for (int ke = nb; ke < r; ke += nb) words += 2.0 * (m - ke) * (n - ke);
-                by += words * sizeof(T);
+                by += (m * n + r * n + m * r) * sizeof(T);
             }
             pend_[rq].flops = f;
             pend_[rq].bytes = by;
@@ -1540,7 +1551,7 @@ private:
                     fq.a12.push_back(A12{b.p, m, e->A.cols, e->n1});
                     coff += e->A.cols;
                 }
-                if (spm > 0) e2q.push_back(QRTask<T>{V, G, tau, tp, m, r, spm, 1});
+                if (spm > 0) e2q.push_back(QRTask<T>{V, G, tau, tp, m, r, spm, 1, d_status_});
                 tape_.push_back(std::move(fq));  // QR(cf) right after the SplitD, as the reference
             }
             // new shapes

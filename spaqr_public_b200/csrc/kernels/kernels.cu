@@ -8,6 +8,7 @@
 // downdating) so that ranks and reflectors agree with the reference's LAPACK
 // calls up to rounding.
 #include "kernels.hpp"
+#include "status.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -226,6 +227,7 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
         if (tid == 0) {
             pj[j] = beta;
             s_tau[j] = tau;
+            note_qr_pivot(t.status, beta);
         }
         // d[c] = P[j, c] + sum_{r > j} v_j[r] P[r, c] for every panel column c != j
         // (loads issued unconditionally from columns clamped to the panel, so
@@ -434,6 +436,289 @@ __global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, c
     }
 }
 
+// ------------------------------------------------------------------ trailing update on tensor cores
+// The same C <- C - V (T^T (V^T C)) on one tile of kTN columns, with both
+// products on the tensor pipe (warp-level mma.sync):
+//   FP32: 3xTF32 (each operand split into a TF32 head and a TF32 tail,
+//         hi*hi + hi*lo + lo*hi accumulated in FP32: FP32-level accuracy);
+//   FP64: DMMA m8n8k4 (IEEE FP64 products and sums).
+// Rows are staged in kRC-row chunks, column-major in shared memory (stride
+// kTCS: the fragment loads of both products and the coalesced staging and
+// write-back hit distinct banks). Y^T = C^T V: every warp owns fixed output
+// tiles and sums its tiles over all rows in order (no cross-warp reduction,
+// deterministic). Z = T^T Y on SIMT. C -= V Z per chunk: every warp owns
+// fixed tiles of the chunk, subtracted from the staged C, written back.
+constexpr int kTCS = kRC + 4;  // 68: column stride of the staged chunk (elements)
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+    hi = to_tf32(x);
+    lo = to_tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// acc += A B in 3xTF32: the two small cross terms first, then the head product
+__device__ __forceinline__ void mma_3xtf32(float (&d)[4], const uint32_t (&ah)[4], const uint32_t (&al)[4],
+                                           uint32_t bh0, uint32_t bh1, uint32_t bl0, uint32_t bl1) {
+    mma_tf32(d, al, bh0, bh1);
+    mma_tf32(d, ah, bl0, bl1);
+    mma_tf32(d, ah, bh0, bh1);
+}
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// Y^T(j, i) = sum over the chunk's rows r of C(r, j) V(r, i), accumulated into
+// the warp's tiles. Cs, Vs: column-major chunk (stride kTCS).
+// FP32: warp w owns the 16 x 8 tile (j0 = 16 (w >> 2), i0 = 8 (w & 3)).
+__device__ __forceinline__ void tc_yt_chunk(float (&acc)[4], const float* Cs, const float* Vs, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int j0 = 16 * (warp >> 2), i0 = 8 * (warp & 3);
+#pragma unroll 2
+    for (int k0 = 0; k0 < kRC; k0 += 8) {
+        uint32_t ah[4], al[4], bh0, bl0, bh1, bl1;
+        split_tf32(Cs[(j0 + g) * kTCS + k0 + t], ah[0], al[0]);
+        split_tf32(Cs[(j0 + g + 8) * kTCS + k0 + t], ah[1], al[1]);
+        split_tf32(Cs[(j0 + g) * kTCS + k0 + t + 4], ah[2], al[2]);
+        split_tf32(Cs[(j0 + g + 8) * kTCS + k0 + t + 4], ah[3], al[3]);
+        split_tf32(Vs[(i0 + g) * kTCS + k0 + t], bh0, bl0);
+        split_tf32(Vs[(i0 + g) * kTCS + k0 + t + 4], bh1, bl1);
+        mma_3xtf32(acc, ah, al, bh0, bh1, bl0, bl1);
+    }
+}
+// FP64: warp w owns the two 8 x 8 tiles (j0 = 8 (w >> 1), i0 = 16 (w & 1) + {0, 8}).
+__device__ __forceinline__ void tc_yt_chunk(double (&acc)[4], const double* Cs, const double* Vs, int warp,
+                                            int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int j0 = 8 * (warp >> 1), i0 = 16 * (warp & 1);
+    double d0[2] = {acc[0], acc[1]}, d1[2] = {acc[2], acc[3]};
+#pragma unroll 4
+    for (int k0 = 0; k0 < kRC; k0 += 4) {
+        const double a = Cs[(j0 + g) * kTCS + k0 + t];
+        mma_f64(d0, a, Vs[(i0 + g) * kTCS + k0 + t]);
+        mma_f64(d1, a, Vs[(i0 + 8 + g) * kTCS + k0 + t]);
+    }
+    acc[0] = d0[0];
+    acc[1] = d0[1];
+    acc[2] = d1[0];
+    acc[3] = d1[1];
+}
+// The warp's accumulated Y^T tiles into Ys as Y(i, j) = Ys[i * (kTN + 1) + j].
+__device__ __forceinline__ void tc_yt_store(const float (&acc)[4], float* Ys, int warp, int lane) {
+    constexpr int CP = kTN + 1;
+    const int g = lane >> 2, t = lane & 3;
+    const int j0 = 16 * (warp >> 2), i0 = 8 * (warp & 3);
+    Ys[(i0 + 2 * t) * CP + j0 + g] = acc[0];
+    Ys[(i0 + 2 * t + 1) * CP + j0 + g] = acc[1];
+    Ys[(i0 + 2 * t) * CP + j0 + g + 8] = acc[2];
+    Ys[(i0 + 2 * t + 1) * CP + j0 + g + 8] = acc[3];
+}
+__device__ __forceinline__ void tc_yt_store(const double (&acc)[4], double* Ys, int warp, int lane) {
+    constexpr int CP = kTN + 1;
+    const int g = lane >> 2, t = lane & 3;
+    const int j0 = 8 * (warp >> 1), i0 = 16 * (warp & 1);
+    Ys[(i0 + 2 * t) * CP + j0 + g] = acc[0];
+    Ys[(i0 + 2 * t + 1) * CP + j0 + g] = acc[1];
+    Ys[(i0 + 8 + 2 * t) * CP + j0 + g] = acc[2];
+    Ys[(i0 + 8 + 2 * t + 1) * CP + j0 + g] = acc[3];
+}
+
+// Z operand fragments of C -= V Z, kept in registers across the chunks.
+// FP32: warp w owns rows m0 = 16 (w >> 1) of the chunk and columns
+// n0 = 16 (w & 1) + {0, 8}; zf[nt][ks][0..3] = {hi(k0+t), hi(k0+t+4), lo(k0+t), lo(k0+t+4)}.
+struct ZFragF32 {
+    uint32_t z[2][4][4];
+};
+__device__ __forceinline__ void tc_z_load(ZFragF32& f, const float* Zs, int warp, int lane) {
+    constexpr int CP = kTN + 1;
+    const int g = lane >> 2, t = lane & 3;
+    const int n0 = 16 * (warp & 1);
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int c = n0 + 8 * nt + g, k0 = 8 * ks;
+            split_tf32(Zs[(k0 + t) * CP + c], f.z[nt][ks][0], f.z[nt][ks][2]);
+            split_tf32(Zs[(k0 + t + 4) * CP + c], f.z[nt][ks][1], f.z[nt][ks][3]);
+        }
+}
+// Cs(r, c) -= (V Z)(r, c) over the chunk (Vs, Cs column-major, stride kTCS).
+__device__ __forceinline__ void tc_cvz_chunk(float* Cs, const float* Vs, const ZFragF32& f, const float*, int warp,
+                                             int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = 16 * (warp >> 1), n0 = 16 * (warp & 1);
+    float d[2][4] = {};
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+        const int k0 = 8 * ks;
+        uint32_t ah[4], al[4];
+        split_tf32(Vs[(k0 + t) * kTCS + m0 + g], ah[0], al[0]);
+        split_tf32(Vs[(k0 + t) * kTCS + m0 + g + 8], ah[1], al[1]);
+        split_tf32(Vs[(k0 + t + 4) * kTCS + m0 + g], ah[2], al[2]);
+        split_tf32(Vs[(k0 + t + 4) * kTCS + m0 + g + 8], ah[3], al[3]);
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+            mma_3xtf32(d[nt], ah, al, f.z[nt][ks][0], f.z[nt][ks][1], f.z[nt][ks][2], f.z[nt][ks][3]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+        const int c = n0 + 8 * nt + 2 * t;
+        Cs[c * kTCS + m0 + g] -= d[nt][0];
+        Cs[(c + 1) * kTCS + m0 + g] -= d[nt][1];
+        Cs[c * kTCS + m0 + g + 8] -= d[nt][2];
+        Cs[(c + 1) * kTCS + m0 + g + 8] -= d[nt][3];
+    }
+}
+struct ZFragF64 {};
+__device__ __forceinline__ void tc_z_load(ZFragF64&, const double*, int, int) {}
+// FP64: warp w owns rows m0 = 8 w of the chunk and all four 8-column tiles;
+// the Z fragments are read from shared memory (Zs = Y(i, j) layout).
+__device__ __forceinline__ void tc_cvz_chunk(double* Cs, const double* Vs, const ZFragF64&, const double* Zs,
+                                             int warp, int lane) {
+    constexpr int CP = kTN + 1;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = 8 * warp;
+    double d[4][2] = {};
+#pragma unroll
+    for (int k0 = 0; k0 < kNB; k0 += 4) {
+        const double a = Vs[(k0 + t) * kTCS + m0 + g];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_f64(d[nt], a, Zs[(k0 + t) * CP + 8 * nt + g]);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        const int c = 8 * nt + 2 * t;
+        Cs[c * kTCS + m0 + g] -= d[nt][0];
+        Cs[(c + 1) * kTCS + m0 + g] -= d[nt][1];
+    }
+}
+
+template <class T>
+struct TcTraits;
+template <>
+struct TcTraits<float> {
+    using ZF = ZFragF32;
+};
+template <>
+struct TcTraits<double> {
+    using ZF = ZFragF64;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks, const TileRef* tiles, int p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int CP = kTN + 1, TP = kNB + 1;
+    constexpr int EPT = kRC * kNB / kThreads;  // 8 elements per thread per chunk (V and C each)
+    T* Vs = reinterpret_cast<T*>(smem_raw);  // kNB columns x kTCS, column-major
+    T* Cs = Vs + kNB * kTCS;                  // kTN columns x kTCS
+    T* Ys = Cs + kTN * kTCS;                  // kNB x CP: Y, then Z
+    T* Tsh = Ys + kNB * CP;                   // kNB x TP
+    __shared__ T* colp[kTN];
+    const TileRef tr = tiles[blockIdx.x];
+    const QRTask<T> t = tasks[tr.task];
+    const int m = t.m, k = t.k;
+    const int w = min(kNB, k - p);
+    const int R = m - p;
+    const int nf = t.tr_only ? 0 : k - p - w;
+    const int ntot = nf + t.ntr;
+    const int c0 = tr.tile * kTN;
+    const int tn = min(kTN, ntot - c0);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid < kTN) {
+        int vc = c0 + tid;
+        T* ptr = nullptr;
+        if (tid < tn) ptr = vc < nf ? t.fac + (size_t)(p + w + vc) * m : t.tr + (size_t)(vc - nf) * m;
+        colp[tid] = ptr;
+    }
+    const T* V0 = t.fac + (size_t)p * m;
+    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        int i = e % kNB, j = e / kNB;
+        Tsh[i * TP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
+    }
+    __syncthreads();
+    T vr[EPT], cr[EPT];
+    // element u of thread tid: row r = e % kRC, column q = e / kRC (coalesced along rows)
+    auto fetch = [&](int r0) {
+        const int rc = min(kRC, R - r0);
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            const int gr = r0 + r;
+            const T x = V0[p + min(gr, R - 1) + (size_t)min(q, w - 1) * m];
+            vr[u] = (r < rc && q < w) ? (gr < q ? T(0) : (gr == q ? T(1) : x)) : T(0);
+            const T y = colp[min(q, tn - 1)][p + r0 + min(r, rc - 1)];
+            cr[u] = (r < rc && q < tn) ? y : T(0);
+        }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            Vs[q * kTCS + r] = vr[u];
+            Cs[q * kTCS + r] = cr[u];
+        }
+    };
+    // Y^T = C^T V over all rows
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    fetch(0);
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+        stash();
+        __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC);
+        tc_yt_chunk(acc, Cs, Vs, warp, lane);
+        __syncthreads();
+    }
+    tc_yt_store(acc, Ys, warp, lane);
+    __syncthreads();
+    // Z = T^T Y (SIMT, 32 x 32 x 32)
+    {
+        const int c = tid % kTN, jq = tid / kTN;
+        constexpr int QPT = kNB / (kThreads / kTN);
+        T z[QPT];
+#pragma unroll
+        for (int u = 0; u < QPT; ++u) {
+            const int i = jq * QPT + u;
+            T s = T(0);
+            for (int l = 0; l <= i; ++l) s += Tsh[l * TP + i] * Ys[l * CP + c];
+            z[u] = s;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = z[u];
+        __syncthreads();
+    }
+    typename TcTraits<T>::ZF zf;
+    tc_z_load(zf, Ys, warp, lane);
+    // C -= V Z chunk by chunk, written back after each chunk
+    fetch(0);
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+        const int rc = min(kRC, R - r0);
+        stash();
+        __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC);
+        tc_cvz_chunk(Cs, Vs, zf, Ys, warp, lane);
+        __syncthreads();
+        for (int e = tid; e < kRC * kTN; e += blockDim.x) {
+            const int r = e % kRC, cc = e / kRC;
+            if (r < rc && cc < tn) colp[cc][p + r0 + r] = Cs[cc * kTCS + r];
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ TRSM (right, upper)
 template <class T>
 __global__ void __launch_bounds__(128) k_trsm(const TrsmTask<T>* tasks, const TileRef* tiles) {
@@ -476,6 +761,158 @@ __global__ void __launch_bounds__(128) k_trsm(const TrsmTask<T>* tasks, const Ti
         }
         if (active)
             for (int jj = 0; jj < wj; ++jj) t.X[row + (size_t)(J0 + jj) * t.ldx] = acc[jj];
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ TRSM on tensor cores
+// X(rows x k) <- X R^-1 (R upper k x k) on 128-row tiles, blocked by 32
+// columns: for block J, S = X(:, 0:J) R(0:J, J) on the tensor pipe (3xTF32 /
+// DMMA mma.sync, the finished blocks of X staged 32 columns at a time), then
+// each thread solves its row of (X(:, J) - S) against the 32 x 32 diagonal
+// block of R and stores it (the next blocks read it back).
+constexpr int kTrXS = 136;  // column stride of the staged X chunk (128 rows + pad)
+constexpr int kTrRS = 40;   // row stride of the staged R chunk (32 columns + pad)
+
+// S(32 rows of the warp, 32 columns) += Xc(:, 0:32) Rc(0:32, :)
+__device__ __forceinline__ void trsm_mma_chunk(float (&acc)[2][4][4], const float* Xs, const float* Rs, int warp,
+                                               int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = 32 * warp;
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 8) {
+        uint32_t ah[2][4], al[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int r = r0 + 16 * mt + g;
+            split_tf32(Xs[(k0 + t) * kTrXS + r], ah[mt][0], al[mt][0]);
+            split_tf32(Xs[(k0 + t) * kTrXS + r + 8], ah[mt][1], al[mt][1]);
+            split_tf32(Xs[(k0 + t + 4) * kTrXS + r], ah[mt][2], al[mt][2]);
+            split_tf32(Xs[(k0 + t + 4) * kTrXS + r + 8], ah[mt][3], al[mt][3]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            uint32_t bh0, bl0, bh1, bl1;
+            split_tf32(Rs[(k0 + t) * kTrRS + 8 * nt + g], bh0, bl0);
+            split_tf32(Rs[(k0 + t + 4) * kTrRS + 8 * nt + g], bh1, bl1);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) mma_3xtf32(acc[mt][nt], ah[mt], al[mt], bh0, bh1, bl0, bl1);
+        }
+    }
+}
+__device__ __forceinline__ void trsm_mma_store(const float (&acc)[2][4][4], float* Ss, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int r = 32 * warp + 16 * mt + g, c = 8 * nt + 2 * t;
+            Ss[r * (kNB + 1) + c] = acc[mt][nt][0];
+            Ss[r * (kNB + 1) + c + 1] = acc[mt][nt][1];
+            Ss[(r + 8) * (kNB + 1) + c] = acc[mt][nt][2];
+            Ss[(r + 8) * (kNB + 1) + c + 1] = acc[mt][nt][3];
+        }
+}
+// FP64: 4 x 4 tiles of 8 x 8 per warp (acc[mt][nt][2] viewed through the same shape)
+__device__ __forceinline__ void trsm_mma_chunk(double (&acc)[2][4][4], const double* Xs, const double* Rs, int warp,
+                                               int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = 32 * warp;
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) a[mt] = Xs[(k0 + t) * kTrXS + r0 + 8 * mt + g];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) b[nt] = Rs[(k0 + t) * kTrRS + 8 * nt + g];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                double* d = &acc[mt >> 1][nt][2 * (mt & 1)];
+                double dd[2] = {d[0], d[1]};
+                mma_f64(dd, a[mt], b[nt]);
+                d[0] = dd[0];
+                d[1] = dd[1];
+            }
+    }
+}
+__device__ __forceinline__ void trsm_mma_store(const double (&acc)[2][4][4], double* Ss, int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int r = 32 * warp + 8 * mt + g, c = 8 * nt + 2 * t;
+            const double* d = &acc[mt >> 1][nt][2 * (mt & 1)];
+            Ss[r * (kNB + 1) + c] = d[0];
+            Ss[r * (kNB + 1) + c + 1] = d[1];
+        }
+}
+
+template <class T>
+size_t trsm_tc_smem() {
+    return sizeof(T) * ((size_t)kNB * kTrXS + (size_t)kNB * kTrRS + (size_t)128 * (kNB + 1) + (size_t)kNB * (kNB + 1));
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const TileRef* tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* Xs = reinterpret_cast<T*>(smem_raw);  // 32 columns x kTrXS (column-major chunk of X)
+    T* Rs = Xs + kNB * kTrXS;                 // 32 rows x kTrRS (chunk of R)
+    T* Ss = Rs + kNB * kTrRS;                 // 128 x (kNB + 1): S, row-major
+    T* Rd = Ss + 128 * (kNB + 1);             // kNB x (kNB + 1): diagonal block
+    const TileRef tr = tiles[blockIdx.x];
+    const TrsmTask<T> t = tasks[tr.task];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = tr.tile * 128 + tid;
+    const bool active = row < t.rows;
+    const int rclamp = min(row, t.rows - 1);
+    for (int J0 = 0; J0 < t.k; J0 += kNB) {
+        const int wj = min(kNB, t.k - J0);
+        T acc[2][4][4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][b][c] = T(0);
+        for (int i0 = 0; i0 < J0; i0 += kNB) {  // J0 is a multiple of kNB: every chunk is full
+            // X(tile rows, i0:i0+32): thread = row, coalesced along rows
+#pragma unroll 4
+            for (int c = 0; c < kNB; ++c) {
+                const T x = t.X[rclamp + (size_t)(i0 + c) * t.ldx];
+                Xs[c * kTrXS + tid] = active ? x : T(0);
+            }
+            for (int e = tid; e < kNB * kNB; e += 128) {
+                const int i = e % kNB, jj = e / kNB;
+                Rs[i * kTrRS + jj] = jj < wj ? t.R[(i0 + i) + (size_t)(J0 + jj) * t.ldr] : T(0);
+            }
+            __syncthreads();
+            trsm_mma_chunk(acc, Xs, Rs, warp, lane);
+            __syncthreads();
+        }
+        trsm_mma_store(acc, Ss, warp, lane);
+        for (int e = tid; e < kNB * kNB; e += 128) {
+            const int i = e % kNB, jj = e / kNB;
+            Rd[i * (kNB + 1) + jj] = (i < wj && jj < wj) ? t.R[(J0 + i) + (size_t)(J0 + jj) * t.ldr] : T(1);
+        }
+        __syncthreads();
+        T x[kNB];
+#pragma unroll
+        for (int jj = 0; jj < kNB; ++jj)
+            x[jj] = (jj < wj ? t.X[rclamp + (size_t)(J0 + min(jj, wj - 1)) * t.ldx] : T(0)) - Ss[tid * (kNB + 1) + jj];
+#pragma unroll
+        for (int jj = 0; jj < kNB; ++jj) {
+            x[jj] = x[jj] / Rd[jj * (kNB + 1) + jj];
+#pragma unroll
+            for (int ll = jj + 1; ll < kNB; ++ll) x[ll] -= x[jj] * Rd[jj * (kNB + 1) + ll];
+        }
+        if (active) {
+#pragma unroll
+            for (int jj = 0; jj < kNB; ++jj)
+                if (jj < wj) t.X[row + (size_t)(J0 + jj) * t.ldx] = x[jj];
+        }
         __syncthreads();
     }
 }
@@ -1040,6 +1477,10 @@ size_t trailing_smem() {
     return sizeof(T) * ((size_t)kRC * TVP<T>::v + (size_t)kRC * (kTN + 1) + (size_t)kNB * (kTN + 1) +
                         (size_t)kNB * (kNB + 1));
 }
+template <class T>
+size_t trailing_tc_smem() {
+    return sizeof(T) * ((size_t)(kNB + kTN) * kTCS + (size_t)kNB * (kTN + 1) + (size_t)kNB * (kNB + 1));
+}
 
 }  // namespace
 
@@ -1061,13 +1502,13 @@ void launch_panel(const QRTask<T>* tasks, const int* ids, int ntasks, int p, int
 template <class T>
 void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s) {
     if (ntiles <= 0) return;
-    k_trailing<T><<<ntiles, kThreads, trailing_smem<T>(), s>>>(tasks, tiles, p);
+    k_trailing_tc<T><<<ntiles, kThreads, trailing_tc_smem<T>(), s>>>(tasks, tiles, p);
 }
 
 template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
     if (ntiles <= 0) return;
-    k_trsm<T><<<ntiles, 128, 0, s>>>(tasks, tiles);
+    k_trsm_tc<T><<<ntiles, 128, trsm_tc_smem<T>(), s>>>(tasks, tiles);
 }
 
 template <class T>
@@ -1158,6 +1599,9 @@ void prepare_kernels() {
     once_per_device(reinterpret_cast<const void*>(&k_panel<T>), [] {
         cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
         cudaFuncSetAttribute(k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem<T>());
+        cudaFuncSetAttribute(k_trailing_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)trailing_tc_smem<T>());
+        cudaFuncSetAttribute(k_trsm_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_tc_smem<T>());
         cudaFuncSetAttribute(k_solve_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     });
 }

@@ -44,8 +44,13 @@ struct QRTask {
     T* tau;
     T* tp;
     int m, k, ntr;
-    int tr_only;  // 1: the trailing updates touch tr only (fac holds finished reflectors: V of a sparsified interface)
+    int tr_only;          // 1: the trailing updates touch tr only (fac holds finished reflectors: V of a sparsified interface)
+    int* status = nullptr;  // device status word (kStat* bits), or none
 };
+// Bits of the device status word of a factorization.
+constexpr int kStatNonFinite = 1;  // NaN or Inf in a pivot (R_kk) of a QR or RRQR
+constexpr int kStatZeroPivot = 2;  // an exactly zero R_kk in an elimination or scaling QR
+constexpr int kStatRRQRNaN = 4;    // a sparsification RRQR found no finite column norm left
 struct TileRef {
     int task, tile;
 };
@@ -113,6 +118,7 @@ struct RRQRTaskRM {
     int* rank;
     int m, n, ldc, pad;
     double tol;
+    int* status = nullptr;  // device status word (kStat* bits), or none
 };
 template <class T>
 cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntasks, int cluster, int max_m,

@@ -30,6 +30,7 @@
 #include <algorithm>
 
 #include "kernels.hpp"
+#include "status.cuh"
 
 namespace spq {
 
@@ -181,7 +182,10 @@ __global__ void __launch_bounds__(kPThreads) k_panel_cl(const QRTask<T>* tasks, 
         s_d[warp][lane] = dm;
         if (cr == 0 && warp == 0) {
             if (lane < j) G[lane * kPS + j] = dm;  // v_lane^T v_j
-            if (lane == 0) s_tau[j] = tau;
+            if (lane == 0) {
+                s_tau[j] = tau;
+                note_qr_pivot(t.status, beta);
+            }
         }
         __syncwarp();
     }
@@ -350,6 +354,7 @@ __global__ void __launch_bounds__(kPThreads, ((sizeof(T) == 4 && kRPL < 16) || k
             tau = (beta - alpha) / beta;
             scal = T(1) / (alpha - beta);
         }
+        if (threadIdx.x == 0 && (!kCl || cr == 0)) note_qr_pivot(t.status, beta);
         T coef[CPW];
 #pragma unroll
         for (int q = 0; q < CPW; ++q) {

@@ -27,6 +27,7 @@
 
 #include "kernels.hpp"
 #include "rrqr_common.cuh"
+#include "status.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
         const int pc = gc;
         if (pc < 0) {  // no finite partial norm left (NaN input): stop here, uniformly over the cluster
             rank = k;
+            if (cr == 0 && tid == 0) note_rrqr_nan(t.status);
             break;
         }
         const int owner = pc / W;
@@ -186,6 +188,7 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
                 C[k * ld + pc] = beta;
                 t.tau[k] = tau;
             }
+            note_rrqr_pivot(tid == 0 ? t.status : nullptr, beta);
         }
         cl.sync();
         const T beta = *cl.map_shared_rank(&s_beta, owner);
