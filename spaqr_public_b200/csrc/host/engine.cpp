@@ -89,6 +89,7 @@ public:
         Cluster* f = nullptr;
         const T* fac = nullptr;
         const T* tp = nullptr;
+        const T* rinv = nullptr;  // R^-1 (k x k) of a QR / ScaleD op, formed after the factorization
         int m = 0, k = 0, ld = 0;
         std::vector<std::pair<Cluster*, int>> segs;
         std::vector<A12> a12;
@@ -2001,12 +2002,44 @@ private:
     }
 
     // ------------------------------------------------------------- solve plan
+    // R^-1 of every QR and ScaleD op with k <= kRinvMax: the identity (zeroed
+    // arena memory plus a unit diagonal) run through the TRSM, X <- X R^-1,
+    // once per factorization. The solve's triangular ops then apply R^-1 (or
+    // R^-T) as one product instead of a chain of diagonal blocks.
+    void form_rinv() {
+        std::vector<TrsmTask<T>> tasks;
+        std::vector<TileRef> tiles;
+        double f = 0, by = 0;
+        for (TapeOp& t : tape_) {
+            if (!((t.kind == TK_QR || t.kind == TK_SCALED) && t.fac != nullptr)) continue;
+            if (t.k < 1 || t.k > kRinvMax) continue;
+            T* X = arena_.template alloc_n<T>((size_t)t.k * t.k);
+            t.rinv = X;
+            const int id = (int)tasks.size();
+            tasks.push_back(TrsmTask<T>{t.fac, X, t.ld, t.k, t.k, t.k});
+            for (int r = 0; r < t.k; r += 128) tiles.push_back(TileRef{id, r / 128});
+            f += (double)t.k * t.k * t.k;
+            by += (1.5 * t.k * t.k) * sizeof(T);
+        }
+        if (tasks.empty()) return;
+        Upload up;
+        const size_t o_t = up.add(tasks), o_l = up.add(tiles);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
+        const TrsmTask<T>* dt = reinterpret_cast<const TrsmTask<T>*>(d + o_t);
+        launch_unit_diag<T>(dt, (int)tasks.size(), stream_);
+        timed(KF_TRSM, f, by, [&] {
+            launch_trsm<T>(dt, reinterpret_cast<const TileRef*>(d + o_l), (int)tiles.size(), stream_);
+        });
+        launches_fact_ += 2;
+    }
+
     void build_solve_plan() {
         if (rect_) {
             build_nrml_plan();
             return;
         }
         const double tq0 = wall();
+        form_rinv();
         int64_t xtot = 0;
         for (auto& c : clusters_) {
             c->xoff = xtot;
@@ -2049,24 +2082,24 @@ private:
                         f.wr.push_back(s.first);
                     }
                     f.smem = t.m;
-                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, (int)gemv.size(),
-                                   (int)t.a12.size()};
+                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0,
+                                   (int)gemv.size(), (int)t.a12.size()};
                     for (auto& a : t.a12) {
                         gemv.push_back(GemvRef<T>{ptr(a.B), a.n1->xoff, a.ld, a.s});
                         b.rd.push_back(a.n1);
                     }
                     b.rd.push_back(t.c);
                     b.wr.push_back(t.c);
-                    b.smem = t.k;
+                    b.smem = t.rinv ? 2 * t.k : t.k;
                     break;
                 }
                 case TK_SCALED:
                     f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
                     f.rd = f.wr = {t.c};
                     f.smem = t.m;
-                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, 0, 0};
+                    b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0, 0, 0};
                     b.rd = b.wr = {t.c};
-                    b.smem = t.k;
+                    b.smem = t.rinv ? 2 * t.k : t.k;
                     break;
                 case TK_ORTHD:
                     f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
@@ -2214,15 +2247,15 @@ private:
             switch (t.kind) {
                 case TK_QR: {
                     POp a{};
-                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, (int)gemv.size(),
-                                   (int)t.a12.size()};
+                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0,
+                                   (int)gemv.size(), (int)t.a12.size()};
                     for (auto& e : t.a12) {
                         gemv.push_back(GemvRef<T>{ptr(e.B), e.n1->xoff, e.ld, e.s});
                         a.rd.push_back(e.n1);
                     }
                     a.rd.push_back(t.c);
                     a.wr = a.rd;
-                    a.smem = t.k;
+                    a.smem = t.rinv ? 2 * t.k : t.k;
                     POp d = a;
                     d.op.dir = 0;
                     d.wr = {t.c};
@@ -2232,9 +2265,9 @@ private:
                 }
                 case TK_SCALED: {
                     POp a{};
-                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), 0, 0, 0, 0};
+                    a.op = SolveOp{SK_TRI, 1, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0, 0, 0};
                     a.rd = a.wr = {t.c};
-                    a.smem = t.k;
+                    a.smem = t.rinv ? 2 * t.k : t.k;
                     POp d = a;
                     d.op.dir = 0;
                     sa.push_back(a);

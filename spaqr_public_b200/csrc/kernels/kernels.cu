@@ -917,6 +917,14 @@ __global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const
     }
 }
 
+// X(i, i) = 1 for i < k of every task (X zeroed before): the identity that the
+// TRSM turns into R^-1.
+template <class T>
+__global__ void k_unit_diag(const TrsmTask<T>* tasks) {
+    const TrsmTask<T> t = tasks[blockIdx.x];
+    for (int i = threadIdx.x; i < t.k; i += blockDim.x) t.X[i + (size_t)i * t.ldx] = T(1);
+}
+
 // ------------------------------------------------------------------ assembly scatter
 template <class T>
 __global__ void k_scatter_values(const uint64_t* addr, const double* vals, int64_t n) {
@@ -1106,6 +1114,51 @@ __device__ void tri_solve(T* xs, int k, const T* R, int ldr, int trans, SolveSha
     }
 }
 
+// xs(0:k) <- Ri xs (trans 0) or Ri^T xs (trans 1) with Ri = R^-1 (k x k,
+// column-major, exactly zero below the diagonal), the inverse computed at the
+// end of the factorization: the triangular solve as one parallel product
+// instead of a chain of diagonal blocks. ys (k elements of shared memory)
+// holds the result until every thread is done reading xs.
+template <class T>
+__device__ void rinv_apply(T* xs, T* ys, int k, const T* Ri, int trans) {
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+    if (trans == 0) {
+        // thread i: row i of Ri; a warp starts at its first row's diagonal (the
+        // entries left of it are zero), so the warp's loads stay coalesced
+        for (int i0 = 0; i0 < k; i0 += nth) {
+            const int i = i0 + tid;
+            const int ic = min(i, k - 1);
+            const int jb = min(i0 + warp * 32, k - 1);
+            T a[4] = {T(0), T(0), T(0), T(0)};
+            int j = jb;
+            for (; j + 3 < k; j += 4) {
+                T r[4], x[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    r[u] = Ri[ic + (size_t)(j + u) * k];
+                    x[u] = xs[j + u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) a[u] += r[u] * x[u];
+            }
+            for (; j < k; ++j) a[0] += Ri[ic + (size_t)j * k] * xs[j];
+            if (i < k) ys[i] = (a[0] + a[1]) + (a[2] + a[3]);
+        }
+    } else {
+        // warp per row i of Ri^T (column i of Ri, contiguous): lanes stride j <= i
+        for (int i = warp; i < k; i += nw) {
+            const T* col = Ri + (size_t)i * k;
+            T a = T(0);
+            for (int j = lane; j <= i; j += 32) a += col[j] * xs[j];
+            a = warp_sum(a);
+            if (lane == 0) ys[i] = a;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < k; i += nth) xs[i] = ys[i];
+    __syncthreads();
+}
+
 // xs(0:k) -= sum_b B_b x_b over the neighbour blocks of a triangular op (B_b:
 // k x s_b, ld). Threads form G column groups of RT row threads; each thread
 // keeps kGU loads of B in flight (a block's last batch clamped to its last
@@ -1207,13 +1260,20 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_solve_step
             const bool has_r = op.p0 != 0;
             for (int i = tid; i < k; i += blockDim.x) xs[i] = x[op.x0 + i];
             __syncthreads();
+            const T* Ri = op.p1 != 0 ? aptr<T>(op.p1) : nullptr;  // R^-1 when it was formed
             if (op.dir == 0) {
                 gemv_sub(xs, k, gemv + op.seg0, op.nseg, x, sh);
                 __syncthreads();
-                if (has_r) tri_solve(xs, k, R, ldr, 0, sh);
+                if (Ri)
+                    rinv_apply(xs, xs + k, k, Ri, 0);
+                else if (has_r)
+                    tri_solve(xs, k, R, ldr, 0, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
             } else {
-                if (has_r) tri_solve(xs, k, R, ldr, 1, sh);
+                if (Ri)
+                    rinv_apply(xs, xs + k, k, Ri, 1);
+                else if (has_r)
+                    tri_solve(xs, k, R, ldr, 1, sh);
                 for (int i = tid; i < k; i += blockDim.x) x[op.x0 + i] = xs[i];
                 // x_n -= B_n^T xs: a warp takes 8 neighbour columns at a time (their
                 // loads in flight together; columns past the block re-read its last
@@ -1512,6 +1572,12 @@ void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cud
 }
 
 template <class T>
+void launch_unit_diag(const TrsmTask<T>* tasks, int ntasks, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_unit_diag<T><<<ntasks, 256, 0, s>>>(tasks);
+}
+
+template <class T>
 void launch_scatter_values(const uint64_t* addr, const double* vals, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
     k_scatter_values<T><<<grid_for(n, 256), 256, 0, s>>>(addr, vals, n);
@@ -1611,6 +1677,7 @@ void prepare_kernels() {
     template void launch_panel<T>(const QRTask<T>*, const int*, int, int, int, cudaStream_t);                 \
     template void launch_trailing<T>(const QRTask<T>*, const TileRef*, int, int, cudaStream_t);               \
     template void launch_trsm<T>(const TrsmTask<T>*, const TileRef*, int, cudaStream_t);                      \
+    template void launch_unit_diag<T>(const TrsmTask<T>*, int, cudaStream_t);                                   \
     template void launch_scatter_values<T>(const uint64_t*, const double*, int64_t, cudaStream_t);         \
     template void launch_solve_step<T>(const SolveOp*, int, const XSeg*, const GemvRef<T>*, const T*, T*, int, \
                                        cudaStream_t);                                                          \

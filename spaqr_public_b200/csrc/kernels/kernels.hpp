@@ -92,6 +92,11 @@ struct TrsmTask {
 };
 template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s);
+// X(i, i) = 1 for i < k of every task (with X zeroed, the identity whose TRSM by
+// R is R^-1; the solve's triangular ops of size <= kRinvMax use it).
+template <class T>
+void launch_unit_diag(const TrsmTask<T>* tasks, int ntasks, cudaStream_t s);
+constexpr int kRinvMax = 512;
 
 // ---------------------------------------------------------------- truncated RRQR
 // Write-back after the RRQR (sparsifyD, src/tree.cpp:1082-1110): rebuild the

@@ -48,6 +48,7 @@
 
 #include "kernels.hpp"
 #include "rrqr_common.cuh"
+#include "status.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -77,6 +78,52 @@ __host__ __device__ constexpr size_t blk_smem_elems(int Wp, int m) {
     return (size_t)(BlkNB<T>::v + kGMax + 3) * Wp + (size_t)((m + 7) & ~7) * (BlkNB<T>::v + 2);
 }
 
+// Partial products of pivot step k (3a below): part[g * Wp + c] = sum over the
+// rows of chunk g of C_bs(i, c) v(i), lanes owning KBU 16-byte column vectors.
+template <class T, int KBU>
+__device__ __forceinline__ void rrqr_partials(const T* C, size_t ld, int j0, int Wc, int Wp, int k, int m, int Gs,
+                                              int Lr, const T* vsh, T* part, int warp, int nw, int lane) {
+    constexpr int VEC = Vec<T>::n;
+    using VT = typename Vec<T>::type;
+    constexpr int kRowUnroll = sizeof(T) == 4 ? 4 : 2;
+    const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);
+    const int ntg = (nvt + KBU - 1) / KBU;
+    for (int item = warp; item < Gs * ntg; item += nw) {
+        const int g = item % Gs, tg = item / Gs;
+        const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
+        T sv[KBU][VEC];
+        const T* cp[KBU];
+#pragma unroll
+        for (int u = 0; u < KBU; ++u) {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sv[u][q] = T(0);
+            const int jl = ((tg * KBU + u) * 32 + lane) * VEC;
+            cp[u] = C + j0 + (jl < Wc ? jl : 0);  // past the slab: reads its first vector
+        }
+#pragma unroll kRowUnroll
+        for (int i = i0; i < i1; ++i) {
+            const T vi = vsh[i];
+            VT x[KBU];
+#pragma unroll
+            for (int u = 0; u < KBU; ++u) x[u] = *reinterpret_cast<const VT*>(cp[u] + i * ld);
+#pragma unroll
+            for (int u = 0; u < KBU; ++u) {
+                const T* xs = reinterpret_cast<const T*>(&x[u]);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) sv[u][q] += vi * xs[q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < KBU; ++u) {
+            const int jl = ((tg * KBU + u) * 32 + lane) * VEC;
+            if (jl < Wp) {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) part[g * Wp + jl + q] = sv[u][q];
+            }
+        }
+    }
+}
+
 template <class T>
 __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int Wp, int mpad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -92,10 +139,8 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
     T* vsh = vn2 + 2 * (size_t)Wp;                    // mpad: the current reflector (pos takes <= Wp elements)
     T* Vs = vsh + mpad;                               // mpad x VP: V_b(i, l) at i * VP + l
     __shared__ T red[32];
-    __shared__ T wv[32];
-    __shared__ int wp[32], wc[32];
-    __shared__ T s_val[2];
-    __shared__ int s_pos[2], s_col[2];
+    __shared__ T wv[2][32];  // per-warp pivot candidates, alternating slots by step parity
+    __shared__ int wp[2][32], wc[2][32];
     __shared__ T s_alpha;
     __shared__ int s_gp, s_gc, s_c0, s_nflag;
     __shared__ T s_aux[kBNB];    // V_b(k:m, l)^T v for l < jb, zero after
@@ -128,6 +173,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
         vn2[jl] = nv;
         pos[jl] = j0 + jl;
     }
+    if (tid == 0) s_c0 = -1;
     __syncthreads();
 
     const int kmax = min(m, n);
@@ -151,9 +197,8 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             k = k0 + jb;
             const int buf = k & 1;  // candidate slots alternate, so one cluster barrier per step suffices
             // 1. pivot: largest partial norm, ties to the smallest position; the
-            //    column now at position k is noted for the swap
-            if (tid == 0) s_c0 = -1;
-            __syncthreads();
+            //    column now at position k is noted for the swap (s_c0 is -1 here:
+            //    set before the first step, reset by its reader at every step)
             T bv = T(-1);
             int bp = INT_MAX, bc = -1;
             for (int jl = tid; jl < Wc; jl += nth) {
@@ -169,34 +214,51 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             }
             warp_best(bv, bp, bc);
             if (lane == 0) {
-                wv[warp] = bv;
-                wp[warp] = bp;
-                wc[warp] = bc;
+                wv[buf][warp] = bv;
+                wp[buf][warp] = bp;
+                wc[buf][warp] = bc;
             }
-            __syncthreads();
-            if (warp == 0) {
-                bv = lane < nw ? wv[lane] : T(-1);
-                bp = lane < nw ? wp[lane] : INT_MAX;
-                bc = lane < nw ? wc[lane] : -1;
-                warp_best(bv, bp, bc);
-                if (lane == 0) {
-                    s_val[buf] = bv;
-                    s_pos[buf] = bp;
-                    s_col[buf] = bc;
-                }
-            }
+            // the cluster barrier also orders this CTA's warps: every warp's candidate
+            // of every CTA is visible to all after it
             cl.sync();
-            if (warp == 0) {  // every CTA reduces the cluster's candidates (lane r reads CTA r)
+            // every CTA reduces all warps' candidates of the cluster (candidate q: CTA
+            // q / nw, warp q % nw; the order is immaterial, (value, position) is a
+            // strict order), then warp 0 fetches F(:, pc) from the pivot's owner
+            if (warp == 0) {
+                // all of a lane's candidate loads are issued before any is used,
+                // so the DSMEM round trips overlap
+                constexpr int kCand = (16 * (kBT / 32) + 31) / 32;  // <= 16 CTAs x warps per CTA, per lane
+                constexpr int kBatch = 4;
                 T v = T(-1);
                 int p = INT_MAX, c = -1;
-                if (lane < CL) {
-                    c = *cl.map_shared_rank(&s_col[buf], lane);
-                    if (c >= 0) {
-                        v = *cl.map_shared_rank(&s_val[buf], lane);
-                        p = *cl.map_shared_rank(&s_pos[buf], lane);
+#pragma unroll
+                for (int u0 = 0; u0 < kCand; u0 += kBatch) {
+                    if (32 * u0 >= CL * nw) break;  // uniform over the warp: no candidate left
+                    T vq[kBatch];
+                    int pq[kBatch], cq[kBatch];
+#pragma unroll
+                    for (int u = 0; u < kBatch; ++u) {
+                        const int q = lane + 32 * (u0 + u);
+                        const bool in = q < CL * nw;
+                        const int rk = in ? q / nw : 0, wq = in ? q % nw : 0;
+                        cq[u] = *cl.map_shared_rank(&wc[buf][wq], rk);
+                        vq[u] = *cl.map_shared_rank(&wv[buf][wq], rk);
+                        pq[u] = *cl.map_shared_rank(&wp[buf][wq], rk);
+                        if (!in) cq[u] = -1;
                     }
+#pragma unroll
+                    for (int u = 0; u < kBatch; ++u)
+                        if (cq[u] >= 0 && better(vq[u], pq[u], v, p)) {
+                            v = vq[u];
+                            p = pq[u];
+                            c = cq[u];
+                        }
                 }
                 warp_best(v, p, c);
+                if (c >= 0 && lane < kBNB) {
+                    const int ow = c / W;
+                    s_fp[lane] = *cl.map_shared_rank(&F[lane * Wp + (c - ow * W)], ow);
+                }
                 if (lane == 0) {
                     s_gp = p;
                     s_gc = c;
@@ -207,16 +269,14 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             if (pc < 0) {  // no finite partial norm left (NaN input): stop, uniformly over the cluster
                 rank = k;
                 done = true;
+                if (cr == 0 && tid == 0) note_rrqr_nan(t.status);
                 break;
             }
-            const int owner = pc / W;
             // 2. every CTA brings the pivot column up to date (C_bs - V_b F(pc, :)^T, F
             //    from the owner's shared memory) and builds the same reflector: the
             //    same inputs and the same arithmetic give bitwise the same v in every
             //    CTA, so v needs no broadcast. The owner stores the column at the end
             //    of the block, once no CTA reads its block-start values any more.
-            if (tid < kBNB) s_fp[tid] = *cl.map_shared_rank(&F[tid * Wp + (pc - owner * W)], owner);
-            __syncthreads();
             T acc = T(0);
             for (int i = k + tid; i < m; i += nth) {
                 T x = C[i * ld + pc];
@@ -228,7 +288,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 else
                     acc += x * x;
             }
-            const T xn2 = bsum(acc, red);
+            const T xn2 = bsum1(acc, red);
             const T alpha = s_alpha;
             T tau, beta, scal;
             if (xn2 == T(0)) {
@@ -277,6 +337,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 for (int q = 0; q < nw; ++q) sacc += s_wpart[q * kBNB + tid];
                 s_aux[tid] = tid < jb ? sacc : T(0);
             }
+            if (cr == 0 && tid == 0) note_rrqr_pivot(t.status, beta);
             if (tol != 0.0 && kmax > 1) {
                 if (k == 0) {
                     r00 = fabs(beta);
@@ -293,51 +354,26 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 // LAPACK's column swap, as positions of the slab's own columns
                 if (s_c0 >= 0) pos[s_c0 - j0] = gp;
                 if (pc >= j0 && pc < j1) pos[pc - j0] = k;
+                s_c0 = -1;
             }
             steps = jb + 1;
-            __syncthreads();
-            // 3a. partials of C_bs(k+1:m, slab)^T v: lanes own 16-byte column vectors
-            //     (kBU per lane), the rows are cut in Gs chunks taken by different warps
-            const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);
-            const int ntg = (nvt + kBU - 1) / kBU;
-            const int Gs = max(1, min(kGMax, (m - k - 1 + 31) / 32));
+            // no barrier here: 3a reads only the reflector (complete since the
+            // s_wpart barrier) and C; the positions, s_aux and the partials are
+            // read in 3b, after the barrier that closes 3a
+            // 3a. partials of C_bs(k+1:m, slab)^T v: lanes own 16-byte column vectors,
+            //     the rows are cut in Gs chunks of about 16 rows taken by different
+            //     warps; narrow slabs give each lane one vector (kBU = 1) so that more
+            //     warps share the pass. Each column's chunk sum runs over its rows in
+            //     order in one lane either way (bitwise the same), and Gs depends on
+            //     (m, k) only, so the result does not depend on the cluster size.
+            const int Gs = max(1, min(kGMax, (m - k - 1 + 15) / 16));
             const int Lr = (m - k - 1 + Gs - 1) / Gs;
-            constexpr int kRowUnroll = sizeof(T) == 4 ? 4 : 2;
             if (tau != T(0)) {
-                for (int item = warp; item < Gs * ntg; item += nw) {
-                    const int g = item % Gs, tg = item / Gs;
-                    const int i0 = k + 1 + g * Lr, i1 = min(m, i0 + Lr);
-                    T sv[kBU][VEC];
-                    const T* cp[kBU];
-#pragma unroll
-                    for (int u = 0; u < kBU; ++u) {
-#pragma unroll
-                        for (int q = 0; q < VEC; ++q) sv[u][q] = T(0);
-                        const int jl = ((tg * kBU + u) * 32 + lane) * VEC;
-                        cp[u] = C + j0 + (jl < Wc ? jl : 0);  // past the slab: reads its first vector
-                    }
-#pragma unroll kRowUnroll
-                    for (int i = i0; i < i1; ++i) {
-                        const T vi = vsh[i];
-                        VT x[kBU];
-#pragma unroll
-                        for (int u = 0; u < kBU; ++u) x[u] = *reinterpret_cast<const VT*>(cp[u] + i * ld);
-#pragma unroll
-                        for (int u = 0; u < kBU; ++u) {
-                            const T* xs = reinterpret_cast<const T*>(&x[u]);
-#pragma unroll
-                            for (int q = 0; q < VEC; ++q) sv[u][q] += vi * xs[q];
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < kBU; ++u) {
-                        const int jl = ((tg * kBU + u) * 32 + lane) * VEC;
-                        if (jl < Wp) {
-#pragma unroll
-                            for (int q = 0; q < VEC; ++q) part[g * Wp + jl + q] = sv[u][q];
-                        }
-                    }
-                }
+                const int nvt = (Wc + 32 * VEC - 1) / (32 * VEC);
+                if (Gs * ((nvt + kBU - 1) / kBU) >= nw)
+                    rrqr_partials<T, kBU>(C, ld, j0, Wc, Wp, k, m, Gs, Lr, vsh, part, warp, nw, lane);
+                else
+                    rrqr_partials<T, 1>(C, ld, j0, Wc, Wp, k, m, Gs, Lr, vsh, part, warp, nw, lane);
             }
             if (tid == 0) s_nflag = 0;
             __syncthreads();

@@ -32,6 +32,19 @@ __device__ __forceinline__ T bsum(T v, T* red) {
     return red[0];
 }
 
+// The same sum with one barrier: every warp reduces the per-warp slots itself
+// (the same butterfly over the same slots as bsum's warp 0, so bitwise the
+// same value). The caller guarantees a barrier between two calls on the same
+// red (no thread may still be reading the slots of the previous call).
+template <class T>
+__device__ __forceinline__ T bsum1(T v, T* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = wsum(v);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    return wsum(lane < nw ? red[lane] : T(0));
+}
+
 // LAPACK's tol3z = sqrt(unit roundoff): below it a downdated partial column
 // norm is recomputed (dlaqp2 / dlaqps).
 template <class T>
