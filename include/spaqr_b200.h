@@ -41,7 +41,7 @@ enum spq_status {
     SPQ_ERR_CUDA = 3,        /* CUDA runtime error (no device, launch failure, ...) */
     SPQ_ERR_NUMERIC = 4,     /* NaN/Inf or a zero pivot reported by a kernel */
     SPQ_ERR_ALLOC = 5,       /* device or host allocation failed */
-    SPQ_ERR_UNSUPPORTED = 6, /* option outside the built path (e.g. --scale 0, --hsl 1) */
+    SPQ_ERR_UNSUPPORTED = 6, /* option outside the built path (e.g. --hsl 1, --scale 0 on a least-squares system) */
     SPQ_ERR_NOCONV = 7       /* Krylov solver did not reach the tolerance */
 };
 
@@ -59,7 +59,8 @@ int spq_create(spq_tree** out, int nlevels, int skip);
 int spq_destroy(spq_tree* t);
 
 int spq_set_tol(spq_tree* t, double tol);      /* -t   (default 1e-1 in the CLI; 0 in Tree) */
-int spq_set_scale(spq_tree* t, int scale);     /* --scale */
+int spq_set_scale(spq_tree* t, int scale);     /* --scale: 1 sparsifyD after diagScale, 0 sparsify
+                                                  (src/tree.cpp:887-989; square systems) */
 int spq_set_order(spq_tree* t, float order);   /* --order 1 (sparsifyD) or 1.5 (sparsifyD_imp: keeps the E2 term) */
 int spq_set_hsl(spq_tree* t, int hsl);         /* --hsl (0 only) */
 int spq_set_square(spq_tree* t, int square);
@@ -74,6 +75,12 @@ int spq_set_coords_grid(spq_tree* t, int n, int d);             /* -n/-d tensor 
  * spq_partition computes it with spq_graph_parts, this library's recursive
  * bisection of the A^T A graph (host only; needs no GPU and no handle). */
 int spq_set_parts(spq_tree* t, int n, const int* parts);
+/* Fill rule of the ordering without coordinates. numeric = 1 (default): the
+ * reference's test, a fill candidate is kept only if the coupling product
+ * ||A(n, c)^T A(n, nin)|| exceeds 1e-14 (src/tree.cpp:856-859), evaluated on
+ * the device with one readback per level; 0: every candidate that passes the
+ * separator tests is kept (no readback). Ignored with coordinates. */
+int spq_set_fill_rule(spq_tree* t, int numeric);
 int spq_graph_parts(int m, int n, const int* colptr, const int* rowind, int nlevels, int* parts);
 int spq_set_precision(spq_tree* t, int precision);              /* spq_precision */
 int spq_set_device(spq_tree* t, int device);

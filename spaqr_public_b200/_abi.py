@@ -43,6 +43,7 @@ SIGNATURES = {
     "spq_set_coords": (_i, [_p, _i, _i, _dp]),
     "spq_set_coords_grid": (_i, [_p, _i, _i]),
     "spq_set_parts": (_i, [_p, _i, _ip]),
+    "spq_set_fill_rule": (_i, [_p, _i]),
     "spq_graph_parts": (_i, [_i, _i, _ip, _ip, _i, _ip]),
     "spq_set_precision": (_i, [_p, _i]),
     "spq_set_device": (_i, [_p, _i]),

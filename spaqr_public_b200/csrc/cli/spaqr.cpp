@@ -15,9 +15,10 @@
 // and its residual, then GMRES (square) or CGLS (more rows than columns) with
 // b = that random vector or --rhs.
 //
-// Flags the reference has and this build does not run: --hsl != 0 and
-// --scale 0 (the library returns SPQ_ERR_UNSUPPORTED), and the Eigen
-// comparison solvers --useEigenLSCG / --useEigenQR / --useCholesky.
+// Flags the reference has and this build does not run: --hsl != 0 (the library
+// returns SPQ_ERR_UNSUPPORTED) and the Eigen comparison solvers --useEigenLSCG /
+// --useEigenQR / --useCholesky. --scale 0 runs on square systems; on least
+// squares the driver switches it to 1, as the reference's does.
 // Added: --precision fp32 (FP32 factorization, FP64 Krylov), --target r (the
 // time-to-residual driver: refinement with GMRES corrections until the true
 // ||Ax - b|| / ||b|| <= r; square systems), --device k.

@@ -216,6 +216,12 @@ int spq_set_parts(spq_tree* t, int n, const int* parts) {
     t->cfg.parts.assign(parts, parts + n);
     return SPQ_OK;
 }
+int spq_set_fill_rule(spq_tree* t, int numeric) {
+    SPQ_SETTER_GUARD
+    if (numeric != 0 && numeric != 1) return fail(SPQ_ERR_ARG, "fill rule must be 0 or 1");
+    t->cfg.numeric_fill = numeric;
+    return SPQ_OK;
+}
 int spq_graph_parts(int m, int n, const int* cp, const int* ri, int nlevels, int* parts) {
     int rc = check_csc(m, n, cp, ri, nullptr, false);
     if (rc) return rc;

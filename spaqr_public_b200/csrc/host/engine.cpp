@@ -10,6 +10,7 @@
 #include "autotune.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,6 +19,7 @@
 #include <map>
 #include <numeric>
 #include <thread>
+#include <unordered_map>
 
 namespace spq {
 namespace {
@@ -77,7 +79,7 @@ public:
         int64_t xoff = -1;
         int level() const { return id.self.lvl; }
     };
-    enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE, TK_REASSIGN };
+    enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE, TK_REASSIGN, TK_ORTH, TK_SPLIT0 };
     struct A12 {
         const T* B;
         int ld, s;
@@ -260,7 +262,8 @@ public:
         if (factorized_) throw std::logic_error("factorize called twice");
         if (cfg_.order != 1.0f && cfg_.order != 1.5f)
             throw std::invalid_argument("--order must be 1 or 1.5");
-        if (!cfg_.scale && cfg_.tol != 0) throw std::invalid_argument("--scale 0 is not supported by this build");
+        if (!cfg_.scale && cfg_.tol != 0 && rect_)
+            throw std::invalid_argument("--scale 0 is supported for square systems only");
         double t0 = wall();
         launches_fact_ = 0;
         t_rank_wait_ = 0;
@@ -289,9 +292,12 @@ public:
             for (Cluster* s : cur())
                 if (s->level() == ilvl_) fill.push_back(s);
             // (threads) each cluster's fill set reads the graph and writes only its own set
+            const bool numeric = !geo_ && cfg_.numeric_fill;
+            std::vector<std::vector<FillCand>> cand(numeric ? fill.size() : 0);
             host_parallel_for(fill.size(), [&](size_t b, size_t e) {
-                for (size_t i = b; i < e; ++i) get_sparsity(fill[i]);
+                for (size_t i = b; i < e; ++i) get_sparsity(fill[i], numeric ? &cand[i] : nullptr);
             });
+            if (numeric) numeric_fill(fill, cand);
             const size_t nfill = fill.size();
             if (cfg_.verbose >= 3)
                 std::fprintf(stderr, "[lvl %d] fill host: %zu of %zu clusters, %.2f ms\n", ilvl_, nfill, cur().size(),
@@ -312,7 +318,12 @@ public:
             cudaEventRecord(ev[4], stream_);
             phase_ = 4;
             if (rect_ && cfg_.scale && window) extra_phase();
-            if (window) sparsify_phase();
+            if (window) {
+                if (cfg_.scale)
+                    sparsify_phase();
+                else
+                    sparsify0_phase();
+            }
             lap(4);
             cudaEventRecord(ev[5], stream_);
             phase_ = 5;
@@ -695,7 +706,13 @@ private:
         return true;
     }
     // src/tree.cpp:834-870 (purely symbolic, with or without coordinates)
-    void get_sparsity(Cluster* c) {
+    // A fill candidate left to the numeric test: nin joins c's fill set if
+    // ||A(n, c)^T A(n, nin)|| > 1e-14 for some shared row cluster n.
+    struct FillCand {
+        Cluster* nin;
+        Blk a1, a2;
+    };
+    void get_sparsity(Cluster* c, std::vector<FillCand>* numeric = nullptr) {
         std::vector<Cluster*> rs;
         std::vector<Sep> cols;
         for (Edge* e : c->out) cols.push_back(e->n2->id.self);
@@ -705,13 +722,67 @@ private:
             if (!e->live) continue;
             Cluster* n = e->n2;
             rs.push_back(n);
-            for (Edge* ein : n->in)
-                if (ein->live && ein->n1 != c && !ein->n1->elim && valid_fill(c->id, ein->n1->id, cols))
-                    rs.push_back(ein->n1);
+            for (Edge* ein : n->in) {
+                if (!(ein->live && ein->n1 != c && !ein->n1->elim && valid_fill(c->id, ein->n1->id, cols))) continue;
+                Cluster* nin = ein->n1;
+                // without coordinates the reference also asks the coupling to be
+                // numerically nonzero (src/tree.cpp:856-859), unless nin is one of
+                // c's own interfaces
+                if (numeric && !(nin->id.l == c->id.self || nin->id.r == c->id.self))
+                    numeric->push_back(FillCand{nin, e->A, ein->A});
+                else
+                    rs.push_back(nin);
+            }
         }
         std::sort(rs.begin(), rs.end(), [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
         rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
         c->rsparsity = std::move(rs);
+        if (numeric) {  // candidates already in the set need no test
+            auto in_rs = [&](const Cluster* x) {
+                return std::binary_search(c->rsparsity.begin(), c->rsparsity.end(), x,
+                                          [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
+            };
+            numeric->erase(std::remove_if(numeric->begin(), numeric->end(),
+                                          [&](const FillCand& f) { return in_rs(f.nin); }),
+                           numeric->end());
+        }
+    }
+
+    // The numeric fill test of the level's candidates: one batched launch of
+    // ||A1^T A2|| (FP64 sums) and one readback; passing candidates join their
+    // cluster's fill set.
+    void numeric_fill(const std::vector<Cluster*>& fill, std::vector<std::vector<FillCand>>& cand) {
+        std::vector<ProdNormTask<T>> tasks;
+        for (auto& v : cand)
+            for (auto& f : v)
+                tasks.push_back(ProdNormTask<T>{f.a1.p, f.a2.p, f.a1.ld, f.a2.ld, f.a1.rows, f.a1.cols, f.a2.cols, 0});
+        if (tasks.empty()) return;
+        double* d_out = desc_arena_.alloc_n<double>(tasks.size());
+        Upload up;
+        const size_t o = up.add(tasks);
+        char* d = up.commit(desc_arena_, stream_, pinned_);
+        launch_product_norms<T>(reinterpret_cast<const ProdNormTask<T>*>(d + o), (int)tasks.size(), d_out, stream_);
+        ++launches_fact_;
+        std::vector<double> norms(tasks.size());
+        cuda_check(cudaMemcpyAsync(norms.data(), d_out, norms.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+                   "fill norms");
+        cuda_check(cudaStreamSynchronize(stream_), "fill norms");
+        pinned_.reset();
+        size_t q = 0;
+        for (size_t i = 0; i < fill.size(); ++i) {
+            bool added = false;
+            for (auto& f : cand[i]) {
+                if (norms[q++] > 1e-14) {
+                    fill[i]->rsparsity.push_back(f.nin);
+                    added = true;
+                }
+            }
+            if (added) {
+                auto& rs = fill[i]->rsparsity;
+                std::sort(rs.begin(), rs.end(), [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
+                rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
+            }
+        }
     }
 
     // ------------------------------------------------------------- batched QR execution
@@ -1024,87 +1095,277 @@ private:
             QRJob job;
             std::vector<int> uids;
         };
+        // The level's interiors in order. Graph changes (fill blocks: arena
+        // addresses, uids, edge order) are made on this thread in that order;
+        // the read-only block search and the descriptor lists, which are most of
+        // the host work, run on host threads. Same blocks, same order, same
+        // descriptors as one task after another.
+        std::vector<Cluster*> lv;
+        for (Cluster* c : cur())
+            if (c->level() == ilvl_) lv.push_back(c);
+        const size_t nl = lv.size();
+        std::unordered_map<const Cluster*, int> pos_in_level;
+        pos_in_level.reserve(nl * 2);
+        for (size_t i = 0; i < nl; ++i) pos_in_level[lv[i]] = (int)i;
+        struct Plan {
+            std::vector<Edge*> H;           // stacked column blocks
+            std::vector<Cluster*> upd;      // updated clusters, rsparsity order
+            std::vector<Edge*> blk;         // upd.size() x H.size(): the block of (upd, H row cluster), null if missing
+            int m = 0, k = 0;
+        };
+        std::vector<Plan> plans(nl);
+        // The split below relies on no interior of this level lying in another's
+        // column or fill set (true of nested dissection, whose interiors are cut
+        // apart by separators): then no task's fill lands in another task's
+        // column. Otherwise the tasks are built one after another.
+        std::atomic<bool> coupled{false};
+        // 1. (threads) blocks that already exist: a neighbour n is updated unless
+        //    eliminated before this phase or earlier in it (lower position)
+        host_parallel_for(
+            nl,
+            [&](size_t b, size_t e) {
+                std::vector<std::pair<const Cluster*, int>> hs;
+                for (size_t i = b; i < e; ++i) {
+                    Cluster* c = lv[i];
+                    Plan& P = plans[i];
+                    if (c->csize == 0) continue;
+                    for (Edge* ed : c->out)
+                        if (ed->live) {
+                            P.H.push_back(ed);
+                            P.m += ed->A.rows;
+                            if (ed->n2 != c && pos_in_level.count(ed->n2)) coupled = true;
+                        }
+                    P.k = P.H.front()->A.cols;
+                    // H's row clusters by address: one pass over a neighbour's edges
+                    // finds all of its blocks in those rows (the first edge per row
+                    // cluster, as a scan per row cluster would)
+                    hs.clear();
+                    for (size_t h = 0; h < P.H.size(); ++h) hs.emplace_back(P.H[h]->n2, (int)h);
+                    std::sort(hs.begin(), hs.end());
+                    for (size_t h = 1; h < hs.size(); ++h)
+                        if (hs[h].first == hs[h - 1].first) coupled = true;  // two blocks in one row cluster
+                    const size_t nh = P.H.size();
+                    for (Cluster* n : c->rsparsity) {
+                        if (n == c || n->elim) continue;
+                        auto it = pos_in_level.find(n);
+                        if (it != pos_in_level.end()) {
+                            coupled = true;
+                            if (it->second < (int)i) continue;
+                        }
+                        P.upd.push_back(n);
+                        const size_t base = P.blk.size();
+                        P.blk.resize(base + nh, nullptr);
+                        for (Edge* e2 : n->out) {
+                            auto f = std::lower_bound(hs.begin(), hs.end(), std::make_pair((const Cluster*)e2->n2, -1));
+                            if (f != hs.end() && f->first == e2->n2 && !P.blk[base + f->second])
+                                P.blk[base + f->second] = e2;
+                        }
+                    }
+                }
+            },
+            64);
         std::vector<Task> tasks;
-        for (Cluster* c : cur()) {
-            if (c->level() != ilvl_) continue;
+        if (!coupled) {
+        // 2. (this thread, level order) arena memory of every job and the missing
+        //    fill blocks, created in the order of a task-by-task elimination; a
+        //    block an earlier task of this phase created is found in `made`
+        struct PairHash {
+            size_t operator()(const std::pair<const Cluster*, const Cluster*>& p) const {
+                return std::hash<const void*>()(p.first) * 31 + std::hash<const void*>()(p.second);
+            }
+        };
+        std::unordered_map<std::pair<const Cluster*, const Cluster*>, Edge*, PairHash> made;
+        std::vector<Task> all(nl);
+        for (size_t i = 0; i < nl; ++i) {
+            Cluster* c = lv[i];
+            Plan& P = plans[i];
             if (c->csize == 0) {
                 c->elim = true;
+                continue;
+            }
+            QRJob& j = all[i].job;
+            j.m = P.m;
+            j.k = P.k;
+            j.fac = arena_.alloc_n<T>((size_t)P.m * P.k);
+            j.tau = arena_.alloc_n<T>(P.k);
+            j.tp = arena_.alloc_n<T>((size_t)npanels(P.k) * kNB * kNB);
+            const size_t nh = P.H.size();
+            for (size_t u = 0; u < P.upd.size(); ++u) {
+                Cluster* n = P.upd[u];
+                for (size_t h = 0; h < nh; ++h) {
+                    Edge*& b = P.blk[u * nh + h];
+                    if (b) continue;
+                    const auto key = std::make_pair((const Cluster*)n, (const Cluster*)P.H[h]->n2);
+                    auto f = made.find(key);
+                    if (f != made.end()) {
+                        b = f->second;
+                    } else {
+                        b = add_edge(n, P.H[h]->n2);
+                        made.emplace(key, b);
+                    }
+                }
+            }
+            c->elim = true;
+        }
+        // 3. (threads) each job's copy descriptors and block uids
+        host_parallel_for(
+            nl,
+            [&](size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i) {
+                    Cluster* c = lv[i];
+                    Plan& P = plans[i];
+                    if (c->csize == 0) continue;
+                    Task& t = all[i];
+                    QRJob& j = t.job;
+                    const int m = P.m, k = P.k;
+                    const size_t nh = P.H.size();
+                    j.gather.reserve(nh * (1 + P.upd.size()));
+                    j.scatter.reserve(nh * P.upd.size());
+                    t.uids.reserve(nh * (1 + P.upd.size()));
+                    int off = 0;
+                    for (Edge* ed : P.H) {
+                        j.gather.push_back(cp(ed->A.p, j.fac + off, ed->A.ld, m, ed->A.rows, k));
+                        t.uids.push_back(ed->A.uid);
+                        off += ed->A.rows;
+                    }
+                    int co = 0;
+                    for (size_t u = 0; u < P.upd.size(); ++u) {
+                        Cluster* n = P.upd[u];
+                        off = 0;
+                        for (size_t h = 0; h < nh; ++h) {
+                            Edge* ecn = P.blk[u * nh + h];
+                            const int pad = off + co * m;  // relative to the wave scratch of this job
+                            j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
+                            j.scatter.push_back(cp(nullptr, ecn->A.p, m, ecn->A.ld, ecn->A.rows, n->csize, 0, pad));
+                            t.uids.push_back(ecn->A.uid);
+                            off += ecn->A.rows;
+                        }
+                        co += n->csize;
+                    }
+                    j.ntr = co;
+                }
+            },
+            64);
+        // 4. (this thread, level order) the tape, counters, log and, for least
+        //    squares, the column blocks a finished elimination drops
+        for (size_t i = 0; i < nl; ++i) {
+            Cluster* c = lv[i];
+            Plan& P = plans[i];
+            if (c->csize == 0) {
                 rec(1, 0, 0, 0, 0, 0, c->order);
                 continue;
             }
-            std::vector<Edge*> H;
-            int m = 0;
-            for (Edge* e : c->out)
-                if (e->live) { H.push_back(e); m += e->A.rows; }
-            const int k = H.front()->A.cols;
-            Task t;
-            QRJob& j = t.job;
-            j.m = m;
-            j.k = k;
-            j.fac = arena_.alloc_n<T>((size_t)m * k);
-            j.tau = arena_.alloc_n<T>(k);
-            j.tp = arena_.alloc_n<T>((size_t)npanels(k) * kNB * kNB);
-            int off = 0;
-            for (Edge* e : H) {
-                j.gather.push_back(cp(e->A.p, j.fac + off, e->A.ld, m, e->A.rows, k));
-                t.uids.push_back(e->A.uid);
-                off += e->A.rows;
-            }
-            int nupd = 0, co = 0;
-            // H's row clusters by address: one pass over a neighbour's edges finds
-            // all of its blocks in those rows (the first edge per row cluster, as a
-            // scan per row cluster would); missing ones are added in H's order
-            std::vector<std::pair<const Cluster*, int>> hs;
-            hs.reserve(H.size());
-            for (size_t i = 0; i < H.size(); ++i) hs.emplace_back(H[i]->n2, (int)i);
-            std::sort(hs.begin(), hs.end());
-            std::vector<Edge*> found(H.size());
-            for (Cluster* n : c->rsparsity) {
-                if (n->elim || n == c) continue;
-                std::fill(found.begin(), found.end(), nullptr);
-                for (Edge* e2 : n->out) {
-                    auto it = std::lower_bound(hs.begin(), hs.end(), std::make_pair((const Cluster*)e2->n2, -1));
-                    if (it != hs.end() && it->first == e2->n2 && !found[it->second]) found[it->second] = e2;
-                }
-                off = 0;
-                for (size_t hi = 0; hi < H.size(); ++hi) {
-                    Edge* e = H[hi];
-                    Edge* ecn = found[hi];
-                    if (!ecn) ecn = add_edge(n, e->n2);
-                    const int pad = off + co * m;  // relative to the wave scratch of this job
-                    j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
-                    j.scatter.push_back(cp(nullptr, ecn->A.p, m, ecn->A.ld, ecn->A.rows, n->csize, 0, pad));
-                    t.uids.push_back(ecn->A.uid);
-                    off += ecn->A.rows;
-                }
-                co += n->csize;
+            const int m = P.m, k = P.k;
+            int co = 0;
+            for (Cluster* n : P.upd) {
                 nnzR_ += (unsigned long long)(c->csize * n->csize);
-                ++nupd;
+                co += n->csize;
             }
-            j.ntr = co;
             nnzH_ += (unsigned long long)(m * k);
             TapeOp op;
             op.kind = TK_QR;
             op.c = c;
-            op.fac = j.fac;
-            op.tp = j.tp;
+            op.fac = all[i].job.fac;
+            op.tp = all[i].job.tp;
             op.m = m;
             op.k = k;
             op.ld = m;
-            for (Edge* e : H) op.segs.emplace_back(e->n2, e->n2->rsize);
-            for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
+            for (Edge* ed : P.H) op.segs.emplace_back(ed->n2, ed->n2->rsize);
+            for (Edge* ed : c->in) op.a12.push_back(A12{ed->A.p, ed->A.ld, ed->A.cols, ed->n1});
             tape_.push_back(std::move(op));
-            c->elim = true;
             if (rect_) {  // least squares keeps R only: the self block shrinks to k rows, the rest goes
-                for (Edge* e : c->out) {
-                    if (e->n2 == c)
-                        e->A.rows = std::min(e->A.rows, k);
+                for (Edge* ed : c->out) {
+                    if (ed->n2 == c)
+                        ed->A.rows = std::min(ed->A.rows, k);
                     else
-                        e->live = false;
+                        ed->live = false;
                 }
             }
-            rec(1, m, k, nupd, (long long)H.size(), co, c->order);
-            tasks.push_back(std::move(t));
+            rec(1, m, k, (long long)P.upd.size(), (long long)P.H.size(), co, c->order);
+            tasks.push_back(std::move(all[i]));
+        }
+        } else {
+            for (Cluster* c : cur()) {
+                if (c->level() != ilvl_) continue;
+                if (c->csize == 0) {
+                    c->elim = true;
+                    rec(1, 0, 0, 0, 0, 0, c->order);
+                    continue;
+                }
+                std::vector<Edge*> H;
+                int m = 0;
+                for (Edge* e : c->out)
+                    if (e->live) { H.push_back(e); m += e->A.rows; }
+                const int k = H.front()->A.cols;
+                Task t;
+                QRJob& j = t.job;
+                j.m = m;
+                j.k = k;
+                j.fac = arena_.alloc_n<T>((size_t)m * k);
+                j.tau = arena_.alloc_n<T>(k);
+                j.tp = arena_.alloc_n<T>((size_t)npanels(k) * kNB * kNB);
+                int off = 0;
+                for (Edge* e : H) {
+                    j.gather.push_back(cp(e->A.p, j.fac + off, e->A.ld, m, e->A.rows, k));
+                    t.uids.push_back(e->A.uid);
+                    off += e->A.rows;
+                }
+                int nupd = 0, co = 0;
+                // H's row clusters by address: one pass over a neighbour's edges finds
+                // all of its blocks in those rows (the first edge per row cluster, as a
+                // scan per row cluster would); missing ones are added in H's order
+                std::vector<std::pair<const Cluster*, int>> hs;
+                hs.reserve(H.size());
+                for (size_t i = 0; i < H.size(); ++i) hs.emplace_back(H[i]->n2, (int)i);
+                std::sort(hs.begin(), hs.end());
+                std::vector<Edge*> found(H.size());
+                for (Cluster* n : c->rsparsity) {
+                    if (n->elim || n == c) continue;
+                    std::fill(found.begin(), found.end(), nullptr);
+                    for (Edge* e2 : n->out) {
+                        auto it = std::lower_bound(hs.begin(), hs.end(), std::make_pair((const Cluster*)e2->n2, -1));
+                        if (it != hs.end() && it->first == e2->n2 && !found[it->second]) found[it->second] = e2;
+                    }
+                    off = 0;
+                    for (size_t hi = 0; hi < H.size(); ++hi) {
+                        Edge* e = H[hi];
+                        Edge* ecn = found[hi];
+                        if (!ecn) ecn = add_edge(n, e->n2);
+                        const int pad = off + co * m;  // relative to the wave scratch of this job
+                        j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
+                        j.scatter.push_back(cp(nullptr, ecn->A.p, m, ecn->A.ld, ecn->A.rows, n->csize, 0, pad));
+                        t.uids.push_back(ecn->A.uid);
+                        off += ecn->A.rows;
+                    }
+                    co += n->csize;
+                    nnzR_ += (unsigned long long)(c->csize * n->csize);
+                    ++nupd;
+                }
+                j.ntr = co;
+                nnzH_ += (unsigned long long)(m * k);
+                TapeOp op;
+                op.kind = TK_QR;
+                op.c = c;
+                op.fac = j.fac;
+                op.tp = j.tp;
+                op.m = m;
+                op.k = k;
+                op.ld = m;
+                for (Edge* e : H) op.segs.emplace_back(e->n2, e->n2->rsize);
+                for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
+                tape_.push_back(std::move(op));
+                c->elim = true;
+                if (rect_) {  // least squares keeps R only: the self block shrinks to k rows, the rest goes
+                    for (Edge* e : c->out) {
+                        if (e->n2 == c)
+                            e->A.rows = std::min(e->A.rows, k);
+                        else
+                            e->live = false;
+                    }
+                }
+                rec(1, m, k, nupd, (long long)H.size(), co, c->order);
+                tasks.push_back(std::move(t));
+            }
         }
         if (tasks.empty()) return;
         const double te1 = wall();
@@ -1217,6 +1478,420 @@ private:
     }
 
     // ------------------------------------------------------------- sparsification (src/tree.cpp:992-1114)
+    // ------------------------------------------------------------- --scale 0 (sparsify, src/tree.cpp:887-989)
+    // Per interface c (square systems): sinv = 1 / sigma_min([A_pp; A_mp]) (QR
+    // of the stacked column, then one-sided Jacobi on its R); the RRQR of
+    // C = [A_mp^T | sinv A_pp^T A_pm]; A_mp <- rows of R P^T (the same
+    // write-back as sparsifyD), A_pp <- A_pp Q (the reflectors applied to
+    // A_pp^T, transposed back); the fine cluster takes the last rows of every
+    // block in c's row and the corners of the diagonal block (split_edges,
+    // src/tree.cpp:480-530), and is eliminated at once. Waves as sparsifyD:
+    // every block a task touches lies in its interface's own row or column.
+    void sparsify0_phase() {
+        std::vector<Cluster*> list;
+        std::vector<std::vector<int>> touched;
+        for (Cluster* c : cur()) {
+            if (!want_sparsify(c)) continue;
+            std::vector<int> u;
+            for (Edge* e : c->in)
+                if (!e->n1->elim) u.push_back(e->A.uid);
+            for (Edge* e : c->out)
+                if (!e->n2->elim) u.push_back(e->A.uid);
+            list.push_back(c);
+            touched.push_back(std::move(u));
+        }
+        if (list.empty()) return;
+        int nw = 0;
+        auto wave = assign_waves(touched, next_uid_, &nw);
+        print_waves("sparsify0", wave, nw);
+        std::vector<std::vector<std::vector<long long>>> recs(list.size());
+        const int order0 = max_order_;
+        fine_of_.assign(list.size(), nullptr);
+        for (int w = 0; w < nw; ++w) {
+            std::vector<Spars0Job> jobs;
+            size_t celems = 0, ielems = 0;
+            for (size_t t = 0; t < list.size(); ++t) {
+                if (wave[t] != w) continue;
+                Cluster* c = list[t];
+                if (c->csize == 0) {
+                    recs[t] = {{3, 0, 0, 0, c->rsize, 0, c->order}};
+                    continue;
+                }
+                Spars0Job j;
+                j.idx = t;
+                j.c = c;
+                for (Edge* e : c->in)
+                    if (!e->n1->elim) { j.apm.push_back(e); j.spm += e->A.cols; }
+                for (Edge* e : c->out) {
+                    if (e->n2->elim) continue;
+                    if (e->n2 != c) { j.amp.push_back(e); j.smp += e->A.rows; }
+                    else j.self = e;
+                }
+                if (!j.self) throw std::runtime_error("sparsify (scale 0): interface without its diagonal block");
+                j.m = c->csize;
+                j.n = j.smp + j.spm;
+                j.ld = std::max((j.n + 3) & ~3, 4);
+                j.c_off = celems;
+                celems += (size_t)j.m * j.ld;
+                j.i_off = ielems;
+                ielems += 3 * (size_t)std::max(j.n, 1) + 1;
+                celems += 3 * (size_t)std::max(j.n, 1);
+                celems = (celems + 31) & ~size_t(31);
+                jobs.push_back(std::move(j));
+            }
+            if (!jobs.empty()) run_sparsify0_wave(jobs, celems, ielems, recs);
+        }
+        // The fine clusters were created wave by wave; the reference creates them
+        // in the interfaces' order, and the order is what its records show: the
+        // k-th compressed interface of the list gets the k-th new order.
+        int next = order0;
+        for (size_t t = 0; t < list.size(); ++t) {
+            Cluster* cf = fine_of_[t];
+            if (!cf) continue;
+            cf->order = next++;
+            recs[t][0][6] = cf->order;  // the fine cluster's elimination record
+        }
+        if (next != max_order_) throw std::logic_error("sparsify (scale 0): fine cluster count");
+        for (size_t t = 0; t < list.size(); ++t)
+            for (const auto& r : recs[t]) rec(r[0], r[1], r[2], r[3], r[4], r[5], r[6]);
+    }
+    std::vector<Cluster*> fine_of_;  // sparsify0_phase: the fine cluster of each listed interface
+
+    struct Spars0Job {
+        size_t idx = 0;
+        Cluster* c = nullptr;
+        std::vector<Edge*> apm, amp;
+        Edge* self = nullptr;
+        int m = 0, n = 0, smp = 0, spm = 0, ld = 0;
+        size_t c_off = 0, i_off = 0;
+    };
+
+    // One elimination QR job of the listed column blocks H (stacked in order)
+    // updating the blocks blk[u][h] of every cluster upd[u]; the tape op and
+    // the counters as elim_phase. Returns the job (its descriptors built).
+    QRJob fine_elim_job(Cluster* c, const std::vector<Edge*>& H, const std::vector<Cluster*>& upd,
+                        const std::vector<std::vector<Edge*>>& blk, std::vector<int>& uids) {
+        QRJob j;
+        int m = 0;
+        for (Edge* e : H) m += e->A.rows;
+        const int k = H.front()->A.cols;
+        j.m = m;
+        j.k = k;
+        j.fac = arena_.alloc_n<T>((size_t)m * k);
+        j.tau = arena_.alloc_n<T>(k);
+        j.tp = arena_.alloc_n<T>((size_t)npanels(k) * kNB * kNB);
+        int off = 0;
+        for (Edge* e : H) {
+            j.gather.push_back(cp(e->A.p, j.fac + off, e->A.ld, m, e->A.rows, k));
+            uids.push_back(e->A.uid);
+            off += e->A.rows;
+        }
+        int co = 0;
+        for (size_t u = 0; u < upd.size(); ++u) {
+            Cluster* n = upd[u];
+            off = 0;
+            for (Edge* ecn : blk[u]) {
+                const int pad = off + co * m;
+                j.gather.push_back(cp(ecn->A.p, nullptr, ecn->A.ld, m, ecn->A.rows, n->csize, 0, pad));
+                j.scatter.push_back(cp(nullptr, ecn->A.p, m, ecn->A.ld, ecn->A.rows, n->csize, 0, pad));
+                uids.push_back(ecn->A.uid);
+                off += ecn->A.rows;
+            }
+            co += n->csize;
+            nnzR_ += (unsigned long long)(c->csize * n->csize);
+        }
+        j.ntr = co;
+        nnzH_ += (unsigned long long)(m * k);
+        TapeOp op;
+        op.kind = TK_QR;
+        op.c = c;
+        op.fac = j.fac;
+        op.tp = j.tp;
+        op.m = m;
+        op.k = k;
+        op.ld = m;
+        for (Edge* e : H) op.segs.emplace_back(e->n2, e->n2->rsize);
+        for (Edge* e : c->in) op.a12.push_back(A12{e->A.p, e->A.ld, e->A.cols, e->n1});
+        tape_.push_back(std::move(op));
+        c->elim = true;
+        return j;
+    }
+
+    // Runs a set of conflict-free QR jobs (the elimination machinery).
+    void run_qr_jobs(std::vector<QRJob>& jobs) {
+        if (jobs.empty()) return;
+        const size_t e = wave_scratch_elems(jobs);
+        T* trbase = static_cast<T*>(scratch_.get(std::max<size_t>(e, 1) * sizeof(T), stream_));
+        WaveBuild B;
+        const std::vector<TrsmTask<T>> no_trsm;
+        const std::vector<CopyDesc<T>> no_post;
+        build_wave(jobs, no_trsm, trbase, d_status_, B);
+        issue_wave(B, no_trsm, no_post, wall());
+    }
+
+    void run_sparsify0_wave(std::vector<Spars0Job>& jobs, size_t celems, size_t ielems,
+                            std::vector<std::vector<std::vector<long long>>>& recs) {
+        const size_t nj = jobs.size();
+        // 1. QR of every stacked [A_pp; A_mp] (copies, the factor kept in the arena)
+        std::vector<QRJob> apq(nj);
+        std::vector<int> ra(nj, 0);
+        for (size_t q = 0; q < nj; ++q) {
+            auto& j = jobs[q];
+            Cluster* c = j.c;
+            int rows = j.self->A.rows;
+            for (Edge* e : j.amp) rows += e->A.rows;
+            ra[q] = rows;
+            QRJob& a = apq[q];
+            a.m = rows;
+            a.k = j.m;
+            a.fac = arena_.alloc_n<T>((size_t)rows * j.m);
+            a.tau = arena_.alloc_n<T>(j.m);
+            a.tp = arena_.alloc_n<T>((size_t)npanels(j.m) * kNB * kNB);
+            int off = 0;
+            a.gather.push_back(cp(j.self->A.p, a.fac, j.self->A.ld, rows, j.self->A.rows, j.m));
+            off += j.self->A.rows;
+            for (Edge* e : j.amp) {
+                a.gather.push_back(cp(e->A.p, a.fac + off, e->A.ld, rows, e->A.rows, j.m));
+                off += e->A.rows;
+            }
+            (void)c;
+        }
+        run_qr_jobs(apq);
+        // 2. sinv per job (one-sided Jacobi on R), 3. A_pm gathered column-major
+        double* d_sinv = desc_arena_.alloc_n<double>(nj);
+        std::vector<SigmaTask<T>> sig;
+        std::vector<AtbTask<T>> atb;
+        std::vector<TileRef> atb_tiles;
+        std::vector<CopyDesc<T>> pmg;
+        for (size_t q = 0; q < nj; ++q) {
+            auto& j = jobs[q];
+            T* work = arena_.alloc_n<T>((size_t)j.m * j.m);
+            sig.push_back(SigmaTask<T>{apq[q].fac, work, d_sinv + q, ra[q], j.m});
+            const int rows = j.self->A.rows;
+            T* bpm = j.spm > 0 ? arena_.alloc_n<T>((size_t)rows * j.spm) : nullptr;
+            int off = 0;
+            for (Edge* e : j.apm) {
+                pmg.push_back(cp(e->A.p, bpm + (size_t)off * rows, e->A.ld, rows, rows, e->A.cols));
+                off += e->A.cols;
+            }
+            if (j.spm > 0) {
+                const int id = (int)atb.size();
+                atb.push_back(AtbTask<T>{j.self->A.p, bpm, nullptr, d_sinv + q, j.self->A.ld, rows, j.ld, rows, j.m,
+                                         j.spm, j.smp, 0});
+                for (int t0 = 0; t0 < j.spm; t0 += 32) atb_tiles.push_back(TileRef{id, t0 / 32});
+            }
+        }
+        {
+            Upload u;
+            const size_t o_s = u.add(sig), o_c = u.add(pmg);
+            char* d = u.commit(desc_arena_, stream_, pinned_);
+            launch_sigma_min<T>(reinterpret_cast<const SigmaTask<T>*>(d + o_s), (int)sig.size(), stream_);
+            ++launches_fact_;
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_c), pmg);
+        }
+        // 4. C = [A_mp^T | sinv A_pp^T A_pm] and its RRQR
+        std::vector<RRQRTaskRM<T>> rt;
+        const std::vector<int> ranks = rrqr_batch(
+            jobs, celems, ielems, rt,
+            [&](const Spars0Job& j, T* C, std::vector<CopyDesc<T>>& g) {
+                int cur = 0;
+                for (Edge* e : j.amp) {
+                    g.push_back(cp(e->A.p, C + cur, e->A.ld, j.ld, e->A.rows, e->A.cols));
+                    cur += e->A.rows;
+                }
+            },
+            [&](T* cb) {
+                if (atb.empty()) return;
+                for (auto& a : atb) {
+                    const size_t q = (size_t)(a.sinv - d_sinv);
+                    a.C = cb + jobs[q].c_off;
+                }
+                Upload u;
+                const size_t o_a = u.add(atb), o_t = u.add(atb_tiles);
+                char* d = u.commit(desc_arena_, stream_, pinned_);
+                launch_atb_scaled<T>(reinterpret_cast<const AtbTask<T>*>(d + o_a),
+                                     reinterpret_cast<const TileRef*>(d + o_t), (int)atb_tiles.size(), stream_);
+                ++launches_fact_;
+            });
+        // 5. write-back of A_mp, reflectors of C; A_pp <- A_pp Q; split; fine eliminations
+        std::vector<SparsWBRM<T>> wb;
+        std::vector<SpBlock<T>> blocks;
+        std::vector<CopyDesc<T>> tr_in, tr_out, splits;
+        std::vector<QRTask<T>> rq;  // A_pp^T <- Q^T A_pp^T
+        struct Fine {
+            size_t q;
+            Cluster* cf;
+            int r, rows_old, cols_old;
+            T* V;
+            T* tp;
+        };
+        std::vector<Fine> fines;
+        double wb_bytes = 0;
+        for (size_t q = 0; q < nj; ++q) {
+            auto& j = jobs[q];
+            Cluster* c = j.c;
+            const int r = ranks[q], m = j.m;
+            if (r < 0) throw std::runtime_error("sparsify: invalid rank from device");
+            if (r >= m) {
+                recs[j.idx] = {{3, m, c->csize, j.n, c->rsize, 0, c->order}};
+                continue;
+            }
+            T* V = arena_.alloc_n<T>((size_t)m * std::max(r, 1));
+            T* tau = arena_.alloc_n<T>(std::max(r, 1));
+            T* tp = arena_.alloc_n<T>((size_t)std::max(npanels(r), 1) * kNB * kNB);
+            SparsWBRM<T> w{rt[q].C, rt[q].pos, rt[q].colat, rt[q].tau, V, tau, tp, m, j.ld, r, 0, (int)blocks.size(), 0};
+            int cur = 0;
+            for (Edge* e : j.amp) {
+                blocks.push_back(SpBlock<T>{e->A.p, e->A.ld, e->A.rows, e->A.cols, cur, 0});
+                cur += e->A.rows;
+            }
+            w.nblk = (int)blocks.size() - w.blk0;
+            wb.push_back(w);
+            wb_bytes += ((double)r * j.n + 2.0 * m * r) * sizeof(T);
+            const int rows = j.self->A.rows;
+            T* At = arena_.alloc_n<T>((size_t)m * rows);  // A_pp^T (m x rows)
+            tr_in.push_back(cp(j.self->A.p, At, j.self->A.ld, m, rows, m, 2));
+            rq.push_back(QRTask<T>{V, At, tau, tp, m, r, rows, 1, d_status_});
+            tr_out.push_back(cp(At, j.self->A.p, m, j.self->A.ld, m, rows, 2));
+            const int nf = m - r;
+            Cluster* cf = new_cluster(c->cstart + r, nf, c->rstart + rows - nf, nf, c->id);
+            fines.push_back(Fine{q, cf, r, rows, m, V, tp});
+        }
+        if (!wb.empty()) {
+            Upload u2;
+            size_t o_w = u2.add(wb), o_b = u2.add(blocks), o_i = u2.add(tr_in), o_q = u2.add(rq);
+            int maxr = 0;
+            for (auto& x : rq) maxr = std::max(maxr, x.k);
+            std::vector<std::vector<TileRef>> tl;
+            for (int p = 0; p < maxr; p += kNB) {
+                std::vector<TileRef> v;
+                for (size_t t = 0; t < rq.size(); ++t) {
+                    if (rq[t].k <= p) continue;
+                    for (int c0 = 0, ti = 0; c0 < rq[t].ntr; c0 += kTN, ++ti) v.push_back(TileRef{(int)t, ti});
+                }
+                tl.push_back(std::move(v));
+            }
+            std::vector<size_t> o_t;
+            for (auto& v : tl) o_t.push_back(u2.add(v));
+            const size_t o_o = u2.add(tr_out);
+            char* d2 = u2.commit(desc_arena_, stream_, pinned_);
+            int parts = 1;
+            for (const auto& x : wb) parts = std::max(parts, std::max(x.nblk, (x.r + kNB - 1) / kNB));
+            timed(KF_SPARS_WB, 0, wb_bytes, [&] {
+                launch_spars_wb_rm<T>(reinterpret_cast<const SparsWBRM<T>*>(d2 + o_w),
+                                      reinterpret_cast<const SpBlock<T>*>(d2 + o_b), (int)wb.size(), parts, stream_);
+            });
+            ++launches_fact_;
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d2 + o_i), tr_in);
+            for (size_t i = 0; i < tl.size(); ++i) {
+                if (tl[i].empty()) continue;
+                timed(KF_TRAILING, 0, 0, [&] {
+                    launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d2 + o_q),
+                                       reinterpret_cast<const TileRef*>(d2 + o_t[i]), (int)tl[i].size(), (int)i * kNB,
+                                       stream_);
+                });
+                ++launches_fact_;
+            }
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d2 + o_o), tr_out);
+        }
+        // split_edges and the fine clusters' eliminations
+        std::vector<QRJob> fjobs;
+        for (const Fine& F : fines) {
+            auto& j = jobs[F.q];
+            Cluster* c = j.c;
+            Cluster* cf = F.cf;
+            const int r = F.r, nf = F.cols_old - r, rows_new = F.rows_old - nf;
+            // tape: Orthogonal (backward part only), Split (with c's sizes before the
+            // split), then the fine cluster's QR below, as the reference records them
+            TapeOp ot;
+            ot.kind = TK_ORTH;
+            ot.c = c;
+            ot.fac = F.V;
+            ot.tp = F.tp;
+            ot.m = F.cols_old;
+            ot.k = r;
+            ot.ld = F.cols_old;
+            tape_.push_back(std::move(ot));
+            TapeOp st;
+            st.kind = TK_SPLIT0;
+            st.c = c;
+            st.f = cf;
+            st.crows = F.rows_old;
+            st.ccols = F.cols_old;
+            st.rank = nf;
+            tape_.push_back(std::move(st));
+            // the fine cluster's rows of every block in c's row (A_pm): new blocks
+            for (Edge* e : j.apm) {
+                Blk b = new_block(nf, e->A.cols);
+                splits.push_back(cp(e->A.p + rows_new, b.p, e->A.ld, b.ld, nf, e->A.cols));
+                e->A.rows = rows_new;
+                Edge* ef = new_edge(e->n1, cf, b);
+                cf->in.push_back(ef);
+                e->n1->out.push_back(ef);
+            }
+            // the diagonal block's corners (A_pp after A_pp Q)
+            Edge* es = j.self;
+            Blk bff = new_block(nf, nf), bfc = new_block(rows_new, nf), bcf = new_block(nf, r);
+            splits.push_back(cp(es->A.p + rows_new + (size_t)r * es->A.ld, bff.p, es->A.ld, bff.ld, nf, nf));
+            splits.push_back(cp(es->A.p + (size_t)r * es->A.ld, bfc.p, es->A.ld, bfc.ld, rows_new, nf));
+            splits.push_back(cp(es->A.p + rows_new, bcf.p, es->A.ld, bcf.ld, nf, r));
+            es->A.rows = rows_new;
+            es->A.cols = r;
+            Edge* eff = new_edge(cf, cf, bff);
+            Edge* efc = new_edge(cf, c, bfc);
+            Edge* ecf = new_edge(c, cf, bcf);
+            cf->out.push_back(eff);  // by order, descending: the fine cluster first, then c
+            cf->out.push_back(efc);
+            cf->in.push_back(ecf);
+            c->out.push_back(ecf);
+            // new shapes of c and its column blocks
+            for (Edge* e : j.amp) e->A.cols = r;
+            c->rsize = rows_new;
+            c->csize = r;
+            fine_[ilvl_].push_back(cf);
+            // eliminate_cluster(cf): H = [cf rows; c rows], updates of its fill set
+            std::vector<Cluster*> upd;
+            std::vector<std::vector<Edge*>> blk;
+            for (Edge* e : j.apm) upd.push_back(e->n1);
+            upd.push_back(c);
+            std::vector<size_t> order(upd.size());
+            for (size_t i = 0; i < upd.size(); ++i) order[i] = i;
+            std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return upd[a]->order < upd[b]->order; });
+            std::vector<Cluster*> upd_s;
+            for (size_t i : order) {
+                Cluster* n = upd[i];
+                if (n->elim || n == cf) continue;
+                if (!upd_s.empty() && upd_s.back() == n) continue;
+                upd_s.push_back(n);
+                Edge* to_f = n == c ? ecf : find_edge(n, cf);
+                Edge* to_c = n == c ? es : find_edge(n, c);
+                if (!to_f || !to_c) throw std::runtime_error("sparsify (scale 0): missing block of the fine elimination");
+                blk.push_back({to_f, to_c});
+            }
+            std::vector<int> uids;
+            fjobs.push_back(fine_elim_job(cf, {eff, efc}, upd_s, blk, uids));
+            int wtr = 0;
+            for (Cluster* n : upd_s) wtr += n->csize;
+            recs[j.idx] = {{1, cf->rsize + rows_new, nf, (long long)upd_s.size(), 2, wtr, cf->order},
+                           {3, F.cols_old, r, j.n, rows_new, 0, c->order}};
+            fine_of_[j.idx] = cf;
+        }
+        if (!splits.empty()) {
+            Upload u3;
+            const size_t o = u3.add(splits);
+            char* d3 = u3.commit(desc_arena_, stream_, pinned_);
+            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d3 + o), splits);
+        }
+        run_qr_jobs(fjobs);
+    }
+
+    // The first edge of n's out list into the row cluster r.
+    static Edge* find_edge(Cluster* n, Cluster* r) {
+        for (Edge* e : n->out)
+            if (e->n2 == r) return e;
+        return nullptr;
+    }
+
     void sparsify_phase() {
         std::vector<Cluster*> list;
         std::vector<std::vector<int>> touched;
@@ -1297,9 +1972,12 @@ private:
     // size; larger interfaces get more CTAs) and reads the ranks back. rt
     // receives the device task descriptors (C, positions, tau) for the
     // write-back.
-    template <class Job, class Gather>
+    struct NoPre {
+        void operator()(T*) const {}
+    };
+    template <class Job, class Gather, class Pre = NoPre>
     std::vector<int> rrqr_batch(std::vector<Job>& jobs, size_t celems, size_t ielems, std::vector<RRQRTaskRM<T>>& rt,
-                                Gather&& gather) {
+                                Gather&& gather, Pre&& pre = Pre()) {
         const size_t ibytes = (((ielems + jobs.size()) * sizeof(int)) + 255) & ~size_t(255);
         char* base = static_cast<char*>(scratch_.get(ibytes + celems * sizeof(T), stream_));
         int* ib = reinterpret_cast<int*>(base);
@@ -1337,6 +2015,7 @@ private:
         for (auto& kv : groups) o_ids[kv.first] = up.add(kv.second);
         char* d = up.commit(desc_arena_, stream_, pinned_);
         issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o_g), g);
+        pre(cb);  // device work that completes the C matrices (in stream order, before the RRQR)
         Autotuner& tuner = Autotuner::get();
         const bool tuning = tuner.mode() == 1;
         int dev = 0;
@@ -2070,22 +2749,38 @@ private:
         fwd.reserve(tape_.size());
         bwd.reserve(tape_.size());
         auto ptr = [](const T* p) { return (int64_t)reinterpret_cast<uintptr_t>(p); };
-        for (const TapeOp& t : tape_) {
-            POp f{}, b{};
+        // every op's segment and GEMV entries at offsets fixed in tape order, so
+        // the ops are built on host threads into the same arrays
+        const size_t ntape = tape_.size();
+        std::vector<size_t> seg_off(ntape + 1, 0), gemv_off(ntape + 1, 0);
+        for (size_t i = 0; i < ntape; ++i) {
+            const TapeOp& t = tape_[i];
+            seg_off[i + 1] = seg_off[i] + (t.kind == TK_QR ? t.segs.size() : t.kind == TK_MERGE ? t.c->children.size() : 0);
+            gemv_off[i + 1] = gemv_off[i] + (t.kind == TK_QR ? t.a12.size() : 0);
+        }
+        segs.resize(seg_off[ntape]);
+        gemv.resize(gemv_off[ntape]);
+        std::vector<POp> F(ntape), B(ntape);
+        host_parallel_for(ntape, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            const TapeOp& t = tape_[i];
+            POp& f = F[i];
+            POp& b = B[i];
+            size_t sq = seg_off[i], gq = gemv_off[i];
             switch (t.kind) {
                 case TK_QR: {
                     f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, 0, 0, ptr(t.fac), ptr(t.tp), 0,
-                                   (int)segs.size(), (int)t.segs.size()};
+                                   (int)seg_off[i], (int)t.segs.size()};
                     for (auto& s : t.segs) {
-                        segs.push_back(XSeg{s.first->xoff, s.second, 0});
+                        segs[sq++] = XSeg{s.first->xoff, s.second, 0};
                         f.rd.push_back(s.first);
                         f.wr.push_back(s.first);
                     }
                     f.smem = t.m;
                     b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0,
-                                   (int)gemv.size(), (int)t.a12.size()};
+                                   (int)gemv_off[i], (int)t.a12.size()};
                     for (auto& a : t.a12) {
-                        gemv.push_back(GemvRef<T>{ptr(a.B), a.n1->xoff, a.ld, a.s});
+                        gemv[gq++] = GemvRef<T>{ptr(a.B), a.n1->xoff, a.ld, a.s};
                         b.rd.push_back(a.n1);
                     }
                     b.rd.push_back(t.c);
@@ -2121,11 +2816,27 @@ private:
                     b.wr = {t.c};
                     b.smem = t.crows;
                     break;
+                case TK_ORTH:  // backward only: x(c)[0, m) <- Q x(c)[0, m)
+                    b.op = SolveOp{SK_APPLYQ, 1, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    b.rd = b.wr = {t.c};
+                    b.smem = t.m;
+                    break;
+                case TK_SPLIT0:
+                    f.op = SolveOp{SK_SPLIT0, 0, t.crows, t.ccols, t.rank, 0, t.c->xoff, t.f->xoff, 0, 0, 0, 0, 0};
+                    f.rd = {t.c};
+                    f.wr = {t.f};
+                    f.smem = 0;
+                    b.op = f.op;
+                    b.op.dir = 1;
+                    b.rd = {t.f};
+                    b.wr = {t.c};
+                    b.smem = 0;
+                    break;
                 case TK_MERGE: {
-                    f.op = SolveOp{SK_MERGE, 0, 0, 0, 0, 0, t.c->xoff, 0, 0, 0, 0, (int)segs.size(),
+                    f.op = SolveOp{SK_MERGE, 0, 0, 0, 0, 0, t.c->xoff, 0, 0, 0, 0, (int)seg_off[i],
                                    (int)t.c->children.size()};
                     for (Cluster* ch : t.c->children) {
-                        segs.push_back(XSeg{ch->xoff, ch->rsize, ch->csize});
+                        segs[sq++] = XSeg{ch->xoff, ch->rsize, ch->csize};
                         f.rd.push_back(ch);
                         b.wr.push_back(ch);
                     }
@@ -2137,9 +2848,14 @@ private:
                     break;
                 }
             }
-            // the QR op of an order-1.5 fine cluster has no forward part (its T is zero)
-            if (!(t.kind == TK_QR && t.fac == nullptr)) fwd.push_back(std::move(f));
-            bwd.push_back(std::move(b));
+        }
+        }, 256);
+        for (size_t i = 0; i < ntape; ++i) {
+            // the QR op of an order-1.5 fine cluster has no forward part (its T is zero),
+            // and neither has the Orthogonal op of --scale 0
+            if (!(tape_[i].kind == TK_QR && tape_[i].fac == nullptr) && tape_[i].kind != TK_ORTH)
+                fwd.push_back(std::move(F[i]));
+            bwd.push_back(std::move(B[i]));
         }
         std::reverse(bwd.begin(), bwd.end());
         const double tq2 = wall();
@@ -2508,6 +3224,9 @@ private:
                     break;
                 case SK_MERGE:
                     t.op.kind = SK_MERGE_T;
+                    break;
+                case SK_SPLIT0:
+                    t.op.kind = SK_SPLIT0_T;
                     break;
                 default:
                     throw std::logic_error("adjoint: op without a transpose");

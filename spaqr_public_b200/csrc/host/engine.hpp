@@ -36,6 +36,10 @@ struct Config {
     // Leaf part of every column for the ordering without coordinates (empty:
     // graph_bisection computes it); ignored when coordinates are set.
     std::vector<int> parts;
+    // Ordering without coordinates: the reference's numeric fill test (a fill
+    // candidate is kept only if ||A1^T A2|| > 1e-14, src/tree.cpp:856-859);
+    // 0 keeps every candidate that passes the separator tests.
+    int numeric_fill = 1;
 };
 
 // Event log record: [type, ilvl, order, a, b, c, d, e] (same layout as the

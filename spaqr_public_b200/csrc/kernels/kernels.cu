@@ -300,142 +300,6 @@ __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, cons
     }
 }
 
-// ------------------------------------------------------------------ trailing update
-// C <- (I - V T V^T)^T C = C - V (T^T (V^T C)) on one tile of kTN columns, the
-// rows in kRC-row chunks staged in shared memory (the next chunk's loads are
-// issued before the current chunk's arithmetic). Y = V^T C: each thread owns a
-// 2 x 2 block of Y and sums it over the rows in order; C -= V Z: each thread
-// keeps its column of Z in registers and walks rows of V (V rows padded to an
-// even stride, so pairs and quads load together). Per element the sums run in
-// the same order as a plain row-by-row product.
-// Row stride of the staged V chunk: a multiple of 16 bytes (FP32) or 16 bytes
-// per pair (FP64), so a thread's pair and a row's quads are aligned loads.
-template <class T>
-struct TVP {
-    static constexpr int v = sizeof(T) == 4 ? 36 : 34;
-};
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_trailing(const QRTask<T>* tasks, const TileRef* tiles, int p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int VP = TVP<T>::v, CP = kTN + 1, TP = kNB + 1;
-    constexpr int EPT = kRC * kNB / kThreads;  // 8 elements per thread per chunk (V and C each)
-    T* Vs = reinterpret_cast<T*>(smem_raw);  // kRC x VP
-    T* Cs = Vs + kRC * VP;                    // kRC x CP
-    T* Ys = Cs + kRC * CP;                    // kNB x CP
-    T* Tsh = Ys + kNB * CP;                   // kNB x TP
-    __shared__ T* colp[kTN];
-    const TileRef tr = tiles[blockIdx.x];
-    const QRTask<T> t = tasks[tr.task];
-    const int m = t.m, k = t.k;
-    const int w = min(kNB, k - p);
-    const int R = m - p;
-    const int nf = t.tr_only ? 0 : k - p - w;
-    const int ntot = nf + t.ntr;
-    const int c0 = tr.tile * kTN;
-    const int tn = min(kTN, ntot - c0);
-    const int tid = threadIdx.x;
-    if (tid < kTN) {
-        int vc = c0 + tid;
-        T* ptr = nullptr;
-        if (tid < tn) ptr = vc < nf ? t.fac + (size_t)(p + w + vc) * m : t.tr + (size_t)(vc - nf) * m;
-        colp[tid] = ptr;
-    }
-    const T* V0 = t.fac + (size_t)p * m;
-    for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-        int i = e % kNB, j = e / kNB;
-        Tsh[i * TP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
-    }
-    __syncthreads();
-    T vr[EPT], cr[EPT];
-    auto fetch = [&](int r0, bool want_c) {
-        const int rc = min(kRC, R - r0);
-#pragma unroll
-        for (int u = 0; u < EPT; ++u) {
-            const int e = tid + u * kThreads;
-            const int r = e % kRC, q = e / kRC;
-            const int gr = r0 + r;
-            const T x = V0[p + min(gr, R - 1) + (size_t)min(q, w - 1) * m];
-            vr[u] = (r < rc && q < w) ? (gr < q ? T(0) : (gr == q ? T(1) : x)) : T(0);
-            if (want_c) {
-                const T y = colp[min(q, tn - 1)][p + r0 + min(r, rc - 1)];
-                cr[u] = (r < rc && q < tn) ? y : T(0);
-            }
-        }
-    };
-    auto stash = [&](bool want_c) {
-#pragma unroll
-        for (int u = 0; u < EPT; ++u) {
-            const int e = tid + u * kThreads;
-            const int r = e % kRC, q = e / kRC;
-            Vs[r * VP + q] = vr[u];
-            if (want_c) Cs[r * CP + q] = cr[u];
-        }
-    };
-    // Y = V^T C: thread (qp, cp) owns Y(2qp..2qp+1, 2cp..2cp+1), summed over the rows in order
-    const int qp = tid / 16, cp = tid % 16;
-    T a00 = T(0), a01 = T(0), a10 = T(0), a11 = T(0);
-    fetch(0, true);
-    for (int r0 = 0; r0 < R; r0 += kRC) {
-        const int rc = min(kRC, R - r0);
-        stash(true);
-        __syncthreads();
-        if (r0 + kRC < R) fetch(r0 + kRC, true);
-        for (int r = 0; r < rc; ++r) {
-            const T v0 = Vs[r * VP + 2 * qp], v1 = Vs[r * VP + 2 * qp + 1];
-            const T x0 = Cs[r * CP + 2 * cp], x1 = Cs[r * CP + 2 * cp + 1];
-            a00 += v0 * x0;
-            a01 += v0 * x1;
-            a10 += v1 * x0;
-            a11 += v1 * x1;
-        }
-        __syncthreads();
-    }
-    Ys[(2 * qp) * CP + 2 * cp] = a00;
-    Ys[(2 * qp) * CP + 2 * cp + 1] = a01;
-    Ys[(2 * qp + 1) * CP + 2 * cp] = a10;
-    Ys[(2 * qp + 1) * CP + 2 * cp + 1] = a11;
-    __syncthreads();
-    // Z = T^T Y
-    const int c = tid % kTN, jq = tid / kTN;
-    constexpr int QPT = kNB / (kThreads / kTN);
-    T z[QPT];
-#pragma unroll
-    for (int u = 0; u < QPT; ++u) {
-        const int i = jq * QPT + u;
-        T s = T(0);
-        for (int l = 0; l <= i; ++l) s += Tsh[l * TP + i] * Ys[l * CP + c];
-        z[u] = s;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < QPT; ++u) Ys[(jq * QPT + u) * CP + c] = z[u];
-    __syncthreads();
-    T zc[kNB];
-#pragma unroll
-    for (int q = 0; q < kNB; ++q) zc[q] = Ys[q * CP + c];
-    // C -= V Z: thread (c, jq) rows jq, jq + 8, ... of each chunk
-    constexpr int RG = kThreads / kTN;
-    fetch(0, true);
-    for (int r0 = 0; r0 < R; r0 += kRC) {
-        const int rc = min(kRC, R - r0);
-        stash(true);
-        __syncthreads();
-        if (r0 + kRC < R) fetch(r0 + kRC, true);
-        for (int r = jq; r < rc; r += RG) {
-            T s = T(0);
-#pragma unroll
-            for (int q = 0; q < kNB; ++q) s += Vs[r * VP + q] * zc[q];
-            Cs[r * CP + c] -= s;
-        }
-        __syncthreads();
-        for (int e = tid; e < kRC * kTN; e += blockDim.x) {
-            int r = e % kRC, cc = e / kRC;
-            if (r < rc && cc < tn) colp[cc][p + r0 + r] = Cs[r * CP + cc];
-        }
-        __syncthreads();
-    }
-}
-
 // ------------------------------------------------------------------ trailing update on tensor cores
 // The same C <- C - V (T^T (V^T C)) on one tile of kTN columns, with both
 // products on the tensor pipe (warp-level mma.sync):
@@ -719,52 +583,6 @@ __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks
     }
 }
 
-// ------------------------------------------------------------------ TRSM (right, upper)
-template <class T>
-__global__ void __launch_bounds__(128) k_trsm(const TrsmTask<T>* tasks, const TileRef* tiles) {
-    __shared__ T Rs[64][kNB + 1];
-    __shared__ T Rd[kNB][kNB + 1];
-    const TileRef tr = tiles[blockIdx.x];
-    const TrsmTask<T> t = tasks[tr.task];
-    const int tid = threadIdx.x;
-    const int row = tr.tile * 128 + tid;
-    const bool active = row < t.rows;
-    for (int J0 = 0; J0 < t.k; J0 += kNB) {
-        const int wj = min(kNB, t.k - J0);
-        T acc[kNB];
-#pragma unroll
-        for (int jj = 0; jj < kNB; ++jj) acc[jj] = (active && jj < wj) ? t.X[row + (size_t)(J0 + jj) * t.ldx] : T(0);
-        for (int i0 = 0; i0 < J0; i0 += 64) {
-            const int ic = min(64, J0 - i0);
-            for (int e = tid; e < 64 * kNB; e += blockDim.x) {
-                int i = e % 64, jj = e / 64;
-                Rs[i][jj] = (i < ic && jj < wj) ? t.R[(i0 + i) + (size_t)(J0 + jj) * t.ldr] : T(0);
-            }
-            __syncthreads();
-            for (int i = 0; i < ic; ++i) {
-                const T xi = active ? t.X[row + (size_t)(i0 + i) * t.ldx] : T(0);
-#pragma unroll
-                for (int jj = 0; jj < kNB; ++jj) acc[jj] -= xi * Rs[i][jj];
-            }
-            __syncthreads();
-        }
-        for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-            int i = e % kNB, jj = e / kNB;
-            Rd[i][jj] = (i < wj && jj < wj) ? t.R[(J0 + i) + (size_t)(J0 + jj) * t.ldr] : T(1);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int jj = 0; jj < kNB; ++jj) {
-            acc[jj] = acc[jj] / Rd[jj][jj];
-#pragma unroll
-            for (int ll = jj + 1; ll < kNB; ++ll) acc[ll] -= acc[jj] * Rd[jj][ll];
-        }
-        if (active)
-            for (int jj = 0; jj < wj; ++jj) t.X[row + (size_t)(J0 + jj) * t.ldx] = acc[jj];
-        __syncthreads();
-    }
-}
-
 // ------------------------------------------------------------------ TRSM on tensor cores
 // X(rows x k) <- X R^-1 (R upper k x k) on 128-row tiles, blocked by 32
 // columns: for block J, S = X(:, 0:J) R(0:J, J) on the tensor pipe (3xTF32 /
@@ -923,6 +741,123 @@ template <class T>
 __global__ void k_unit_diag(const TrsmTask<T>* tasks) {
     const TrsmTask<T> t = tasks[blockIdx.x];
     for (int i = threadIdx.x; i < t.k; i += blockDim.x) t.X[i + (size_t)i * t.ldx] = T(1);
+}
+
+// One CTA per fill candidate: the squared entries of A1^T A2 (each entry a
+// dot product over the rows), summed over the CTA, square-rooted.
+template <class T>
+__global__ void __launch_bounds__(256) k_product_norm(const ProdNormTask<T>* tasks, double* out) {
+    __shared__ double red[32];
+    const ProdNormTask<T> t = tasks[blockIdx.x];
+    double s = 0.0;
+    const int pairs = t.c1 * t.c2;
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+        const int a = q % t.c1, b = q / t.c1;
+        const T* x = t.a1 + (size_t)a * t.ld1;
+        const T* y = t.a2 + (size_t)b * t.ld2;
+        double dot = 0.0;
+        for (int r = 0; r < t.rows; ++r) dot += (double)x[r] * (double)y[r];
+        s += dot * dot;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
+}
+
+// ------------------------------------------------------------------ --scale 0 helpers
+// One-sided (Hestenes) Jacobi on the columns of a copy W of R: round-robin
+// pairs (i, j), one pair per warp at a time, rotated until every pair is
+// orthogonal to working precision (or 30 sweeps); the singular values are then
+// the column norms. Writes 1 / sigma_min (sum of squares in FP64).
+template <class T>
+__global__ void __launch_bounds__(256) k_sigma_min(const SigmaTask<T>* tasks) {
+    __shared__ double red[32];
+    __shared__ int s_rot;
+    const SigmaTask<T> t = tasks[blockIdx.x];
+    const int n = t.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    T* W = t.work;
+    for (int e = tid; e < n * n; e += blockDim.x) {
+        const int i = e % n, j = e / n;
+        W[e] = i <= j ? t.R[i + (size_t)j * t.ld] : T(0);
+    }
+    __syncthreads();
+    const int np = n + (n & 1);  // players of the round-robin (a dummy when n is odd)
+    const double eps = sizeof(T) == 8 ? 1e-15 : 1e-7;
+    for (int sweep = 0; sweep < 30 && n > 1; ++sweep) {
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        for (int round = 0; round < np - 1; ++round) {
+            for (int pr = warp; pr < np / 2; pr += nw) {
+                // circle method: player np-1 fixed, the others rotate
+                int a = pr == 0 ? np - 1 : (round + pr) % (np - 1);
+                int b = (round + np - 1 - pr) % (np - 1);
+                if (a >= n || b >= n) continue;
+                if (a > b) { const int x = a; a = b; b = x; }
+                T* x = W + (size_t)a * n;
+                T* y = W + (size_t)b * n;
+                double al = 0, be = 0, ga = 0;
+                for (int r = lane; r < n; r += 32) {
+                    const double xr = x[r], yr = y[r];
+                    al += xr * xr;
+                    be += yr * yr;
+                    ga += xr * yr;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
+                if (fabs(ga) <= eps * sqrt(al * be) || ga == 0.0) continue;
+                const double zeta = (be - al) / (2.0 * ga);
+                const double tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
+                for (int r = lane; r < n; r += 32) {
+                    const double xr = x[r], yr = y[r];
+                    x[r] = (T)(cs * xr - sn * yr);
+                    y[r] = (T)(sn * xr + cs * yr);
+                }
+                if (lane == 0) s_rot = 1;
+            }
+            __syncthreads();
+        }
+        if (!s_rot) break;
+        __syncthreads();
+    }
+    double mn = 1e308;
+    for (int j = warp; j < n; j += nw) {
+        const T* x = W + (size_t)j * n;
+        double ss = 0;
+        for (int r = lane; r < n; r += 32) ss += (double)x[r] * (double)x[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        mn = fmin(mn, sqrt(ss));
+    }
+    if (lane == 0) red[warp] = mn;
+    __syncthreads();
+    if (tid == 0) {
+        double m2 = red[0];
+        for (int q = 1; q < nw; ++q) m2 = fmin(m2, red[q]);
+        *t.sinv = 1.0 / m2;
+    }
+}
+
+// One CTA per (task, 32-column tile of B): thread (i, jj) sums over the rows.
+template <class T>
+__global__ void __launch_bounds__(256) k_atb_scaled(const AtbTask<T>* tasks, const TileRef* tiles) {
+    const TileRef tr = tiles[blockIdx.x];
+    const AtbTask<T> t = tasks[tr.task];
+    const int j0 = tr.tile * 32;
+    const T sc = (T)*t.sinv;
+    for (int e = threadIdx.x; e < t.ni * 32; e += blockDim.x) {
+        const int jj = e / t.ni, i = e % t.ni;
+        const int j = j0 + jj;
+        if (j >= t.nj) continue;
+        const T* a = t.A + (size_t)i * t.lda;
+        const T* b = t.B + (size_t)j * t.ldb;
+        T acc = T(0);
+        for (int r = 0; r < t.rows; ++r) acc += a[r] * b[r];
+        t.C[(size_t)i * t.ldc + t.off + j] = sc * acc;
+    }
 }
 
 // ------------------------------------------------------------------ assembly scatter
@@ -1330,6 +1265,34 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_solve_step
             }
             break;
         }
+        case SK_SPLIT0: {
+            const int cfull = op.a, chead = op.b, fs = op.c;
+            T* xc = x + op.x0;
+            T* xf = x + op.x1;
+            if (op.dir == 0) {
+                for (int q = tid; q < fs; q += blockDim.x) xf[q] = xc[cfull - fs + q];
+            } else {
+                for (int q = tid; q < fs; q += blockDim.x) xc[chead - fs + q] = xf[q];
+            }
+            break;
+        }
+        case SK_SPLIT0_T: {
+            const int cfull = op.a, chead = op.b, fs = op.c;
+            T* xc = x + op.x0;
+            T* xf = x + op.x1;
+            if (op.dir == 0) {
+                for (int q = tid; q < fs; q += blockDim.x) {
+                    xc[cfull - fs + q] += xf[q];
+                    xf[q] = T(0);
+                }
+            } else {
+                for (int q = tid; q < fs; q += blockDim.x) {
+                    xf[q] += xc[chead - fs + q];
+                    xc[chead - fs + q] = T(0);
+                }
+            }
+            break;
+        }
         case SK_MERGE: {
             // dir 0: parent <- children rows; dir 1: children cols <- parent
             int cur = 0;
@@ -1533,11 +1496,6 @@ inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
 }
 
 template <class T>
-size_t trailing_smem() {
-    return sizeof(T) * ((size_t)kRC * TVP<T>::v + (size_t)kRC * (kTN + 1) + (size_t)kNB * (kTN + 1) +
-                        (size_t)kNB * (kNB + 1));
-}
-template <class T>
 size_t trailing_tc_smem() {
     return sizeof(T) * ((size_t)(kNB + kTN) * kTCS + (size_t)kNB * (kTN + 1) + (size_t)kNB * (kNB + 1));
 }
@@ -1569,6 +1527,23 @@ template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
     if (ntiles <= 0) return;
     k_trsm_tc<T><<<ntiles, 128, trsm_tc_smem<T>(), s>>>(tasks, tiles);
+}
+
+template <class T>
+void launch_product_norms(const ProdNormTask<T>* tasks, int ntasks, double* out, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_product_norm<T><<<ntasks, 256, 0, s>>>(tasks, out);
+}
+
+template <class T>
+void launch_sigma_min(const SigmaTask<T>* tasks, int ntasks, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    k_sigma_min<T><<<ntasks, 256, 0, s>>>(tasks);
+}
+template <class T>
+void launch_atb_scaled(const AtbTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
+    if (ntiles <= 0) return;
+    k_atb_scaled<T><<<ntiles, 256, 0, s>>>(tasks, tiles);
 }
 
 template <class T>
@@ -1664,7 +1639,6 @@ template <class T>
 void prepare_kernels() {
     once_per_device(reinterpret_cast<const void*>(&k_panel<T>), [] {
         cudaFuncSetAttribute(k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        cudaFuncSetAttribute(k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem<T>());
         cudaFuncSetAttribute(k_trailing_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)trailing_tc_smem<T>());
         cudaFuncSetAttribute(k_trsm_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_tc_smem<T>());
@@ -1678,6 +1652,9 @@ void prepare_kernels() {
     template void launch_trailing<T>(const QRTask<T>*, const TileRef*, int, int, cudaStream_t);               \
     template void launch_trsm<T>(const TrsmTask<T>*, const TileRef*, int, cudaStream_t);                      \
     template void launch_unit_diag<T>(const TrsmTask<T>*, int, cudaStream_t);                                   \
+    template void launch_product_norms<T>(const ProdNormTask<T>*, int, double*, cudaStream_t);                  \
+    template void launch_sigma_min<T>(const SigmaTask<T>*, int, cudaStream_t);                                  \
+    template void launch_atb_scaled<T>(const AtbTask<T>*, const TileRef*, int, cudaStream_t);                   \
     template void launch_scatter_values<T>(const uint64_t*, const double*, int64_t, cudaStream_t);         \
     template void launch_solve_step<T>(const SolveOp*, int, const XSeg*, const GemvRef<T>*, const T*, T*, int, \
                                        cudaStream_t);                                                          \

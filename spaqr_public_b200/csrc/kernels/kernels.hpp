@@ -92,11 +92,48 @@ struct TrsmTask {
 };
 template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s);
+// ||A1^T A2||_F of fill candidates (the numeric fill test of the ordering
+// without coordinates, src/tree.cpp:856-859): A1 rows x c1 and A2 rows x c2,
+// column-major, summed in FP64.
+template <class T>
+struct ProdNormTask {
+    const T* a1;
+    const T* a2;
+    int ld1, ld2, rows, c1, c2, pad;
+};
+template <class T>
+void launch_product_norms(const ProdNormTask<T>* tasks, int ntasks, double* out, cudaStream_t s);
+// --scale 0 sparsification (sparsify, src/tree.cpp:887-989):
+// sinv = 1 / sigma_min(R) of an upper-triangular n x n R (ld), the smallest
+// singular value of the stacked [A_pp; A_mp] after its QR (gesvd_values,
+// src/util.cpp:767-782), by one-sided Jacobi on a copy in work (n x n).
+template <class T>
+struct SigmaTask {
+    const T* R;
+    T* work;
+    double* sinv;
+    int ld, n;
+};
+template <class T>
+void launch_sigma_min(const SigmaTask<T>* tasks, int ntasks, cudaStream_t s);
+// C(i, off + j) = sinv * sum_r A(r, i) B(r, j) into a row-major C (row stride
+// ldc): the A_pp^T A_pm columns of the sparsification matrix. A rows x ni,
+// B rows x nj, column-major.
+template <class T>
+struct AtbTask {
+    const T* A;
+    const T* B;
+    T* C;
+    const double* sinv;
+    int lda, ldb, ldc, rows, ni, nj, off, pad;
+};
+template <class T>
+void launch_atb_scaled(const AtbTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s);
 // X(i, i) = 1 for i < k of every task (with X zeroed, the identity whose TRSM by
 // R is R^-1; the solve's triangular ops of size <= kRinvMax use it).
 template <class T>
 void launch_unit_diag(const TrsmTask<T>* tasks, int ntasks, cudaStream_t s);
-constexpr int kRinvMax = 512;
+constexpr int kRinvMax = 1024;
 
 // ---------------------------------------------------------------- truncated RRQR
 // Write-back after the RRQR (sparsifyD, src/tree.cpp:1082-1110): rebuild the
@@ -169,7 +206,11 @@ enum SolveKind : int {
     SK_MERGE = 3,   // Merge fwd/bwd copies
     SK_REASSIGN = 4, // rectangular row reassignment: dir 0 x(n)[nstart + i] = x(c)[idx[i]], dir 1 back
     SK_SPLIT_T = 5, // transpose of SK_SPLIT (same dir)
-    SK_MERGE_T = 6  // transpose of SK_MERGE (same dir): add into the source, zero the target
+    SK_MERGE_T = 6, // transpose of SK_MERGE (same dir): add into the source, zero the target
+    SK_SPLIT0 = 7,  // Split of --scale 0 (src/operations.cpp:118-119): dir 0 x(f) <- last a.. rows of
+                    // x(c)'s full segment (a = its length, c = x(f)'s length); dir 1 the last entries
+                    // of x(c)'s head (b = its length) <- x(f)
+    SK_SPLIT0_T = 8 // transpose of SK_SPLIT0 (same dir): add into the source, zero the target
 };
 struct SolveOp {
     int kind, dir;

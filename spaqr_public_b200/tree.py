@@ -99,6 +99,12 @@ class Tree:
         p = np.ascontiguousarray(parts, dtype=np.int32)
         check(lib().spq_set_parts(self._h, int(p.size), iptr(p)))
 
+    def set_fill_rule(self, numeric):
+        """Ordering without coordinates: 1 (default) keeps a fill candidate only
+        if ||A1^T A2|| > 1e-14 (the reference, src/tree.cpp:856-859); 0 keeps
+        every candidate that passes the separator tests."""
+        check(lib().spq_set_fill_rule(self._h, int(numeric)))
+
     # main steps (include/tree.h:139-147)
     def partition(self, A):
         m, n, cp, ri, va = _csc(A)

@@ -2,8 +2,10 @@
 
 No coordinates are set: the library orders the matrix from its own bisection of
 the A^T A graph through the reference's MetisPartition / getInterfacesUsingATA
-steps, and keeps every fill candidate that passes the separator tests. The
-oracle gets the same part vector and the same fill rule (numeric_fill off).
+steps, and applies the reference's numeric fill test (a candidate is kept only
+if ||A1^T A2|| > 1e-14, src/tree.cpp:856-859) on the device. The oracle gets
+the same part vector and the same fill rule; the second rule (keep every
+candidate, spq_set_fill_rule 0) is checked against the oracle with the test off.
 
 Bar (FP64): event log identical, one-shot solve within 1e-10 relative, GMRES
 (square) or CGLS (least squares) iteration counts identical. FP32 factor: the
@@ -25,26 +27,29 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "spaqr_public_b200", "_build", "spaqr")
 
 
-def _pair(A, levels, tol, skip, square=1, prec=FP64):
+def _pair(A, levels, tol, skip, square=1, prec=FP64, numeric=True):
     t = Tree(levels, skip, precision=prec)
     t.set_tol(tol)
     t.set_scale(1)
     t.set_square(square)
+    if not numeric:
+        t.set_fill_rule(0)
     t.partition(A)
     t.assemble(A)
     t.factorize()
     o = O.OracleTree(levels, skip, tol, 1, 1.0, square)
-    o.set_parts(graph_parts(A, levels), numeric_fill=False)
+    o.set_parts(graph_parts(A, levels), numeric_fill=numeric)
     o.partition(A)
     o.assemble(A)
     o.factorize()
     return t, o
 
 
+@pytest.mark.parametrize("numeric", [True, False])
 @pytest.mark.parametrize("kind,n,levels,tol,skip", [("2d", 64, 6, 1e-3, 0), ("3d", 16, 6, 1e-2, 1)])
-def test_graph_ordering_log_solve_gmres_match_oracle(gpu, kind, n, levels, tol, skip):
+def test_graph_ordering_log_solve_gmres_match_oracle(gpu, kind, n, levels, tol, skip, numeric):
     A = matgen.column_normalize(matgen.advdiff2d(n, seed=5) if kind == "2d" else matgen.advdiff3d(n, seed=5))
-    t, o = _pair(A, levels, tol, skip)
+    t, o = _pair(A, levels, tol, skip, numeric=numeric)
     assert np.array_equal(t.log(), o.log())
     b = np.random.default_rng(n).standard_normal(A[0])
     x = t.solve(b)

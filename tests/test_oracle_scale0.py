@@ -7,10 +7,8 @@ singular value of [A_pp; A_mp] (gesvd_values), A_pp <- A_pp Q
 fine cluster eliminated at once through split_edges. The reference has no tests
 or golden vectors for this path, so the restatement is checked for internal
 consistency: at a tolerance near zero the preconditioner is an exact solve, the
-one-shot error follows the tolerance, and GMRES converges. The GPU library
-has no device path for it yet (its factorize refuses --scale 0 with
-SPQ_ERR_UNSUPPORTED); this restatement is the checker such a path is built
-against.
+one-shot error follows the tolerance, and GMRES converges. It is the checker
+of the library's device path for --scale 0 (tests/test_gpu_scale0.py).
 """
 import numpy as np
 import pytest
