@@ -77,6 +77,7 @@ public:
         std::vector<Edge*> out, in;
         int xcap = 0;
         int64_t xoff = -1;
+        int out_mark = 0;  // elimination build: out edges before the phase's fill blocks
         int level() const { return id.self.lvl; }
     };
     enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE, TK_REASSIGN, TK_ORTH, TK_SPLIT0 };
@@ -92,6 +93,7 @@ public:
         const T* fac = nullptr;
         const T* tp = nullptr;
         const T* rinv = nullptr;  // R^-1 (k x k) of a QR / ScaleD op, formed after the factorization
+        const T* qt = nullptr;    // Q^T (m x m) of a ScaleD op, formed after the factorization
         int m = 0, k = 0, ld = 0;
         std::vector<std::pair<Cluster*, int>> segs;
         std::vector<A12> a12;
@@ -118,8 +120,10 @@ public:
         scratch_.hand_off(stream_);
         cudaStreamSynchronize(stream_);
         if (side_) cudaStreamDestroy(side_);
+        if (side2_) cudaStreamDestroy(side2_);
         if (ev_fork_) cudaEventDestroy(ev_fork_);
         if (ev_join_) cudaEventDestroy(ev_join_);
+        if (ev_join2_) cudaEventDestroy(ev_join2_);
         cudaStreamDestroy(stream_);
     }
     void open_device() {
@@ -127,8 +131,10 @@ public:
         cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaStreamCreateWithFlags(&side2_, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "event");
         cuda_check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "event");
+        cuda_check(cudaEventCreateWithFlags(&ev_join2_, cudaEventDisableTiming), "event");
         cudaMemPool_t pool = device_pool(cfg_.device);
         arena_.set_stream(stream_, pool);
         desc_arena_.set_stream(stream_, pool);
@@ -443,8 +449,9 @@ public:
 private:
     Config cfg_;
     cudaStream_t stream_ = nullptr;
-    cudaStream_t side_ = nullptr;  // second branch of a solve wave (forked from and joined to stream_)
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    cudaStream_t side_ = nullptr;   // branches of a solve wave (forked from and joined to stream_):
+    cudaStream_t side2_ = nullptr;  // tall Q applications and large triangular ops
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_join2_ = nullptr;
     Arena arena_;
     int* d_status_ = nullptr;  // device status word of the current factorization
     int status_ = 0;           // its value at the end of the factorization
@@ -488,6 +495,8 @@ private:
         int hkind, ha, hb;
         size_t boff;  // tall Q applications (cluster kernel): ops [boff, boff + nbig)
         int nbig, bcl;
+        size_t toff;  // large triangular ops (cluster kernel): ops [toff, toff + ntri)
+        int ntri, tcl, tk;
     };
     std::vector<POp> plan_fwd_, plan_bwd_;  // host copies, kept for the adjoint plan
     std::vector<int> gemv_cols_;            // columns of every neighbour block (work counts)
@@ -498,28 +507,46 @@ private:
         int hkind, ha, hb;   // kind and sizes of its largest op
         const SolveOp* big;  // tall Q applications, one cluster of bcl CTAs each
         int nbig, bcl;
+        const SolveOp* tri;  // large triangular ops, one cluster of tcl CTAs each (k <= tk)
+        int ntri, tcl, tk;
     };
     static constexpr int kApplyqBigRows = 384;
+    // A backward triangular op goes to the cluster kernel from kTriClWords
+    // words of R^-1 and neighbour blocks, on ceil(words / kTriClPerCta) CTAs
+    // (the wave's largest op sets the launch's cluster size).
+    static constexpr double kTriClWords = 32768, kTriClPerCta = 16384;
     Wave make_wave(const SolveOp* d_ops, const WMeta& mt) const {
-        return Wave{d_ops + mt.off, mt.n, mt.smem, mt.words, mt.hkind, mt.ha, mt.hb, d_ops + mt.boff, mt.nbig, mt.bcl};
+        return Wave{d_ops + mt.off, mt.n,     mt.smem,  mt.words, mt.hkind, mt.ha,  mt.hb,
+                    d_ops + mt.boff, mt.nbig, mt.bcl,  d_ops + mt.toff, mt.ntri, mt.tcl, mt.tk};
     }
-    // One sweep wave: the one-CTA ops and the tall Q applications (independent
-    // ops: the cluster launch runs on a branch forked from the stream).
+    // One sweep wave: the one-CTA ops, the tall Q applications and the large
+    // triangular ops (independent ops: each cluster launch runs on a branch
+    // forked from the stream).
     int launch_wave(const Wave& w, T* xb) {
-        const bool fork = w.nops > 0 && w.nbig > 0;
+        const bool fork = (w.nops > 0) + (w.nbig > 0) + (w.ntri > 0) > 1;
         if (fork) {
             cuda_check(cudaEventRecord(ev_fork_, stream_), "fork");
-            cuda_check(cudaStreamWaitEvent(side_, ev_fork_, 0), "fork");
+            if (w.nbig > 0) cuda_check(cudaStreamWaitEvent(side_, ev_fork_, 0), "fork");
+            if (w.ntri > 0) cuda_check(cudaStreamWaitEvent(side2_, ev_fork_, 0), "fork");
         }
         if (w.nbig > 0)
             cuda_check(launch_applyq_cl<T>(w.big, w.nbig, w.bcl, d_segs_, xb, fork ? side_ : stream_),
                        "solve cluster launch");
+        if (w.ntri > 0)
+            cuda_check(launch_tri_cl<T>(w.tri, w.ntri, w.tcl, w.tk, d_gemv_, xb, fork ? side2_ : stream_),
+                       "solve cluster launch");
         if (w.nops > 0) launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, stream_);
         if (fork) {
-            cuda_check(cudaEventRecord(ev_join_, side_), "join");
-            cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+            if (w.nbig > 0) {
+                cuda_check(cudaEventRecord(ev_join_, side_), "join");
+                cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+            }
+            if (w.ntri > 0) {
+                cuda_check(cudaEventRecord(ev_join2_, side2_), "join");
+                cuda_check(cudaStreamWaitEvent(stream_, ev_join2_, 0), "join");
+            }
         }
-        return (w.nops > 0) + (w.nbig > 0);
+        return (w.nops > 0) + (w.nbig > 0) + (w.ntri > 0);
     }
     std::vector<Wave> fwd_waves_, bwd_waves_, adj_waves_;
     int64_t xtot_ = 0;
@@ -1164,17 +1191,17 @@ private:
                 }
             },
             64);
+        const double ts1 = wall();
+        double ts2 = ts1, ts3 = ts1;
+        const size_t nedges0 = edges_.size();
         std::vector<Task> tasks;
         if (!coupled) {
         // 2. (this thread, level order) arena memory of every job and the missing
         //    fill blocks, created in the order of a task-by-task elimination; a
-        //    block an earlier task of this phase created is found in `made`
-        struct PairHash {
-            size_t operator()(const std::pair<const Cluster*, const Cluster*>& p) const {
-                return std::hash<const void*>()(p.first) * 31 + std::hash<const void*>()(p.second);
-            }
-        };
-        std::unordered_map<std::pair<const Cluster*, const Cluster*>, Edge*, PairHash> made;
+        //    block an earlier task of this phase created is among n's out edges
+        //    past out_mark (a few per cluster)
+        for (const Plan& P : plans)
+            for (Cluster* n : P.upd) n->out_mark = (int)n->out.size();
         std::vector<Task> all(nl);
         for (size_t i = 0; i < nl; ++i) {
             Cluster* c = lv[i];
@@ -1195,18 +1222,18 @@ private:
                 for (size_t h = 0; h < nh; ++h) {
                     Edge*& b = P.blk[u * nh + h];
                     if (b) continue;
-                    const auto key = std::make_pair((const Cluster*)n, (const Cluster*)P.H[h]->n2);
-                    auto f = made.find(key);
-                    if (f != made.end()) {
-                        b = f->second;
-                    } else {
-                        b = add_edge(n, P.H[h]->n2);
-                        made.emplace(key, b);
-                    }
+                    Cluster* r = P.H[h]->n2;
+                    for (size_t q = n->out_mark; q < n->out.size(); ++q)
+                        if (n->out[q]->n2 == r) {
+                            b = n->out[q];
+                            break;
+                        }
+                    if (!b) b = add_edge(n, r);
                 }
             }
             c->elim = true;
         }
+        ts2 = wall();
         // 3. (threads) each job's copy descriptors and block uids
         host_parallel_for(
             nl,
@@ -1246,6 +1273,7 @@ private:
                 }
             },
             64);
+        ts3 = wall();
         // 4. (this thread, level order) the tape, counters, log and, for least
         //    squares, the column blocks a finished elimination drops
         for (size_t i = 0; i < nl; ++i) {
@@ -1375,7 +1403,11 @@ private:
         auto wave = assign_waves(touched, next_uid_, &nw);
         print_waves("elim", wave, nw);
         if (cfg_.verbose >= 3)
-            std::fprintf(stderr, "[lvl %d] elim host: tasks %.2f ms, waves %.2f ms\n", ilvl_, (te1 - te0) * 1e3,
+            std::fprintf(stderr,
+                         "[lvl %d] elim host: tasks %.2f ms%s (plans %.2f, graph %.2f with %zu fill blocks, "
+                         "descriptors %.2f, tape %.2f), waves %.2f ms\n",
+                         ilvl_, (te1 - te0) * 1e3, coupled ? " (coupled: serial build)" : "", (ts1 - te0) * 1e3,
+                         (ts2 - ts1) * 1e3, edges_.size() - nedges0, (ts3 - ts2) * 1e3, (te1 - ts3) * 1e3,
                          (wall() - te1) * 1e3);
         // every wave's descriptors first (host threads, one scratch sized for the
         // largest wave), then the uploads and launches in wave order
@@ -2712,6 +2744,64 @@ private:
         launches_fact_ += 2;
     }
 
+    // Q^T of every ScaleD op of kDenseQMin..kRinvMax rows with at least half as
+    // many reflectors as rows: the identity run through the compact-WY update
+    // (the elimination's trailing kernel, panel by panel), once per
+    // factorization. The solve's forward sweep then applies Q^T as one dense
+    // product split over a thread-block cluster, instead of a chain of one
+    // reduction per reflector panel.
+    static constexpr int kDenseQMin = 128;
+    void form_qt() {
+        std::vector<QRTask<T>> tasks;
+        std::vector<TrsmTask<T>> diag;
+        double f = 0, by = 0;
+        int maxk = 0;
+        for (TapeOp& t : tape_) {
+            if (!(t.kind == TK_SCALED && t.fac != nullptr && t.k >= 1)) continue;
+            if (t.m < kDenseQMin || t.m > kRinvMax || 2 * t.k < t.m || t.ld != t.m) continue;
+            T* M = arena_.alloc_n<T>((size_t)t.m * t.m);
+            t.qt = M;
+            tasks.push_back(QRTask<T>{const_cast<T*>(t.fac), M, nullptr, const_cast<T*>(t.tp), t.m, t.k, t.m, 1,
+                                      nullptr});
+            diag.push_back(TrsmTask<T>{nullptr, M, t.m, t.m, t.m, t.m});
+            maxk = std::max(maxk, t.k);
+            f += 4.0 * t.m * t.m * t.k - 2.0 * t.m * t.k * t.k;
+            by += (2.0 * t.m * t.m + (double)t.m * t.k) * sizeof(T);
+        }
+        if (tasks.empty()) return;
+        Upload up;
+        const size_t o_q = up.add(tasks), o_d = up.add(diag);
+        // the tile lists of every panel step (alive until the commit: add()
+        // records where they lie)
+        std::vector<std::vector<TileRef>> tl;
+        for (int p = 0; p < maxk; p += kNB) {
+            std::vector<TileRef> v;
+            for (size_t i = 0; i < tasks.size(); ++i) {
+                if (tasks[i].k <= p) continue;
+                for (int c0 = 0, ti = 0; c0 < tasks[i].ntr; c0 += kTN, ++ti) v.push_back(TileRef{(int)i, ti});
+            }
+            tl.push_back(std::move(v));
+        }
+        std::vector<size_t> o_t;
+        for (const auto& v : tl) {
+            o_t.push_back(v.empty() ? size_t(0) : up.add(v));
+            o_t.push_back(v.size());
+        }
+        char* d = up.commit(desc_arena_, stream_, pinned_);
+        launch_unit_diag<T>(reinterpret_cast<const TrsmTask<T>*>(d + o_d), (int)diag.size(), stream_);
+        ++launches_fact_;
+        const double per = f / std::max<size_t>(1, o_t.size() / 2), pby = by / std::max<size_t>(1, o_t.size() / 2);
+        for (size_t i = 0; i < o_t.size(); i += 2) {
+            if (o_t[i + 1] == 0) continue;
+            timed(KF_TRAILING, per, pby, [&] {
+                launch_trailing<T>(reinterpret_cast<const QRTask<T>*>(d + o_q),
+                                   reinterpret_cast<const TileRef*>(d + o_t[i]), (int)o_t[i + 1], (int)(i / 2) * kNB,
+                                   stream_);
+            });
+            ++launches_fact_;
+        }
+    }
+
     void build_solve_plan() {
         if (rect_) {
             build_nrml_plan();
@@ -2719,6 +2809,7 @@ private:
         }
         const double tq0 = wall();
         form_rinv();
+        form_qt();
         int64_t xtot = 0;
         for (auto& c : clusters_) {
             c->xoff = xtot;
@@ -2789,7 +2880,8 @@ private:
                     break;
                 }
                 case TK_SCALED:
-                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), ptr(t.qt),
+                                   0, 0};
                     f.rd = f.wr = {t.c};
                     f.smem = t.m;
                     b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0, 0, 0};
@@ -2847,6 +2939,8 @@ private:
                     f.smem = b.smem = 0;
                     break;
                 }
+                default:  // TK_REASSIGN: least squares only
+                    break;
             }
         }
         }, 256);
@@ -3048,6 +3142,8 @@ private:
                     sc.push_back(f);
                     break;
                 }
+                default:  // TK_ORTH, TK_SPLIT0: --scale 0 runs on square systems only
+                    break;
             }
         }
         std::reverse(sb.begin(), sb.end());
@@ -3168,12 +3264,25 @@ private:
         auto big = [](const SolveOp& o) {
             return o.kind == SK_APPLYQ && o.b > 0 && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows;
         };
+        // backward triangular ops with R^-1 formed (or R = I) and large enough
+        // neighbour blocks or R^-1, and forward ScaleD ops with Q^T formed, go to
+        // the dense cluster kernel
+        auto cl_words = [&](const SolveOp& o) {
+            return o.kind == SK_TRI ? op_words(o) : (double)o.a * o.a;
+        };
+        auto tri = [&](const SolveOp& o) {
+            if (o.dir != 0 || o.a < 1 || o.a > kRinvMax) return false;
+            if (o.kind == SK_APPLYQ) return o.p2 != 0 && o.nseg == 0;
+            if (o.kind != SK_TRI || o.nseg > kTriMaxRefs) return false;
+            if (!(o.p1 != 0 || o.p0 == 0)) return false;
+            return op_words(o) >= kTriClWords;
+        };
         for (auto& w : waves) {
-            WMeta mt{all.size(), 0, 0, 0.0, -1, 0, 0, 0, 0, 0};
-            double hw = -1;
+            WMeta mt{all.size(), 0, 0, 0.0, -1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double hw = -1, tw = 0;
             int maxm = 0;
             for (int i : w)
-                if (!big(ops[i].op)) {
+                if (!big(ops[i].op) && !tri(ops[i].op)) {
                     all.push_back(ops[i].op);
                     mt.smem = std::max(mt.smem, ops[i].smem);
                     ++mt.n;
@@ -3186,6 +3295,15 @@ private:
                     ++mt.nbig;
                 }
             mt.bcl = mt.nbig ? (maxm + kApplyqClRows - 1) / kApplyqClRows : 0;
+            mt.toff = all.size();
+            for (int i : w)
+                if (tri(ops[i].op)) {
+                    all.push_back(ops[i].op);
+                    tw = std::max(tw, cl_words(ops[i].op));
+                    mt.tk = std::max(mt.tk, ops[i].op.a);
+                    ++mt.ntri;
+                }
+            mt.tcl = mt.ntri ? std::min(kTriMaxCl, std::max(2, (int)std::ceil(tw / kTriClPerCta))) : 0;
             for (int i : w) {
                 const double ow = op_words(ops[i].op);
                 mt.words += ow;
@@ -3281,6 +3399,7 @@ public:
         for (const Wave* w : all) {
             Wave a = *w, b = *w;
             a.nbig = 0;
+            a.ntri = 0;
             b.nops = 0;
             launch_wave(a, xbuf_);
             cudaEvent_t e;
@@ -3294,11 +3413,13 @@ public:
         for (size_t i = 0; i < all.size(); ++i) {
             float ms = 0;
             cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-            if (cfg_.verbose >= 3 && all[i]->nbig > 0) {
+            if (cfg_.verbose >= 3 && all[i]->nbig + all[i]->ntri > 0) {
                 float m1 = 0;
                 cudaEventElapsedTime(&m1, ev[i], mid[i]);
-                std::fprintf(stderr, "solve wave %zu: %d ops %.4f ms, %d tall Q ops (cluster %d) %.4f ms\n", i,
-                             all[i]->nops, m1, all[i]->nbig, all[i]->bcl, ms - m1);
+                std::fprintf(stderr,
+                             "solve wave %zu: %d ops %.4f ms, %d tall Q ops (cluster %d) and %d triangular ops "
+                             "(cluster %d) %.4f ms\n",
+                             i, all[i]->nops, m1, all[i]->nbig, all[i]->bcl, all[i]->ntri, all[i]->tcl, ms - m1);
             }
             out.push_back(ms);
             out.push_back(all[i]->nops);
@@ -3310,7 +3431,54 @@ public:
         }
         for (auto e : ev) cudaEventDestroy(e);
         for (auto e : mid) cudaEventDestroy(e);
+        if (cfg_.verbose >= 4) profile_solve_ops(all);
         return out;
+    }
+
+    // Diagnostics: every op of every sweep wave launched alone (5 times between
+    // two events), one line per op on stderr: wave, kind, dir, sizes, neighbour
+    // columns (triangular ops), the cluster size (tall Q ops, else 0) and the
+    // time of one launch. x is scratch here.
+    void profile_solve_ops(const std::vector<const Wave*>& all) {
+        cudaEvent_t e0, e1;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        constexpr int kRep = 5;
+        std::vector<SolveOp> h;
+        for (size_t i = 0; i < all.size(); ++i) {
+            const Wave& w = *all[i];
+            for (int part = 0; part < 3; ++part) {
+                const int n = part == 0 ? w.nops : part == 1 ? w.nbig : w.ntri;
+                if (n == 0) continue;
+                const SolveOp* d = part == 0 ? w.ops : part == 1 ? w.big : w.tri;
+                h.resize(n);
+                cuda_check(cudaMemcpy(h.data(), d, n * sizeof(SolveOp), cudaMemcpyDeviceToHost), "profile ops");
+                for (int j = 0; j < n; ++j) {
+                    const SolveOp& o = h[j];
+                    cudaEventRecord(e0, stream_);
+                    for (int r = 0; r < kRep; ++r) {
+                        if (part == 0)
+                            launch_solve_step<T>(d + j, 1, d_segs_, d_gemv_, nullptr, xbuf_, w.smem, stream_);
+                        else if (part == 1)
+                            cuda_check(launch_applyq_cl<T>(d + j, 1, w.bcl, d_segs_, xbuf_, stream_), "profile op");
+                        else
+                            cuda_check(launch_tri_cl<T>(d + j, 1, w.tcl, w.tk, d_gemv_, xbuf_, stream_), "profile op");
+                    }
+                    cudaEventRecord(e1, stream_);
+                    cuda_check(cudaEventSynchronize(e1), "profile op");
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    long long gc = 0;
+                    if (o.kind == SK_TRI)
+                        for (int q = 0; q < o.nseg; ++q) gc += gemv_cols_[o.seg0 + q];
+                    std::fprintf(stderr, "op %zu kind %d dir %d a %d b %d c %d nseg %d gcols %lld cl %d us %.2f\n", i,
+                                 o.kind, o.dir, o.a, o.b, o.c, o.nseg, gc, part == 0 ? 0 : part == 1 ? w.bcl : w.tcl,
+                                 ms * 1e3 / kRep);
+                }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
     }
 
 private:

@@ -237,6 +237,16 @@ void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const Gem
 constexpr int kApplyqClRows = 256;
 template <class T>
 cudaError_t launch_applyq_cl(const SolveOp* ops, int nops, int cluster, const XSeg* segs, T* x, cudaStream_t s);
+// SK_TRI ops of dir 0 whose R^-1 was formed (p1) or whose R is the identity
+// (p0 == 0), with at most kTriMaxRefs neighbour blocks and k <= kmax <=
+// kRinvMax, on thread-block clusters of `cluster` CTAs: the neighbour columns
+// and then the rows of R^-1 are split over the cluster (a DSMEM reduction
+// between the two).
+constexpr int kTriMaxCl = 16;
+constexpr int kTriMaxRefs = 64;
+template <class T>
+cudaError_t launch_tri_cl(const SolveOp* ops, int nops, int cluster, int kmax, const GemvRef<T>* gemv, T* x,
+                          cudaStream_t s);
 // dst[pos[k]] = src[pos[k]] (one x buffer into the other at the given positions)
 template <class T>
 void launch_seg_copy(const T* src, T* dst, const int64_t* pos, int n, cudaStream_t s);

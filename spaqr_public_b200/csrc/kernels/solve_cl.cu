@@ -154,6 +154,153 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
     if (has) *xp = xr;
 }
 
+
+// One backward triangular op (SK_TRI, dir 0: x_c <- R^-1 (x_c - sum_b B_b x_b),
+// the R^-1 solve of Tree::solve after the neighbour products, src/tree.cpp:
+// 1440-1466 with the QR / ScaleD operations' backward steps) or one forward
+// ScaleD op whose Q^T was formed (SK_APPLYQ with p2 = Q^T, m x m column-major:
+// x_c <- Q^T x_c, the Q^T step of the scaling, src/tree.cpp:557) on a cluster
+// of CL CTAs, for ops whose matrices are too large for one CTA's load stream:
+//   1. CTA cr sums B(:, j) x_j over its slice of the op's neighbour columns
+//      (the blocks' columns concatenated, ceil(gc / CL) per CTA) for all k
+//      rows into its shared memory;
+//   2. one cluster barrier; every CTA forms xs = x_c - (p_0 + ... + p_{CL-1})
+//      from the slices' partials read over DSMEM in rank order (the same
+//      values in every CTA); a second barrier, after which no CTA reads
+//      another's shared memory and x_c may be written;
+//   3. CTA cr writes rows [cr S, (cr + 1) S) of R^-1 xs or Q^T xs (S =
+//      ceil(k / CL)), or of xs itself where R is the identity (p0 == 0).
+// Results are deterministic for a given cluster size; they differ from the
+// one-CTA form only by the order of the neighbour sums.
+constexpr int kTThreads = 256;
+constexpr int kTGU = 16;  // loads in flight per thread in the neighbour products
+
+template <class T>
+__global__ void __launch_bounds__(kTThreads) k_tri_cl(const SolveOp* ops, const GemvRef<T>* gemv, T* x) {
+    extern __shared__ __align__(16) unsigned char tri_raw[];
+    __shared__ GemvRef<T> refs[kTriMaxRefs];
+    __shared__ int cstart[kTriMaxRefs + 1];
+    __shared__ T red[kTThreads];
+    cg::cluster_group cl = cg::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int cr = (int)cl.block_rank();
+    const SolveOp op = ops[blockIdx.x / CL];
+    const bool dense = op.kind == SK_APPLYQ;  // Q^T, full; else R^-1, upper triangular
+    const int k = op.a, nb = dense ? 0 : op.nseg;
+    T* part = reinterpret_cast<T*>(tri_raw);  // this CTA's partial sums (k)
+    T* xs = part + k;                         // the reduced right-hand side (k)
+    T* xc = x + op.x0;
+    const int tid = threadIdx.x;
+    for (int b = tid; b < nb; b += kTThreads) refs[b] = gemv[op.seg0 + b];
+    __syncthreads();
+    if (tid == 0) {
+        int c = 0;
+        for (int b = 0; b < nb; ++b) {
+            cstart[b] = c;
+            c += refs[b].s;
+        }
+        cstart[nb] = c;
+    }
+    __syncthreads();
+    // 1. partial neighbour products over this CTA's column slice
+    const int gc = cstart[nb];
+    const int sc = (gc + CL - 1) / CL;
+    const int c0 = min(gc, cr * sc), c1 = min(gc, c0 + sc);
+    {
+        const int RT = min(kTThreads, (k + 31) & ~31);
+        const int G = kTThreads / RT;
+        const int ri = tid % RT, g = tid / RT;
+        for (int i0 = 0; i0 < k; i0 += RT) {
+            const int i = i0 + ri;
+            const int ic = min(i, k - 1);
+            T a[4] = {T(0), T(0), T(0), T(0)};
+            if (g < G) {
+                for (int b = 0; b < nb; ++b) {
+                    const int lo = max(c0, cstart[b]) - cstart[b], hi = min(c1, cstart[b + 1]) - cstart[b];
+                    if (lo >= hi) continue;
+                    const GemvRef<T> r = refs[b];
+                    const T* B = reinterpret_cast<const T*>(r.boff) + ic;
+                    const T* xn = x + r.xoff;
+                    const size_t ld = (size_t)r.ld;
+                    const int last = hi - 1;
+                    for (int j = lo + g; j < hi; j += kTGU * G) {
+                        T bv[kTGU], xv[kTGU];
+#pragma unroll
+                        for (int u = 0; u < kTGU; ++u) {
+                            const int jj = min(j + u * G, last);
+                            bv[u] = B[(size_t)jj * ld];
+                            xv[u] = xn[jj];
+                        }
+#pragma unroll
+                        for (int u = 0; u < kTGU; ++u)
+                            if (j + u * G <= last) a[u & 3] += bv[u] * xv[u];
+                    }
+                }
+            }
+            red[tid] = (a[0] + a[1]) + (a[2] + a[3]);
+            __syncthreads();
+            if (g == 0 && i < k) {
+                T sum = T(0);
+                for (int q = 0; q < G; ++q) sum += red[q * RT + ri];
+                part[i] = sum;
+            }
+            __syncthreads();
+        }
+    }
+    cl.sync();
+    // 2. xs = x_c - the partials in rank order
+    if (gc == 0) {
+        for (int i = tid; i < k; i += kTThreads) xs[i] = xc[i];
+    } else {
+        for (int i = tid; i < k; i += kTThreads) {
+            T sum = T(0);
+            for (int q = 0; q < CL; ++q) sum += *cl.map_shared_rank(part + i, q);
+            xs[i] = xc[i] - sum;
+        }
+    }
+    cl.sync();
+    // 3. this CTA's rows of R^-1 xs (column-major, exactly zero below the
+    //    diagonal: a warp starts at its first row) or of Q^T xs
+    const int S = (k + CL - 1) / CL;
+    const int r0 = min(k, cr * S), r1 = min(k, r0 + S);
+    const T* Ri = dense ? reinterpret_cast<const T*>(op.p2)
+                        : op.p1 != 0 ? reinterpret_cast<const T*>(op.p1) : nullptr;
+    if (!Ri) {
+        for (int i = r0 + tid; i < r1; i += kTThreads) xc[i] = xs[i];
+        return;
+    }
+    const int nr = r1 - r0;
+    if (nr <= 0) return;
+    const int RT = min(kTThreads, (nr + 31) & ~31);
+    const int G = kTThreads / RT;
+    const int ri = tid % RT, g = tid / RT;
+    for (int i0 = r0; i0 < r1; i0 += RT) {
+        const int i = i0 + ri;
+        const int ic = min(i, k - 1);
+        const int jb = dense ? 0 : min(i0 + (ri & ~31), k - 1);
+        T a[4] = {T(0), T(0), T(0), T(0)};
+        if (g < G) {
+            int j = jb + g;
+            for (; j + (kTGU - 1) * G < k; j += kTGU * G) {
+                T rv[kTGU];
+#pragma unroll
+                for (int u = 0; u < kTGU; ++u) rv[u] = Ri[ic + (size_t)(j + u * G) * k];
+#pragma unroll
+                for (int u = 0; u < kTGU; ++u) a[u & 3] += rv[u] * xs[j + u * G];
+            }
+            for (; j < k; j += G) a[0] += Ri[ic + (size_t)j * k] * xs[j];
+        }
+        red[tid] = (a[0] + a[1]) + (a[2] + a[3]);
+        __syncthreads();
+        if (g == 0 && i < r1) {
+            T sum = T(0);
+            for (int q = 0; q < G; ++q) sum += red[q * RT + ri];
+            xc[i] = sum;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 template <class T>
@@ -180,5 +327,33 @@ cudaError_t launch_applyq_cl(const SolveOp* ops, int nops, int cluster, const XS
 
 template cudaError_t launch_applyq_cl<double>(const SolveOp*, int, int, const XSeg*, double*, cudaStream_t);
 template cudaError_t launch_applyq_cl<float>(const SolveOp*, int, int, const XSeg*, float*, cudaStream_t);
+
+template <class T>
+cudaError_t launch_tri_cl(const SolveOp* ops, int nops, int cluster, int kmax, const GemvRef<T>* gemv, T* x,
+                          cudaStream_t s) {
+    if (nops <= 0) return cudaSuccess;
+    if (cluster < 1 || cluster > kTriMaxCl || kmax < 1 || kmax > kRinvMax) return cudaErrorInvalidValue;
+    once_per_device(reinterpret_cast<const void*>(&k_tri_cl<T>), [] {
+        cudaFuncSetAttribute(k_tri_cl<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nops * cluster), 1, 1);
+    cfg.blockDim = dim3(kTThreads, 1, 1);
+    cfg.dynamicSmemBytes = 2 * (size_t)kmax * sizeof(T);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_tri_cl<T>, ops, gemv, x);
+}
+
+template cudaError_t launch_tri_cl<double>(const SolveOp*, int, int, int, const GemvRef<double>*, double*,
+                                           cudaStream_t);
+template cudaError_t launch_tri_cl<float>(const SolveOp*, int, int, int, const GemvRef<float>*, float*,
+                                          cudaStream_t);
 
 }  // namespace spq
