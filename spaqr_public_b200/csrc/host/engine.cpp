@@ -2744,12 +2744,13 @@ private:
         launches_fact_ += 2;
     }
 
-    // Q^T of every ScaleD op of kDenseQMin..kRinvMax rows with at least half as
-    // many reflectors as rows: the identity run through the compact-WY update
-    // (the elimination's trailing kernel, panel by panel), once per
-    // factorization. The solve's forward sweep then applies Q^T as one dense
-    // product split over a thread-block cluster, instead of a chain of one
-    // reduction per reflector panel.
+    // Q^T of every ScaleD and OrthD op, and of every elimination QR op whose
+    // rows are one cluster's segment, of kDenseQMin..kRinvMax rows with at
+    // least half as many reflectors as rows: the identity run through the
+    // compact-WY update (the elimination's trailing kernel, panel by panel),
+    // once per factorization. The solve's sweeps then apply Q^T (and OrthD's
+    // Q, as its transpose) as one dense product split over a thread-block
+    // cluster, instead of a chain of one reduction per reflector panel.
     static constexpr int kDenseQMin = 128;
     void form_qt() {
         std::vector<QRTask<T>> tasks;
@@ -2757,7 +2758,9 @@ private:
         double f = 0, by = 0;
         int maxk = 0;
         for (TapeOp& t : tape_) {
-            if (!(t.kind == TK_SCALED && t.fac != nullptr && t.k >= 1)) continue;
+            // elimination QR ops qualify when their rows are one cluster's segment
+            const bool qr1 = t.kind == TK_QR && t.segs.size() == 1 && t.segs[0].second == t.m;
+            if (!((t.kind == TK_SCALED || t.kind == TK_ORTHD || qr1) && t.fac != nullptr && t.k >= 1)) continue;
             if (t.m < kDenseQMin || t.m > kRinvMax || 2 * t.k < t.m || t.ld != t.m) continue;
             T* M = arena_.alloc_n<T>((size_t)t.m * t.m);
             t.qt = M;
@@ -2867,6 +2870,11 @@ private:
                         f.rd.push_back(s.first);
                         f.wr.push_back(s.first);
                     }
+                    if (t.qt) {  // one segment (form_qt): contiguous x, Q^T formed
+                        f.op.x0 = t.segs[0].first->xoff;
+                        f.op.nseg = 0;
+                        f.op.p2 = ptr(t.qt);
+                    }
                     f.smem = t.m;
                     b.op = SolveOp{SK_TRI, 0, t.k, 0, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.rinv), 0,
                                    (int)gemv_off[i], (int)t.a12.size()};
@@ -2889,7 +2897,8 @@ private:
                     b.smem = t.rinv ? 2 * t.k : t.k;
                     break;
                 case TK_ORTHD:
-                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), 0, 0, 0};
+                    f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, t.c->xoff, 0, ptr(t.fac), ptr(t.tp), ptr(t.qt),
+                                   0, 0};
                     f.rd = f.wr = {t.c};
                     f.smem = t.m;
                     b.op = f.op;
@@ -3259,23 +3268,25 @@ private:
     }
     void pack_waves(const std::vector<POp>& ops, const std::vector<std::vector<int>>& waves,
                     std::vector<SolveOp>& all, std::vector<WMeta>& meta) const {
-        // Q applications of at least kApplyqBigRows rows go to the cluster kernel
-        // (after the wave's other ops in the array)
-        auto big = [](const SolveOp& o) {
-            return o.kind == SK_APPLYQ && o.b > 0 && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows;
-        };
-        // backward triangular ops with R^-1 formed (or R = I) and large enough
-        // neighbour blocks or R^-1, and forward ScaleD ops with Q^T formed, go to
-        // the dense cluster kernel
+        // Every op goes to exactly one of three launches (after the wave's
+        // one-CTA ops in the array: the tall Q applications, then the dense ops).
+        // Backward triangular ops with R^-1 formed (or R = I) and large enough
+        // neighbour blocks or R^-1, and ScaleD / OrthD steps with Q^T formed, go
+        // to the dense cluster kernel
         auto cl_words = [&](const SolveOp& o) {
             return o.kind == SK_TRI ? op_words(o) : (double)o.a * o.a;
         };
         auto tri = [&](const SolveOp& o) {
-            if (o.dir != 0 || o.a < 1 || o.a > kRinvMax) return false;
-            if (o.kind == SK_APPLYQ) return o.p2 != 0 && o.nseg == 0;
-            if (o.kind != SK_TRI || o.nseg > kTriMaxRefs) return false;
+            if (o.a < 1 || o.a > kRinvMax) return false;
+            if (o.kind == SK_APPLYQ) return o.p2 != 0 && o.nseg == 0;  // Q^T x (dir 0) or Q x (dir 1)
+            if (o.kind != SK_TRI || o.dir != 0 || o.nseg > kTriMaxRefs) return false;
             if (!(o.p1 != 0 || o.p0 == 0)) return false;
             return op_words(o) >= kTriClWords;
+        };
+        // other Q applications of at least kApplyqBigRows rows go to the tall-Q
+        // cluster kernel
+        auto big = [&](const SolveOp& o) {
+            return o.kind == SK_APPLYQ && o.b > 0 && o.a >= kApplyqBigRows && o.a <= 16 * kApplyqClRows && !tri(o);
         };
         for (auto& w : waves) {
             WMeta mt{all.size(), 0, 0, 0.0, -1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -3304,6 +3315,8 @@ private:
                     ++mt.ntri;
                 }
             mt.tcl = mt.ntri ? std::min(kTriMaxCl, std::max(2, (int)std::ceil(tw / kTriClPerCta))) : 0;
+            if ((size_t)(mt.n + mt.nbig + mt.ntri) != w.size())
+                throw std::logic_error("solve plan: an op was routed to more or fewer than one launch");
             for (int i : w) {
                 const double ow = op_words(ops[i].op);
                 mt.words += ow;

@@ -157,10 +157,12 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
 
 // One backward triangular op (SK_TRI, dir 0: x_c <- R^-1 (x_c - sum_b B_b x_b),
 // the R^-1 solve of Tree::solve after the neighbour products, src/tree.cpp:
-// 1440-1466 with the QR / ScaleD operations' backward steps) or one forward
-// ScaleD op whose Q^T was formed (SK_APPLYQ with p2 = Q^T, m x m column-major:
-// x_c <- Q^T x_c, the Q^T step of the scaling, src/tree.cpp:557) on a cluster
-// of CL CTAs, for ops whose matrices are too large for one CTA's load stream:
+// 1440-1466 with the QR / ScaleD operations' backward steps) or one ScaleD /
+// OrthD step whose Q^T was formed (SK_APPLYQ with p2 = Q^T, m x m column-major:
+// x_c <- Q^T x_c for dir 0, x_c <- Q x_c as the transposed product for dir 1;
+// the Q^T / Q steps of the scaling and the sparsification, src/tree.cpp:557,
+// src/operations.cpp) on a cluster of CL CTAs, for ops whose matrices are too
+// large for one CTA's load stream:
 //   1. CTA cr sums B(:, j) x_j over its slice of the op's neighbour columns
 //      (the blocks' columns concatenated, ceil(gc / CL) per CTA) for all k
 //      rows into its shared memory;
@@ -168,8 +170,9 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
 //      from the slices' partials read over DSMEM in rank order (the same
 //      values in every CTA); a second barrier, after which no CTA reads
 //      another's shared memory and x_c may be written;
-//   3. CTA cr writes rows [cr S, (cr + 1) S) of R^-1 xs or Q^T xs (S =
-//      ceil(k / CL)), or of xs itself where R is the identity (p0 == 0).
+//   3. CTA cr writes rows [cr S, (cr + 1) S) of R^-1 xs, Q^T xs or Q xs (S =
+//      ceil(k / CL)), or of xs itself where R is the identity (p0 == 0); Q xs
+//      reads columns of Q^T, a warp per row with the lanes along the column.
 // Results are deterministic for a given cluster size; they differ from the
 // one-CTA form only by the order of the neighbour sums.
 constexpr int kTThreads = 256;
@@ -271,6 +274,27 @@ __global__ void __launch_bounds__(kTThreads) k_tri_cl(const SolveOp* ops, const 
     }
     const int nr = r1 - r0;
     if (nr <= 0) return;
+    if (dense && op.dir == 1) {
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int i = r0 + warp; i < r1; i += kTThreads / 32) {
+            const T* col = Ri + (size_t)i * k;
+            T a[4] = {T(0), T(0), T(0), T(0)};
+            int j = lane;
+            for (; j + 32 * (kTGU - 1) < k; j += 32 * kTGU) {
+                T cv[kTGU];
+#pragma unroll
+                for (int u = 0; u < kTGU; ++u) cv[u] = col[j + 32 * u];
+#pragma unroll
+                for (int u = 0; u < kTGU; ++u) a[u & 3] += cv[u] * xs[j + 32 * u];
+            }
+            for (; j < k; j += 32) a[0] += col[j] * xs[j];
+            T sum = (a[0] + a[1]) + (a[2] + a[3]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) xc[i] = sum;
+        }
+        return;
+    }
     const int RT = min(kTThreads, (nr + 31) & ~31);
     const int G = kTThreads / RT;
     const int ri = tid % RT, g = tid / RT;
