@@ -510,7 +510,7 @@ private:
         const SolveOp* tri;  // large triangular ops, one cluster of tcl CTAs each (k <= tk)
         int ntri, tcl, tk;
     };
-    static constexpr int kApplyqBigRows = 384;
+    static constexpr int kApplyqBigRows = 192;
     // A backward triangular op goes to the cluster kernel from kTriClWords
     // words of R^-1 and neighbour blocks, on ceil(words / kTriClPerCta) CTAs
     // (the wave's largest op sets the launch's cluster size).

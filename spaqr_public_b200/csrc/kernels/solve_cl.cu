@@ -6,13 +6,13 @@
 // from unit-lower V with one kNB x kNB T factor per panel) runs on a cluster
 // of CL CTAs, CTA cr holding rows [cr S, (cr + 1) S) with S = ceil(m / CL) <=
 // 256: one row per thread, its x value in a register. A panel costs one pass
-// that loads the row's kNB entries of V into registers and forms the kNB
-// products v x (the next panel's V and T loads are issued right after, so
-// they are in flight during this panel's exchange), a warp transpose-sum and
-// a CTA sum, the CTA's kNB sums stored
+// that takes the row's kNB entries of V from registers and forms the kNB
+// products v x, a warp transpose-sum and a CTA sum, the CTA's kNB sums stored
 // into slot cr of every CTA of the cluster (DSMEM, double-buffered by panel
-// parity), one cluster barrier, then in every warp y = the slots summed in
-// rank order, z = T^T y (dir 0) or T y (dir 1) by lane shuffles, and
+// parity) and released by a fence, then the next panel's V and T loads, one
+// relaxed cluster barrier (the loads stay in flight through it: a releasing
+// arrive would first wait for them), then in every warp y = the slots summed
+// in rank order, z = T^T y (dir 0) or T y (dir 1) by lane shuffles, and
 // x -= v^T z from the registers. V is read once per panel (the one-CTA form
 // reads it twice and walks m / 256 rows per thread in each pass).
 #include <cooperative_groups.h>
@@ -115,7 +115,6 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
             const T vq = q < rr ? vraw[q] : (q == rr ? T(1) : T(0));
             v[q] = (has && q < w) ? vq : T(0);
         }
-        if (pi + 1 < np) load_panel(pi + 1, vraw, traw);  // in flight during the exchange
         T a[kNB];
 #pragma unroll
         for (int q = 0; q < kNB; ++q) a[q] = v[q] * xr;
@@ -127,7 +126,10 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
             for (int q = 0; q < kAWarps; ++q) s += wred[q][lane];
             for (int dst = warp; dst < CL; dst += kAWarps) *cl.map_shared_rank(&part[buf][cr][lane], dst) = s;
         }
-        cl.sync();
+        asm volatile("fence.acq_rel.cluster;" ::: "memory");
+        if (pi + 1 < np) load_panel(pi + 1, vraw, traw);
+        asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+        asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
         T y = T(0);
         for (int q = 0; q < CL; ++q) y += part[buf][q][lane];
         T z = T(0);  // lane j: z_j = sum_l T(l, j) y_l (dir 0) or T(j, l) y_l (dir 1); zero past w
