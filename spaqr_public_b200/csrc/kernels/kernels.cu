@@ -632,6 +632,12 @@ __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks
 // each thread solves its row of (X(:, J) - S) against the 32 x 32 diagonal
 // block of R and stores it (the next blocks read it back).
 constexpr int kTrXS = 136;  // column stride of the staged X chunk (128 rows + pad)
+// Stages of the chunk pipeline: 3 in FP32 (89 KB of shared memory with S and the
+// diagonal block), 2 in FP64 (111 KB): two CTAs per SM either way.
+template <class T>
+struct TrsmStages {
+    static constexpr int v = sizeof(T) == 4 ? 3 : 2;
+};
 constexpr int kTrRS = 40;   // row stride of the staged R chunk (32 columns + pad)
 
 // S(32 rows of the warp, 32 columns) += Xc(:, 0:32) Rc(0:32, :)
@@ -712,16 +718,18 @@ __device__ __forceinline__ void trsm_mma_store(const double (&acc)[2][4][4], dou
 
 template <class T>
 size_t trsm_tc_smem() {
-    return sizeof(T) * ((size_t)kNB * kTrXS + (size_t)kNB * kTrRS + (size_t)128 * (kNB + 1) + (size_t)kNB * (kNB + 1));
+    return sizeof(T) * ((size_t)TrsmStages<T>::v * (kNB * kTrXS + kNB * kTrRS) + (size_t)128 * (kNB + 1) +
+                        (size_t)kNB * (kNB + 1));
 }
 
 template <class T>
 __global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const TileRef* tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Xs = reinterpret_cast<T*>(smem_raw);  // 32 columns x kTrXS (column-major chunk of X)
-    T* Rs = Xs + kNB * kTrXS;                 // 32 rows x kTrRS (chunk of R)
-    T* Ss = Rs + kNB * kTrRS;                 // 128 x (kNB + 1): S, row-major
-    T* Rd = Ss + 128 * (kNB + 1);             // kNB x (kNB + 1): diagonal block
+    constexpr int S = TrsmStages<T>::v;
+    constexpr int STG = kNB * kTrXS + kNB * kTrRS;  // one stage: X chunk, then R chunk
+    T* stg = reinterpret_cast<T*>(smem_raw);       // S stages
+    T* Ss = stg + S * STG;                          // 128 x (kNB + 1): S, row-major
+    T* Rd = Ss + 128 * (kNB + 1);                   // kNB x (kNB + 1): diagonal block
     const TileRef tr = tiles[blockIdx.x];
     const TrsmTask<T> t = tasks[tr.task];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -737,21 +745,37 @@ __global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const
             for (int b = 0; b < 4; ++b)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[a][b][c] = T(0);
-        for (int i0 = 0; i0 < J0; i0 += kNB) {  // J0 is a multiple of kNB: every chunk is full
-            // X(tile rows, i0:i0+32): thread = row, coalesced along rows
-#pragma unroll 4
-            for (int c = 0; c < kNB; ++c) {
-                const T x = t.X[rclamp + (size_t)(i0 + c) * t.ldx];
-                Xs[c * kTrXS + tid] = active ? x : T(0);
+        // chunks i0 = 32 ch < J0 (every chunk full), S - 1 in flight: X(tile
+        // rows, i0:i0+32) with thread = row (coalesced along rows; this thread
+        // wrote those entries itself), R(i0:i0+32, J0:J0+wj), zero-filled past
+        const int nch = J0 / kNB;
+        auto issue = [&](int ch) {
+            if (ch < nch) {
+                T* Xs = stg + (ch % S) * STG;
+                T* Rs = Xs + kNB * kTrXS;
+                const int i0 = ch * kNB;
+#pragma unroll 8
+                for (int c = 0; c < kNB; ++c)
+                    cp_async_el(Xs + c * kTrXS + tid, t.X + rclamp + (size_t)(i0 + c) * t.ldx, active);
+                for (int e = tid; e < kNB * kNB; e += 128) {
+                    const int i = e % kNB, jj = e / kNB;
+                    cp_async_el(Rs + i * kTrRS + jj, t.R + (i0 + i) + (size_t)(J0 + min(jj, wj - 1)) * t.ldr,
+                                jj < wj);
+                }
             }
-            for (int e = tid; e < kNB * kNB; e += 128) {
-                const int i = e % kNB, jj = e / kNB;
-                Rs[i * kTrRS + jj] = jj < wj ? t.R[(i0 + i) + (size_t)(J0 + jj) * t.ldr] : T(0);
-            }
-            __syncthreads();
-            trsm_mma_chunk(acc, Xs, Rs, warp, lane);
-            __syncthreads();
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int ch = 0; ch < S - 1; ++ch) issue(ch);
+        for (int ch = 0; ch < nch; ++ch) {
+            cp_async_wait<S - 2>();
+            __syncthreads();  // chunk ch landed for every thread; stage (ch - 1) % S is free
+            issue(ch + S - 1);
+            const T* Xs = stg + (ch % S) * STG;
+            trsm_mma_chunk(acc, Xs, Xs + kNB * kTrXS, warp, lane);
         }
+        cp_async_wait<0>();
+        __syncthreads();
         trsm_mma_store(acc, Ss, warp, lane);
         for (int e = tid; e < kNB * kNB; e += 128) {
             const int i = e % kNB, jj = e / kNB;
