@@ -479,37 +479,15 @@ struct TcTraits<double> {
     using ZF = ZFragF64;
 };
 
-// Stages of the chunk pipeline (cp.async, zero-filled past the tile): 4 in
-// FP32 (78 KB of shared memory with Y and T: two CTAs per SM), 3 in FP64
-// (121 KB: one CTA per SM, three chunks in flight).
-template <class T>
-struct TrailStages {
-    static constexpr int v = sizeof(T) == 4 ? 4 : 3;
-};
-// One element global -> shared without registers; src_ok false writes zero.
-template <class T>
-__device__ __forceinline__ void cp_async_el(T* dst, const T* src, bool src_ok) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(sizeof(T)),
-                 "r"(src_ok ? (int)sizeof(T) : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks, const TileRef* tiles, int p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int S = TrailStages<T>::v;
     constexpr int CP = kTN + 1, TP = kNB + 1;
     constexpr int EPT = kRC * kNB / kThreads;  // 8 elements per thread per chunk (V and C each)
-    constexpr int STG = (kNB + kTN) * kTCS;    // one stage: V then C, column-major (stride kTCS)
-    T* stg = reinterpret_cast<T*>(smem_raw);   // S stages
-    T* Ys = stg + S * STG;                     // kNB x CP: Y, then Z
-    T* Tsh = Ys + kNB * CP;                    // kNB x TP
+    T* Vs = reinterpret_cast<T*>(smem_raw);  // kNB columns x kTCS, column-major
+    T* Cs = Vs + kNB * kTCS;                  // kTN columns x kTCS
+    T* Ys = Cs + kTN * kTCS;                  // kNB x CP: Y, then Z
+    T* Tsh = Ys + kNB * CP;                   // kNB x TP
     __shared__ T* colp[kTN];
     const TileRef tr = tiles[blockIdx.x];
     const QRTask<T> t = tasks[tr.task];
@@ -533,52 +511,40 @@ __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks
         Tsh[i * TP + j] = (i < w && j < w) ? t.tp[(size_t)(p / kNB) * kNB * kNB + e] : T(0);
     }
     __syncthreads();
-    const int nch = (R + kRC - 1) / kRC;
-    // chunk ch into stage ch % S: element u of thread tid is row r = e % kRC,
-    // column q = e / kRC (coalesced along rows); rows past R and columns past
-    // the panel / tile are zero-filled
-    auto issue = [&](int ch) {
-        if (ch < nch) {
-            T* Vs = stg + (ch % S) * STG;
-            T* Cs = Vs + kNB * kTCS;
-            const int r0 = ch * kRC;
-            const int rc = min(kRC, R - r0);
+    T vr[EPT], cr[EPT];
+    // element u of thread tid: row r = e % kRC, column q = e / kRC (coalesced along rows)
+    auto fetch = [&](int r0) {
+        const int rc = min(kRC, R - r0);
 #pragma unroll
-            for (int u = 0; u < EPT; ++u) {
-                const int e = tid + u * kThreads;
-                const int r = e % kRC, q = e / kRC;
-                const int gr = r0 + r;
-                cp_async_el(Vs + q * kTCS + r, V0 + p + min(gr, R - 1) + (size_t)min(q, w - 1) * m, r < rc && q < w);
-                cp_async_el(Cs + q * kTCS + r, colp[min(q, tn - 1)] + p + r0 + min(r, rc - 1), r < rc && q < tn);
-            }
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            const int gr = r0 + r;
+            const T x = V0[p + min(gr, R - 1) + (size_t)min(q, w - 1) * m];
+            vr[u] = (r < rc && q < w) ? (gr < q ? T(0) : (gr == q ? T(1) : x)) : T(0);
+            const T y = colp[min(q, tn - 1)][p + r0 + min(r, rc - 1)];
+            cr[u] = (r < rc && q < tn) ? y : T(0);
         }
-        cp_async_commit();  // an empty group past the last chunk keeps the wait count uniform
     };
-    // the unit-lower structure of the panel's reflectors in chunk 0: zero above
-    // the diagonal, one on it
-    auto unit_lower = [&](T* Vs) {
-        for (int e = tid; e < kNB * kNB; e += blockDim.x) {
-            const int q = e / kNB, r = e % kNB;
-            if (q < w && r <= q) Vs[q * kTCS + r] = r == q ? T(1) : T(0);
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * kThreads;
+            const int r = e % kRC, q = e / kRC;
+            Vs[q * kTCS + r] = vr[u];
+            Cs[q * kTCS + r] = cr[u];
         }
     };
     // Y^T = C^T V over all rows
     T acc[4] = {T(0), T(0), T(0), T(0)};
-#pragma unroll
-    for (int ch = 0; ch < S - 1; ++ch) issue(ch);
-    for (int ch = 0; ch < nch; ++ch) {
-        cp_async_wait<S - 2>();
-        __syncthreads();  // chunk ch landed for every thread; stage (ch - 1) % S is free
-        T* Vs = stg + (ch % S) * STG;
-        if (ch == 0) {
-            unit_lower(Vs);
-            __syncthreads();
-        }
-        issue(ch + S - 1);
-        tc_yt_chunk(acc, Vs + kNB * kTCS, Vs, warp, lane);
+    fetch(0);
+    for (int r0 = 0; r0 < R; r0 += kRC) {
+        stash();
+        __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC);
+        tc_yt_chunk(acc, Cs, Vs, warp, lane);
+        __syncthreads();
     }
-    cp_async_wait<0>();
-    __syncthreads();
     tc_yt_store(acc, Ys, warp, lane);
     __syncthreads();
     // Z = T^T Y (SIMT, 32 x 32 x 32)
@@ -601,28 +567,34 @@ __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks
     typename TcTraits<T>::ZF zf;
     tc_z_load(zf, Ys, warp, lane);
     // C -= V Z chunk by chunk, written back after each chunk
-#pragma unroll
-    for (int ch = 0; ch < S - 1; ++ch) issue(ch);
-    for (int ch = 0; ch < nch; ++ch) {
-        cp_async_wait<S - 2>();
-        __syncthreads();  // chunk ch landed; the write-back of chunk ch - 1 is done
-        T* Vs = stg + (ch % S) * STG;
-        T* Cs = Vs + kNB * kTCS;
-        if (ch == 0) {
-            unit_lower(Vs);
-            __syncthreads();
-        }
-        issue(ch + S - 1);
-        const int r0 = ch * kRC;
+    fetch(0);
+    for (int r0 = 0; r0 < R; r0 += kRC) {
         const int rc = min(kRC, R - r0);
+        stash();
+        __syncthreads();
+        if (r0 + kRC < R) fetch(r0 + kRC);
         tc_cvz_chunk(Cs, Vs, zf, Ys, warp, lane);
         __syncthreads();
         for (int e = tid; e < kRC * kTN; e += blockDim.x) {
             const int r = e % kRC, cc = e / kRC;
             if (r < rc && cc < tn) colp[cc][p + r0 + r] = Cs[cc * kTCS + r];
         }
+        __syncthreads();
     }
-    cp_async_wait<0>();
+}
+
+// One element global -> shared without registers; src_ok false writes zero.
+template <class T>
+__device__ __forceinline__ void cp_async_el(T* dst, const T* src, bool src_ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(sizeof(T)),
+                 "r"(src_ok ? (int)sizeof(T) : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // ------------------------------------------------------------------ TRSM on tensor cores
@@ -1563,8 +1535,7 @@ inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
 
 template <class T>
 size_t trailing_tc_smem() {
-    return sizeof(T) * ((size_t)TrailStages<T>::v * (kNB + kTN) * kTCS + (size_t)kNB * (kTN + 1) +
-                        (size_t)kNB * (kNB + 1));
+    return sizeof(T) * ((size_t)(kNB + kTN) * kTCS + (size_t)kNB * (kTN + 1) + (size_t)kNB * (kNB + 1));
 }
 
 }  // namespace
