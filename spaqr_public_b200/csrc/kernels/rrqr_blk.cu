@@ -139,12 +139,12 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
     T* vsh = vn2 + 2 * (size_t)Wp;                    // mpad: the current reflector (pos takes <= Wp elements)
     T* Vs = vsh + mpad;                               // mpad x VP: V_b(i, l) at i * VP + l
     __shared__ T red[32];
-    __shared__ T wv[2][32];  // per-warp pivot candidates, alternating slots by step parity
-    __shared__ int wp[2][32], wc[2][32];
+    __shared__ Cand<T> wcand[2][32];  // per-warp pivot candidates, alternating slots by step parity
+    __shared__ int s_gp, s_gc;
+    __shared__ T s_fp[kBNB];  // F(l, pivot column), zero for l >= jb
     __shared__ T s_alpha;
-    __shared__ int s_gp, s_gc, s_c0, s_nflag;
+    __shared__ int s_c0, s_nflag;
     __shared__ T s_aux[kBNB];    // V_b(k:m, l)^T v for l < jb, zero after
-    __shared__ T s_fp[kBNB];     // F(l, pivot column), zero for l >= jb
     __shared__ int s_pcs[kBNB];  // pivot column of each step of the block
     __shared__ T s_betas[kBNB];  // R_kk of each step of the block
     __shared__ T s_wpart[(kBT / 32) * kBNB];
@@ -213,17 +213,14 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 }
             }
             warp_best(bv, bp, bc);
-            if (lane == 0) {
-                wv[buf][warp] = bv;
-                wp[buf][warp] = bp;
-                wc[buf][warp] = bc;
-            }
+            if (lane == 0) wcand[buf][warp] = Cand<T>{bv, bp, bc};
             // the cluster barrier also orders this CTA's warps: every warp's candidate
             // of every CTA is visible to all after it
             cl.sync();
             // every CTA reduces all warps' candidates of the cluster (candidate q: CTA
-            // q / nw, warp q % nw; the order is immaterial, (value, position) is a
-            // strict order), then warp 0 fetches F(:, pc) from the pivot's owner
+            // q / nw, warp q % nw, one 16-byte record; the order is immaterial,
+            // (value, position) is a strict order), then warp 0 fetches F(:, pc) from
+            // the pivot's owner
             if (warp == 0) {
                 // all of a lane's candidate loads are issued before any is used,
                 // so the DSMEM round trips overlap
@@ -234,24 +231,21 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
 #pragma unroll
                 for (int u0 = 0; u0 < kCand; u0 += kBatch) {
                     if (32 * u0 >= CL * nw) break;  // uniform over the warp: no candidate left
-                    T vq[kBatch];
-                    int pq[kBatch], cq[kBatch];
+                    Cand<T> cq[kBatch];
 #pragma unroll
                     for (int u = 0; u < kBatch; ++u) {
                         const int q = lane + 32 * (u0 + u);
                         const bool in = q < CL * nw;
                         const int rk = in ? q / nw : 0, wq = in ? q % nw : 0;
-                        cq[u] = *cl.map_shared_rank(&wc[buf][wq], rk);
-                        vq[u] = *cl.map_shared_rank(&wv[buf][wq], rk);
-                        pq[u] = *cl.map_shared_rank(&wp[buf][wq], rk);
-                        if (!in) cq[u] = -1;
+                        cq[u] = *cl.map_shared_rank(&wcand[buf][wq], rk);
+                        if (!in) cq[u].c = -1;
                     }
 #pragma unroll
                     for (int u = 0; u < kBatch; ++u)
-                        if (cq[u] >= 0 && better(vq[u], pq[u], v, p)) {
-                            v = vq[u];
-                            p = pq[u];
-                            c = cq[u];
+                        if (cq[u].c >= 0 && better(cq[u].v, cq[u].p, v, p)) {
+                            v = cq[u].v;
+                            p = cq[u].p;
+                            c = cq[u].c;
                         }
                 }
                 warp_best(v, p, c);
@@ -385,17 +379,40 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 const int c = j0 + jl;
                 if (c == pc || pos[jl] < k) continue;
                 const T ck0 = C[k * ld + c];
-                if (tau != T(0)) {
-                    T g = ck0;
-                    for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
-                    T corr = T(0);
-#pragma unroll
-                    for (int l = 0; l < kBNB; ++l) corr += F[l * Wp + jl] * s_aux[l];
-                    F[jb * Wp + jl] = tau * (g - corr);
-                }
                 T upd = T(0);
+                if constexpr (sizeof(T) == 4) {
+                    // F(:, c) read once: F(jb, c) is still zero, and V_b(k, jb) = 1,
+                    // so the update is the sum over l != jb plus the new entry (the
+                    // same sum term by term, zeros included). FP64 reads F twice
+                    // (its 16 entries in registers would spill).
+                    T fr[kBNB];
 #pragma unroll
-                for (int l = 0; l < kBNB; ++l) upd += vk[l] * F[l * Wp + jl];
+                    for (int l = 0; l < kBNB; ++l) fr[l] = F[l * Wp + jl];
+                    T fnew = T(0);
+                    if (tau != T(0)) {
+                        T g = ck0;
+                        for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
+                        T corr = T(0);
+#pragma unroll
+                        for (int l = 0; l < kBNB; ++l) corr += fr[l] * s_aux[l];
+                        fnew = tau * (g - corr);
+                        F[jb * Wp + jl] = fnew;
+                    }
+#pragma unroll
+                    for (int l = 0; l < kBNB; ++l) upd += vk[l] * fr[l];
+                    upd += fnew;
+                } else {
+                    if (tau != T(0)) {
+                        T g = ck0;
+                        for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
+                        T corr = T(0);
+#pragma unroll
+                        for (int l = 0; l < kBNB; ++l) corr += F[l * Wp + jl] * s_aux[l];
+                        F[jb * Wp + jl] = tau * (g - corr);
+                    }
+#pragma unroll
+                    for (int l = 0; l < kBNB; ++l) upd += vk[l] * F[l * Wp + jl];
+                }
                 const T ck = ck0 - upd;
                 C[k * ld + c] = ck;
                 const T n1 = vn1[jl];

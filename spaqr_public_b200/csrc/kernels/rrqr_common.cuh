@@ -82,6 +82,13 @@ __device__ __forceinline__ bool better(T v, int p, T bv, int bp) {
     return v > bv || (v == bv && p < bp);
 }
 
+// One pivot candidate as a 16-byte record (one DSMEM load).
+template <class T>
+struct __align__(16) Cand {
+    T v;
+    int p, c;
+};
+
 // Warp arg-max of (value, position, column) candidates; every lane gets the winner.
 template <class T>
 __device__ __forceinline__ void warp_best(T& v, int& p, int& c) {
