@@ -20,6 +20,7 @@
 #include <numeric>
 #include <set>
 #include <stdexcept>
+#include <unordered_map>
 
 namespace spq {
 
@@ -196,17 +197,51 @@ void rows_by_norm(const Csc& At_perm, const std::vector<Cid>& cid_of_pos, std::v
 // column of its largest-norm run of equal ids (form_rmap, src/tree.cpp:57-98).
 Ordering finish_ordering(const Csc& A, int nlevels, const std::vector<Cid>& ids, bool square) {
     const int n = A.n, m = A.m;
-    // Hierarchical column sort: by id, then by the id lifted to each level.
+    // Hierarchical column sort: stable by id, then stable by the id lifted to
+    // each level in turn. Every key is a function of the id, so the columns of
+    // one id keep their order and the ids' relative order is that of the same
+    // sorts run on the distinct ids: those (a few per bottom cluster) are
+    // sorted, and the columns follow by a stable counting sort on their id's
+    // rank. Same permutation as the sorts over all columns.
     Ordering o;
-    o.cperm.resize(n);
-    std::iota(o.cperm.begin(), o.cperm.end(), 0);
-    std::vector<Cid> key(ids);
+    std::vector<int> slot(n);
+    std::vector<Cid> uniq;
+    {
+        struct CidHash {
+            size_t operator()(const Cid& c) const {
+                uint64_t h = 1469598103934665603ull;
+                for (int v : {c.self.lvl, c.self.sep, c.l.lvl, c.l.sep, c.r.lvl, c.r.sep, c.part, c.section})
+                    h = (h ^ (uint32_t)v) * 1099511628211ull;
+                return (size_t)h;
+            }
+        };
+        std::unordered_map<Cid, int, CidHash> at;
+        at.reserve(1024);
+        for (int j = 0; j < n; ++j) {
+            auto it = at.find(ids[j]);
+            if (it == at.end()) {
+                it = at.emplace(ids[j], (int)uniq.size()).first;
+                uniq.push_back(ids[j]);
+            }
+            slot[j] = it->second;
+        }
+    }
+    const int D = (int)uniq.size();
+    std::vector<int> ord(D);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::vector<Cid> key(uniq);
     auto by_key = [&key](int a, int b) { return key[a] < key[b]; };
-    std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
+    std::stable_sort(ord.begin(), ord.end(), by_key);
     for (int lvl = 1; lvl < nlevels; ++lvl) {
         for (auto& k : key) k = lift(k, lvl);
-        std::stable_sort(o.cperm.begin(), o.cperm.end(), by_key);
+        std::stable_sort(ord.begin(), ord.end(), by_key);
     }
+    std::vector<int> rank(D), start(D + 1, 0);
+    for (int q = 0; q < D; ++q) rank[ord[q]] = q;
+    for (int j = 0; j < n; ++j) ++start[rank[slot[j]] + 1];
+    for (int q = 0; q < D; ++q) start[q + 1] += start[q];
+    o.cperm.resize(n);
+    for (int j = 0; j < n; ++j) o.cperm[start[rank[slot[j]]]++] = j;
     o.cid_of_pos.resize(n);
     for (int k = 0; k < n; ++k) o.cid_of_pos[k] = ids[o.cperm[k]];
 
@@ -255,13 +290,31 @@ Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<
     // Separators, top level first; a column on the even side of a cut that
     // touches an unassigned column on the odd side joins that separator. The
     // sweep is sequential in column order (assignments feed later tests).
+    // A column can join the separator of level l only if some neighbour lies on
+    // the odd sibling side at l (sides part >> (l - 1) differing in the last
+    // bit only: the highest differing bit of the two parts is l - 1, and the
+    // column's is 0); one pass marks those levels per column (bit l), and each
+    // sweep visits only the marked columns, in column order as before.
+    std::vector<std::vector<int>> cand(nlevels);
+    {
+        std::vector<uint32_t> mask(n, 0);
+        for (int i = 0; i < n; ++i)
+            for (int64_t q = G.p[i]; q < G.p[i + 1]; ++q) {
+                const unsigned x = (unsigned)(part[i] ^ part[G.i[q]]);
+                if (x == 0) continue;
+                const int h = 31 - __builtin_clz(x);
+                if (h + 1 < nlevels && !((part[i] >> h) & 1)) mask[i] |= 1u << (h + 1);
+            }
+        for (int i = 0; i < n; ++i)
+            for (int l = 1; l < nlevels; ++l)
+                if (mask[i] >> l & 1) cand[l].push_back(i);
+    }
     std::vector<Cid> cmap(n);
     for (int depth = 0; depth + 1 < nlevels; ++depth) {
         const int l = nlevels - depth - 1;
-        for (int i = 0; i < n; ++i) {
+        for (int i : cand[l]) {
             if (cmap[i].self.lvl != -1) continue;
             const int pi = side_at(part[i], l);
-            if (pi & 1) continue;
             for (int64_t q = G.p[i]; q < G.p[i + 1]; ++q) {
                 const int j = G.i[q];
                 if (cmap[j].self.lvl == -1 && side_at(part[j], l) == pi + 1) {
