@@ -20,6 +20,7 @@
 #include <numeric>
 #include <set>
 #include <stdexcept>
+#include <thread>
 #include <unordered_map>
 
 namespace spq {
@@ -117,23 +118,58 @@ struct Adjacency {
     std::vector<int> i;
 };
 
+// fn(t, begin, end) over [0, n) in contiguous ranges on up to 8 host threads
+// (one call on this thread for small n).
+template <class F>
+void par_ranges(int n, F&& fn) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = n < 16384 ? 1 : std::min(hw, 8);
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t)
+        th.emplace_back([&, t] { fn(t, (int)((int64_t)n * t / nt), (int)((int64_t)n * (t + 1) / nt)); });
+    fn(0, 0, (int)((int64_t)n / nt));
+    for (auto& x : th) x.join();
+}
+
+// Column adjacency of A^T A (sorted neighbour lists), built in column ranges
+// on host threads and concatenated.
 Adjacency ata_adjacency(const Csc& A, const Csc& At) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = A.n < 16384 ? 1 : std::min(hw, 8);
+    std::vector<std::vector<int>> li(nt);
+    std::vector<std::vector<int64_t>> lp(nt);
+    std::vector<int> lo(nt + 1);
+    par_ranges(A.n, [&](int t, int b, int e) {
+        lo[t] = b;
+        if (t == nt - 1) lo[nt] = e;
+        std::vector<int> stamp(A.n, -1), list;
+        auto& gi = li[t];
+        auto& gp = lp[t];
+        gi.reserve((size_t)(A.p[e] - A.p[b]) * 4);
+        gp.reserve((size_t)(e - b));
+        for (int j = b; j < e; ++j) {
+            list.clear();
+            for (int q = A.p[j]; q < A.p[j + 1]; ++q) {
+                int r = A.i[q];
+                for (int t2 = At.p[r]; t2 < At.p[r + 1]; ++t2) {
+                    int c = At.i[t2];
+                    if (stamp[c] != j) { stamp[c] = j; list.push_back(c); }
+                }
+            }
+            std::sort(list.begin(), list.end());
+            gi.insert(gi.end(), list.begin(), list.end());
+            gp.push_back((int64_t)gi.size());
+        }
+    });
     Adjacency G;
     G.p.assign((size_t)A.n + 1, 0);
-    std::vector<int> stamp(A.n, -1), list;
-    G.i.reserve(A.i.size() * 4);
-    for (int j = 0; j < A.n; ++j) {
-        list.clear();
-        for (int q = A.p[j]; q < A.p[j + 1]; ++q) {
-            int r = A.i[q];
-            for (int t = At.p[r]; t < At.p[r + 1]; ++t) {
-                int c = At.i[t];
-                if (stamp[c] != j) { stamp[c] = j; list.push_back(c); }
-            }
-        }
-        std::sort(list.begin(), list.end());
-        G.i.insert(G.i.end(), list.begin(), list.end());
-        G.p[j + 1] = (int64_t)G.i.size();
+    size_t tot = 0;
+    for (auto& v : li) tot += v.size();
+    G.i.reserve(tot);
+    for (int t = 0; t < nt; ++t) {
+        const int64_t base = (int64_t)G.i.size();
+        for (int j = lo[t]; j < lo[t + 1]; ++j) G.p[j + 1] = base + lp[t][j - lo[t]];
+        G.i.insert(G.i.end(), li[t].begin(), li[t].end());
     }
     return G;
 }
