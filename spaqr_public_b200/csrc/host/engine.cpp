@@ -218,46 +218,80 @@ public:
         if (bottoms_[0].empty()) throw std::logic_error("assemble before partition");
         open_device();
         nnzA_ = A.i.size();
-        const Csc App = csc_gather_rows(csc_gather_cols(A, cperm_), rperm_);
+        // permuted matrix: its column k is column cperm_[k] of A, row irow[r] is row r of A
+        std::vector<int> irow(A.m);
+        for (int k = 0; k < A.m; ++k) irow[rperm_[k]] = k;
         std::vector<Cluster*> rowcl(A.m);
         for (Cluster* s : bottoms_[0])
             for (int i = s->rstart; i < s->rstart + s->rsize; ++i) rowcl[i] = s;
-        std::vector<uint64_t> addr;
-        std::vector<double> vals;
-        addr.reserve(A.i.size());
-        vals.reserve(A.i.size());
-        for (Cluster* self : bottoms_[0]) {
-            std::set<Cluster*, ByOrder> cn;
-            for (int j = self->cstart; j < self->cstart + self->csize; ++j)
-                for (int q = App.p[j]; q < App.p[j + 1]; ++q) cn.insert(rowcl[App.i[q]]);
-            cn.insert(self);
+        // (this thread, cluster order) each bottom cluster's row-cluster
+        // neighbours by order, their blocks and edges
+        const auto& B = bottoms_[0];
+        const size_t nb = B.size();
+        std::vector<size_t> first(nb + 1, 0);
+        std::vector<std::vector<std::pair<Cluster*, Blk>>> nblk(nb);
+        std::vector<Cluster*> cn;
+        for (size_t s = 0; s < nb; ++s) {
+            Cluster* self = B[s];
+            cn.clear();
+            size_t cnt = 0;
+            for (int j = self->cstart; j < self->cstart + self->csize; ++j) {
+                const int oc = cperm_[j];
+                for (int q = A.p[oc]; q < A.p[oc + 1]; ++q) cn.push_back(rowcl[irow[A.i[q]]]);
+                cnt += (size_t)(A.p[oc + 1] - A.p[oc]);
+            }
+            cn.push_back(self);
+            std::sort(cn.begin(), cn.end(), ByOrder());
+            cn.erase(std::unique(cn.begin(), cn.end()), cn.end());
             for (Cluster* nbr : cn) {
                 Blk b = new_block(nbr->rsize, self->csize);
-                for (int col = 0; col < self->csize; ++col) {
-                    const int j = self->cstart + col;
-                    for (int q = App.p[j]; q < App.p[j + 1]; ++q) {
-                        const int r = App.i[q];
-                        if (r >= nbr->rstart && r < nbr->rstart + nbr->rsize) {
-                            addr.push_back(reinterpret_cast<uint64_t>(b.p + (r - nbr->rstart) + (size_t)col * b.ld));
-                            vals.push_back(App.v[q]);
-                        }
-                    }
-                }
+                nblk[s].emplace_back(nbr, b);
                 Edge* e = new_edge(self, nbr, b);
                 self->out.push_back(e);
                 if (self != nbr) nbr->in.push_back(e);
             }
-            std::stable_sort(self->out.begin(), self->out.end(),
-                             [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
+            first[s + 1] = first[s] + cnt;
         }
-        uint64_t* d_addr = desc_arena_.alloc_n<uint64_t>(addr.size());
-        double* d_vals = desc_arena_.alloc_n<double>(vals.size());
-        cuda_check(cudaMemcpyAsync(d_addr, addr.data(), addr.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
-        cuda_check(cudaMemcpyAsync(d_vals, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice, stream_), "upload");
-        timed(KF_ASSEMBLE, 0, (double)addr.size() * (16 + sizeof(T)),
-              [&] { launch_scatter_values<T>(d_addr, d_vals, (int64_t)addr.size(), stream_); });
-        ++launches_fact_;
+        // (threads) the block address and value of every entry, straight into
+        // pinned staging; the scatter is a permutation, so the order is free
+        const size_t nnz = first[nb];
+        char* h = pinned_.get(std::max<size_t>(nnz, 1) * 16);
+        uint64_t* haddr = reinterpret_cast<uint64_t*>(h);
+        double* hvals = reinterpret_cast<double*>(h + std::max<size_t>(nnz, 1) * 8);
+        host_parallel_for(
+            nb,
+            [&](size_t b0, size_t e0) {
+                for (size_t s = b0; s < e0; ++s) {
+                    const Cluster* self = B[s];
+                    const auto& nbl = nblk[s];
+                    size_t o = first[s];
+                    for (int col = 0; col < self->csize; ++col) {
+                        const int oc = cperm_[self->cstart + col];
+                        for (int q = A.p[oc]; q < A.p[oc + 1]; ++q) {
+                            const int r = irow[A.i[q]];
+                            const Cluster* nbr = rowcl[r];
+                            size_t u = 0;
+                            while (nbl[u].first != nbr) ++u;
+                            const Blk& b = nbl[u].second;
+                            haddr[o] = reinterpret_cast<uint64_t>(b.p + (r - nbr->rstart) + (size_t)col * b.ld);
+                            hvals[o] = A.v[q];
+                            ++o;
+                        }
+                    }
+                }
+            },
+            64);
+        if (nnz > 0) {
+            uint64_t* d_addr = desc_arena_.alloc_n<uint64_t>(nnz);
+            double* d_vals = desc_arena_.alloc_n<double>(nnz);
+            cuda_check(cudaMemcpyAsync(d_addr, haddr, nnz * 8, cudaMemcpyHostToDevice, stream_), "upload");
+            cuda_check(cudaMemcpyAsync(d_vals, hvals, nnz * 8, cudaMemcpyHostToDevice, stream_), "upload");
+            timed(KF_ASSEMBLE, 0, (double)nnz * (16 + sizeof(T)),
+                  [&] { launch_scatter_values<T>(d_addr, d_vals, (int64_t)nnz, stream_); });
+            ++launches_fact_;
+        }
         cuda_check(cudaStreamSynchronize(stream_), "assemble");
+        pinned_.reset();
         assembled_ = true;
         t_asm_ = wall() - t0;
     }

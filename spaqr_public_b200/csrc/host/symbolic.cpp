@@ -118,12 +118,12 @@ struct Adjacency {
     std::vector<int> i;
 };
 
-// fn(t, begin, end) over [0, n) in contiguous ranges on up to 8 host threads
-// (one call on this thread for small n).
+// fn(t, begin, end) over [0, n) in contiguous ranges on up to 8 host threads,
+// at least min_items items per thread (one call on this thread below that).
 template <class F>
-void par_ranges(int n, F&& fn) {
+void par_ranges(int n, F&& fn, int min_items = 2048) {
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int nt = n < 16384 ? 1 : std::min(hw, 8);
+    const int nt = std::max(1, std::min({hw, 8, n / std::max(1, min_items)}));
     std::vector<std::thread> th;
     for (int t = 1; t < nt; ++t)
         th.emplace_back([&, t] { fn(t, (int)((int64_t)n * t / nt), (int)((int64_t)n * (t + 1) / nt)); });
@@ -135,7 +135,7 @@ void par_ranges(int n, F&& fn) {
 // on host threads and concatenated.
 Adjacency ata_adjacency(const Csc& A, const Csc& At) {
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int nt = A.n < 16384 ? 1 : std::min(hw, 8);
+    const int nt = std::max(1, std::min({hw, 8, A.n / 2048}));
     std::vector<std::vector<int>> li(nt);
     std::vector<std::vector<int64_t>> lp(nt);
     std::vector<int> lo(nt + 1);
@@ -176,33 +176,70 @@ Adjacency ata_adjacency(const Csc& A, const Csc& At) {
 
 // Recursive geometric bisection: at each depth every part is split at the
 // (N/2)-th smallest coordinate along its widest coordinate (ties: lowest dim).
+// The members of every part are kept as one ascending range of `order`; a
+// split is a stable partition of the range (ascending on both sides, as a
+// scan of all indices would list them), and the parts of a depth are split on
+// host threads.
 std::vector<int> bisect(int n, int nlevels, int d, const std::vector<double>& X) {
-    std::vector<int> part(n, 0);
-    std::vector<double> vals;
+    std::vector<int> part(n, 0), order(n), tmp(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int> st{0, n};  // part k: order[st[k], st[k + 1])
     for (int depth = 0; depth + 1 < nlevels; ++depth) {
         const int nparts = 1 << depth;
-        std::vector<std::vector<int>> members(nparts);
-        for (int i = 0; i < n; ++i) members[part[i]].push_back(i);
-        for (int k = 0; k < nparts; ++k) {
-            const auto& mem = members[k];
-            if (mem.empty()) continue;
+        std::vector<int> mid(nparts);
+        auto split = [&](int k, std::vector<double>& vals) {
+            const int b = st[k], e = st[k + 1];
+            mid[k] = b;
+            if (b == e) return;
             int best = -1;
             double widest = -1.0;
             for (int a = 0; a < d; ++a) {
                 double lo = std::numeric_limits<double>::max(), hi = std::numeric_limits<double>::lowest();
-                for (int i : mem) {
-                    double x = X[(size_t)i * d + a];
+                for (int t = b; t < e; ++t) {
+                    double x = X[(size_t)order[t] * d + a];
                     lo = std::min(lo, x);
                     hi = std::max(hi, x);
                 }
                 if (hi - lo > widest) { widest = hi - lo; best = a; }
             }
-            vals.resize(mem.size());
-            for (size_t t = 0; t < mem.size(); ++t) vals[t] = X[(size_t)mem[t] * d + best];
-            std::nth_element(vals.begin(), vals.begin() + mem.size() / 2, vals.end());
-            const double cut = vals[mem.size() / 2];
-            for (int i : mem) part[i] = (X[(size_t)i * d + best] <= cut) ? 2 * k : 2 * k + 1;
+            const int cnt = e - b;
+            vals.resize(cnt);
+            for (int t = 0; t < cnt; ++t) vals[t] = X[(size_t)order[b + t] * d + best];
+            std::nth_element(vals.begin(), vals.begin() + cnt / 2, vals.end());
+            const double cut = vals[cnt / 2];
+            int l = b, r = 0;
+            for (int t = b; t < e; ++t) {
+                const int i = order[t];
+                if (X[(size_t)i * d + best] <= cut) {
+                    part[i] = 2 * k;
+                    order[l++] = i;
+                } else {
+                    part[i] = 2 * k + 1;
+                    tmp[b + r++] = i;
+                }
+            }
+            std::copy(tmp.begin() + b, tmp.begin() + b + r, order.begin() + l);
+            mid[k] = l;
+        };
+        if (nparts < 8) {
+            std::vector<double> vals;
+            for (int k = 0; k < nparts; ++k) split(k, vals);
+        } else {
+            par_ranges(
+                nparts,
+                [&](int, int kb, int ke) {
+                    std::vector<double> vals;
+                    for (int k = kb; k < ke; ++k) split(k, vals);
+                },
+                1);
         }
+        std::vector<int> nst(2 * nparts + 1);
+        for (int k = 0; k < nparts; ++k) {
+            nst[2 * k] = st[k];
+            nst[2 * k + 1] = mid[k];
+        }
+        nst[2 * nparts] = n;
+        st.swap(nst);
     }
     return part;
 }
@@ -378,40 +415,46 @@ Ordering geometric_ordering(const Csc& A, int nlevels, int d, const std::vector<
 
     // Interface sides of separator rows from their lower-level neighbours
     // (lowest level wins, first seen wins on ties).
-    for (int r = 0; r < m; ++r) {
-        const Sep self = rmap[r].self;
-        if (self.lvl <= 0) continue;
-        Sep left, right;
-        for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
-            const Sep nb = cmap[At.i[q]].self;
-            if (nb.lvl >= self.lvl) continue;
-            int pj = (int)(nb.sep / std::pow(2.0, self.lvl - nb.lvl - 1));
-            Sep& side = (pj % 2 == 0) ? left : right;
-            if (side.lvl == -1 || nb.lvl < side.lvl) side = nb;
+    // (threads: each row reads cmap and writes its own entry)
+    par_ranges(m, [&](int, int rb, int re) {
+        for (int r = rb; r < re; ++r) {
+            const Sep self = rmap[r].self;
+            if (self.lvl <= 0) continue;
+            Sep left, right;
+            for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
+                const Sep nb = cmap[At.i[q]].self;
+                if (nb.lvl >= self.lvl) continue;
+                int pj = (int)(nb.sep / std::pow(2.0, self.lvl - nb.lvl - 1));
+                Sep& side = (pj % 2 == 0) ? left : right;
+                if (side.lvl == -1 || nb.lvl < side.lvl) side = nb;
+            }
+            rmap[r].l = left;
+            rmap[r].r = right;
         }
-        rmap[r].l = left;
-        rmap[r].r = right;
-    }
+    });
     // Columns take the ids of the rows with the same index (identity matching);
-    // a missing side is completed from same-separator neighbours.
+    // a missing side is completed from same-separator neighbours (threads: each
+    // row reads the copy cm2 and writes its own entry).
     std::vector<Cid> cm2(rmap);
-    for (int r = 0; r < m; ++r) {
-        const Sep self = rmap[r].self;
-        Sep left = rmap[r].l, right = rmap[r].r;
-        if (right == Sep()) {
-            for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
-                const Cid& c = cm2[At.i[q]];
-                if (c.self == self && c.r != Sep()) right = (right == Sep()) ? c.r : common_ancestor(right, c.r);
+    par_ranges(m, [&](int, int rb, int re) {
+        for (int r = rb; r < re; ++r) {
+            const Sep self = rmap[r].self;
+            Sep left = rmap[r].l, right = rmap[r].r;
+            if (right == Sep()) {
+                for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
+                    const Cid& c = cm2[At.i[q]];
+                    if (c.self == self && c.r != Sep()) right = (right == Sep()) ? c.r : common_ancestor(right, c.r);
+                }
+            } else if (left == Sep()) {
+                for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
+                    const Cid& c = cm2[At.i[q]];
+                    if (c.self == self && c.l != Sep()) left = (left == Sep()) ? c.l : common_ancestor(left, c.l);
+                }
             }
-        } else if (left == Sep()) {
-            for (int q = At.p[r]; q < At.p[r + 1]; ++q) {
-                const Cid& c = cm2[At.i[q]];
-                if (c.self == self && c.l != Sep()) left = (left == Sep()) ? c.l : common_ancestor(left, c.l);
-            }
+            rmap[r].l = left;
+            rmap[r].r = right;
         }
-        rmap[r].l = left;
-        rmap[r].r = right;
-    }
+    });
     for (int r = 0; r < m; ++r) {
         if (rmap[r].l == Sep()) rmap[r].l = rmap[r].self;
         if (rmap[r].r == Sep()) rmap[r].r = rmap[r].self;
