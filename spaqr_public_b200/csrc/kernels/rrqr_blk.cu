@@ -27,10 +27,12 @@
 //      candidates in alternating slots, cluster barrier, each CTA reduces the
 //      candidates through DSMEM;
 //   2. every CTA brings the pivot column up to date (C_bs(k:m, pc) -
-//      V_b F(pc, :)^T, reading F(pc, :) from the owner's shared memory), builds
-//      the reflector (dlarfg) and s_aux = V_b(k:m, 0:jb)^T v: same inputs and
-//      arithmetic give bitwise the same v in every CTA, so nothing is
-//      broadcast; the swap is applied to the positions each CTA keeps;
+//      V_b F(pc, :)^T, reading F(pc, :) from the owner's shared memory) and,
+//      in the same pass and one block reduction, its norm and V_b^T of it;
+//      the reflector (dlarfg) is v = (1, scal x) and s_aux = V_b(k:m, 0:jb)^T v
+//      follows from those sums: same inputs and arithmetic give bitwise the
+//      same v in every CTA, so nothing is broadcast; the swap is applied to the
+//      positions each CTA keeps;
 //   3. every CTA forms F(jb, c) over its slab (one pass over C_bs(k+1:m, slab),
 //      row chunks whose count depends only on m and k, so the result does not
 //      depend on the cluster size), updates pivot row k of its columns and
@@ -271,44 +273,27 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             //    same inputs and the same arithmetic give bitwise the same v in every
             //    CTA, so v needs no broadcast. The owner stores the column at the end
             //    of the block, once no CTA reads its block-start values any more.
+            // One pass and one block reduction: the pivot column x (kept unscaled in
+            //    vsh), its squared norm below row k and the sums V_b(k+1:m, l)^T x;
+            //    after the reduction the reflector is v = (1, scal x(k+1:m)), so
+            //    s_aux = V_b(k, :) + scal V_b(k+1:m, :)^T x, and the partial products
+            //    of 3a run on x and are scaled in 3b.
             T acc = T(0);
+            T sa[kBNB];
+#pragma unroll
+            for (int l = 0; l < kBNB; ++l) sa[l] = T(0);
             for (int i = k + tid; i < m; i += nth) {
                 T x = C[i * ld + pc];
 #pragma unroll
                 for (int l = 0; l < kBNB; ++l) x -= Vs[i * VP + l] * s_fp[l];  // zero past jb
                 vsh[i] = x;
-                if (i == k)
+                if (i == k) {
                     s_alpha = x;
-                else
+                } else {
                     acc += x * x;
-            }
-            const T xn2 = bsum1(acc, red);
-            const T alpha = s_alpha;
-            T tau, beta, scal;
-            if (xn2 == T(0)) {
-                tau = T(0);
-                beta = alpha;
-                scal = T(1);
-            } else {
-                const T nrm = dhypot(alpha, (T)sqrt(xn2));
-                beta = alpha >= T(0) ? -nrm : nrm;
-                tau = (beta - alpha) / beta;
-                scal = T(1) / (alpha - beta);
-            }
-            // the reflector, V_b(:, jb) and the rows of s_aux in one pass (same row mapping)
-            T sa[kBNB];
 #pragma unroll
-            for (int l = 0; l < kBNB; ++l) sa[l] = T(0);
-            for (int i = k + tid; i < m; i += nth) {
-                T v = T(1);
-                if (i != k) {
-                    v = vsh[i];
-                    if (tau != T(0)) v *= scal;
+                    for (int l = 0; l < kBNB; ++l) sa[l] += Vs[i * VP + l] * x;  // columns >= jb are zero
                 }
-#pragma unroll
-                for (int l = 0; l < kBNB; ++l) sa[l] += Vs[i * VP + l] * v;  // columns >= jb are zero
-                vsh[i] = v;
-                Vs[i * VP + jb] = v;
             }
             // warp transpose-sum: lane l (mod kBNB) ends with the warp's sum of sa[l]
 #pragma unroll
@@ -324,13 +309,32 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             // with kBNB < 32, lanes l and l + kBNB hold halves of the same sum
             T part0 = sa[0];
             if (kBNB < 32) part0 += __shfl_xor_sync(0xffffffffu, part0, kBNB);
+            acc = wsum(acc);
             if (lane < kBNB) s_wpart[warp * kBNB + lane] = part0;
+            if (lane == 0) red[warp] = acc;
             __syncthreads();
+            T xn2 = T(0);
+            for (int q = 0; q < nw; ++q) xn2 += red[q];
+            const T alpha = s_alpha;
+            T tau, beta, scal;
+            if (xn2 == T(0)) {
+                tau = T(0);
+                beta = alpha;
+                scal = T(1);
+            } else {
+                const T nrm = dhypot(alpha, (T)sqrt(xn2));
+                beta = alpha >= T(0) ? -nrm : nrm;
+                tau = (beta - alpha) / beta;
+                scal = T(1) / (alpha - beta);
+            }
+            const T sc = tau != T(0) ? scal : T(1);  // v(k+1:m) = sc x(k+1:m)
             if (tid < kBNB) {
                 T sacc = T(0);
                 for (int q = 0; q < nw; ++q) sacc += s_wpart[q * kBNB + tid];
-                s_aux[tid] = tid < jb ? sacc : T(0);
+                s_aux[tid] = tid < jb ? Vs[k * VP + tid] + sc * sacc : T(0);
             }
+            // V_b(:, jb) = v (read after the barriers that follow)
+            for (int i = k + tid; i < m; i += nth) Vs[i * VP + jb] = i == k ? T(1) : sc * vsh[i];
             if (cr == 0 && tid == 0) note_rrqr_pivot(t.status, beta);
             if (tol != 0.0 && kmax > 1) {
                 if (k == 0) {
@@ -351,10 +355,10 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 s_c0 = -1;
             }
             steps = jb + 1;
-            // no barrier here: 3a reads only the reflector (complete since the
-            // s_wpart barrier) and C; the positions, s_aux and the partials are
+            // no barrier here: 3a reads only x (complete since the reduction
+            // barrier) and C; the positions, s_aux, V_b(:, jb) and the partials are
             // read in 3b, after the barrier that closes 3a
-            // 3a. partials of C_bs(k+1:m, slab)^T v: lanes own 16-byte column vectors,
+            // 3a. partials of C_bs(k+1:m, slab)^T x (v / sc): lanes own 16-byte column vectors,
             //     the rows are cut in Gs chunks of about 16 rows taken by different
             //     warps; narrow slabs give each lane one vector (kBU = 1) so that more
             //     warps share the pass. Each column's chunk sum runs over its rows in
@@ -390,8 +394,9 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                     for (int l = 0; l < kBNB; ++l) fr[l] = F[l * Wp + jl];
                     T fnew = T(0);
                     if (tau != T(0)) {
-                        T g = ck0;
+                        T g = T(0);
                         for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
+                        g = ck0 + sc * g;
                         T corr = T(0);
 #pragma unroll
                         for (int l = 0; l < kBNB; ++l) corr += fr[l] * s_aux[l];
@@ -403,8 +408,9 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                     upd += fnew;
                 } else {
                     if (tau != T(0)) {
-                        T g = ck0;
+                        T g = T(0);
                         for (int q = 0; q < Gs; ++q) g += part[q * Wp + jl];
+                        g = ck0 + sc * g;
                         T corr = T(0);
 #pragma unroll
                         for (int l = 0; l < kBNB; ++l) corr += F[l * Wp + jl] * s_aux[l];

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, con
 // Results are deterministic for a given cluster size; they differ from the
 // one-CTA form only by the order of the neighbour sums.
 constexpr int kTThreads = 256;
-constexpr int kTGU = 32;  // loads in flight per thread in the products
+constexpr int kTGU = 16;  // loads in flight per thread in the products
 
 template <class T>
 __global__ void __launch_bounds__(kTThreads) k_tri_cl(const SolveOp* ops, const GemvRef<T>* gemv, T* x) {
