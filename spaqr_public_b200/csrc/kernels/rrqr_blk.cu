@@ -54,6 +54,31 @@
 
 namespace cg = cooperative_groups;
 
+// Phase clocks of the pivot steps (built only with -DSPQ_RRQR_CLOCKS, as the
+// separate library libspaqr_b200_rrqrclk.so): thread 0 of every CTA adds the
+// clock64() span of each phase of each pivot step to a device counter.
+#ifdef SPQ_RRQR_CLOCKS
+__device__ unsigned long long g_rrqr_clocks[16];
+#define SPQ_CLK(name) const long long name = clock64()
+#define SPQ_CLK_ADD(slot, v) atomicAdd(&g_rrqr_clocks[slot], (unsigned long long)(v))
+// Reads (and with reset != 0 zeroes) the 16 counters: slots 0-6 the phase
+// spans (arg-max, cluster barrier, candidate reduction, pivot column and
+// reflector, partial products, row update and norms, norm recomputation), 7 the
+// block ends, 8 the CTA steps, 9 the CTA blocks.
+extern "C" int spq_rrqr_phase_clocks(unsigned long long* out16, int reset) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return 1;
+    if (cudaMemcpyFromSymbol(out16, g_rrqr_clocks, sizeof(unsigned long long) * 16) != cudaSuccess) return 1;
+    if (reset) {
+        const unsigned long long z[16] = {0};
+        if (cudaMemcpyToSymbol(g_rrqr_clocks, z, sizeof(z)) != cudaSuccess) return 1;
+    }
+    return 0;
+}
+#else
+#define SPQ_CLK(name)
+#define SPQ_CLK_ADD(slot, v)
+#endif
+
 namespace spq {
 namespace {
 
@@ -197,6 +222,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
         int steps = 0;
         for (int jb = 0; jb < nbk; ++jb) {
             k = k0 + jb;
+            SPQ_CLK(tq0);
             const int buf = k & 1;  // candidate slots alternate, so one cluster barrier per step suffices
             // 1. pivot: largest partial norm, ties to the smallest position; the
             //    column now at position k is noted for the swap (s_c0 is -1 here:
@@ -216,9 +242,11 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             }
             warp_best(bv, bp, bc);
             if (lane == 0) wcand[buf][warp] = Cand<T>{bv, bp, bc};
+            SPQ_CLK(tq1);
             // the cluster barrier also orders this CTA's warps: every warp's candidate
             // of every CTA is visible to all after it
             cl.sync();
+            SPQ_CLK(tq2);
             // every CTA reduces all warps' candidates of the cluster (candidate q: CTA
             // q / nw, warp q % nw, one 16-byte record; the order is immaterial,
             // (value, position) is a strict order), then warp 0 fetches F(:, pc) from
@@ -262,6 +290,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             }
             __syncthreads();
             const int gp = s_gp, pc = s_gc;
+            SPQ_CLK(tq3);
             if (pc < 0) {  // no finite partial norm left (NaN input): stop, uniformly over the cluster
                 rank = k;
                 done = true;
@@ -355,6 +384,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 s_c0 = -1;
             }
             steps = jb + 1;
+            SPQ_CLK(tq4);
             // no barrier here: 3a reads only x (complete since the reduction
             // barrier) and C; the positions, s_aux, V_b(:, jb) and the partials are
             // read in 3b, after the barrier that closes 3a
@@ -375,6 +405,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
             }
             if (tid == 0) s_nflag = 0;
             __syncthreads();
+            SPQ_CLK(tq5);
             // 3b. F(jb, c), pivot row k, partial norms
             T vk[kBNB];  // V_b(k, 0:jb], zero after
 #pragma unroll
@@ -437,6 +468,7 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 }
             }
             __syncthreads();
+            SPQ_CLK(tq6);
             // 3c. norms whose downdate lost accuracy, from C_bs(k+1:m, c) - V_b F(:, c)^T
             //     (one warp per column)
             if (s_nflag > 0) {
@@ -462,10 +494,24 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
                 }
                 __syncthreads();
             }
+#ifdef SPQ_RRQR_CLOCKS
+            if (tid == 0) {
+                SPQ_CLK(tq7);
+                SPQ_CLK_ADD(0, tq1 - tq0);
+                SPQ_CLK_ADD(1, tq2 - tq1);
+                SPQ_CLK_ADD(2, tq3 - tq2);
+                SPQ_CLK_ADD(3, tq4 - tq3);
+                SPQ_CLK_ADD(4, tq5 - tq4);
+                SPQ_CLK_ADD(5, tq6 - tq5);
+                SPQ_CLK_ADD(6, tq7 - tq6);
+                SPQ_CLK_ADD(8, 1);
+            }
+#endif
         }
         // every CTA is past its last read of this block's block-start pivot columns
         // and of the owners' F: the owners store R_kk and the reflector of each
         // accepted pivot in its column
+        SPQ_CLK(tb0);
         cl.sync();
         for (int j = 0; j < steps; ++j) {
             const int pcj = s_pcs[j], kj = k0 + j;
@@ -531,6 +577,13 @@ __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, co
         }
         // the next block's first pivot columns are read (global) by every CTA
         cl.sync();
+#ifdef SPQ_RRQR_CLOCKS
+        if (tid == 0) {
+            SPQ_CLK(tb1);
+            SPQ_CLK_ADD(7, tb1 - tb0);
+            SPQ_CLK_ADD(9, 1);
+        }
+#endif
     }
     __syncthreads();
     // positions out: pos, and colat as their inverse (positions are a permutation)
