@@ -2999,8 +2999,19 @@ private:
         gemv_cols_.clear();
         for (auto& g : gemv) gemv_cols_.push_back(g.s);
         std::vector<std::vector<int>> fw, bw;
-        schedule_ops(fwd, fw);
-        schedule_ops(bwd, bw);
+        {  // the two sweeps are scheduled independently: the backward one on a second thread
+            std::exception_ptr err;
+            std::thread tb([&] {
+                try {
+                    schedule_ops(bwd, bw);
+                } catch (...) {
+                    err = std::current_exception();
+                }
+            });
+            schedule_ops(fwd, fw);
+            tb.join();
+            if (err) std::rethrow_exception(err);
+        }
         std::vector<SolveOp> all;
         std::vector<WMeta> fm, bm;
         pack_waves(fwd, fw, all, fm);
