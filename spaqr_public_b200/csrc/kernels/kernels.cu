@@ -8,6 +8,7 @@
 // downdating) so that ranks and reflectors agree with the reference's LAPACK
 // calls up to rounding.
 #include "kernels.hpp"
+#include "pdl.cuh"
 #include "status.cuh"
 
 #include <algorithm>
@@ -15,6 +16,8 @@
 #include <cmath>
 #include <mutex>
 #include <set>
+#include <stdexcept>
+#include <string>
 #include <utility>
 
 namespace spq {
@@ -123,6 +126,7 @@ __device__ void build_tfac(const T* Vp, int ldv, int R, int w, const T* taus, T*
 // along dst columns.
 template <class T>
 __global__ void __launch_bounds__(256) k_copy(const CopyDesc<T>* descs, int n) {
+    pdl_enter();
     __shared__ T tile[32][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int d = blockIdx.x; d < n; d += gridDim.x) {
@@ -182,6 +186,7 @@ __global__ void __launch_bounds__(256) k_copy(const CopyDesc<T>* descs, int n) {
 // dlarft, forward columnwise), so T needs no extra pass.
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_panel(const QRTask<T>* tasks, const int* ids, int p, int smem_rows) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     __shared__ T red[32];
@@ -481,6 +486,7 @@ struct TcTraits<double> {
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_trailing_tc(const QRTask<T>* tasks, const TileRef* tiles, int p) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int CP = kTN + 1, TP = kNB + 1;
     constexpr int EPT = kRC * kNB / kThreads;  // 8 elements per thread per chunk (V and C each)
@@ -696,6 +702,7 @@ size_t trsm_tc_smem() {
 
 template <class T>
 __global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const TileRef* tiles) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int S = TrsmStages<T>::v;
     constexpr int STG = kNB * kTrXS + kNB * kTrRS;  // one stage: X chunk, then R chunk
@@ -777,6 +784,7 @@ __global__ void __launch_bounds__(128) k_trsm_tc(const TrsmTask<T>* tasks, const
 // TRSM turns into R^-1.
 template <class T>
 __global__ void k_unit_diag(const TrsmTask<T>* tasks) {
+    pdl_enter();
     const TrsmTask<T> t = tasks[blockIdx.x];
     for (int i = threadIdx.x; i < t.k; i += blockDim.x) t.X[i + (size_t)i * t.ldx] = T(1);
 }
@@ -785,6 +793,7 @@ __global__ void k_unit_diag(const TrsmTask<T>* tasks) {
 // dot product over the rows), summed over the CTA, square-rooted.
 template <class T>
 __global__ void __launch_bounds__(256) k_product_norm(const ProdNormTask<T>* tasks, double* out) {
+    pdl_enter();
     __shared__ double red[32];
     const ProdNormTask<T> t = tasks[blockIdx.x];
     double s = 0.0;
@@ -808,6 +817,7 @@ __global__ void __launch_bounds__(256) k_product_norm(const ProdNormTask<T>* tas
 // the column norms. Writes 1 / sigma_min (sum of squares in FP64).
 template <class T>
 __global__ void __launch_bounds__(256) k_sigma_min(const SigmaTask<T>* tasks) {
+    pdl_enter();
     __shared__ double red[32];
     __shared__ int s_rot;
     const SigmaTask<T> t = tasks[blockIdx.x];
@@ -882,6 +892,7 @@ __global__ void __launch_bounds__(256) k_sigma_min(const SigmaTask<T>* tasks) {
 // One CTA per (task, 32-column tile of B): thread (i, jj) sums over the rows.
 template <class T>
 __global__ void __launch_bounds__(256) k_atb_scaled(const AtbTask<T>* tasks, const TileRef* tiles) {
+    pdl_enter();
     const TileRef tr = tiles[blockIdx.x];
     const AtbTask<T> t = tasks[tr.task];
     const int j0 = tr.tile * 32;
@@ -901,6 +912,7 @@ __global__ void __launch_bounds__(256) k_atb_scaled(const AtbTask<T>* tasks, con
 // ------------------------------------------------------------------ assembly scatter
 template <class T>
 __global__ void k_scatter_values(const uint64_t* addr, const double* vals, int64_t n) {
+    pdl_enter();
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
         *reinterpret_cast<T*>(addr[e]) = (T)vals[e];
 }
@@ -1193,6 +1205,7 @@ __device__ void gemv_sub(T* xs, int k, const GemvRef<T>* gv, int nb, const T* x,
 template <class T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_solve_step(const SolveOp* ops, const XSeg* segs,
                                                         const GemvRef<T>* gemv, T* x) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* xs = reinterpret_cast<T*>(smem_raw);
     __shared__ SolveShared<T> sh;
@@ -1416,12 +1429,14 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_solve_step
 
 template <class T>
 __global__ void k_seg_copy(const T* src, T* dst, const int64_t* pos, int n) {
+    pdl_enter();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[pos[i]] = src[pos[i]];
 }
 
 // out[t][i] = || row (row0 + i) of block t || (FP64 sums), one warp per row.
 template <class T>
 __global__ void k_row_norms(const RowNormTask<T>* tasks, int ntasks, double* out) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int t = 0; t < ntasks; ++t) {
@@ -1441,10 +1456,12 @@ __global__ void k_row_norms(const RowNormTask<T>* tasks, int ntasks, double* out
 
 template <class T>
 __global__ void k_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n) {
+    pdl_enter();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[xpos[i]] = (T)b[src[i]];
 }
 template <class T>
 __global__ void k_scatter_out(const T* x, const int64_t* xpos, const int* dst, double* out, int n) {
+    pdl_enter();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[dst[i]] = (double)x[xpos[i]];
 }
@@ -1541,59 +1558,65 @@ size_t trailing_tc_smem() {
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+static void pdl_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + " launch: " + cudaGetErrorString(e));
+}
+
 template <class T>
 void launch_copy(const CopyDesc<T>* d, int n, int max_cols, cudaStream_t s) {
     if (n <= 0) return;
     const int chunks = std::max(1, std::min(32, (max_cols + 31) / 32));
-    k_copy<T><<<dim3(n < 65535 ? n : 65535, chunks), 256, 0, s>>>(d, n);
+    pdl_check(launch_pdl(k_copy<T>, dim3(n < 65535 ? n : 65535, chunks), dim3(256), 0, s, 0, d, n), "k_copy");
 }
 
 template <class T>
 void launch_panel(const QRTask<T>* tasks, const int* ids, int ntasks, int p, int smem_rows, cudaStream_t s) {
     if (ntasks <= 0) return;
     size_t smem = (size_t)smem_rows * kNB * sizeof(T);
-    k_panel<T><<<ntasks, kThreads, smem, s>>>(tasks, ids, p, smem_rows);
+    pdl_check(launch_pdl(k_panel<T>, dim3(ntasks), dim3(kThreads), smem, s, 0, tasks, ids, p, smem_rows), "k_panel");
 }
 
 template <class T>
 void launch_trailing(const QRTask<T>* tasks, const TileRef* tiles, int ntiles, int p, cudaStream_t s) {
     if (ntiles <= 0) return;
-    k_trailing_tc<T><<<ntiles, kThreads, trailing_tc_smem<T>(), s>>>(tasks, tiles, p);
+    pdl_check(launch_pdl(k_trailing_tc<T>, dim3(ntiles), dim3(kThreads), trailing_tc_smem<T>(), s, 0, tasks, tiles, p),
+              "k_trailing_tc");
 }
 
 template <class T>
 void launch_trsm(const TrsmTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
     if (ntiles <= 0) return;
-    k_trsm_tc<T><<<ntiles, 128, trsm_tc_smem<T>(), s>>>(tasks, tiles);
+    pdl_check(launch_pdl(k_trsm_tc<T>, dim3(ntiles), dim3(128), trsm_tc_smem<T>(), s, 0, tasks, tiles), "k_trsm_tc");
 }
 
 template <class T>
 void launch_product_norms(const ProdNormTask<T>* tasks, int ntasks, double* out, cudaStream_t s) {
     if (ntasks <= 0) return;
-    k_product_norm<T><<<ntasks, 256, 0, s>>>(tasks, out);
+    pdl_check(launch_pdl(k_product_norm<T>, dim3(ntasks), dim3(256), 0, s, 0, tasks, out), "k_product_norm");
 }
 
 template <class T>
 void launch_sigma_min(const SigmaTask<T>* tasks, int ntasks, cudaStream_t s) {
     if (ntasks <= 0) return;
-    k_sigma_min<T><<<ntasks, 256, 0, s>>>(tasks);
+    pdl_check(launch_pdl(k_sigma_min<T>, dim3(ntasks), dim3(256), 0, s, 0, tasks), "k_sigma_min");
 }
 template <class T>
 void launch_atb_scaled(const AtbTask<T>* tasks, const TileRef* tiles, int ntiles, cudaStream_t s) {
     if (ntiles <= 0) return;
-    k_atb_scaled<T><<<ntiles, 256, 0, s>>>(tasks, tiles);
+    pdl_check(launch_pdl(k_atb_scaled<T>, dim3(ntiles), dim3(256), 0, s, 0, tasks, tiles), "k_atb_scaled");
 }
 
 template <class T>
 void launch_unit_diag(const TrsmTask<T>* tasks, int ntasks, cudaStream_t s) {
     if (ntasks <= 0) return;
-    k_unit_diag<T><<<ntasks, 256, 0, s>>>(tasks);
+    pdl_check(launch_pdl(k_unit_diag<T>, dim3(ntasks), dim3(256), 0, s, 0, tasks), "k_unit_diag");
 }
 
 template <class T>
 void launch_scatter_values(const uint64_t* addr, const double* vals, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
-    k_scatter_values<T><<<grid_for(n, 256), 256, 0, s>>>(addr, vals, n);
+    pdl_check(launch_pdl(k_scatter_values<T>, dim3(grid_for(n, 256)), dim3(256), 0, s, 0, addr, vals, n),
+              "k_scatter_values");
 }
 
 template <class T>
@@ -1602,27 +1625,30 @@ void launch_solve_step(const SolveOp* ops, int nops, const XSeg* segs, const Gem
     (void)arena;
     if (nops <= 0) return;
     size_t smem = (size_t)(smem_elems < 32 ? 32 : smem_elems) * sizeof(T);
-    k_solve_step<T><<<nops, kThreads, smem, s>>>(ops, segs, gemv, x);
+    pdl_check(launch_pdl(k_solve_step<T>, dim3(nops), dim3(kThreads), smem, s, 0, ops, segs, gemv, x), "k_solve_step");
 }
 
 template <class T>
 void launch_seg_copy(const T* src, T* dst, const int64_t* pos, int n, cudaStream_t s) {
     if (n <= 0) return;
-    k_seg_copy<T><<<grid_for(n, 256), 256, 0, s>>>(src, dst, pos, n);
+    pdl_check(launch_pdl(k_seg_copy<T>, dim3(grid_for(n, 256)), dim3(256), 0, s, 0, src, dst, pos, n), "k_seg_copy");
 }
 template <class T>
 void launch_row_norms(const RowNormTask<T>* tasks, int ntasks, int total_rows, double* out, cudaStream_t s) {
     if (ntasks <= 0 || total_rows <= 0) return;
-    k_row_norms<T><<<grid_for((int64_t)total_rows * 32, 256, 148 * 8), 256, 0, s>>>(tasks, ntasks, out);
+    pdl_check(launch_pdl(k_row_norms<T>, dim3(grid_for((int64_t)total_rows * 32, 256, 148 * 8)), dim3(256), 0, s, 0,
+                         tasks, ntasks, out),
+              "k_row_norms");
 }
 
 template <class T>
 void launch_gather_in(const double* b, const int* src, const int64_t* xpos, T* x, int n, cudaStream_t s) {
-    k_gather_in<T><<<grid_for(n, 256), 256, 0, s>>>(b, src, xpos, x, n);
+    pdl_check(launch_pdl(k_gather_in<T>, dim3(grid_for(n, 256)), dim3(256), 0, s, 0, b, src, xpos, x, n), "k_gather_in");
 }
 template <class T>
 void launch_scatter_out(const T* x, const int64_t* xpos, const int* dst, double* out, int n, cudaStream_t s) {
-    k_scatter_out<T><<<grid_for(n, 256), 256, 0, s>>>(x, xpos, dst, out, n);
+    pdl_check(launch_pdl(k_scatter_out<T>, dim3(grid_for(n, 256)), dim3(256), 0, s, 0, x, xpos, dst, out, n),
+              "k_scatter_out");
 }
 
 void launch_spmv_csr(int m, const int* rp, const int* ci, const double* v, const double* x, double* y,

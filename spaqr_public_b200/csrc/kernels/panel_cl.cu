@@ -30,6 +30,7 @@
 #include <algorithm>
 
 #include "kernels.hpp"
+#include "pdl.cuh"
 #include "status.cuh"
 
 namespace spq {
@@ -70,6 +71,7 @@ __device__ __forceinline__ T tsum32(T (&a)[kNB]) {  // lane q returns sum over l
 // ids[0:n] task indices, ids[n:2n] their cluster sizes (1 <= CLt <= cluster)
 template <class T>
 __global__ void __launch_bounds__(kPThreads) k_panel_cl(const QRTask<T>* tasks, const int* ids, int n, int p) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* P = reinterpret_cast<T*>(smem_raw);  // slab rows x kPS
     // column sums by sender rank (2 x kMaxCl x kNB), then the warp partials
@@ -246,6 +248,7 @@ __global__ void __launch_bounds__(kPThreads) k_panel_cl(const QRTask<T>* tasks, 
 //      finished columns), the owner then writing v and beta into column j.
 template <class T, bool kCl, int kRPL>
 __global__ void __launch_bounds__(kPThreads, ((sizeof(T) == 4 && kRPL < 16) || kRPL < 8) ? 2 : 1) k_panel_reg(const QRTask<T>* tasks, const int* ids, int n, int p) {
+    pdl_enter();
     constexpr int CPW = kNB / kPWarps;  // columns per warp
     constexpr int SR = 32 * kRPL;       // slab rows
     static_assert(CPW == 4, "the transposed reduction assumes four columns per warp");
@@ -448,13 +451,15 @@ cudaError_t launch_panel_cl(const QRTask<T>* tasks, const int* ids, int ntasks, 
     cfg.blockDim = dim3(kPThreads, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_panel_cl<T>, tasks, ids, ntasks, p);
 }
 
@@ -462,8 +467,7 @@ template <class T, int RPL>
 cudaError_t launch_panel_reg_rpl(const QRTask<T>* tasks, const int* ids, int ntasks, int cluster, int p,
                                  cudaStream_t s) {
     if (cluster == 1) {
-        k_panel_reg<T, false, RPL><<<ntasks, kPThreads, 0, s>>>(tasks, ids, ntasks, p);
-        return cudaGetLastError();
+        return launch_pdl(k_panel_reg<T, false, RPL>, dim3(ntasks), dim3(kPThreads), 0, s, 0, tasks, ids, ntasks, p);
     }
     once_per_device(reinterpret_cast<const void*>(&k_panel_reg<T, true, RPL>), [] {
         cudaFuncSetAttribute(k_panel_reg<T, true, RPL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -473,13 +477,15 @@ cudaError_t launch_panel_reg_rpl(const QRTask<T>* tasks, const int* ids, int nta
     cfg.blockDim = dim3(kPThreads, 1, 1);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_panel_reg<T, true, RPL>, tasks, ids, ntasks, p);
 }
 

@@ -26,6 +26,10 @@
 #include <climits>
 
 #include "kernels.hpp"
+#include "pdl.cuh"
+
+#include <stdexcept>
+#include <string>
 #include "rrqr_common.cuh"
 #include "status.cuh"
 
@@ -42,6 +46,7 @@ using namespace rrqr;
 template <class T>
 __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids,
                                                          size_t smem_bytes) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* vsh = reinterpret_cast<T*>(smem_raw);
     __shared__ T red[32];
@@ -358,6 +363,7 @@ __global__ void __launch_bounds__(kRRThreads) k_rrqr_rm(const RRQRTaskRM<T>* tas
 // turned into the panel's T factor (LAPACK dlarft, forward, columnwise).
 template <class T>
 __global__ void __launch_bounds__(256) k_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks) {
+    pdl_enter();
     constexpr int P = kNB + 1;
     __shared__ T G[kNB * P];
     __shared__ T Ts[kNB * P];
@@ -493,13 +499,15 @@ cudaError_t launch_rrqr_rm(const RRQRTaskRM<T>* tasks, const int* ids, int ntask
     cfg.blockDim = dim3(kRRThreads, 1, 1);
     cfg.dynamicSmemBytes = smem_bytes;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_rrqr_rm<T>, tasks, ids, smem_bytes);
 }
 
@@ -507,7 +515,8 @@ template <class T>
 void launch_spars_wb_rm(const SparsWBRM<T>* tasks, const SpBlock<T>* blocks, int ntasks, int parts, cudaStream_t s) {
     if (ntasks <= 0) return;
     const int ny = parts < 1 ? 1 : (parts > 32 ? 32 : parts);
-    k_spars_wb_rm<T><<<dim3(ntasks, ny), 256, 0, s>>>(tasks, blocks);
+    const cudaError_t e = launch_pdl(k_spars_wb_rm<T>, dim3(ntasks, ny), dim3(256), 0, s, 0, tasks, blocks);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("k_spars_wb_rm launch: ") + cudaGetErrorString(e));
 }
 
 template cudaError_t launch_rrqr_rm<double>(const RRQRTaskRM<double>*, const int*, int, int, int, int,

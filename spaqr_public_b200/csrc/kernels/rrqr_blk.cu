@@ -49,6 +49,7 @@
 #include <climits>
 
 #include "kernels.hpp"
+#include "pdl.cuh"
 #include "rrqr_common.cuh"
 #include "status.cuh"
 
@@ -153,6 +154,7 @@ __device__ __forceinline__ void rrqr_partials(const T* C, size_t ld, int j0, int
 
 template <class T>
 __global__ void __launch_bounds__(kBT) k_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int Wp, int mpad) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int VEC = Vec<T>::n;
     constexpr int kBNB = BlkNB<T>::v;
@@ -627,13 +629,15 @@ cudaError_t launch_rrqr_blk(const RRQRTaskRM<T>* tasks, const int* ids, int ntas
     cfg.blockDim = dim3(kBT, 1, 1);
     cfg.dynamicSmemBytes = smem_bytes;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_rrqr_blk<T>, tasks, ids, Wp, mpad);
 }
 

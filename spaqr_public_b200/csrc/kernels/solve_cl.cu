@@ -18,6 +18,7 @@
 #include <cooperative_groups.h>
 
 #include "kernels.hpp"
+#include "pdl.cuh"
 
 namespace spq {
 
@@ -47,6 +48,7 @@ __device__ __forceinline__ T tsum32(T (&a)[kNB]) {  // lane q returns sum over l
 
 template <class T>
 __global__ void __launch_bounds__(kAThreads) k_applyq_cl(const SolveOp* ops, const XSeg* segs, T* x) {
+    pdl_enter();
     __shared__ T part[2][kAMaxCl][kNB];
     __shared__ T wred[kAWarps][kNB];
     __shared__ T tsh[2][kNB][kNB + 1];
@@ -182,6 +184,7 @@ constexpr int kTGU = 16;  // loads in flight per thread in the products
 
 template <class T>
 __global__ void __launch_bounds__(kTThreads) k_tri_cl(const SolveOp* ops, const GemvRef<T>* gemv, T* x) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char tri_raw[];
     __shared__ GemvRef<T> refs[kTriMaxRefs];
     __shared__ int cstart[kTriMaxRefs + 1];
@@ -341,13 +344,15 @@ cudaError_t launch_applyq_cl(const SolveOp* ops, int nops, int cluster, const XS
     cfg.blockDim = dim3(kAThreads, 1, 1);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_applyq_cl<T>, ops, segs, x);
 }
 
@@ -367,13 +372,15 @@ cudaError_t launch_tri_cl(const SolveOp* ops, int nops, int cluster, int kmax, c
     cfg.blockDim = dim3(kTThreads, 1, 1);
     cfg.dynamicSmemBytes = 2 * (size_t)kmax * sizeof(T);
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = (unsigned)cluster;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // the kernel starts with pdl_enter()
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_tri_cl<T>, ops, gemv, x);
 }
 
