@@ -36,22 +36,71 @@ Csc csc_from(int m, int n, const int* cp, const int* ri, const double* va) {
     return A;
 }
 
+// Column r of the result lists the columns j of A with A(r, j) != 0 in
+// increasing j. On host threads for large matrices: each thread counts its
+// column range's entries per row, a prefix over (row, thread) places every
+// thread's entries of a row after those of the lower ranges, and each thread
+// scatters its own range: the same arrays as one pass in column order.
 Csc csc_transpose(const Csc& A) {
     Csc T;
     T.m = A.n;
     T.n = A.m;
     T.p.assign((size_t)A.m + 1, 0);
-    for (int r : A.i) ++T.p[(size_t)r + 1];
-    std::partial_sum(T.p.begin(), T.p.end(), T.p.begin());
     T.i.resize(A.i.size());
     T.v.resize(A.v.size());
-    std::vector<int> next(T.p.begin(), T.p.end() - 1);
-    for (int j = 0; j < A.n; ++j)
-        for (int q = A.p[j]; q < A.p[j + 1]; ++q) {
-            int dst = next[A.i[q]]++;
-            T.i[dst] = j;
-            T.v[dst] = A.v[q];
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = A.i.size() < (size_t)(1 << 18) ? 1 : std::max(1, std::min({hw, 8, A.n / 2048}));
+    if (nt == 1) {
+        for (int r : A.i) ++T.p[(size_t)r + 1];
+        std::partial_sum(T.p.begin(), T.p.end(), T.p.begin());
+        std::vector<int> next(T.p.begin(), T.p.end() - 1);
+        for (int j = 0; j < A.n; ++j)
+            for (int q = A.p[j]; q < A.p[j + 1]; ++q) {
+                int dst = next[A.i[q]]++;
+                T.i[dst] = j;
+                T.v[dst] = A.v[q];
+            }
+        return T;
+    }
+    std::vector<std::vector<int>> cnt(nt, std::vector<int>(A.m, 0));
+    auto range = [&](int t, int& lo, int& hi) {
+        lo = (int)((int64_t)A.n * t / nt);
+        hi = (int)((int64_t)A.n * (t + 1) / nt);
+    };
+    std::vector<std::thread> th;
+    auto run = [&](auto&& fn) {
+        th.clear();
+        for (int t = 1; t < nt; ++t) th.emplace_back([&, t] { fn(t); });
+        fn(0);
+        for (auto& x : th) x.join();
+    };
+    run([&](int t) {
+        int lo, hi;
+        range(t, lo, hi);
+        auto& c = cnt[t];
+        for (int q = A.p[lo]; q < A.p[hi]; ++q) ++c[A.i[q]];
+    });
+    // row pointers, then each thread's first slot in every row
+    for (int r = 0; r < A.m; ++r) {
+        int64_t s = T.p[r];
+        for (int t = 0; t < nt; ++t) {
+            const int c = cnt[t][r];
+            cnt[t][r] = (int)s;
+            s += c;
         }
+        T.p[(size_t)r + 1] = s;
+    }
+    run([&](int t) {
+        int lo, hi;
+        range(t, lo, hi);
+        auto& next = cnt[t];
+        for (int j = lo; j < hi; ++j)
+            for (int q = A.p[j]; q < A.p[j + 1]; ++q) {
+                int dst = next[A.i[q]]++;
+                T.i[dst] = j;
+                T.v[dst] = A.v[q];
+            }
+    });
     return T;
 }
 
