@@ -548,7 +548,7 @@ private:
     // A backward triangular op goes to the cluster kernel from kTriClWords
     // words of R^-1 and neighbour blocks, on ceil(words / kTriClPerCta) CTAs
     // (the wave's largest op sets the launch's cluster size).
-    static constexpr double kTriClWords = 32768, kTriClPerCta = 16384;
+    static constexpr double kTriClWords = 16384, kTriClPerCta = 16384;
     Wave make_wave(const SolveOp* d_ops, const WMeta& mt) const {
         return Wave{d_ops + mt.off, mt.n,     mt.smem,  mt.words, mt.hkind, mt.ha,  mt.hb,
                     d_ops + mt.boff, mt.nbig, mt.bcl,  d_ops + mt.toff, mt.ntri, mt.tcl, mt.tk};
@@ -2785,7 +2785,7 @@ private:
     // once per factorization. The solve's sweeps then apply Q^T (and OrthD's
     // Q, as its transpose) as one dense product split over a thread-block
     // cluster, instead of a chain of one reduction per reflector panel.
-    static constexpr int kDenseQMin = 128;
+    static constexpr int kDenseQMin = 64;
     void form_qt() {
         std::vector<QRTask<T>> tasks;
         std::vector<TrsmTask<T>> diag;
