@@ -109,9 +109,10 @@ public:
         stream_ = s;
         pool_ = pool;
     }
+    // The bytes alloc(bytes) takes from a chunk: whole 128-byte lines, at least one.
+    static size_t rounded(size_t bytes) { return bytes ? (bytes + 127) & ~size_t(127) : 128; }
     void* alloc(size_t bytes) {
-        bytes = (bytes + 127) & ~size_t(127);
-        if (bytes == 0) bytes = 128;
+        bytes = rounded(bytes);
         if (chunks_.empty() || used_ + bytes > cap_) {
             const double t0 = wall_seconds();
             size_t sz = bytes > chunk_ ? bytes : chunk_;

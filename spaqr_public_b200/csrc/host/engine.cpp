@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <deque>
 #include <exception>
+#include <limits>
 #include <map>
 #include <numeric>
 #include <thread>
@@ -679,12 +680,13 @@ private:
         clusters_.emplace_back(c);
         return c;
     }
+    static size_t block_elems(int rows, int cols) { return (size_t)std::max(rows, 1) * std::max(cols, 1); }
     Blk new_block(int rows, int cols) {
         Blk b;
         b.rows = rows;
         b.cols = cols;
         b.ld = std::max(rows, 1);
-        b.p = arena_.alloc_n<T>((size_t)b.ld * std::max(cols, 1));
+        b.p = arena_.alloc_n<T>(block_elems(rows, cols));
         b.uid = next_uid_++;
         return b;
     }
@@ -2644,12 +2646,15 @@ private:
         };
         const std::vector<Cluster*>& par = cur();
         const size_t np = par.size();
+        std::unordered_map<const Cluster*, int> pidx;  // parent -> position in par
+        pidx.reserve(np * 2);
+        for (size_t pi = 0; pi < np; ++pi) pidx[par[pi]] = (int)pi;
         std::vector<std::vector<Cluster*>> nbs(np);
         std::vector<std::vector<Move>> moves(np);
         std::vector<std::vector<std::pair<Cluster*, Edge*>>> pes(np);  // parent edges by neighbour address
-        std::vector<std::vector<CopyDesc<T>>> cps(np);
-        // 1. (threads) each parent's neighbour parents and child-block moves: reads only
-        //    its own children's edges
+        std::vector<size_t> pbytes(np, 0);
+        // 1. (threads) each parent's neighbour parents, the bytes of its new blocks
+        //    and its child-block moves: reads only its own children's edges
         host_parallel_for(np, [&](size_t b, size_t e) {
             for (size_t pi = b; pi < e; ++pi) {
                 Cluster* s = par[pi];
@@ -2667,20 +2672,79 @@ private:
                 std::sort(nb.begin(), nb.end(),
                           [](const Cluster* a, const Cluster* b) { return a->order < b->order; });
                 nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+                for (Cluster* n : nb) pbytes[pi] += Arena::rounded(block_elems(n->rsize, s->csize) * sizeof(T));
             }
         });
         const double tb = wall();
         t_nb = tb - tm1;
-        // 2. (in order) the parent edges: blocks and uids in the reference's order
-        for (size_t pi = 0; pi < np; ++pi) {
-            Cluster* s = par[pi];
-            s->out.reserve(s->out.size() + nbs[pi].size());
-            pes[pi].reserve(nbs[pi].size());
-            for (Cluster* n : nbs[pi]) pes[pi].emplace_back(n, add_edge(s, n));
+        // 2. the parent edges in the reference's order (parents in order, each
+        //    parent's neighbours by order): uids and edge slots by prefix sums,
+        //    each parent's blocks from one arena range in that order. Then (threads)
+        //    the edges and out lists per parent, and the in lists per neighbour,
+        //    each list in the order one parent after another gives it.
+        std::vector<size_t> ebase(np + 1, 0);
+        for (size_t pi = 0; pi < np; ++pi) ebase[pi + 1] = ebase[pi] + nbs[pi].size();
+        const size_t ne = ebase[np], e0 = edges_.size();
+        if (ne > size_t(std::numeric_limits<int>::max() - next_uid_))
+            throw std::runtime_error("merge: block uid overflow");
+        const int uid0 = next_uid_;
+        next_uid_ += (int)ne;
+        std::vector<char*> pbase(np, nullptr);
+        for (size_t pi = 0; pi < np; ++pi)
+            if (pbytes[pi]) pbase[pi] = static_cast<char*>(arena_.alloc(pbytes[pi]));
+        edges_.resize(e0 + ne);
+        std::vector<int> tgt(ne);  // the neighbour's position in par
+        host_parallel_for(np, [&](size_t b, size_t e) {
+            for (size_t pi = b; pi < e; ++pi) {
+                Cluster* s = par[pi];
+                char* p = pbase[pi];
+                s->out.reserve(s->out.size() + nbs[pi].size());
+                pes[pi].reserve(nbs[pi].size());
+                for (size_t j = 0; j < nbs[pi].size(); ++j) {
+                    Cluster* n = nbs[pi][j];
+                    const size_t q = ebase[pi] + j;
+                    Blk bk;
+                    bk.rows = n->rsize;
+                    bk.cols = s->csize;
+                    bk.ld = std::max(bk.rows, 1);
+                    bk.p = reinterpret_cast<T*>(p);
+                    bk.uid = uid0 + (int)q;
+                    p += Arena::rounded(block_elems(bk.rows, bk.cols) * sizeof(T));
+                    Edge& ed = edges_[e0 + q];
+                    ed = Edge{s, n, bk, true};
+                    s->out.push_back(&ed);
+                    pes[pi].emplace_back(n, &ed);
+                    const auto it = pidx.find(n);
+                    if (it == pidx.end()) throw std::runtime_error("merge: neighbour outside the level");
+                    tgt[q] = n == s ? -1 : it->second;
+                }
+            }
+        });
+        {
+            std::vector<int> nin(np, 0);
+            for (int t : tgt)
+                if (t >= 0) ++nin[t];
+            for (size_t t = 0; t < np; ++t) par[t]->in.reserve(par[t]->in.size() + nin[t]);
+            const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+            const size_t nth = std::max<size_t>(1, std::min<size_t>({hw, 8, np / 256}));
+            host_parallel_for(nth, [&](size_t b, size_t e) {
+                for (size_t k = b; k < e; ++k) {  // neighbours [np k / nth, np (k + 1) / nth)
+                    const int lo = (int)(np * k / nth), hi = (int)(np * (k + 1) / nth);
+                    for (size_t q = 0; q < ne; ++q)
+                        if (tgt[q] >= lo && tgt[q] < hi) par[tgt[q]]->in.push_back(&edges_[e0 + q]);
+                }
+            }, 1);
         }
         const double tc = wall();
         t_add = tc - tb;
-        // 3. (threads) each parent sorts its out list and lists its copies
+        // 3. (threads) each parent sorts its out list and writes its copies into
+        //    the pinned stage at its prefix-sum position
+        std::vector<size_t> cbase(np + 1, 0);
+        for (size_t pi = 0; pi < np; ++pi) cbase[pi + 1] = cbase[pi] + moves[pi].size();
+        const size_t ncp = cbase[np];
+        CopyDesc<T>* hcp = ncp ? reinterpret_cast<CopyDesc<T>*>(pinned_.get(ncp * sizeof(CopyDesc<T>))) : nullptr;
+        std::vector<double> pby(np, 0);
+        std::vector<int> pmaxc(np, 0);
         host_parallel_for(np, [&](size_t b, size_t e) {
             for (size_t pi = b; pi < e; ++pi) {
                 Cluster* s = par[pi];
@@ -2688,40 +2752,42 @@ private:
                                  [](Edge* a, Edge* b) { return a->n2->order < b->n2->order; });
                 auto& pe = pes[pi];
                 std::sort(pe.begin(), pe.end());
-                cps[pi].reserve(moves[pi].size());
+                CopyDesc<T>* o = hcp + cbase[pi];
                 for (const Move& mv : moves[pi]) {
                     auto it = std::lower_bound(pe.begin(), pe.end(), std::make_pair(mv.np, (Edge*)nullptr));
                     if (it == pe.end() || it->first != mv.np) throw std::runtime_error("merge: missing parent edge");
                     Edge* f = it->second;
                     Edge* eo = mv.eo;
-                    cps[pi].push_back(cp(eo->A.p, f->A.p + mv.roff + (size_t)mv.so->cposparent * f->A.ld, eo->A.ld,
-                                         f->A.ld, eo->A.rows, eo->A.cols));
+                    *o++ = cp(eo->A.p, f->A.p + mv.roff + (size_t)mv.so->cposparent * f->A.ld, eo->A.ld, f->A.ld,
+                              eo->A.rows, eo->A.cols);
+                    pby[pi] += 2.0 * eo->A.rows * eo->A.cols * sizeof(T);
+                    pmaxc[pi] = std::max(pmaxc[pi], eo->A.cols);
                     eo->live = false;
                 }
             }
         });
         const double td = wall();
         t_sort = td - tc;
-        std::vector<CopyDesc<T>> copies;
-        {
-            size_t ne = 0;
-            for (auto& v : cps) ne += v.size();
-            copies.reserve(ne);
-            for (auto& v : cps) copies.insert(copies.end(), v.begin(), v.end());
-        }
-        t_cp = wall() - td;
+        t_cp = 0;
         const double tm2 = wall();
-        if (!copies.empty()) {
-            Upload up;
-            size_t o = up.add(copies);
-            char* d = up.commit(desc_arena_, stream_, pinned_);
-            issue_copies(reinterpret_cast<const CopyDesc<T>*>(d + o), copies);
+        if (ncp) {
+            double by = 0;
+            int maxc = 0;
+            for (size_t pi = 0; pi < np; ++pi) {
+                by += pby[pi];
+                maxc = std::max(maxc, pmaxc[pi]);
+            }
+            const size_t bytes = ncp * sizeof(CopyDesc<T>);
+            auto* d = static_cast<CopyDesc<T>*>(desc_arena_.alloc(bytes));
+            cuda_check(cudaMemcpyAsync(d, hcp, bytes, cudaMemcpyHostToDevice, stream_), "merge copy list upload");
+            timed(KF_COPY, 0, by, [&] { launch_copy<T>(d, (int)ncp, maxc, stream_); });
+            ++launches_fact_;
         }
         if (cfg_.verbose >= 3)
             std::fprintf(stderr,
                          "[lvl %d] merge host: %zu clusters, %zu copies, sizes %.2f ms, neighbours %.2f, edges %.2f, "
                          "sort + copy list %.2f, concatenate %.2f, upload+launch %.2f\n",
-                         ilvl_, cur().size(), copies.size(), (tm1 - tm0) * 1e3, t_nb * 1e3, t_add * 1e3,
+                         ilvl_, cur().size(), ncp, (tm1 - tm0) * 1e3, t_nb * 1e3, t_add * 1e3,
                          t_sort * 1e3, t_cp * 1e3, (wall() - tm2) * 1e3);
     }
 
