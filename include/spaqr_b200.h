@@ -200,7 +200,11 @@ int spq_get_launches(spq_tree* t, long long* factorize, long long* krylov, long 
  * returns, for kernel family f (0 copy, 1 panel QR, 2 trailing update, 3 trsm,
  * 4 truncated RRQR, 5 sparsification write-back, 6 assembly scatter,
  * 7 preconditioner application), out[0..3] = launches, total ms, algorithmic
- * flops, algorithmic bytes. spq_reset_kernel_stats clears the counters. */
+ * flops, algorithmic bytes. spq_reset_kernel_stats clears the counters.
+ * profile = 2 also prints, when the counters are read, one line per launch to
+ * stderr: "timeline <family> <start ms> <duration ms> L<level> P<phase>", the
+ * start measured from the first launch since the previous read, for locating
+ * the stretches where the device waits for the host. */
 int spq_set_profile(spq_tree* t, int profile);
 int spq_get_kernel_stats(spq_tree* t, int family, double* out4);
 int spq_reset_kernel_stats(spq_tree* t);

@@ -613,7 +613,7 @@ int spq_get_launches(spq_tree* t, long long* factorize, long long* krylov, long 
 int spq_set_profile(spq_tree* t, int profile) {
     if (!t) return fail(SPQ_ERR_ARG, "null handle");
     if (!t->eng) return fail(SPQ_ERR_STATE, "profile before partition");
-    t->eng->set_profile(profile != 0);
+    t->eng->set_profile(profile);
     return SPQ_OK;
 }
 int spq_get_kernel_stats(spq_tree* t, int family, double* out4) {

@@ -13,12 +13,16 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <deque>
 #include <exception>
+#include <functional>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <numeric>
+#include <pthread.h>
 #include <thread>
 #include <unordered_map>
 
@@ -30,6 +34,86 @@ double wall() {
 }
 
 inline int npanels(int k) { return (k + kNB - 1) / kNB; }
+
+// Host worker threads for the engine's parallel passes, started once per
+// process (a factorization makes hundreds of short passes, and starting
+// threads for each costs 10-20 us per thread). One pass at a time: a pass
+// submitted while another holds the pool (a second handle, the backward
+// schedule's thread) runs its chunks on the calling thread, with the same
+// chunk boundaries, so results do not depend on which thread ran a chunk. A
+// child process forked after the workers started has none of them and runs
+// every pass on its own thread.
+class HostPool {
+public:
+    static HostPool& get() {
+        static HostPool* p = new HostPool();  // never destroyed: the workers live until exit
+        return *p;
+    }
+    // Calls body(t) for t in [0, nt) on the caller and the workers and returns
+    // when all have returned; false (nothing called) if the pool is busy.
+    bool run(size_t nt, const std::function<void(size_t)>& body) {
+        if (forked_ || workers_ == 0) return false;
+        std::unique_lock<std::mutex> busy(submit_, std::try_to_lock);
+        if (!busy.owns_lock()) return false;
+        Job job{&body, nt};
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_ = &job;
+            ++gen_;
+        }
+        cv_.notify_all();
+        work(job);
+        std::unique_lock<std::mutex> g(mu_);
+        done_cv_.wait(g, [&] { return job.done.load() == nt && job.active == 0; });
+        job_ = nullptr;
+        return true;
+    }
+
+private:
+    struct Job {
+        const std::function<void(size_t)>* body;
+        size_t nt;
+        std::atomic<size_t> next{0}, done{0};
+        int active = 0;  // workers inside work(), under mu_
+    };
+    HostPool() {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        workers_ = std::min(hw, 8u) - 1;
+        for (unsigned i = 0; i < workers_; ++i) std::thread([this] { loop(); }).detach();
+        pthread_atfork(nullptr, nullptr, [] { get().forked_ = true; });
+    }
+    void work(Job& j) {
+        for (size_t t; (t = j.next.fetch_add(1)) < j.nt;) {
+            (*j.body)(t);
+            if (j.done.fetch_add(1) + 1 == j.nt) {
+                std::lock_guard<std::mutex> g(mu_);
+                done_cv_.notify_all();
+            }
+        }
+    }
+    void loop() {
+        unsigned long long seen = 0;
+        for (;;) {
+            Job* j;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return job_ != nullptr && gen_ != seen; });
+                seen = gen_;
+                j = job_;
+                ++j->active;
+            }
+            work(*j);
+            std::lock_guard<std::mutex> g(mu_);
+            if (--j->active == 0) done_cv_.notify_all();
+        }
+    }
+    unsigned workers_ = 0;
+    bool forked_ = false;
+    std::mutex submit_, mu_;
+    std::condition_variable cv_, done_cv_;
+    Job* job_ = nullptr;
+    unsigned long long gen_ = 0;
+};
 
 // Greedy wave assignment in list order: a task runs one wave after the last
 // task that touched any of its blocks.
@@ -78,7 +162,7 @@ public:
         std::vector<Edge*> out, in;
         int xcap = 0;
         int64_t xoff = -1;
-        int out_mark = 0;  // elimination build: out edges before the phase's fill blocks
+        int pos = -1;  // scratch: position in the current cluster list during a host pass
         int level() const { return id.self.lvl; }
     };
     enum TapeKind { TK_QR, TK_SCALED, TK_ORTHD, TK_SPLITD, TK_MERGE, TK_REASSIGN, TK_ORTH, TK_SPLIT0 };
@@ -108,6 +192,10 @@ public:
     ~Engine() override {
         if (!stream_) return;
         cudaSetDevice(cfg_.device);
+        try {
+            finish_capture();
+        } catch (...) {
+        }
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (graph_) cudaGraphDestroy(graph_);
         if (adj_exec_) cudaGraphExecDestroy(adj_exec_);
@@ -120,22 +208,29 @@ public:
         desc_arena_.release();
         scratch_.hand_off(stream_);
         cudaStreamSynchronize(stream_);
-        if (side_) cudaStreamDestroy(side_);
-        if (side2_) cudaStreamDestroy(side2_);
-        if (ev_fork_) cudaEventDestroy(ev_fork_);
-        if (ev_join_) cudaEventDestroy(ev_join_);
-        if (ev_join2_) cudaEventDestroy(ev_join2_);
+        for (Lanes* ln : {&lanes_, &cap_lanes_}) {
+            if (ln->side) cudaStreamDestroy(ln->side);
+            if (ln->side2) cudaStreamDestroy(ln->side2);
+            if (ln->fork) cudaEventDestroy(ln->fork);
+            if (ln->join) cudaEventDestroy(ln->join);
+            if (ln->join2) cudaEventDestroy(ln->join2);
+        }
+        if (cap_lanes_.main) cudaStreamDestroy(cap_lanes_.main);
         cudaStreamDestroy(stream_);
     }
     void open_device() {
         if (stream_) return;
         cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_check(cudaStreamCreateWithFlags(&side2_, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "event");
-        cuda_check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "event");
-        cuda_check(cudaEventCreateWithFlags(&ev_join2_, cudaEventDisableTiming), "event");
+        lanes_.main = stream_;
+        cuda_check(cudaStreamCreateWithFlags(&cap_lanes_.main, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (Lanes* ln : {&lanes_, &cap_lanes_}) {
+            cuda_check(cudaStreamCreateWithFlags(&ln->side, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaStreamCreateWithFlags(&ln->side2, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaEventCreateWithFlags(&ln->fork, cudaEventDisableTiming), "event");
+            cuda_check(cudaEventCreateWithFlags(&ln->join, cudaEventDisableTiming), "event");
+            cuda_check(cudaEventCreateWithFlags(&ln->join2, cudaEventDisableTiming), "event");
+        }
         cudaMemPool_t pool = device_pool(cfg_.device);
         arena_.set_stream(stream_, pool);
         desc_arena_.set_stream(stream_, pool);
@@ -335,9 +430,12 @@ public:
             // (threads) each cluster's fill set reads the graph and writes only its own set
             const bool numeric = !geo_ && cfg_.numeric_fill;
             std::vector<std::vector<FillCand>> cand(numeric ? fill.size() : 0);
-            host_parallel_for(fill.size(), [&](size_t b, size_t e) {
-                for (size_t i = b; i < e; ++i) get_sparsity(fill[i], numeric ? &cand[i] : nullptr);
-            });
+            host_parallel_for(
+                fill.size(),
+                [&](size_t b, size_t e) {
+                    for (size_t i = b; i < e; ++i) get_sparsity(fill[i], numeric ? &cand[i] : nullptr);
+                },
+                16);
             if (numeric) numeric_fill(fill, cand);
             const size_t nfill = fill.size();
             if (cfg_.verbose >= 3)
@@ -377,6 +475,7 @@ public:
         }
         rec(6, (long long)nnzA_, (long long)nnzR_, (long long)nnzH_, (long long)nnzQ_);
         const double tp0 = wall();
+        phase_ = 6;
         build_solve_plan();
         t_plan_ = wall() - tp0;
         int status = 0;
@@ -406,14 +505,22 @@ public:
         if (!factorized_) throw std::logic_error("solve before factorize");
         if (rect_) throw std::invalid_argument("least-squares factorization: use solve_nrml / cgls");
         double t0 = wall();
+        phase_ = 7;
         cuda_check(cudaMemcpyAsync(d_bin_, d_b, sizeof(double) * nrows_, cudaMemcpyDeviceToDevice, stream_), "solve in");
-        if (!graph_exec_) {
-            cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-            run_solve_sweeps();
-            cuda_check(cudaStreamEndCapture(stream_, &graph_), "capture end");
-            cuda_check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+        // Until the solve graph is ready the application launches its sweeps
+        // directly (the same kernels in the same order: the same result), so
+        // the device starts at once instead of waiting for the graph's capture
+        // and instantiation.
+        // The capture starts after the first application's launches are issued,
+        // so the two do not contend for the driver.
+        if (!graph_exec_ && cap_done_) finish_capture();
+        if (graph_exec_) {
+            timed(KF_SOLVE, 0, solve_bytes_,
+                  [&] { cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch"); });
+        } else {
+            timed(KF_SOLVE, 0, solve_bytes_, [&] { launches_solve_ = run_solve_sweeps(lanes_); });
+            if (!cap_thread_.joinable()) start_capture();
         }
-        timed(KF_SOLVE, 0, solve_bytes_, [&] { cuda_check(cudaGraphLaunch(graph_exec_, stream_), "graph launch"); });
         cuda_check(cudaMemcpyAsync(d_x, d_xout_, sizeof(double) * ncols_, cudaMemcpyDeviceToDevice, stream_),
                    "solve out");
         t_solve_ = wall() - t0;
@@ -484,9 +591,20 @@ public:
 private:
     Config cfg_;
     cudaStream_t stream_ = nullptr;
-    cudaStream_t side_ = nullptr;   // branches of a solve wave (forked from and joined to stream_):
-    cudaStream_t side2_ = nullptr;  // tall Q applications and large triangular ops
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_join2_ = nullptr;
+    // The streams a solve sweep launches on: the origin stream and two branches
+    // forked from and joined to it (tall Q applications, large triangular ops).
+    // lanes_ runs on stream_; cap_lanes_ is a second set on which a host thread
+    // captures the solve graph while stream_ runs the first applications.
+    struct Lanes {
+        cudaStream_t main = nullptr, side = nullptr, side2 = nullptr;
+        cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
+    };
+    Lanes lanes_, cap_lanes_;
+    std::thread cap_thread_;
+    std::atomic<bool> cap_done_{false};
+    std::exception_ptr cap_err_;
+    cudaGraph_t cap_graph_ = nullptr;
+    cudaGraphExec_t cap_exec_ = nullptr;
     Arena arena_;
     int* d_status_ = nullptr;  // device status word of the current factorization
     int status_ = 0;           // its value at the end of the factorization
@@ -557,28 +675,29 @@ private:
     // One sweep wave: the one-CTA ops, the tall Q applications and the large
     // triangular ops (independent ops: each cluster launch runs on a branch
     // forked from the stream).
-    int launch_wave(const Wave& w, T* xb) {
+    int launch_wave(const Wave& w, T* xb) { return launch_wave(w, xb, lanes_); }
+    int launch_wave(const Wave& w, T* xb, const Lanes& ln) {
         const bool fork = (w.nops > 0) + (w.nbig > 0) + (w.ntri > 0) > 1;
         if (fork) {
-            cuda_check(cudaEventRecord(ev_fork_, stream_), "fork");
-            if (w.nbig > 0) cuda_check(cudaStreamWaitEvent(side_, ev_fork_, 0), "fork");
-            if (w.ntri > 0) cuda_check(cudaStreamWaitEvent(side2_, ev_fork_, 0), "fork");
+            cuda_check(cudaEventRecord(ln.fork, ln.main), "fork");
+            if (w.nbig > 0) cuda_check(cudaStreamWaitEvent(ln.side, ln.fork, 0), "fork");
+            if (w.ntri > 0) cuda_check(cudaStreamWaitEvent(ln.side2, ln.fork, 0), "fork");
         }
         if (w.nbig > 0)
-            cuda_check(launch_applyq_cl<T>(w.big, w.nbig, w.bcl, d_segs_, xb, fork ? side_ : stream_),
+            cuda_check(launch_applyq_cl<T>(w.big, w.nbig, w.bcl, d_segs_, xb, fork ? ln.side : ln.main),
                        "solve cluster launch");
         if (w.ntri > 0)
-            cuda_check(launch_tri_cl<T>(w.tri, w.ntri, w.tcl, w.tk, d_gemv_, xb, fork ? side2_ : stream_),
+            cuda_check(launch_tri_cl<T>(w.tri, w.ntri, w.tcl, w.tk, d_gemv_, xb, fork ? ln.side2 : ln.main),
                        "solve cluster launch");
-        if (w.nops > 0) launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, stream_);
+        if (w.nops > 0) launch_solve_step<T>(w.ops, w.nops, d_segs_, d_gemv_, nullptr, xb, w.smem, ln.main);
         if (fork) {
             if (w.nbig > 0) {
-                cuda_check(cudaEventRecord(ev_join_, side_), "join");
-                cuda_check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+                cuda_check(cudaEventRecord(ln.join, ln.side), "join");
+                cuda_check(cudaStreamWaitEvent(ln.main, ln.join, 0), "join");
             }
             if (w.ntri > 0) {
-                cuda_check(cudaEventRecord(ev_join2_, side2_), "join");
-                cuda_check(cudaStreamWaitEvent(stream_, ev_join2_, 0), "join");
+                cuda_check(cudaEventRecord(ln.join2, ln.side2), "join");
+                cuda_check(cudaStreamWaitEvent(ln.main, ln.join2, 0), "join");
             }
         }
         return (w.nops > 0) + (w.nbig > 0) + (w.ntri > 0);
@@ -606,8 +725,8 @@ private:
         std::string tag;
         int level, phase;
     };
-    int phase_ = 0;  // factorization phase of the launches being issued (profiling trace)
-    bool prof_ = false;
+    int phase_ = 0;  // phase of the launches being issued (profiling trace): 0-5 level phases, 6 solve plan, 7 solve
+    bool prof_ = false, timeline_ = false;
     std::vector<Pending> pend_;
     std::string tag_;  // launch shape printed beside its time (profiling with verbose >= 4)
     bool tracing() const { return prof_ && cfg_.verbose >= 4; }
@@ -641,6 +760,13 @@ private:
             fam_[p.fam].bytes += p.bytes;
             if (prof_ && cfg_.verbose >= 4)
                 std::fprintf(stderr, "    trace %d %.4f ms L%d P%d %s\n", p.fam, ms, p.level, p.phase, p.tag.c_str());
+            if (timeline_) {
+                float st = 0;
+                cudaEventElapsedTime(&st, pend_.front().a, p.a);
+                std::fprintf(stderr, "timeline %d %.4f %.4f L%d P%d\n", p.fam, st, ms, p.level, p.phase);
+            }
+        }
+        for (auto& p : pend_) {
             cudaEventDestroy(p.a);
             cudaEventDestroy(p.b);
         }
@@ -648,7 +774,10 @@ private:
     }
 
 public:
-    void set_profile(bool on) override { prof_ = on; }
+    void set_profile(int level) override {
+        prof_ = level > 0;
+        timeline_ = level > 1;
+    }
     double* krylov_workspace(size_t elems) override {
         open_device();
         return static_cast<double*>(scratch_.get(std::max<size_t>(elems, 1) * sizeof(double), stream_));
@@ -711,22 +840,16 @@ private:
             fn(size_t(0), n);
             return;
         }
-        std::vector<std::thread> th;
         std::vector<std::exception_ptr> err(nt);
-        for (size_t t = 1; t < nt; ++t)
-            th.emplace_back([&, t] {
-                try {
-                    fn(n * t / nt, n * (t + 1) / nt);
-                } catch (...) {
-                    err[t] = std::current_exception();
-                }
-            });
-        try {
-            fn(size_t(0), n / nt);
-        } catch (...) {
-            err[0] = std::current_exception();
-        }
-        for (auto& x : th) x.join();
+        const std::function<void(size_t)> body = [&](size_t t) {
+            try {
+                fn(n * t / nt, n * (t + 1) / nt);
+            } catch (...) {
+                err[t] = std::current_exception();
+            }
+        };
+        if (!HostPool::get().run(nt, body))
+            for (size_t t = 0; t < nt; ++t) body(t);
         for (auto& e : err)
             if (e) std::rethrow_exception(e);
     }
@@ -1226,49 +1349,146 @@ private:
                     }
                 }
             },
-            64);
+            16);
         const double ts1 = wall();
         double ts2 = ts1, ts3 = ts1;
         const size_t nedges0 = edges_.size();
         std::vector<Task> tasks;
         if (!coupled) {
-        // 2. (this thread, level order) arena memory of every job and the missing
-        //    fill blocks, created in the order of a task-by-task elimination; a
-        //    block an earlier task of this phase created is among n's out edges
-        //    past out_mark (a few per cluster)
-        for (const Plan& P : plans)
-            for (Cluster* n : P.upd) n->out_mark = (int)n->out.size();
+        // 2. arena memory of every job and the missing fill blocks, the same
+        //    blocks, uids, edges and list orders as a task-by-task elimination
+        //    (a block is made by the first task that misses it, in level order,
+        //    and found by the later ones):
+        //    a. (threads) each task's missing (updated cluster n, row cluster r)
+        //       slots in (u, h) order, at its prefix-sum position
+        const std::vector<Cluster*>& all_c = cur();
+        for (size_t q = 0; q < all_c.size(); ++q) all_c[q]->pos = (int)q;
+        struct Miss {
+            int task, slot, n, r;  // n, r: positions in cur()
+        };
+        std::vector<size_t> mbase(nl + 1, 0);
+        host_parallel_for(
+            nl,
+            [&](size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i)
+                    mbase[i + 1] = (size_t)std::count(plans[i].blk.begin(), plans[i].blk.end(), nullptr);
+            },
+            64);
+        for (size_t i = 0; i < nl; ++i) mbase[i + 1] += mbase[i];
+        const size_t nm = mbase[nl];
+        std::vector<Miss> miss(nm);
+        host_parallel_for(
+            nl,
+            [&](size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i) {
+                    const Plan& P = plans[i];
+                    const size_t nh = P.H.size();
+                    size_t q = mbase[i];
+                    for (size_t s = 0; s < P.blk.size(); ++s)
+                        if (!P.blk[s]) miss[q++] = Miss{(int)i, (int)s, P.upd[s / nh]->pos, P.H[s % nh]->n2->pos};
+                }
+            },
+            64);
+        //    b. the slots of each n in that order; (threads) per n, the first
+        //       slot of each r makes the block (creator[m] == m), the rest use it
+        const size_t ncl = all_c.size();
+        std::vector<size_t> nb0(ncl + 1, 0);
+        for (const Miss& m : miss) ++nb0[m.n + 1];
+        for (size_t q = 0; q < ncl; ++q) nb0[q + 1] += nb0[q];
+        std::vector<int> byn(nm), creator(nm);
+        {
+            std::vector<size_t> cur_n(nb0.begin(), nb0.end() - 1);
+            for (size_t m = 0; m < nm; ++m) byn[cur_n[miss[m].n]++] = (int)m;
+        }
+        host_parallel_for(
+            ncl,
+            [&](size_t b, size_t e) {
+                std::vector<std::pair<int, int>> rs;
+                for (size_t q = b; q < e; ++q) {
+                    if (nb0[q] == nb0[q + 1]) continue;
+                    rs.clear();
+                    for (size_t x = nb0[q]; x < nb0[q + 1]; ++x) rs.emplace_back(miss[byn[x]].r, byn[x]);
+                    std::sort(rs.begin(), rs.end());
+                    for (size_t x = 0; x < rs.size(); ++x)
+                        creator[rs[x].second] = (x && rs[x].first == rs[x - 1].first) ? creator[rs[x - 1].second]
+                                                                                       : rs[x].second;
+                }
+            },
+            256);
+        //    c. (level order) job memory, then the task's new blocks: uids and
+        //       arena addresses in creation order
         std::vector<Task> all(nl);
+        std::vector<int> rank(nm, -1);
+        std::vector<T*> bptr;
+        bptr.reserve(nm);
+        const size_t e0 = edges_.size();
+        const int uid0 = next_uid_;
         for (size_t i = 0; i < nl; ++i) {
             Cluster* c = lv[i];
-            Plan& P = plans[i];
-            if (c->csize == 0) {
-                c->elim = true;
-                continue;
-            }
+            const Plan& P = plans[i];
+            if (c->csize == 0) continue;
             QRJob& j = all[i].job;
             j.m = P.m;
             j.k = P.k;
             j.fac = arena_.alloc_n<T>((size_t)P.m * P.k);
             j.tau = arena_.alloc_n<T>(P.k);
             j.tp = arena_.alloc_n<T>((size_t)npanels(P.k) * kNB * kNB);
-            const size_t nh = P.H.size();
-            for (size_t u = 0; u < P.upd.size(); ++u) {
-                Cluster* n = P.upd[u];
-                for (size_t h = 0; h < nh; ++h) {
-                    Edge*& b = P.blk[u * nh + h];
-                    if (b) continue;
-                    Cluster* r = P.H[h]->n2;
-                    for (size_t q = n->out_mark; q < n->out.size(); ++q)
-                        if (n->out[q]->n2 == r) {
-                            b = n->out[q];
-                            break;
-                        }
-                    if (!b) b = add_edge(n, r);
+            for (size_t m = mbase[i]; m < mbase[i + 1]; ++m)
+                if (creator[m] == (int)m) {
+                    rank[m] = (int)bptr.size();
+                    bptr.push_back(arena_.alloc_n<T>(block_elems(all_c[miss[m].r]->rsize, all_c[miss[m].n]->csize)));
                 }
-            }
-            c->elim = true;
         }
+        const size_t nnew = bptr.size();
+        if (nnew > size_t(std::numeric_limits<int>::max() - next_uid_))
+            throw std::runtime_error("elimination: block uid overflow");
+        next_uid_ += (int)nnew;
+        edges_.resize(e0 + nnew);
+        std::vector<int> cr(nnew);  // the new block's row cluster (position in cur()), -1 on the diagonal
+        //    d. (threads) the new edges, each n's out list and the tasks' slots;
+        //       then each r's in list, in creation order
+        host_parallel_for(
+            ncl,
+            [&](size_t b, size_t e) {
+                for (size_t q = b; q < e; ++q) {
+                    Cluster* n = all_c[q];
+                    for (size_t x = nb0[q]; x < nb0[q + 1]; ++x) {
+                        const int m = byn[x];
+                        if (creator[m] != m) continue;
+                        Cluster* r = all_c[miss[m].r];
+                        Blk bk;
+                        bk.rows = r->rsize;
+                        bk.cols = n->csize;
+                        bk.ld = std::max(bk.rows, 1);
+                        bk.p = bptr[rank[m]];
+                        bk.uid = uid0 + rank[m];
+                        Edge& ed = edges_[e0 + rank[m]];
+                        ed = Edge{n, r, bk, true};
+                        n->out.push_back(&ed);
+                        cr[rank[m]] = r == n ? -1 : miss[m].r;
+                    }
+                    for (size_t x = nb0[q]; x < nb0[q + 1]; ++x) {
+                        const int m = byn[x];
+                        plans[miss[m].task].blk[miss[m].slot] = &edges_[e0 + rank[creator[m]]];
+                    }
+                }
+            },
+            256);
+        {
+            const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+            const size_t nth = std::max<size_t>(1, std::min<size_t>({hw, 8, nnew / 4096}));
+            host_parallel_for(
+                nth,
+                [&](size_t b, size_t e) {
+                    for (size_t k = b; k < e; ++k) {  // row clusters [ncl k / nth, ncl (k + 1) / nth)
+                        const int lo = (int)(ncl * k / nth), hi = (int)(ncl * (k + 1) / nth);
+                        for (size_t x = 0; x < nnew; ++x)
+                            if (cr[x] >= lo && cr[x] < hi) all_c[cr[x]]->in.push_back(&edges_[e0 + x]);
+                    }
+                },
+                1);
+        }
+        for (size_t i = 0; i < nl; ++i) lv[i]->elim = true;
         ts2 = wall();
         // 3. (threads) each job's copy descriptors and block uids
         host_parallel_for(
@@ -1310,8 +1530,32 @@ private:
             },
             64);
         ts3 = wall();
-        // 4. (this thread, level order) the tape, counters, log and, for least
-        //    squares, the column blocks a finished elimination drops
+        // 4. (threads) each task's tape op; then (this thread, level order) the
+        //    tape, counters, log and, for least squares, the column blocks a
+        //    finished elimination drops
+        std::vector<TapeOp> qops(nl);
+        host_parallel_for(
+            nl,
+            [&](size_t b, size_t e) {
+                for (size_t i = b; i < e; ++i) {
+                    Cluster* c = lv[i];
+                    const Plan& P = plans[i];
+                    if (c->csize == 0) continue;
+                    TapeOp& op = qops[i];
+                    op.kind = TK_QR;
+                    op.c = c;
+                    op.fac = all[i].job.fac;
+                    op.tp = all[i].job.tp;
+                    op.m = P.m;
+                    op.k = P.k;
+                    op.ld = P.m;
+                    op.segs.reserve(P.H.size());
+                    for (Edge* ed : P.H) op.segs.emplace_back(ed->n2, ed->n2->rsize);
+                    op.a12.reserve(c->in.size());
+                    for (Edge* ed : c->in) op.a12.push_back(A12{ed->A.p, ed->A.ld, ed->A.cols, ed->n1});
+                }
+            },
+            64);
         for (size_t i = 0; i < nl; ++i) {
             Cluster* c = lv[i];
             Plan& P = plans[i];
@@ -1326,17 +1570,7 @@ private:
                 co += n->csize;
             }
             nnzH_ += (unsigned long long)(m * k);
-            TapeOp op;
-            op.kind = TK_QR;
-            op.c = c;
-            op.fac = all[i].job.fac;
-            op.tp = all[i].job.tp;
-            op.m = m;
-            op.k = k;
-            op.ld = m;
-            for (Edge* ed : P.H) op.segs.emplace_back(ed->n2, ed->n2->rsize);
-            for (Edge* ed : c->in) op.a12.push_back(A12{ed->A.p, ed->A.ld, ed->A.cols, ed->n1});
-            tape_.push_back(std::move(op));
+            tape_.push_back(std::move(qops[i]));
             if (rect_) {  // least squares keeps R only: the self block shrinks to k rows, the rest goes
                 for (Edge* ed : c->out) {
                     if (ed->n2 == c)
@@ -2965,6 +3199,9 @@ private:
                 case TK_QR: {
                     f.op = SolveOp{SK_APPLYQ, 0, t.m, t.k, t.ld, 0, 0, 0, ptr(t.fac), ptr(t.tp), 0,
                                    (int)seg_off[i], (int)t.segs.size()};
+                    f.rd.reserve(t.segs.size());
+                    f.wr.reserve(t.segs.size());
+                    b.rd.reserve(t.a12.size() + 1);
                     for (auto& s : t.segs) {
                         segs[sq++] = XSeg{s.first->xoff, s.second, 0};
                         f.rd.push_back(s.first);
@@ -3502,7 +3739,10 @@ private:
     }
 
 public:
-    bool solve_ready() const override { return graph_exec_ != nullptr; }
+    bool solve_ready() override {
+        finish_capture();
+        return graph_exec_ != nullptr;
+    }
 
     std::vector<double> profile_solve_waves() override {
         if (!factorized_) throw std::logic_error("profile before factorize");
@@ -3606,14 +3846,49 @@ public:
     }
 
 private:
-    void run_solve_sweeps() {
-        launches_solve_ = 0;
-        launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, stream_);
-        ++launches_solve_;
-        for (auto& w : fwd_waves_) launches_solve_ += launch_wave(w, xbuf_);
-        for (auto& w : bwd_waves_) launches_solve_ += launch_wave(w, xbuf_);
-        launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, stream_);
-        ++launches_solve_;
+    // One application's launches on ln; returns how many kernels it launched.
+    int run_solve_sweeps(const Lanes& ln) {
+        int n = 0;
+        launch_gather_in<T>(d_bin_, d_src_, d_xin_, xbuf_, nin_, ln.main);
+        ++n;
+        for (auto& w : fwd_waves_) n += launch_wave(w, xbuf_, ln);
+        for (auto& w : bwd_waves_) n += launch_wave(w, xbuf_, ln);
+        launch_scatter_out<T>(xbuf_, d_xout_pos_, d_dst_, d_xout_, nout_, ln.main);
+        return n + 1;
+    }
+    // The solve graph: captured from the same launches on cap_lanes_ by a host
+    // thread (capture records, it does not run) and instantiated there, while
+    // the first applications run their launches directly on stream_.
+    void start_capture() {
+        cap_done_ = false;
+        cap_err_ = nullptr;
+        cap_thread_ = std::thread([this] {
+            try {
+                cuda_check(cudaSetDevice(cfg_.device), "cudaSetDevice");
+                cuda_check(cudaStreamBeginCapture(cap_lanes_.main, cudaStreamCaptureModeThreadLocal), "capture");
+                run_solve_sweeps(cap_lanes_);
+                cuda_check(cudaStreamEndCapture(cap_lanes_.main, &cap_graph_), "capture end");
+                cuda_check(cudaGraphInstantiate(&cap_exec_, cap_graph_, 0), "graph instantiate");
+            } catch (...) {
+                cap_err_ = std::current_exception();
+            }
+            cap_done_ = true;
+        });
+    }
+    // Waits for a capture in flight and adopts its graph (a capture error is
+    // rethrown here).
+    void finish_capture() {
+        if (!cap_thread_.joinable()) return;
+        cap_thread_.join();
+        graph_ = cap_graph_;
+        graph_exec_ = cap_exec_;
+        cap_graph_ = nullptr;
+        cap_exec_ = nullptr;
+        if (cap_err_) {
+            std::exception_ptr e = cap_err_;
+            cap_err_ = nullptr;
+            std::rethrow_exception(e);
+        }
     }
     // M^T = G_in^T (sweeps)^T S_out^T: start from zero, place g where the solve
     // reads x out, run the transposed waves, read y where the solve puts b in.

@@ -66,7 +66,7 @@ struct KernelStat {
 class EngineBase {
 public:
     virtual ~EngineBase() = default;
-    virtual void set_profile(bool on) = 0;
+    virtual void set_profile(int level) = 0;  // 0 off, 1 per-family timing, 2 plus a launch timeline
     virtual KernelStat kernel_stat(int family) = 0;
     virtual void reset_kernel_stats() = 0;
     virtual void partition(const Csc& A) = 0;
@@ -100,7 +100,7 @@ public:
     virtual std::vector<double> profile_solve_waves() = 0;
     // True once the preconditioner's solve graph exists (built by the first
     // application); from then on an application allocates nothing.
-    virtual bool solve_ready() const = 0;
+    virtual bool solve_ready() = 0;  // the solve graph exists (waits for a capture in flight)
     // Device workspace of at least `elems` doubles on the handle's stream for a
     // Krylov solve (the factorization's scratch buffer, idle between
     // factorizations): valid until the next call or factorization.
