@@ -15,11 +15,11 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
-#include <deque>
 #include <exception>
 #include <functional>
 #include <limits>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <pthread.h>
@@ -34,6 +34,30 @@ double wall() {
 }
 
 inline int npanels(int k) { return (k + kNB - 1) / kNB; }
+
+// Grow-only storage with stable element addresses, in chunks of 4096 elements
+// (a std::deque allocates one small block per few elements, which made the
+// 189k fill blocks of a level cost a malloc each ten).
+template <class E>
+class ChunkedStore {
+public:
+    static constexpr size_t kChunk = 4096;
+    size_t size() const { return n_; }
+    E& operator[](size_t i) { return chunks_[i / kChunk][i % kChunk]; }
+    E& back() { return (*this)[n_ - 1]; }
+    void push_back(const E& e) {
+        resize(n_ + 1);
+        back() = e;
+    }
+    void resize(size_t n) {  // grows only
+        while (chunks_.size() * kChunk < n) chunks_.emplace_back(new E[kChunk]);
+        n_ = std::max(n_, n);
+    }
+
+private:
+    std::vector<std::unique_ptr<E[]>> chunks_;
+    size_t n_ = 0;
+};
 
 // Host worker threads for the engine's parallel passes, started once per
 // process (a factorization makes hundreds of short passes, and starting
@@ -507,12 +531,10 @@ public:
         double t0 = wall();
         phase_ = 7;
         cuda_check(cudaMemcpyAsync(d_bin_, d_b, sizeof(double) * nrows_, cudaMemcpyDeviceToDevice, stream_), "solve in");
-        // Until the solve graph is ready the application launches its sweeps
-        // directly (the same kernels in the same order: the same result), so
-        // the device starts at once instead of waiting for the graph's capture
-        // and instantiation.
-        // The capture starts after the first application's launches are issued,
-        // so the two do not contend for the driver.
+        // Until the solve graph is ready an application launches its sweeps
+        // directly (the same kernels in the same order as the graph: the same
+        // result), so the device does not wait for the graph; a host thread
+        // captures it after the first application's launches are issued.
         if (!graph_exec_ && cap_done_) finish_capture();
         if (graph_exec_) {
             timed(KF_SOLVE, 0, solve_bytes_,
@@ -615,7 +637,7 @@ private:
     double t_phase_[6] = {0, 0, 0, 0, 0, 0};  // host time per phase: fill, elim, shift, scale, sparsify, merge
     std::vector<std::vector<Cluster*>> bottoms_, fine_;
     std::vector<std::unique_ptr<Cluster>> clusters_;
-    std::deque<Edge> edges_;  // stable addresses
+    ChunkedStore<Edge> edges_;
     std::vector<TapeOp> tape_;
     std::vector<int> cperm_, rperm_;
     bool rect_ = false;  // least squares (no identity row matching): rows move, R^T R solves
@@ -725,6 +747,7 @@ private:
         std::string tag;
         int level, phase;
     };
+    double tg_[5] = {0, 0, 0, 0, 0};  // elimination build: host time of the fill-block steps (verbose 3)
     int phase_ = 0;  // phase of the launches being issued (profiling trace): 0-5 level phases, 6 solve plan, 7 solve
     bool prof_ = false, timeline_ = false;
     std::vector<Pending> pend_;
@@ -1389,6 +1412,7 @@ private:
                 }
             },
             64);
+        const double tg1 = wall();
         //    b. the slots of each n in that order; (threads) per n, the first
         //       slot of each r makes the block (creator[m] == m), the rest use it
         const size_t ncl = all_c.size();
@@ -1415,6 +1439,7 @@ private:
                 }
             },
             256);
+        const double tg2 = wall();
         //    c. (level order) job memory, then the task's new blocks: uids and
         //       arena addresses in creation order
         std::vector<Task> all(nl);
@@ -1443,6 +1468,7 @@ private:
         if (nnew > size_t(std::numeric_limits<int>::max() - next_uid_))
             throw std::runtime_error("elimination: block uid overflow");
         next_uid_ += (int)nnew;
+        const double tg3 = wall();
         edges_.resize(e0 + nnew);
         std::vector<int> cr(nnew);  // the new block's row cluster (position in cur()), -1 on the diagonal
         //    d. (threads) the new edges, each n's out list and the tasks' slots;
@@ -1474,6 +1500,7 @@ private:
                 }
             },
             256);
+        const double tg4 = wall();
         {
             const size_t hw = std::max(1u, std::thread::hardware_concurrency());
             const size_t nth = std::max<size_t>(1, std::min<size_t>({hw, 8, nnew / 4096}));
@@ -1490,6 +1517,11 @@ private:
         }
         for (size_t i = 0; i < nl; ++i) lv[i]->elim = true;
         ts2 = wall();
+        tg_[0] = tg1 - ts1;
+        tg_[1] = tg2 - tg1;
+        tg_[2] = tg3 - tg2;
+        tg_[3] = tg4 - tg3;
+        tg_[4] = ts2 - tg4;
         // 3. (threads) each job's copy descriptors and block uids
         host_parallel_for(
             nl,
@@ -1674,11 +1706,12 @@ private:
         print_waves("elim", wave, nw);
         if (cfg_.verbose >= 3)
             std::fprintf(stderr,
-                         "[lvl %d] elim host: tasks %.2f ms%s (plans %.2f, graph %.2f with %zu fill blocks, "
+                         "[lvl %d] elim host: tasks %.2f ms%s (plans %.2f, graph %.2f with %zu fill blocks "
+                         "[slots %.2f, first makers %.2f, memory %.2f, edges %.2f, in lists %.2f], "
                          "descriptors %.2f, tape %.2f), waves %.2f ms\n",
                          ilvl_, (te1 - te0) * 1e3, coupled ? " (coupled: serial build)" : "", (ts1 - te0) * 1e3,
-                         (ts2 - ts1) * 1e3, edges_.size() - nedges0, (ts3 - ts2) * 1e3, (te1 - ts3) * 1e3,
-                         (wall() - te1) * 1e3);
+                         (ts2 - ts1) * 1e3, edges_.size() - nedges0, tg_[0] * 1e3, tg_[1] * 1e3, tg_[2] * 1e3,
+                         tg_[3] * 1e3, tg_[4] * 1e3, (ts3 - ts2) * 1e3, (te1 - ts3) * 1e3, (wall() - te1) * 1e3);
         // every wave's descriptors first (host threads, one scratch sized for the
         // largest wave), then the uploads and launches in wave order
         std::vector<std::vector<QRJob>> wjobs(nw);
@@ -1690,15 +1723,53 @@ private:
         std::vector<WaveBuild> builds(nw);
         const std::vector<TrsmTask<T>> no_trsm;
         const std::vector<CopyDesc<T>> no_post;
-        host_parallel_for(
-            (size_t)nw,
-            [&](size_t b, size_t e) {
-                for (size_t w = b; w < e; ++w) build_wave(wjobs[w], no_trsm, trbase, d_status_, builds[w]);
-            },
-            4);
+        // The wave builds (pure functions of their jobs) run on host threads,
+        // wave w on lane w mod lanes so that they finish about in wave order,
+        // while this thread uploads and launches each wave as soon as it is
+        // built, in wave order: the device starts on the first wave instead of
+        // waiting for the last build.
+        const size_t lanes = std::min<size_t>(std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 8),
+                                              (size_t)nw);
+        std::unique_ptr<std::atomic<bool>[]> ready(new std::atomic<bool>[nw]);
+        for (int w = 0; w < nw; ++w) ready[w] = false;
+        std::atomic<bool> failed{false};
+        std::exception_ptr berr;
+        std::thread producer([&] {
+            try {
+                host_parallel_for(
+                    lanes,
+                    [&](size_t b, size_t e) {
+                        for (size_t l = b; l < e; ++l)
+                            for (size_t w = l; w < (size_t)nw && !failed; w += lanes) {
+                                build_wave(wjobs[w], no_trsm, trbase, d_status_, builds[w]);
+                                ready[w].store(true, std::memory_order_release);
+                            }
+                    },
+                    1);
+            } catch (...) {
+                berr = std::current_exception();
+                failed = true;
+            }
+        });
+        try {
+            for (int w = 0; w < nw; ++w) {
+                while (!ready[w].load(std::memory_order_acquire)) {
+                    if (failed) break;
+                    std::this_thread::yield();
+                }
+                if (failed) break;
+                issue_wave(builds[w], no_trsm, no_post, wall());
+            }
+        } catch (...) {
+            failed = true;
+            producer.join();
+            throw;
+        }
+        producer.join();
+        if (berr) std::rethrow_exception(berr);
         if (cfg_.verbose >= 3)
-            std::fprintf(stderr, "[lvl %d] elim host: %d wave builds %.2f ms\n", ilvl_, nw, (wall() - tw0) * 1e3);
-        for (int w = 0; w < nw; ++w) issue_wave(builds[w], no_trsm, no_post, wall());
+            std::fprintf(stderr, "[lvl %d] elim host: %d wave builds and launches %.2f ms\n", ilvl_, nw,
+                         (wall() - tw0) * 1e3);
     }
 
     // ------------------------------------------------------------- scaling (src/tree.cpp:533-580)
@@ -3160,6 +3231,10 @@ private:
         d_adj_out_ = arena_.alloc_n<double>(nrows_);
         std::vector<int> src, dst;
         std::vector<int64_t> xin, xo;
+        src.reserve(nrows_);
+        xin.reserve(nrows_);
+        dst.reserve(ncols_);
+        xo.reserve(ncols_);
         for (Cluster* c : bottoms_[0]) {
             for (int i = 0; i < c->rsize_org; ++i) {
                 src.push_back(rperm_[c->rstart + i]);
@@ -3857,8 +3932,8 @@ private:
         return n + 1;
     }
     // The solve graph: captured from the same launches on cap_lanes_ by a host
-    // thread (capture records, it does not run) and instantiated there, while
-    // the first applications run their launches directly on stream_.
+    // thread (capture records, it does not run), instantiated and uploaded
+    // there, while the first applications run their launches on stream_.
     void start_capture() {
         cap_done_ = false;
         cap_err_ = nullptr;
@@ -3869,8 +3944,17 @@ private:
                 run_solve_sweeps(cap_lanes_);
                 cuda_check(cudaStreamEndCapture(cap_lanes_.main, &cap_graph_), "capture end");
                 cuda_check(cudaGraphInstantiate(&cap_exec_, cap_graph_, 0), "graph instantiate");
+                // placed on the device here, not by its first launch
+                cuda_check(cudaGraphUpload(cap_exec_, cap_lanes_.main), "graph upload");
+                cuda_check(cudaStreamSynchronize(cap_lanes_.main), "graph upload");
             } catch (...) {
                 cap_err_ = std::current_exception();
+                cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+                if (cudaStreamIsCapturing(cap_lanes_.main, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(cap_lanes_.main, &g);
+                    if (g) cudaGraphDestroy(g);
+                }
             }
             cap_done_ = true;
         });

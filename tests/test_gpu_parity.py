@@ -160,3 +160,42 @@ def test_device_buffers_loaded(gpu):
     assert "libspaqr_b200.so" in maps
     assert os.path.exists(os.path.join(os.path.dirname(os.path.dirname(__file__)), "spaqr_public_b200", "_build",
                                        "libspaqr_b200.so"))
+
+
+def test_direct_and_graph_applications_agree(gpu):
+    """The first applications launch the sweep kernels directly while a host
+    thread captures the solve graph; the later ones replay the graph. The same
+    kernels run in the same order, so every application gives the same bits."""
+    w, A, t, _ = build("advdiff3d_16")
+    xs = [t.solve(w["b"]) for _ in range(6)]
+    for x in xs[1:]:
+        assert np.array_equal(xs[0], x)
+
+
+def test_launch_timeline_profile(gpu, capfd):
+    """Profile level 2 prints one timeline line per timed launch (family, start,
+    duration, level, phase) when the counters are read."""
+    import ctypes as C
+    from spaqr_public_b200._abi import check, lib
+    w = matgen.workload("advdiff2d_32")
+    A = matgen.column_normalize(w["A"])
+    t = Tree(w["levels"], w["skip"], precision=FP64)
+    t.set_tol(w["tol"])
+    t.set_scale(1)
+    t.set_square(1)
+    t.set_coords_grid(w["n"], w["d"])
+    t.partition(A)
+    check(lib().spq_set_profile(t._h, 2))
+    t.assemble(A)
+    t.factorize()
+    t.solve(w["b"])
+    out = np.zeros(4)
+    check(lib().spq_get_kernel_stats(t._h, 0, out.ctypes.data_as(C.POINTER(C.c_double))))
+    lines = [ln.split() for ln in capfd.readouterr().err.splitlines() if ln.startswith("timeline ")]
+    assert len(lines) > 10
+    phases = set()
+    for _, fam, st, du, lv, ph in lines:
+        assert 0 <= int(fam) < 8 and float(st) >= 0 and float(du) > 0
+        assert lv.startswith("L") and ph.startswith("P")
+        phases.add(int(ph[1:]))
+    assert 1 in phases and 7 in phases  # elimination launches and the solve
