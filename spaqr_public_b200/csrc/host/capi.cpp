@@ -61,7 +61,25 @@ int guard_on(spq_tree* t, F&& f) {
         cudaError_t e = cudaSetDevice(t->cfg.device);
         if (e != cudaSuccess) return fail(SPQ_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     }
-    return guard(std::forward<F>(f));
+    const int rc = guard(std::forward<F>(f));
+    // The first preconditioner application leaves a host thread capturing the
+    // solve graph (it overlaps the applications that follow inside the call).
+    // The capture ends before control returns: while a stream is capturing, a
+    // caller's cudaDeviceSynchronize (torch.cuda.synchronize) fails with
+    // cudaErrorStreamCaptureUnsupported. An error of the call is kept.
+    if (t && t->eng) {
+        const std::string err = g_err;
+        const int rs = guard([&] {
+            t->eng->solve_ready();
+            return SPQ_OK;
+        });
+        if (rc != SPQ_OK) {
+            g_err = err;
+            return rc;
+        }
+        return rs;
+    }
+    return rc;
 }
 
 int check_csc(int m, int n, const int* cp, const int* ri, const double* va, bool need_values = true) {

@@ -240,6 +240,11 @@ public:
             if (ln->join2) cudaEventDestroy(ln->join2);
         }
         if (cap_lanes_.main) cudaStreamDestroy(cap_lanes_.main);
+        for (int i = 0; i < kRqSide; ++i) {
+            if (rq_side_[i]) cudaStreamDestroy(rq_side_[i]);
+            if (rq_join_[i]) cudaEventDestroy(rq_join_[i]);
+        }
+        if (rq_fork_) cudaEventDestroy(rq_fork_);
         cudaStreamDestroy(stream_);
     }
     void open_device() {
@@ -254,6 +259,11 @@ public:
             cuda_check(cudaEventCreateWithFlags(&ln->fork, cudaEventDisableTiming), "event");
             cuda_check(cudaEventCreateWithFlags(&ln->join, cudaEventDisableTiming), "event");
             cuda_check(cudaEventCreateWithFlags(&ln->join2, cudaEventDisableTiming), "event");
+        }
+        cuda_check(cudaEventCreateWithFlags(&rq_fork_, cudaEventDisableTiming), "event");
+        for (int i = 0; i < kRqSide; ++i) {
+            cuda_check(cudaStreamCreateWithFlags(&rq_side_[i], cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaEventCreateWithFlags(&rq_join_[i], cudaEventDisableTiming), "event");
         }
         cudaMemPool_t pool = device_pool(cfg_.device);
         arena_.set_stream(stream_, pool);
@@ -622,6 +632,12 @@ private:
         cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     };
     Lanes lanes_, cap_lanes_;
+    // Branch streams of a sparsification wave's RRQR: the launches of one wave
+    // (one per cluster size) are independent interfaces and run side by side,
+    // forked from stream_ and joined to it before the rank readback.
+    static constexpr int kRqSide = 3;
+    cudaStream_t rq_side_[kRqSide] = {};
+    cudaEvent_t rq_fork_ = nullptr, rq_join_[kRqSide] = {};
     std::thread cap_thread_;
     std::atomic<bool> cap_done_{false};
     std::exception_ptr cap_err_;
@@ -2401,7 +2417,31 @@ private:
         };
         std::vector<Tuned> tuned;
         std::vector<size_t> rqs;
-        for (auto& kv : groups) {
+        // The groups are disjoint sets of interfaces. Without per-launch
+        // profiling they run side by side, stream_ and the branch streams taking
+        // them in turn, the group with the most work first (its clusters are
+        // placed while the SMs are still free); with profiling one after another
+        // on stream_ in map order, so that each launch's events time it alone.
+        // Neither the order nor the stream changes a result.
+        std::vector<decltype(&*groups.begin())> order;
+        for (auto& kv : groups) order.push_back(&kv);
+        const bool conc = !prof_ && order.size() > 1;
+        const int nside = conc ? std::min<int>(kRqSide, (int)order.size() - 1) : 0;
+        if (conc) {
+            auto work = [&](const std::vector<int>& qs) {
+                double w = 0;
+                for (int q : qs) w += (double)jobs[q].m * jobs[q].n * std::min(jobs[q].m, jobs[q].n);
+                return w;
+            };
+            std::stable_sort(order.begin(), order.end(),
+                             [&](const auto* a, const auto* b) { return work(a->second) > work(b->second); });
+            cuda_check(cudaEventRecord(rq_fork_, stream_), "fork");
+            for (int i = 0; i < nside; ++i) cuda_check(cudaStreamWaitEvent(rq_side_[i], rq_fork_, 0), "fork");
+        }
+        for (size_t gi = 0; gi < order.size(); ++gi) {
+            auto& kv = *order[gi];
+            const int lane_of = conc ? (int)(gi % (size_t)(nside + 1)) : 0;
+            cudaStream_t ls = lane_of == 0 ? stream_ : rq_side_[lane_of - 1];
             int maxm = 0, maxn = 0;
             for (int q : kv.second) {
                 maxm = std::max(maxm, jobs[q].m);
@@ -2429,36 +2469,40 @@ private:
                 if (tuning) {
                     cuda_check(cudaEventCreate(&ea), "event");
                     cuda_check(cudaEventCreate(&eb), "event");
-                    cudaEventRecord(ea, stream_);
+                    cudaEventRecord(ea, ls);
                 }
                 if (tracing())
                     tag_ = "rrqr_blk n " + std::to_string(nt) + " cl " + std::to_string(cl) + " m " +
                            std::to_string(maxm) + " k " + std::to_string(maxn);
                 rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
-                    cudaError_t e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                    cudaError_t e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, ls);
                     while (e != cudaSuccess && cl > 1 && rrqr_blk_fits<T>(maxm, maxn, cl / 2)) {
                         cudaGetLastError();  // a cluster this large did not launch here: halve it
                         cl /= 2;
-                        e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                        e = launch_rrqr_blk<T>(dt, di, nt, cl, maxm, maxn, ls);
                     }
                     cuda_check(e, "rrqr launch");
                 }));
                 if (tuning) {
-                    cudaEventRecord(eb, stream_);
+                    cudaEventRecord(eb, ls);
                     tuned.push_back(Tuned{key, cl, ea, eb, &kv.second});
                 }
             } else {
                 const int cl = kv.first.second;
                 rqs.push_back(timed(KF_RRQR, 0, 0, [&] {
-                    cudaError_t e = launch_rrqr_rm<T>(dt, di, nt, cl, maxm, maxn, stream_);
+                    cudaError_t e = launch_rrqr_rm<T>(dt, di, nt, cl, maxm, maxn, ls);
                     if (e != cudaSuccess && cl > 8) {  // 16-CTA clusters are an opt-in; fall back to 8
                         cudaGetLastError();
-                        e = launch_rrqr_rm<T>(dt, di, nt, 8, maxm, maxn, stream_);
+                        e = launch_rrqr_rm<T>(dt, di, nt, 8, maxm, maxn, ls);
                     }
                     cuda_check(e, "rrqr launch");
                 }));
             }
             ++launches_fact_;
+        }
+        for (int i = 0; i < nside; ++i) {
+            cuda_check(cudaEventRecord(rq_join_[i], rq_side_[i]), "join");
+            cuda_check(cudaStreamWaitEvent(stream_, rq_join_[i], 0), "join");
         }
         std::vector<int> ranks(jobs.size());
         const double tw0 = wall();
@@ -2480,6 +2524,7 @@ private:
             cudaEventDestroy(tu.a);
             cudaEventDestroy(tu.b);
         }
+        // rqs is in map order when profiling (the only case with entries to fill)
         size_t gi = 0;
         for (auto& kv : groups) {  // algorithmic work of each launch, now that the ranks are known
             const size_t rq = rqs[gi++];

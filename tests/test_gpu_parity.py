@@ -172,6 +172,22 @@ def test_direct_and_graph_applications_agree(gpu):
         assert np.array_equal(xs[0], x)
 
 
+def test_device_synchronize_right_after_first_application(gpu):
+    """The first application starts the capture of the solve graph on a host
+    thread; the call returns only once that capture has ended, so the caller
+    may synchronize the whole device at once (cudaDeviceSynchronize fails while
+    any stream of the device is capturing)."""
+    import torch
+    for _ in range(3):
+        w, A, t, _ = build("advdiff3d_16")
+        b = torch.tensor(w["b"], dtype=torch.float64, device="cuda")
+        x = torch.zeros_like(b)
+        t.solve_dev(b.data_ptr(), x.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(x.cpu().numpy(), t.solve(w["b"]))
+        t.close()
+
+
 def test_launch_timeline_profile(gpu, capfd):
     """Profile level 2 prints one timeline line per timed launch (family, start,
     duration, level, phase) when the counters are read."""
