@@ -2398,6 +2398,17 @@ private:
             const int blk = rrqr_blk_fits<T>(jobs[q].m, jobs[q].n, 16) ? 1 : 0;
             groups[{blk, cluster_of(jobs[q])}].push_back((int)q);
         }
+        // Within a launch, clusters start in task order: the largest interfaces
+        // first, so that a launch with more clusters than fit at once does not
+        // end on a large one started last. Each task is independent: the order
+        // changes no result.
+        for (auto& kv : groups)
+            std::stable_sort(kv.second.begin(), kv.second.end(), [&](int a, int b) {
+                const auto w = [&](int q) {
+                    return (double)jobs[q].m * jobs[q].n * std::min(jobs[q].m, jobs[q].n);
+                };
+                return w(a) > w(b);
+            });
         Upload up;
         size_t o_g = up.add(g), o_r = up.add(rt);
         std::map<std::pair<int, int>, size_t> o_ids;
