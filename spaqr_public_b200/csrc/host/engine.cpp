@@ -1153,6 +1153,13 @@ private:
                 std::map<int, std::vector<std::pair<int, int>>> by;
                 for (auto& e : list) by[-cls(e.first)].push_back(e);
                 for (auto& kv : by) {
+                    // tallest panels first: clusters start in list order, so a launch
+                    // with more clusters than fit at once does not end on a tall one
+                    // started last (tasks are independent: no result changes)
+                    std::stable_sort(kv.second.begin(), kv.second.end(),
+                                     [&](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                                         return qt[a.second].m > qt[b.second].m;
+                                     });
                     PanelLaunch L;
                     L.kind = kind;
                     for (auto& e : kv.second) {
@@ -1190,6 +1197,15 @@ private:
         auto& trsm_tiles = B.trsm_tiles;
         auto& pgroups = B.pgroups;
         const double tw_built = wall();
+        // One CTA per tile, independent of the others: the tiles of the tallest
+        // tasks (trailing update) and of the widest R (TRSM) first, so that a
+        // launch of more CTAs than fit at once does not end on a long one
+        // started last. The order changes no result.
+        for (auto& tl : tiles)
+            std::stable_sort(tl.begin(), tl.end(),
+                             [&](const TileRef& a, const TileRef& b) { return qt[a.task].m > qt[b.task].m; });
+        std::stable_sort(trsm_tiles.begin(), trsm_tiles.end(),
+                         [&](const TileRef& a, const TileRef& b) { return trsm[a.task].k > trsm[b.task].k; });
         Upload up;
         size_t o_g = up.add(g), o_s = up.add(s), o_q = up.add(qt), o_tr = up.add(trsm), o_tt = up.add(trsm_tiles),
                o_post = up.add(post);
