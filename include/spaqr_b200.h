@@ -104,7 +104,10 @@ int spq_factorize_batch(spq_tree* const* ts, int n, int nthreads);
  * one (square matching off; include/tree.h:147). */
 int spq_solve(spq_tree* t, const double* b, double* x);
 int spq_solve_nrml(spq_tree* t, const double* b, double* x);
-/* Same on DEVICE buffers (FP64, on the handle's device). */
+/* Same on DEVICE buffers (FP64, on the handle's device). The first
+ * application of a factorization also captures its solve graph on a host
+ * thread; like every call on a handle, it returns only once no capture is in
+ * flight, so the caller may synchronize the device right after it. */
 int spq_solve_dev(spq_tree* t, const double* d_b, double* d_x);
 int spq_solve_nrml_dev(spq_tree* t, const double* d_b, double* d_x);
 
